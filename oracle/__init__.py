@@ -1,0 +1,178 @@
+"""ORACLE — test infrastructure only.
+
+Python access to the CPU restatement of mojoBLAS's level-3 routines
+(ref_level3.cpp, built into liboracle_level3.so by the Makefile beside it) plus
+float64 / extended-precision reference products.  Only tests, the smoke check
+and bench.py's CPU-baseline legs import this package; the CUDA library never
+does.
+
+Matrices are numpy arrays holding column-major storage: a matrix with leading
+dimension ld and n columns is a 1-D buffer (or a Fortran-ordered 2-D array)
+whose element (i, j) sits at flat index i + j*ld.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle_level3.so"
+BUG_COMPAT = 1  # reproduce the reference's quirks (v7 alpha, right/trans trsm)
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = C.CDLL(str(LIB_PATH))
+        i64, f32p, f64p = C.c_int64, C.POINTER(C.c_float), C.POINTER(C.c_double)
+        ch = C.c_char
+        sig = {
+            "orc_sgemm": [ch, ch, i64, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_float, f32p, i64, C.c_int],
+            "orc_dgemm": [ch, ch, i64, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64, C.c_int],
+            "orc_sgemm_naive": [ch, ch, i64, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_float, f32p, i64],
+            "orc_dgemm_naive": [ch, ch, i64, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64],
+            "orc_sgemm_v11": [i64, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_float, f32p, i64],
+            "orc_dgemm_v3": [i64, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64],
+            "orc_dgemm_v7": [i64, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64, C.c_int],
+            "orc_ssyrk": [ch, ch, i64, i64, C.c_float, f32p, i64, C.c_float, f32p, i64],
+            "orc_dsyrk": [ch, ch, i64, i64, C.c_double, f64p, i64, C.c_double, f64p, i64],
+            "orc_strsm": [ch, ch, ch, ch, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_int],
+            "orc_dtrsm": [ch, ch, ch, ch, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_int],
+        }
+        for name, argtypes in sig.items():
+            fn = getattr(_lib, name)
+            fn.argtypes = argtypes
+            fn.restype = C.c_int
+        _lib.orc_set_threads.argtypes = [C.c_int]
+        _lib.orc_max_threads.restype = C.c_int
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return lib().orc_max_threads()
+
+
+def _p(x: np.ndarray, dt):
+    assert x.dtype == dt and (x.flags.f_contiguous or x.ndim == 1), "column-major buffer expected"
+    return x.ctypes.data_as(C.POINTER(C.c_float if dt == np.float32 else C.c_double))
+
+
+def _c(t) -> bytes:
+    return t.encode() if isinstance(t, str) else t
+
+
+def _dt(x):
+    return np.float32 if x.dtype == np.float32 else np.float64
+
+
+def gemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, flags=0) -> int:
+    """The reference's gemm dispatch (gemm.mojo:56-124), in place on c."""
+    dt = _dt(c)
+    fn = lib().orc_sgemm if dt == np.float32 else lib().orc_dgemm
+    return fn(_c(ta), _c(tb), m, n, k, alpha, _p(a, dt), lda, _p(b, dt), ldb, beta, _p(c, dt), ldc, flags)
+
+
+def gemm_naive(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> int:
+    dt = _dt(c)
+    fn = lib().orc_sgemm_naive if dt == np.float32 else lib().orc_dgemm_naive
+    return fn(_c(ta), _c(tb), m, n, k, alpha, _p(a, dt), lda, _p(b, dt), ldb, beta, _p(c, dt), ldc)
+
+
+def sgemm_v11(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> int:
+    f = np.float32
+    return lib().orc_sgemm_v11(m, n, k, alpha, _p(a, f), lda, _p(b, f), ldb, beta, _p(c, f), ldc)
+
+
+def dgemm_v7(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, flags=0) -> int:
+    f = np.float64
+    return lib().orc_dgemm_v7(m, n, k, alpha, _p(a, f), lda, _p(b, f), ldb, beta, _p(c, f), ldc, flags)
+
+
+def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc) -> int:
+    dt = _dt(c)
+    fn = lib().orc_ssyrk if dt == np.float32 else lib().orc_dsyrk
+    return fn(_c(uplo), _c(trans), n, k, alpha, _p(a, dt), lda, beta, _p(c, dt), ldc)
+
+
+def trsm(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb, flags=0) -> int:
+    dt = _dt(b)
+    fn = lib().orc_strsm if dt == np.float32 else lib().orc_dtrsm
+    return fn(_c(side), _c(uplo), _c(ta), _c(diag), m, n, alpha, _p(a, dt), lda, _p(b, dt), ldb, flags)
+
+
+# ---------------------------------------------------------------------------
+# float64 references (Netlib semantics, independent of the reference's code)
+# ---------------------------------------------------------------------------
+
+def view(buf: np.ndarray, rows: int, cols: int, ld: int) -> np.ndarray:
+    """The rows x cols column-major matrix stored in buf with leading dimension ld."""
+    flat = buf.reshape(-1, order="F")
+    if rows > 0 and cols > 0:
+        assert rows <= ld and (cols - 1) * ld + rows <= flat.size, "matrix exceeds its buffer"
+    return np.lib.stride_tricks.as_strided(flat, shape=(rows, cols),
+                                           strides=(flat.itemsize, flat.itemsize * ld))
+
+
+def op(x: np.ndarray, t) -> np.ndarray:
+    return x if _c(t) in (b"N", b"n") else x.T
+
+
+def gemm_f64(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> np.ndarray:
+    """float64 C = alpha*op(A)op(B) + beta*C as an m x n array (c untouched)."""
+    A = op(view(a, *( (m, k) if _c(ta) in (b"N", b"n") else (k, m)), lda), ta).astype(np.float64)
+    B = op(view(b, *( (k, n) if _c(tb) in (b"N", b"n") else (n, k)), ldb), tb).astype(np.float64)
+    out = float(alpha) * (A @ B)
+    if beta != 0:
+        out = out + float(beta) * view(c, m, n, ldc).astype(np.float64)
+    return out
+
+
+def tri(x: np.ndarray, uplo, diag) -> np.ndarray:
+    t = np.tril(x) if _c(uplo) in (b"L", b"l") else np.triu(x)
+    if _c(diag) in (b"U", b"u"):
+        t = t.copy()
+        np.fill_diagonal(t, 1.0)
+    return t
+
+
+def trsm_f64(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb) -> np.ndarray:
+    """float64 Netlib trsm result X (m x n); b untouched."""
+    import scipy.linalg as sl
+    na = m if _c(side) in (b"L", b"l") else n
+    A = tri(view(a, na, na, lda).astype(np.float64), uplo, diag)
+    opA = op(A, ta)
+    B = float(alpha) * view(b, m, n, ldb).astype(np.float64)
+    lower = bool(np.allclose(opA, np.tril(opA)))
+    if _c(side) in (b"L", b"l"):
+        return sl.solve_triangular(opA, B, lower=lower)
+    # X opA = B  <=>  opA^T X^T = B^T
+    return sl.solve_triangular(opA.T, B.T, lower=not lower).T
+
+
+def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:
+    """max|x - ref| / max|ref| (normwise, the error metric quoted with every result)."""
+    den = float(np.max(np.abs(ref)))
+    return float(np.max(np.abs(x.astype(np.float64) - ref))) / (den if den > 0 else 1.0)
+
+
+def elementwise_err(x: np.ndarray, ref: np.ndarray, bound: np.ndarray) -> float:
+    """max_ij |x - ref| / bound_ij, with bound = |alpha| |op(A)| |op(B)| (+|beta||C|)."""
+    bound = np.where(bound > 0, bound, 1.0)
+    return float(np.max(np.abs(x.astype(np.float64) - ref) / bound))
