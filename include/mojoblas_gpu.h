@@ -1,0 +1,135 @@
+/*
+ * mojoblas_gpu.h — C ABI of the B200 (sm_100a) level-3 BLAS library.
+ *
+ * Drop-in boundary for mojoBLAS's level-3 hot path.  Every routine keeps the
+ * argument order and meaning of the mojoBLAS routine it replaces (column-major
+ * storage, element (i,j) of a matrix at p[i + j*ld], Netlib transpose / uplo /
+ * side / diag characters), and returns:
+ *     0               success
+ *     > 0             Netlib `info`: the 1-based position of the first invalid
+ *                     argument, numbered as the mojoBLAS routine numbers it
+ *     < 0             an MBG_ERR_* code below (CUDA failure, allocation, ...)
+ * Where mojoBLAS prints "<routine>: Info <n>" and returns, this library returns
+ * n and prints nothing.
+ *
+ * Pointers may be device pointers (the fast path) or ordinary host pointers; the
+ * library detects which with cudaPointerGetAttributes and, for host data, copies
+ * the operands to the device and the result back, so a host caller sees the
+ * same in-place semantics as the reference.  Calls are synchronous unless
+ * mbg_set_sync(0) is in effect and every operand is a device pointer.
+ *
+ * Quick returns, argument checks and the alpha == 0 / k == 0 paths follow the
+ * reference; the arithmetic follows Netlib where the reference departs from it
+ * (gemm_v7 alpha, right-side transposed trsm).
+ */
+#ifndef MOJOBLAS_GPU_H
+#define MOJOBLAS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MBG_OK                 0
+#define MBG_ERR_CUDA          -1  /* a CUDA runtime call failed (mbg_last_error has it) */
+#define MBG_ERR_ALLOC         -2  /* device workspace allocation failed               */
+#define MBG_ERR_UNSUPPORTED   -3  /* valid arguments, combination not implemented     */
+#define MBG_ERR_NO_DEVICE     -4  /* no usable CUDA device / driver                   */
+#define MBG_ERR_TIMEOUT       -5  /* a kernel's bounded wait expired (error flag set)  */
+#define MBG_ERR_INVALID_MODE  -6  /* unknown precision mode or slice count            */
+
+/* ---- precision modes ---------------------------------------------------- */
+#define MBG_MODE_PLAIN   0  /* FP32 / FP64 FMA on the CUDA cores (the drop-in)           */
+#define MBG_MODE_BF16X3  1  /* fp32: a = a1 + a2 in bf16, a1b1 + a1b2 + a2b1 on tcgen05  */
+#define MBG_MODE_BF16X6  2  /* fp32: a = a1 + a2 + a3 in bf16, 6 products on tcgen05     */
+#define MBG_MODE_OZAKI   3  /* fp64: int8 slices, exact int32 tcgen05 products, fp64 sum */
+
+/* ---- level 3: the reference's routines ---------------------------------- */
+
+/* C := alpha*op(A)*op(B) + beta*C.
+ * Replaces mojoBLAS gemm[float32] (src/level3/gemm.mojo:56-124), which routes to
+ * gemm_v11 (NN, :2092) or _gemm_naive (:127). */
+int mbg_sgemm(char trans_a, char trans_b, int64_t m, int64_t n, int64_t k,
+              float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
+              float beta, float* c, int64_t ldc);
+
+/* Replaces mojoBLAS gemm[float64] (src/level3/gemm.mojo:56-124: gemm_v3 :385,
+ * gemm_v7 :817, _gemm_naive :127). */
+int mbg_dgemm(char trans_a, char trans_b, int64_t m, int64_t n, int64_t k,
+              double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+              double beta, double* c, int64_t ldc);
+
+/* C := alpha*A*A^T + beta*C or alpha*A^T*A + beta*C on the `uplo` triangle.
+ * Replaces mojoBLAS syrk (src/level3/syrk.mojo:20-200). */
+int mbg_ssyrk(char uplo, char trans, int64_t n, int64_t k, float alpha,
+              const float* a, int64_t lda, float beta, float* c, int64_t ldc);
+int mbg_dsyrk(char uplo, char trans, int64_t n, int64_t k, double alpha,
+              const double* a, int64_t lda, double beta, double* c, int64_t ldc);
+
+/* op(A)*X = alpha*B or X*op(A) = alpha*B, X overwrites B.
+ * Replaces mojoBLAS trsm (src/level3/trsm.mojo:20-275). */
+int mbg_strsm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t n,
+              float alpha, const float* a, int64_t lda, float* b, int64_t ldb);
+int mbg_dtrsm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t n,
+              double alpha, const double* a, int64_t lda, double* b, int64_t ldb);
+
+/* ---- the same routines with a precision mode ----------------------------
+ * mode: MBG_MODE_PLAIN, MBG_MODE_BF16X3 or MBG_MODE_BF16X6 for float;
+ *       MBG_MODE_PLAIN or MBG_MODE_OZAKI for double.
+ * slices: Ozaki int8 slices per operand (2..8, each carries 7 bits); ignored
+ *         by the other modes.
+ * refine: trsm only — iterative-refinement steps after the solve (0 or more):
+ *         R = alpha*B - op(A)*X in the accurate mode, solve, X += correction.
+ * Same argument numbering for `info` as the plain routine (mode arguments are
+ * not counted). */
+int mbg_sgemm_ex(int mode, char trans_a, char trans_b, int64_t m, int64_t n, int64_t k,
+                 float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
+                 float beta, float* c, int64_t ldc);
+int mbg_dgemm_ex(int mode, int slices, char trans_a, char trans_b, int64_t m, int64_t n,
+                 int64_t k, double alpha, const double* a, int64_t lda, const double* b,
+                 int64_t ldb, double beta, double* c, int64_t ldc);
+int mbg_ssyrk_ex(int mode, char uplo, char trans, int64_t n, int64_t k, float alpha,
+                 const float* a, int64_t lda, float beta, float* c, int64_t ldc);
+int mbg_strsm_ex(int mode, int refine, char side, char uplo, char trans_a, char diag,
+                 int64_t m, int64_t n, float alpha, const float* a, int64_t lda,
+                 float* b, int64_t ldb);
+int mbg_dtrsm_ex(int mode, int slices, int refine, char side, char uplo, char trans_a,
+                 char diag, int64_t m, int64_t n, double alpha, const double* a,
+                 int64_t lda, double* b, int64_t ldb);
+
+/* ---- runtime ------------------------------------------------------------ */
+/* Stream for subsequent calls from any thread (a cudaStream_t; NULL = legacy
+ * default stream, the initial value). */
+int   mbg_set_stream(void* stream);
+void* mbg_get_stream(void);
+/* 1 (default): every call returns after its device work finished.
+ * 0: calls whose operands are all device pointers return after enqueueing. */
+int   mbg_set_sync(int on);
+/* Synchronise the library stream and report a pending kernel error flag. */
+int   mbg_synchronize(void);
+const char* mbg_status_string(int status);
+const char* mbg_last_error(void);
+int   mbg_version(void);
+/* Release cached device workspace. */
+int   mbg_release_workspace(void);
+
+/* ---- kernel timing (CUDA events around each library kernel launch) ------ */
+int mbg_prof_enable(int on);
+int mbg_prof_reset(void);
+/* Total device milliseconds and launch count recorded for kernels whose name
+ * contains `name_substring` since the last reset (events are resolved here). */
+int mbg_prof_query(const char* name_substring, double* total_ms, int64_t* launches);
+/* Launches of library kernels since the last reset, counted on the host. */
+int64_t mbg_launch_count(void);
+
+/* ---- test hooks ----------------------------------------------------------- */
+/* Make the n-th device allocation from now on fail (n >= 1); 0 disables. */
+int mbg_debug_fail_alloc(int nth);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOJOBLAS_GPU_H */

@@ -1,0 +1,207 @@
+// C ABI entry points: argument checks (Netlib numbering as in the mojoBLAS
+// routines), quick returns, host-operand staging and precision-mode dispatch.
+#include "mbg_internal.cuh"
+
+namespace mbg {
+
+// ---- argument checks ----------------------------------------------------------
+// src/level3/gemm.mojo:179-213
+static int gemm_info(char ta, char tb, i64 m, i64 n, i64 k, i64 lda, i64 ldb, i64 ldc) {
+    if (!is_n(ta) && !is_t(ta)) return 1;
+    if (!is_n(tb) && !is_t(tb)) return 2;
+    if (m < 0) return 3;
+    if (n < 0) return 4;
+    if (k < 0) return 5;
+    if (lda < imax(1, is_n(ta) ? m : k)) return 8;
+    if (ldb < imax(1, is_n(tb) ? k : n)) return 10;
+    if (ldc < imax(1, m)) return 13;
+    return 0;
+}
+// src/level3/syrk.mojo:60-83
+static int syrk_info(char uplo, char trans, i64 n, i64 k, i64 lda, i64 ldc) {
+    if (!is_u(uplo) && !is_l(uplo)) return 1;
+    if (!is_n(trans) && !is_t(trans)) return 2;
+    if (n < 0) return 3;
+    if (k < 0) return 4;
+    if (lda < imax(1, is_n(trans) ? n : k)) return 7;
+    if (ldc < imax(1, n)) return 10;
+    return 0;
+}
+// src/level3/trsm.mojo:62-89
+static int trsm_info(char side, char uplo, char ta, char diag, i64 m, i64 n, i64 lda, i64 ldb) {
+    if (!is_l(side) && !is_r(side)) return 1;
+    if (!is_u(uplo) && !is_l(uplo)) return 2;
+    if (!is_n(ta) && !is_t(ta)) return 3;
+    if (!is_u(diag) && !is_n(diag)) return 4;
+    if (m < 0) return 5;
+    if (n < 0) return 6;
+    if (lda < imax(1, is_l(side) ? m : n)) return 9;
+    if (ldb < imax(1, m)) return 11;
+    return 0;
+}
+
+static bool valid_smode(int mode) {
+    return mode == MBG_MODE_PLAIN || mode == MBG_MODE_BF16X3 || mode == MBG_MODE_BF16X6;
+}
+static bool valid_dmode(int mode, int slices) {
+    if (mode == MBG_MODE_PLAIN) return true;
+    return mode == MBG_MODE_OZAKI && slices >= 2 && slices <= 8;
+}
+
+// ---- precision dispatch on device operands -------------------------------------
+int sgemm_mode(int mode, char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a,
+               i64 lda, const float* b, i64 ldb, float beta, float* c, i64 ldc) {
+    if (m == 0 || n == 0) return MBG_OK;
+    if (alpha == 0.0f || k == 0) return scale_matrix<float>(m, n, beta, c, ldc);
+    switch (mode) {
+        case MBG_MODE_PLAIN: return gemm_plain<float>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+        case MBG_MODE_BF16X3: return sgemm_split_tc(2, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, 0);
+        case MBG_MODE_BF16X6: return sgemm_split_tc(3, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, 0);
+        default: return MBG_ERR_INVALID_MODE;
+    }
+}
+
+int dgemm_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
+               const double* a, i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+    if (m == 0 || n == 0) return MBG_OK;
+    if (alpha == 0.0 || k == 0) return scale_matrix<double>(m, n, beta, c, ldc);
+    switch (mode) {
+        case MBG_MODE_PLAIN: return gemm_plain<double>(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+        case MBG_MODE_OZAKI: return dgemm_ozaki_tc(slices, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+        default: return MBG_ERR_INVALID_MODE;
+    }
+}
+
+// ---- staged drivers ------------------------------------------------------------
+template <typename T>
+static int gemm_entry(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, T alpha,
+                      const T* a, i64 lda, const T* b, i64 ldb, T beta, T* c, i64 ldc) {
+    int info = gemm_info(ta, tb, m, n, k, lda, ldb, ldc);
+    if (info) return info;
+    if (m == 0 || n == 0) return MBG_OK;
+    const bool need_ab = !(alpha == T(0) || k == 0);
+    Operand A, B, Cc;
+    if (need_ab) {
+        MBG_TRY(A.prepare(a, is_n(ta) ? m : k, is_n(ta) ? k : m, lda, sizeof(T), true, false));
+        MBG_TRY(B.prepare(b, is_n(tb) ? k : n, is_n(tb) ? n : k, ldb, sizeof(T), true, false));
+    }
+    MBG_TRY(Cc.prepare(c, m, n, ldc, sizeof(T), beta != T(0), true));
+    int st;
+    if (sizeof(T) == 4)
+        st = sgemm_mode(mode, ta, tb, m, n, k, (float)alpha, (const float*)A.dev, A.dev_ld,
+                        (const float*)B.dev, B.dev_ld, (float)beta, (float*)Cc.dev, Cc.dev_ld);
+    else
+        st = dgemm_mode(mode, slices, ta, tb, m, n, k, (double)alpha, (const double*)A.dev, A.dev_ld,
+                        (const double*)B.dev, B.dev_ld, (double)beta, (double*)Cc.dev, Cc.dev_ld);
+    if (st) return st;
+    MBG_TRY(Cc.finish());
+    return finish_call(A.staged || B.staged || Cc.staged);
+}
+
+template <typename T>
+static int syrk_entry(int mode, char uplo, char trans, i64 n, i64 k, T alpha, const T* a, i64 lda,
+                      T beta, T* c, i64 ldc) {
+    int info = syrk_info(uplo, trans, n, k, lda, ldc);
+    if (info) return info;
+    if (n == 0 || (alpha == T(0) && beta == T(1))) return MBG_OK;  // syrk.mojo:85-86
+    const bool need_a = !(alpha == T(0) || k == 0);
+    Operand A, Cc;
+    if (need_a) MBG_TRY(A.prepare(a, is_n(trans) ? n : k, is_n(trans) ? k : n, lda, sizeof(T), true, false));
+    MBG_TRY(Cc.prepare(c, n, n, ldc, sizeof(T), true, true));  // other triangle must survive
+    const T* ad = (const T*)A.dev;
+    T* cd = (T*)Cc.dev;
+    // C := alpha*op(A)*op(A)^T + beta*C; op(A)^T is A with the other transpose
+    const char ta = is_n(trans) ? 'N' : 'T';
+    const char tb = is_n(trans) ? 'T' : 'N';
+    int st;
+    if (!need_a) st = scale_triangle<T>(uplo, n, beta, cd, Cc.dev_ld);
+    else if (mode == MBG_MODE_PLAIN || sizeof(T) == 8)
+        st = gemmt_plain<T>(uplo, ta, tb, n, k, alpha, ad, A.dev_ld, ad, A.dev_ld, beta, cd, Cc.dev_ld);
+    else
+        st = sgemm_split_tc(mode == MBG_MODE_BF16X6 ? 3 : 2, ta, tb, n, n, k, (float)alpha,
+                            (const float*)ad, A.dev_ld, (const float*)ad, A.dev_ld, (float)beta,
+                            (float*)cd, Cc.dev_ld, is_l(uplo) ? 'L' : 'U');
+    if (st) return st;
+    MBG_TRY(Cc.finish());
+    return finish_call(A.staged || Cc.staged);
+}
+
+template <typename T>
+static int trsm_entry(int mode, int slices, int refine, char side, char uplo, char ta, char diag,
+                      i64 m, i64 n, T alpha, const T* a, i64 lda, T* b, i64 ldb) {
+    int info = trsm_info(side, uplo, ta, diag, m, n, lda, ldb);
+    if (info) return info;
+    if (m == 0 || n == 0) return MBG_OK;  // trsm.mojo:91-92
+    const i64 na = is_l(side) ? m : n;
+    Operand A, B;
+    MBG_TRY(A.prepare(a, na, na, lda, sizeof(T), true, false));
+    MBG_TRY(B.prepare(b, m, n, ldb, sizeof(T), true, true));
+    int st = trsm_device<T>(mode, slices, refine, side, uplo, ta, diag, m, n, alpha, (const T*)A.dev,
+                            A.dev_ld, (T*)B.dev, B.dev_ld);
+    if (st) return st;
+    MBG_TRY(B.finish());
+    return finish_call(A.staged || B.staged);
+}
+
+}  // namespace mbg
+
+using namespace mbg;
+
+extern "C" {
+
+int mbg_sgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, float alpha, const float* a,
+              int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc) {
+    return gemm_entry<float>(MBG_MODE_PLAIN, 0, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_dgemm(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha, const double* a,
+              int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc) {
+    return gemm_entry<double>(MBG_MODE_PLAIN, 0, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_sgemm_ex(int mode, char ta, char tb, int64_t m, int64_t n, int64_t k, float alpha,
+                 const float* a, int64_t lda, const float* b, int64_t ldb, float beta, float* c,
+                 int64_t ldc) {
+    if (!valid_smode(mode)) return MBG_ERR_INVALID_MODE;
+    return gemm_entry<float>(mode, 0, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_dgemm_ex(int mode, int slices, char ta, char tb, int64_t m, int64_t n, int64_t k,
+                 double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                 double beta, double* c, int64_t ldc) {
+    if (!valid_dmode(mode, slices)) return MBG_ERR_INVALID_MODE;
+    return gemm_entry<double>(mode, slices, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+int mbg_ssyrk(char uplo, char trans, int64_t n, int64_t k, float alpha, const float* a,
+              int64_t lda, float beta, float* c, int64_t ldc) {
+    return syrk_entry<float>(MBG_MODE_PLAIN, uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+int mbg_dsyrk(char uplo, char trans, int64_t n, int64_t k, double alpha, const double* a,
+              int64_t lda, double beta, double* c, int64_t ldc) {
+    return syrk_entry<double>(MBG_MODE_PLAIN, uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+int mbg_ssyrk_ex(int mode, char uplo, char trans, int64_t n, int64_t k, float alpha,
+                 const float* a, int64_t lda, float beta, float* c, int64_t ldc) {
+    if (!valid_smode(mode)) return MBG_ERR_INVALID_MODE;
+    return syrk_entry<float>(mode, uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+
+int mbg_strsm(char side, char uplo, char ta, char diag, int64_t m, int64_t n, float alpha,
+              const float* a, int64_t lda, float* b, int64_t ldb) {
+    return trsm_entry<float>(MBG_MODE_PLAIN, 0, 0, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int mbg_dtrsm(char side, char uplo, char ta, char diag, int64_t m, int64_t n, double alpha,
+              const double* a, int64_t lda, double* b, int64_t ldb) {
+    return trsm_entry<double>(MBG_MODE_PLAIN, 0, 0, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int mbg_strsm_ex(int mode, int refine, char side, char uplo, char ta, char diag, int64_t m,
+                 int64_t n, float alpha, const float* a, int64_t lda, float* b, int64_t ldb) {
+    if (!valid_smode(mode) || refine < 0) return MBG_ERR_INVALID_MODE;
+    return trsm_entry<float>(mode, 0, refine, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int mbg_dtrsm_ex(int mode, int slices, int refine, char side, char uplo, char ta, char diag,
+                 int64_t m, int64_t n, double alpha, const double* a, int64_t lda, double* b,
+                 int64_t ldb) {
+    if (!valid_dmode(mode, slices) || refine < 0) return MBG_ERR_INVALID_MODE;
+    return trsm_entry<double>(mode, slices, refine, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+
+}  // extern "C"

@@ -1,0 +1,130 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <cstdio>
+#include <string>
+
+#include "../../include/mojoblas_gpu.h"
+
+typedef int64_t i64;
+
+namespace mbg {
+
+// ---- character flags (Netlib spelling, either case; 'C' == 'T' for reals) ----
+inline bool is_n(char t) { return t == 'N' || t == 'n'; }
+inline bool is_t(char t) { return t == 'T' || t == 't' || t == 'C' || t == 'c'; }
+inline bool is_u(char t) { return t == 'U' || t == 'u'; }
+inline bool is_l(char t) { return t == 'L' || t == 'l'; }
+inline bool is_r(char t) { return t == 'R' || t == 'r'; }
+inline i64 imax(i64 a, i64 b) { return a > b ? a : b; }
+inline i64 imin(i64 a, i64 b) { return a < b ? a : b; }
+inline i64 cdiv(i64 a, i64 b) { return (a + b - 1) / b; }
+
+// ---- runtime state ----------------------------------------------------------
+cudaStream_t stream();
+bool sync_mode();
+void set_error(const char* what, cudaError_t e);
+void set_error_msg(const std::string& msg);
+
+// Wraps a CUDA runtime call; on failure records it and returns MBG_ERR_CUDA.
+#define MBG_CUDA(call)                                                         \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess) {                                               \
+            ::mbg::set_error(#call, e_);                                       \
+            return (e_ == cudaErrorNoDevice || e_ == cudaErrorInsufficientDriver) \
+                       ? MBG_ERR_NO_DEVICE : MBG_ERR_CUDA;                     \
+        }                                                                      \
+    } while (0)
+
+#define MBG_TRY(expr)                                                          \
+    do {                                                                       \
+        int s_ = (expr);                                                       \
+        if (s_ != 0) return s_;                                                \
+    } while (0)
+
+// Checks the launch that was just enqueued (configuration errors only).
+int check_launch(const char* name);
+
+// ---- device workspace: a per-device cache of blocks, stream-ordered reuse ---
+// Blocks are handed out for the duration of one library call and returned to
+// the cache when the call finishes enqueueing; all library work runs on one
+// stream, so a block reused by the next call is ordered after its last use.
+struct Workspace {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    Workspace() = default;
+    Workspace(const Workspace&) = delete;
+    Workspace& operator=(const Workspace&) = delete;
+    Workspace(Workspace&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    ~Workspace();
+    int reserve(size_t nbytes);   // MBG_OK or MBG_ERR_ALLOC
+    template <typename T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ---- host/device operand staging ---------------------------------------------
+// A matrix operand of `rows` x `cols` elements with leading dimension `ld`.
+// If the pointer is not device-accessible, a compact device copy (ld = rows) is
+// made (copy_in) and written back on finish() (copy_out).
+struct Operand {
+    const void* user = nullptr;
+    void* dev = nullptr;
+    i64 rows = 0, cols = 0, ld = 0, dev_ld = 0;
+    size_t elem = 0;
+    bool staged = false, copy_out = false;
+    Workspace ws;
+    int prepare(const void* p, i64 rows, i64 cols, i64 ld, size_t elem, bool copy_in, bool copy_out);
+    int finish();  // copies back if staged && copy_out
+};
+bool is_device_pointer(const void* p);
+
+// ---- timing of library kernels (optional) ------------------------------------
+struct ProfScope {
+    int slot = -1;
+    explicit ProfScope(const char* name);
+    ~ProfScope();
+};
+void count_launch(int n = 1);
+
+// Device-side error flag (bounded waits that expired set it): a mapped pinned
+// int[4] — [0] error code, [1] site — or nullptr if it could not be created.
+int* device_error_flag();
+int read_and_clear_device_error();
+int finish_call(bool any_staged);  // synchronises when required, checks flag
+
+// ---- kernels (implemented in the other translation units) --------------------
+template <typename T>
+int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 lda,
+               const T* b, i64 ldb, T beta, T* c, i64 ldc);
+// lower (uplo 'L') or upper triangle of C := alpha*op(A)*op(B) + beta*C
+template <typename T>
+int gemmt_plain(char uplo, char ta, char tb, i64 n, i64 k, T alpha, const T* a, i64 lda,
+                const T* b, i64 ldb, T beta, T* c, i64 ldc);
+template <typename T>
+int scale_matrix(i64 m, i64 n, T beta, T* c, i64 ldc);  // C := beta*C (beta==0 stores 0)
+template <typename T>
+int scale_triangle(char uplo, i64 n, T beta, T* c, i64 ldc);
+
+// precision-mode gemm (dispatch to plain / split / Ozaki), device operands
+int sgemm_mode(int mode, char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a,
+               i64 lda, const float* b, i64 ldb, float beta, float* c, i64 ldc);
+int dgemm_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
+               const double* a, i64 lda, const double* b, i64 ldb, double beta, double* c,
+               i64 ldc);
+// tensor-core paths (tc_gemm.cu)
+int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha,
+                   const float* a, i64 lda, const float* b, i64 ldb, float beta, float* c,
+                   i64 ldc, char tri_uplo);
+int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
+                   const double* a, i64 lda, const double* b, i64 ldb, double beta,
+                   double* c, i64 ldc);
+
+// trsm on device operands (trsm.cu)
+template <typename T>
+int trsm_device(int mode, int slices, int refine, char side, char uplo, char ta, char diag,
+                i64 m, i64 n, T alpha, const T* a, i64 lda, T* b, i64 ldb);
+
+}  // namespace mbg

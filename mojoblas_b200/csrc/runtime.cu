@@ -1,0 +1,308 @@
+// Library runtime: stream, status strings, device workspace cache, host-operand
+// staging, the device error flag and optional per-kernel timing.
+#include "mbg_internal.cuh"
+
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <vector>
+#include <cstring>
+
+namespace mbg {
+
+namespace {
+std::mutex g_mu;
+cudaStream_t g_stream = nullptr;
+std::atomic<bool> g_sync{true};
+thread_local std::string g_last_error;
+std::atomic<int> g_fail_alloc_countdown{0};
+std::atomic<int64_t> g_launches{0};
+
+struct DeviceCache {
+    std::multimap<size_t, void*> free_blocks;  // size -> block
+    std::map<void*, size_t> sizes;
+    int* err_host = nullptr;                    // mapped pinned flag
+    int* err_dev = nullptr;
+};
+std::map<int, DeviceCache> g_cache;
+
+struct ProfRecord {
+    std::string name;
+    cudaEvent_t start, stop;
+};
+std::atomic<bool> g_prof{false};
+std::vector<ProfRecord> g_prof_records;
+std::vector<cudaEvent_t> g_event_pool;
+
+cudaEvent_t take_event() {
+    if (!g_event_pool.empty()) {
+        cudaEvent_t e = g_event_pool.back();
+        g_event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+int current_device() {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return -1;
+    return d;
+}
+}  // namespace
+
+cudaStream_t stream() { return g_stream; }
+bool sync_mode() { return g_sync.load(); }
+
+void set_error(const char* what, cudaError_t e) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    cudaGetLastError();  // clear a sticky launch error so the next call starts clean
+}
+void set_error_msg(const std::string& msg) { g_last_error = msg; }
+
+int check_launch(const char* name) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        g_last_error = std::string("launch of ") + name + ": " + cudaGetErrorString(e);
+        return MBG_ERR_CUDA;
+    }
+    count_launch();
+    return MBG_OK;
+}
+
+void count_launch(int n) { g_launches += n; }
+
+// ---- workspace ---------------------------------------------------------------
+Workspace::~Workspace() {
+    if (!ptr) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    int d = current_device();
+    g_cache[d].free_blocks.emplace(bytes, ptr);
+    ptr = nullptr;
+}
+
+int Workspace::reserve(size_t nbytes) {
+    if (nbytes == 0) nbytes = 256;
+    if (ptr && bytes >= nbytes) return MBG_OK;
+    if (ptr) {  // give back the smaller block
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_cache[current_device()].free_blocks.emplace(bytes, ptr);
+        ptr = nullptr;
+    }
+    const size_t gran = size_t(2) << 20;
+    size_t want = (nbytes + gran - 1) / gran * gran;
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceCache& dc = g_cache[current_device()];
+    auto it = dc.free_blocks.lower_bound(want);
+    if (it != dc.free_blocks.end() && it->first <= 2 * want) {
+        ptr = it->second;
+        bytes = it->first;
+        dc.free_blocks.erase(it);
+        return MBG_OK;
+    }
+    int cd = g_fail_alloc_countdown.load();
+    if (cd > 0) {
+        g_fail_alloc_countdown = cd - 1;
+        if (cd == 1) {
+            set_error_msg("device workspace allocation failed (injected by mbg_debug_fail_alloc)");
+            return MBG_ERR_ALLOC;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        // drop the cache and retry once
+        for (auto& kv : dc.free_blocks) cudaFree(kv.second);
+        dc.free_blocks.clear();
+        cudaGetLastError();
+        e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            set_error("cudaMalloc(workspace)", e);
+            return (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? MBG_ERR_NO_DEVICE
+                                                                                  : MBG_ERR_ALLOC;
+        }
+    }
+    ptr = p;
+    bytes = want;
+    return MBG_OK;
+}
+
+// ---- operands ---------------------------------------------------------------
+bool is_device_pointer(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+int Operand::prepare(const void* p, i64 r, i64 c, i64 l, size_t e, bool copy_in, bool out) {
+    user = p; rows = r; cols = c; ld = l; elem = e; copy_out = out;
+    if (r <= 0 || c <= 0) { dev = const_cast<void*>(p); dev_ld = l; return MBG_OK; }
+    if (is_device_pointer(p)) { dev = const_cast<void*>(p); dev_ld = l; return MBG_OK; }
+    staged = true;
+    dev_ld = r;
+    MBG_TRY(ws.reserve(size_t(r) * size_t(c) * e));
+    dev = ws.ptr;
+    if (copy_in)
+        MBG_CUDA(cudaMemcpy2DAsync(dev, size_t(r) * e, p, size_t(l) * e, size_t(r) * e, size_t(c),
+                                   cudaMemcpyHostToDevice, stream()));
+    return MBG_OK;
+}
+
+int Operand::finish() {
+    if (staged && copy_out)
+        MBG_CUDA(cudaMemcpy2DAsync(const_cast<void*>(user), size_t(ld) * elem, dev, size_t(rows) * elem,
+                                   size_t(rows) * elem, size_t(cols), cudaMemcpyDeviceToHost, stream()));
+    return MBG_OK;
+}
+
+// ---- device error flag ---------------------------------------------------------
+int* device_error_flag() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceCache& dc = g_cache[current_device()];
+    if (!dc.err_host) {
+        if (cudaHostAlloc(&dc.err_host, sizeof(int) * 4, cudaHostAllocMapped) != cudaSuccess) {
+            cudaGetLastError();
+            dc.err_host = nullptr;
+            return nullptr;
+        }
+        std::memset(dc.err_host, 0, sizeof(int) * 4);
+        if (cudaHostGetDevicePointer(&dc.err_dev, dc.err_host, 0) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    return dc.err_dev;
+}
+
+int read_and_clear_device_error() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceCache& dc = g_cache[current_device()];
+    if (!dc.err_host) return 0;
+    volatile int* f = dc.err_host;
+    int v = f[0];
+    if (v) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "a kernel's bounded wait expired (code %d, site %d); results are invalid", v, f[1]);
+        g_last_error = buf;
+        f[0] = 0;
+        f[1] = 0;
+    }
+    return v;
+}
+
+int finish_call(bool any_staged) {
+    if (any_staged || sync_mode()) {
+        MBG_CUDA(cudaStreamSynchronize(stream()));
+        if (read_and_clear_device_error()) return MBG_ERR_TIMEOUT;
+    }
+    return MBG_OK;
+}
+
+// ---- timing ------------------------------------------------------------------
+ProfScope::ProfScope(const char* name) {
+    if (!g_prof.load()) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    ProfRecord r{name, take_event(), take_event()};
+    cudaEventRecord(r.start, stream());
+    g_prof_records.push_back(r);
+    slot = int(g_prof_records.size()) - 1;
+}
+ProfScope::~ProfScope() {
+    if (slot < 0) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    cudaEventRecord(g_prof_records[slot].stop, stream());
+}
+
+}  // namespace mbg
+
+using namespace mbg;
+
+extern "C" {
+
+int mbg_set_stream(void* s) {
+    if (g_stream != static_cast<cudaStream_t>(s)) {
+        // work still queued on the old stream may use cached workspace blocks
+        if (cudaStreamSynchronize(g_stream) != cudaSuccess) cudaGetLastError();
+        g_stream = static_cast<cudaStream_t>(s);
+    }
+    return MBG_OK;
+}
+void* mbg_get_stream(void) { return g_stream; }
+int mbg_set_sync(int on) { g_sync = (on != 0); return MBG_OK; }
+
+int mbg_synchronize(void) {
+    MBG_CUDA(cudaStreamSynchronize(g_stream));
+    if (read_and_clear_device_error()) return MBG_ERR_TIMEOUT;
+    return MBG_OK;
+}
+
+const char* mbg_status_string(int s) {
+    if (s == MBG_OK) return "success";
+    if (s > 0) return "invalid argument (Netlib info = position of the argument)";
+    switch (s) {
+        case MBG_ERR_CUDA: return "CUDA runtime error";
+        case MBG_ERR_ALLOC: return "device workspace allocation failed";
+        case MBG_ERR_UNSUPPORTED: return "unsupported combination";
+        case MBG_ERR_NO_DEVICE: return "no usable CUDA device";
+        case MBG_ERR_TIMEOUT: return "kernel wait limit expired";
+        case MBG_ERR_INVALID_MODE: return "invalid precision mode or slice count";
+        default: return "unknown status";
+    }
+}
+const char* mbg_last_error(void) { return g_last_error.c_str(); }
+int mbg_version(void) { return 100; }
+
+int mbg_release_workspace(void) {
+    MBG_CUDA(cudaStreamSynchronize(g_stream));
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto& kv : g_cache) {
+        for (auto& b : kv.second.free_blocks) cudaFree(b.second);
+        kv.second.free_blocks.clear();
+    }
+    return MBG_OK;
+}
+
+int mbg_prof_enable(int on) { g_prof = (on != 0); return MBG_OK; }
+
+int mbg_prof_reset(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto& r : g_prof_records) {
+        g_event_pool.push_back(r.start);
+        g_event_pool.push_back(r.stop);
+    }
+    g_prof_records.clear();
+    g_launches = 0;
+    return MBG_OK;
+}
+
+int mbg_prof_query(const char* sub, double* total_ms, int64_t* launches) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    double tot = 0.0;
+    int64_t cnt = 0;
+    for (auto& r : g_prof_records) {
+        if (sub && sub[0] && r.name.find(sub) == std::string::npos) continue;
+        if (cudaEventSynchronize(r.stop) != cudaSuccess) { cudaGetLastError(); continue; }
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.start, r.stop) == cudaSuccess) {
+            tot += ms;
+            ++cnt;
+        } else {
+            cudaGetLastError();
+        }
+    }
+    if (total_ms) *total_ms = tot;
+    if (launches) *launches = cnt;
+    return MBG_OK;
+}
+
+int64_t mbg_launch_count(void) { return g_launches.load(); }
+
+int mbg_debug_fail_alloc(int nth) { g_fail_alloc_countdown = nth > 0 ? nth : 0; return MBG_OK; }
+
+}  // extern "C"

@@ -1,0 +1,312 @@
+// Blocked triangular solve — replaces mojoBLAS trsm (src/level3/trsm.mojo:20-275).
+//
+// The reference runs an unblocked, single-threaded substitution per right-hand
+// side column (:105-168).  Here the triangle is split recursively at a multiple
+// of 64 rows until a diagonal block of at most 64 rows is left:
+//     effective lower op(A):  X1 = solve(A11, B1);  B2 -= op(A)21 X1;  X2 = solve(A22, B2)
+//     effective upper op(A):  X2 = solve(A22, B2);  B1 -= op(A)12 X2;  X1 = solve(A11, B1)
+// The off-diagonal updates are gemm calls in the caller's precision mode (plain
+// FP32/FP64, BF16x3/x6 split, or Ozaki int8 slices), so almost all flops run in
+// large GEMMs.  Diagonal blocks are solved by `diag_solve_kernel`: the block is
+// staged once per CTA in shared memory in canonical column-major form, and
+// each warp owns one right-hand-side column, two rows per lane, broadcasting the
+// pivot with a warp shuffle — the reference's column-axpy substitution
+// (:130-148), divide by the diagonal included, with the same skip of zero pivots.
+//
+// Right side: X op(A) = alpha B  <=>  op(A)^T X^T = alpha B^T.  B is transposed
+// into a workspace (alpha folded in), solved from the left with the transpose
+// flag flipped, and transposed back.  This follows Netlib; the reference's
+// right-side Trans branches ignore the transpose (:224-273).
+//
+// Iterative refinement (refine > 0): keep alpha*B, solve, form
+// R = alpha*B - op(A) X with the accurate residual product (FP64 / BF16x6 /
+// 8-slice Ozaki by recursion, diagonal blocks in the input precision), solve
+// op(A) D = R in the caller's mode and add D to X.
+#include "mbg_internal.cuh"
+
+namespace mbg {
+
+namespace {
+
+constexpr int NB = 64;        // diagonal block (leaf) size
+constexpr int DS_WARPS = 8;   // columns per CTA in flight
+
+// Solves op(A)[r0:r0+nb, r0:r0+nb] X = B[r0:r0+nb, :] in place.
+// LOWER: effective op(A) lower triangular (forward), else upper (backward).
+template <typename T, bool LOWER, bool TRANS, bool UNIT>
+__global__ void __launch_bounds__(DS_WARPS * 32)
+diag_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __restrict__ B, i64 ldb) {
+    __shared__ T Ls[NB * (NB + 1)];
+    // stage op(A) block, column-major with a padded leading dimension
+    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+        int i, l;
+        if (TRANS) { l = e % nb; i = e / nb; } else { i = e % nb; l = e / nb; }  // coalesced reads
+        const bool in_tri = LOWER ? (i >= l) : (i <= l);
+        T v = T(0);
+        if (in_tri && !(UNIT && i == l)) v = TRANS ? A[l + (i64)i * lda] : A[i + (i64)l * lda];
+        if (UNIT && i == l) v = T(1);
+        Ls[l * (NB + 1) + i] = v;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (i64 j = (i64)blockIdx.x * DS_WARPS + warp; j < ncols; j += (i64)gridDim.x * DS_WARPS) {
+        T* bj = B + j * ldb;
+        T x0 = lane < nb ? bj[lane] : T(0);
+        T x1 = lane + 32 < nb ? bj[lane + 32] : T(0);
+        for (int s = 0; s < nb; ++s) {
+            const int l = LOWER ? s : nb - 1 - s;
+            const T src = (l < 32) ? x0 : x1;
+            T xl = __shfl_sync(0xffffffffu, src, l & 31);
+            if (xl == T(0)) continue;  // the reference skips zero pivots (:133, :115)
+            if (!UNIT) xl = xl / Ls[l * (NB + 1) + l];
+            if (lane == (l & 31)) { if (l < 32) x0 = xl; else x1 = xl; }
+            const T* col = Ls + l * (NB + 1);
+            if (LOWER) {
+                if (lane > l) x0 -= xl * col[lane];
+                if (lane + 32 > l && lane + 32 < nb) x1 -= xl * col[lane + 32];
+            } else {
+                if (lane < l) x0 -= xl * col[lane];
+                if (lane + 32 < l) x1 -= xl * col[lane + 32];
+            }
+        }
+        if (lane < nb) bj[lane] = x0;
+        if (lane + 32 < nb) bj[lane + 32] = x1;
+    }
+}
+
+// R[0:nb, :] -= tri(op(A)) X[0:nb, :] for one diagonal block (residual leaf).
+template <typename T, bool LOWER, bool TRANS, bool UNIT>
+__global__ void __launch_bounds__(DS_WARPS * 32)
+diag_residual_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, const T* __restrict__ X,
+                     i64 ldx, T* __restrict__ R, i64 ldr) {
+    __shared__ T Ls[NB * (NB + 1)];
+    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+        int i, l;
+        if (TRANS) { l = e % nb; i = e / nb; } else { i = e % nb; l = e / nb; }
+        const bool in_tri = LOWER ? (i >= l) : (i <= l);
+        T v = T(0);
+        if (in_tri && !(UNIT && i == l)) v = TRANS ? A[l + (i64)i * lda] : A[i + (i64)l * lda];
+        if (UNIT && i == l) v = T(1);
+        Ls[l * (NB + 1) + i] = v;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (i64 j = (i64)blockIdx.x * DS_WARPS + warp; j < ncols; j += (i64)gridDim.x * DS_WARPS) {
+        const T* xj = X + j * ldx;
+        T a0 = T(0), a1 = T(0);
+        for (int l = 0; l < nb; ++l) {
+            const T xl = xj[l];
+            a0 = fma(Ls[l * (NB + 1) + lane], xl, a0);
+            if (lane + 32 < nb) a1 = fma(Ls[l * (NB + 1) + lane + 32], xl, a1);
+        }
+        T* rj = R + j * ldr;
+        if (lane < nb) rj[lane] -= a0;
+        if (lane + 32 < nb) rj[lane + 32] -= a1;
+    }
+}
+
+template <typename T>
+__global__ void transpose_scale_kernel(i64 rows, i64 cols, T alpha, const T* __restrict__ src,
+                                       i64 lds, T* __restrict__ dst, i64 ldd) {
+    __shared__ T tile[32][33];
+    const i64 i0 = (i64)blockIdx.x * 32, j0 = (i64)blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const i64 i = i0 + threadIdx.x, j = j0 + r;
+        if (i < rows && j < cols) tile[r][threadIdx.x] = alpha * src[i + j * lds];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const i64 j = j0 + threadIdx.x, i = i0 + r;
+        if (i < rows && j < cols) dst[j + i * ldd] = tile[threadIdx.x][r];
+    }
+}
+
+template <typename T>
+__global__ void axpy_matrix_kernel(i64 m, i64 n, T alpha, const T* __restrict__ x, i64 ldx,
+                                   T* __restrict__ y, i64 ldy) {
+    for (i64 j = blockIdx.y; j < n; j += gridDim.y)
+        for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x)
+            y[i + j * ldy] += alpha * x[i + j * ldx];
+}
+
+template <typename T>
+__global__ void copy_scale_kernel(i64 m, i64 n, T alpha, const T* __restrict__ x, i64 ldx,
+                                  T* __restrict__ y, i64 ldy) {
+    for (i64 j = blockIdx.y; j < n; j += gridDim.y)
+        for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x)
+            y[i + j * ldy] = alpha * x[i + j * ldx];
+}
+
+unsigned ds_grid(i64 ncols) { return (unsigned)imin(cdiv(ncols, DS_WARPS), 148 * 8); }
+
+template <typename T>
+int launch_diag_solve(bool lower, bool trans, bool unit, int nb, i64 n, const T* a, i64 lda, T* b, i64 ldb) {
+    ProfScope prof("trsm_diag_solve");
+    const dim3 g(ds_grid(n)), blk(DS_WARPS * 32);
+    cudaStream_t s = stream();
+#define DS(L, TR, U) diag_solve_kernel<T, L, TR, U><<<g, blk, 0, s>>>(nb, n, a, lda, b, ldb)
+    if (lower) {
+        if (trans) { if (unit) DS(true, true, true); else DS(true, true, false); }
+        else { if (unit) DS(true, false, true); else DS(true, false, false); }
+    } else {
+        if (trans) { if (unit) DS(false, true, true); else DS(false, true, false); }
+        else { if (unit) DS(false, false, true); else DS(false, false, false); }
+    }
+#undef DS
+    return check_launch("trsm_diag_solve");
+}
+
+template <typename T>
+int launch_diag_residual(bool lower, bool trans, bool unit, int nb, i64 n, const T* a, i64 lda,
+                         const T* x, i64 ldx, T* r, i64 ldr) {
+    ProfScope prof("trsm_diag_residual");
+    const dim3 g(ds_grid(n)), blk(DS_WARPS * 32);
+    cudaStream_t s = stream();
+#define DR(L, TR, U) diag_residual_kernel<T, L, TR, U><<<g, blk, 0, s>>>(nb, n, a, lda, x, ldx, r, ldr)
+    if (lower) {
+        if (trans) { if (unit) DR(true, true, true); else DR(true, true, false); }
+        else { if (unit) DR(true, false, true); else DR(true, false, false); }
+    } else {
+        if (trans) { if (unit) DR(false, true, true); else DR(false, true, false); }
+        else { if (unit) DR(false, false, true); else DR(false, false, false); }
+    }
+#undef DR
+    return check_launch("trsm_diag_residual");
+}
+
+// gemm in a precision mode, device operands
+inline int gemm_in_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, float alpha,
+                        const float* a, i64 lda, const float* b, i64 ldb, float beta, float* c, i64 ldc) {
+    (void)slices;
+    return sgemm_mode(mode, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+inline int gemm_in_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
+                        const double* a, i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+    return dgemm_mode(mode, slices, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+inline i64 split_point(i64 m) { return cdiv(cdiv(m, 2), NB) * NB; }
+
+// Pointer to op(A)[r, c] for a column-major A.
+template <typename T>
+inline const T* op_at(const T* a, i64 lda, bool trans, i64 r, i64 c) {
+    return trans ? a + c + r * lda : a + r + c * lda;
+}
+
+// op(A) X = B (in place), left side, op(A) effectively lower/upper.
+template <typename T>
+int solve_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, const T* a,
+               i64 lda, T* b, i64 ldb) {
+    if (m <= NB) return launch_diag_solve<T>(lower, trans, unit, (int)m, n, a, lda, b, ldb);
+    const i64 m1 = split_point(m), m2 = m - m1;
+    const char tc = trans ? 'T' : 'N';
+    const T* a11 = a;
+    const T* a22 = a + m1 + m1 * lda;
+    if (lower) {
+        MBG_TRY(solve_left<T>(mode, slices, lower, trans, unit, m1, n, a11, lda, b, ldb));
+        MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m2, n, m1, T(-1), op_at(a, lda, trans, m1, 0), lda,
+                             b, ldb, T(1), b + m1, ldb));
+        return solve_left<T>(mode, slices, lower, trans, unit, m2, n, a22, lda, b + m1, ldb);
+    }
+    MBG_TRY(solve_left<T>(mode, slices, lower, trans, unit, m2, n, a22, lda, b + m1, ldb));
+    MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m1, n, m2, T(-1), op_at(a, lda, trans, 0, m1), lda,
+                         b + m1, ldb, T(1), b, ldb));
+    return solve_left<T>(mode, slices, lower, trans, unit, m1, n, a11, lda, b, ldb);
+}
+
+// R -= tri(op(A)) X, left side.
+template <typename T>
+int residual_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, const T* a,
+                  i64 lda, const T* x, i64 ldx, T* r, i64 ldr) {
+    if (m <= NB) return launch_diag_residual<T>(lower, trans, unit, (int)m, n, a, lda, x, ldx, r, ldr);
+    const i64 m1 = split_point(m), m2 = m - m1;
+    const char tc = trans ? 'T' : 'N';
+    MBG_TRY(residual_left<T>(mode, slices, lower, trans, unit, m1, n, a, lda, x, ldx, r, ldr));
+    MBG_TRY(residual_left<T>(mode, slices, lower, trans, unit, m2, n, a + m1 + m1 * lda, lda, x + m1,
+                             ldx, r + m1, ldr));
+    if (lower)  // R2 -= op(A)21 X1
+        return gemm_in_mode(mode, slices, tc, 'N', m2, n, m1, T(-1), op_at(a, lda, trans, m1, 0), lda,
+                            x, ldx, T(1), r + m1, ldr);
+    // R1 -= op(A)12 X2
+    return gemm_in_mode(mode, slices, tc, 'N', m1, n, m2, T(-1), op_at(a, lda, trans, 0, m1), lda,
+                        x + m1, ldx, T(1), r, ldr);
+}
+
+template <typename T>
+int launch_transpose(i64 rows, i64 cols, T alpha, const T* src, i64 lds, T* dst, i64 ldd) {
+    ProfScope prof("transpose");
+    dim3 g((unsigned)cdiv(rows, 32), (unsigned)cdiv(cols, 32)), blk(32, 8);
+    if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
+    transpose_scale_kernel<T><<<g, blk, 0, stream()>>>(rows, cols, alpha, src, lds, dst, ldd);
+    return check_launch("transpose");
+}
+
+template <typename T>
+int launch_axpy(i64 m, i64 n, T alpha, const T* x, i64 ldx, T* y, i64 ldy) {
+    ProfScope prof("axpy");
+    dim3 g((unsigned)imin(cdiv(m, 256), 64), (unsigned)imin(n, 65535));
+    axpy_matrix_kernel<T><<<g, 256, 0, stream()>>>(m, n, alpha, x, ldx, y, ldy);
+    return check_launch("axpy");
+}
+
+template <typename T>
+int launch_copy(i64 m, i64 n, T alpha, const T* x, i64 ldx, T* y, i64 ldy) {
+    ProfScope prof("copy");
+    dim3 g((unsigned)imin(cdiv(m, 256), 64), (unsigned)imin(n, 65535));
+    copy_scale_kernel<T><<<g, 256, 0, stream()>>>(m, n, alpha, x, ldx, y, ldy);
+    return check_launch("copy");
+}
+
+int accurate_mode(float) { return MBG_MODE_BF16X6; }
+int accurate_mode(double) { return MBG_MODE_OZAKI; }
+
+// Left-side solve with optional refinement; B already holds alpha*B.
+template <typename T>
+int solve_left_refined(int mode, int slices, int refine, bool lower, bool trans, bool unit, i64 m,
+                       i64 n, const T* a, i64 lda, T* b, i64 ldb) {
+    if (refine <= 0 || mode == MBG_MODE_PLAIN)
+        return solve_left<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb);
+    Workspace w_rhs, w_res;
+    MBG_TRY(w_rhs.reserve(sizeof(T) * size_t(m) * size_t(n)));
+    MBG_TRY(w_res.reserve(sizeof(T) * size_t(m) * size_t(n)));
+    T* rhs = w_rhs.as<T>();
+    T* res = w_res.as<T>();
+    MBG_TRY(launch_copy<T>(m, n, T(1), b, ldb, rhs, m));
+    MBG_TRY(solve_left<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb));
+    const int acc_mode = accurate_mode(T(0));
+    for (int it = 0; it < refine; ++it) {
+        MBG_TRY(launch_copy<T>(m, n, T(1), rhs, m, res, m));
+        MBG_TRY(residual_left<T>(acc_mode, 8, lower, trans, unit, m, n, a, lda, b, ldb, res, m));
+        MBG_TRY(solve_left<T>(mode, slices, lower, trans, unit, m, n, a, lda, res, m));
+        MBG_TRY(launch_axpy<T>(m, n, T(1), res, m, b, ldb));
+    }
+    return MBG_OK;
+}
+
+}  // namespace
+
+template <typename T>
+int trsm_device(int mode, int slices, int refine, char side, char uplo, char ta, char diag, i64 m,
+                i64 n, T alpha, const T* a, i64 lda, T* b, i64 ldb) {
+    if (m == 0 || n == 0) return MBG_OK;
+    const bool trans = is_t(ta), unit = is_u(diag), up = is_u(uplo);
+    if (is_l(side)) {
+        if (alpha != T(1)) MBG_TRY(scale_matrix<T>(m, n, alpha, b, ldb));
+        const bool lower = (!up) != trans;  // effective op(A) lower triangular
+        return solve_left_refined<T>(mode, slices, refine, lower, trans, unit, m, n, a, lda, b, ldb);
+    }
+    // right side: op(A)^T X^T = alpha B^T
+    Workspace wt;
+    MBG_TRY(wt.reserve(sizeof(T) * size_t(m) * size_t(n)));
+    T* bt = wt.as<T>();
+    MBG_TRY(launch_transpose<T>(m, n, alpha, b, ldb, bt, n));   // bt is n x m, ld n
+    const bool trans2 = !trans;
+    const bool lower2 = (!up) != trans2;
+    MBG_TRY(solve_left_refined<T>(mode, slices, refine, lower2, trans2, unit, n, m, a, lda, bt, n));
+    return launch_transpose<T>(n, m, T(1), bt, n, b, ldb);
+}
+
+template int trsm_device<float>(int, int, int, char, char, char, char, i64, i64, float, const float*, i64, float*, i64);
+template int trsm_device<double>(int, int, int, char, char, char, char, i64, i64, double, const double*, i64, double*, i64);
+
+}  // namespace mbg

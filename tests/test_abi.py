@@ -1,0 +1,126 @@
+"""CPU-side checks of the C ABI: the library loads without a GPU, exports every
+symbol include/mojoblas_gpu.h declares, and rejects invalid arguments with the
+reference's Netlib `info` numbering before touching the device."""
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import mojoblas_b200 as mb
+from mojoblas_b200 import _lib as L
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "mojoblas_gpu.h"
+
+
+def declared_symbols():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(mbg_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load()
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    assert set(declared_symbols()) <= set(L.SIGNATURES), set(declared_symbols()) - set(L.SIGNATURES)
+
+
+def test_version_and_status_strings():
+    lib = L.load()
+    assert lib.mbg_version() >= 100
+    assert L.status_string(0) == "success"
+    assert "Netlib" in L.status_string(3)
+    assert L.status_string(L.MBG_ERR_TIMEOUT)
+
+
+Z = np.zeros(64, dtype=np.float32)
+D = np.zeros(64, dtype=np.float64)
+
+
+@pytest.mark.parametrize("args,info", [
+    (("X", "N", 2, 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 1),
+    (("N", "q", 2, 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 2),
+    (("N", "N", -1, 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 3),
+    (("N", "N", 2, -1, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 4),
+    (("N", "N", 2, 2, -1, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 5),
+    (("N", "N", 3, 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 3), 8),
+    (("T", "N", 2, 2, 3, 1.0, Z, 2, Z, 3, 0.0, Z, 2), 8),
+    (("N", "N", 2, 2, 3, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 10),
+    (("N", "T", 2, 3, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 10),
+    (("N", "N", 3, 2, 2, 1.0, Z, 3, Z, 2, 0.0, Z, 2), 13),
+])
+def test_gemm_info_codes(args, info, capsys):
+    assert mb.gemm(*args) == info
+    assert f"gemm: Info {info}" in capsys.readouterr().out
+
+
+def test_gemm_double_and_modes_info():
+    assert mb.gemm("N", "N", 2, 2, 2, 1.0, D, 1, D, 2, 0.0, D, 2) == 8
+    assert mb.gemm("N", "N", 2, 2, 2, 1.0, Z, 1, Z, 2, 0.0, Z, 2, mode=mb.BF16X3) == 8
+    assert mb.gemm("N", "N", 2, 2, 2, 1.0, D, 2, D, 1, 0.0, D, 2, mode=mb.OZAKI) == 10
+
+
+@pytest.mark.parametrize("args,info", [
+    (("X", "N", 2, 2, 1.0, Z, 2, 0.0, Z, 2), 1),
+    (("L", "X", 2, 2, 1.0, Z, 2, 0.0, Z, 2), 2),
+    (("L", "N", -2, 2, 1.0, Z, 2, 0.0, Z, 2), 3),
+    (("L", "N", 2, -2, 1.0, Z, 2, 0.0, Z, 2), 4),
+    (("L", "N", 3, 2, 1.0, Z, 2, 0.0, Z, 3), 7),
+    (("U", "T", 2, 3, 1.0, Z, 2, 0.0, Z, 2), 7),
+    (("U", "N", 3, 2, 1.0, Z, 3, 0.0, Z, 2), 10),
+])
+def test_syrk_info_codes(args, info):
+    assert mb.syrk(*args) == info
+
+
+@pytest.mark.parametrize("args,info", [
+    (("X", "L", "N", "N", 2, 2, 1.0, Z, 2, Z, 2), 1),
+    (("L", "X", "N", "N", 2, 2, 1.0, Z, 2, Z, 2), 2),
+    (("L", "L", "X", "N", 2, 2, 1.0, Z, 2, Z, 2), 3),
+    (("L", "L", "N", "X", 2, 2, 1.0, Z, 2, Z, 2), 4),
+    (("L", "L", "N", "N", -1, 2, 1.0, Z, 2, Z, 2), 5),
+    (("L", "L", "N", "N", 2, -1, 1.0, Z, 2, Z, 2), 6),
+    (("L", "L", "N", "N", 3, 2, 1.0, Z, 2, Z, 3), 9),
+    (("R", "L", "N", "N", 2, 3, 1.0, Z, 2, Z, 2), 9),
+    (("L", "L", "N", "N", 3, 2, 1.0, Z, 3, Z, 2), 11),
+])
+def test_trsm_info_codes(args, info):
+    assert mb.trsm(*args) == info
+
+
+def test_quick_returns_touch_no_device():
+    # m == 0 / n == 0 / syrk alpha == 0 and beta == 1 return before any CUDA call
+    assert mb.gemm("N", "N", 0, 5, 5, 1.0, Z, 1, Z, 5, 0.0, Z, 1) == 0
+    assert mb.gemm("T", "N", 4, 0, 5, 1.0, Z, 5, Z, 5, 0.0, Z, 4) == 0
+    assert mb.syrk("L", "N", 0, 3, 1.0, Z, 1, 0.0, Z, 1) == 0
+    assert mb.syrk("L", "N", 3, 3, 0.0, Z, 3, 1.0, Z, 3) == 0
+    assert mb.trsm("L", "L", "N", "N", 0, 3, 1.0, Z, 1, Z, 1) == 0
+    assert mb.trsm("R", "U", "T", "U", 3, 0, 1.0, Z, 1, Z, 3) == 0
+
+
+def test_invalid_mode_rejected():
+    lib = L.load()
+    assert lib.mbg_sgemm_ex(9, b"N", b"N", 1, 1, 1, 1.0, Z.ctypes.data, 1, Z.ctypes.data, 1, 0.0,
+                            Z.ctypes.data, 1) == L.MBG_ERR_INVALID_MODE
+    assert lib.mbg_dgemm_ex(L.MODE_OZAKI, 1, b"N", b"N", 1, 1, 1, 1.0, D.ctypes.data, 1,
+                            D.ctypes.data, 1, 0.0, D.ctypes.data, 1) == L.MBG_ERR_INVALID_MODE
+    assert lib.mbg_dgemm_ex(L.MODE_OZAKI, 9, b"N", b"N", 1, 1, 1, 1.0, D.ctypes.data, 1,
+                            D.ctypes.data, 1, 0.0, D.ctypes.data, 1) == L.MBG_ERR_INVALID_MODE
+
+
+def test_cuda_failure_is_reported_not_silent():
+    """Without a usable GPU a compute call must fail loudly (no CPU fallback)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    a = np.ones((2, 2), np.float32, order="F")
+    with pytest.raises(mb.MbgError):
+        mb.gemm("N", "N", 2, 2, 2, 1.0, a, 2, a, 2, 0.0, a.copy(order="F"), 2)
