@@ -1,0 +1,408 @@
+"""Benchmark: TFLOP/s at fixed FP64-oracle error, split-precision tensor-core
+GEMM vs the plain FP32/FP64 kernels, on the large-GEMM workload:
+
+    sgemm NT and TN, M = N = K = 8192, float32, alpha = 1, beta = 0,
+    entries uniform[-1, 1) from a seeded generator (synthetic, as the
+    reference publishes no dataset), plus dgemm NN 4096^3 (plain FP64 vs
+    Ozaki int8 slices) reported beside it.
+
+One step = one NT and one TN sgemm 8192^3 in the split-precision mode (BF16x6
+by default: the mode whose error is at or below the plain FP32 kernel's at
+K = 8192).  `value` is whole-job TFLOP/s (2*M*N*K per call) with inputs
+resident in HBM (each input is 256 MiB, larger than the 126 MB L2); `e2e` is
+the same metric through the C ABI with pinned host buffers, so every step
+includes the host->device copies of A and B and the device->host copy of C.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica (the path has no
+data exchange) and rank 0 prints the line; time is the max over ranks.
+`--impl reference` times the reference's own algorithm for the same calls
+(mojoBLAS gemm -> _gemm_naive for NT/TN, restated in C++ with OpenMP) on the
+host cores, on a bounded column sample of each call.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_S = 8192      # sgemm size
+N_D = 4096      # dgemm size
+FLOPS_S = 2.0 * N_S ** 3
+FLOPS_D = 2.0 * N_D ** 3
+SAMPLE_ROWS = 256  # rows of C checked against the float64 oracle
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16": d["bf16_tflops"], "bf16_sustained": d["bf16_tflops_sustained"],
+                "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16": 1590.0, "bf16_sustained": 1400.0, "source": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.dev = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def col_major(torch, rows, cols, gen, dtype, device):
+    """rows x cols column-major matrix (stored as a cols x rows row-major tensor)."""
+    t = torch.rand((cols, rows), generator=gen, dtype=torch.float64 if dtype == "f64" else torch.float32,
+                   device=device)
+    return t.mul_(2).sub_(1)
+
+
+def ref_rows(ta, tb, a, b, rows):
+    """float64 oracle rows of C = op(A) op(B) (a, b: column-major torch tensors)."""
+    A = a.double().cpu().numpy().T  # A[i, l]
+    B = b.double().cpu().numpy().T
+    opA = A if ta == "N" else A.T
+    opB = B if tb == "N" else B.T
+    return opA[rows, :] @ opB
+
+
+def rows_error(c, ref, rows):
+    """max|C - C64| / max|C64| on the sampled rows."""
+    got = c.double().cpu().numpy().T[rows, :]
+    return float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    import mojoblas_b200 as mb
+    from mojoblas_b200 import _lib as L
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    lib = L.load()
+    stream = torch.cuda.current_stream()
+    lib.mbg_set_stream(C.c_void_p(stream.cuda_stream))
+    lib.mbg_set_sync(0)
+    mode = {"bf16x3": L.MODE_BF16X3, "bf16x6": L.MODE_BF16X6}[args.mode]
+    nprod = 3 if args.mode == "bf16x3" else 6
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1234 + rank)
+    A = col_major(torch, N_S, N_S, g, "f32", "cuda")
+    B = col_major(torch, N_S, N_S, g, "f32", "cuda")
+    Cm = torch.empty((N_S, N_S), dtype=torch.float32, device="cuda")
+    n = N_S
+
+    def call(md, ta, tb, c=Cm):
+        st = lib.mbg_sgemm_ex(md, ta.encode(), tb.encode(), n, n, n, 1.0, A.data_ptr(), n, B.data_ptr(), n,
+                              0.0, c.data_ptr(), n)
+        if st:
+            raise RuntimeError(f"mbg_sgemm_ex({md}) failed: {st} {L.last_error()}")
+
+    def step(md):
+        call(md, "N", "T")
+        call(md, "T", "N")
+
+    def timed(md, steps, warmup):
+        for _ in range(warmup):
+            step(md)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        lib.mbg_prof_reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step(md)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = int(lib.mbg_launch_count())
+        ms = e0.elapsed_time(e1) / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches
+
+    # ---- headline: split-precision sgemm ----
+    clocks = Clocks(dev)
+    with clocks:
+        ms, launches = timed(mode, args.steps, args.warmup)
+    value = world * 2 * FLOPS_S / (ms * 1e-3) / 1e12
+
+    # per-kernel timing of the dominant kernel (CUDA events around each launch)
+    lib.mbg_prof_enable(1)
+    lib.mbg_prof_reset()
+    for _ in range(max(2, args.steps // 2)):
+        step(mode)
+    torch.cuda.synchronize()
+    kname = b"tc_gemm_" + args.mode.encode()
+    tot, cnt = C.c_double(), C.c_int64()
+    lib.mbg_prof_query(kname, C.byref(tot), C.byref(cnt))
+    k_ms = tot.value / max(cnt.value, 1)
+    lib.mbg_prof_query(b"split_bf16", C.byref(tot), C.byref(cnt))
+    split_ms = tot.value / max(cnt.value, 1)
+    lib.mbg_prof_enable(0)
+
+    # ---- errors against the float64 oracle (sampled rows) ----
+    rs = np.random.default_rng(7).choice(N_S, SAMPLE_ROWS, replace=False)
+    errs, refs = {}, {}
+    Cp = torch.empty_like(Cm)
+    for ta, tb in (("N", "T"), ("T", "N")):
+        refs[ta + tb] = ref_rows(ta, tb, A, B, rs)
+        call(mode, ta, tb)
+        call(L.MODE_PLAIN, ta, tb, Cp)
+        torch.cuda.synchronize()
+        errs[ta + tb] = {args.mode: rows_error(Cm, refs[ta + tb], rs),
+                         "plain_fp32": rows_error(Cp, refs[ta + tb], rs)}
+    del Cp
+
+    # ---- plain FP32 for the same step ----
+    ms_plain, _ = timed(L.MODE_PLAIN, max(2, args.steps // 4), 1)
+    plain_tflops = world * 2 * FLOPS_S / (ms_plain * 1e-3) / 1e12
+
+    # ---- the other split mode, for reference ----
+    other = "bf16x3" if args.mode == "bf16x6" else "bf16x6"
+    other_mode = L.MODE_BF16X3 if other == "bf16x3" else L.MODE_BF16X6
+    ms_other, _ = timed(other_mode, max(2, args.steps // 2), 1)
+    for ta, tb in (("N", "T"), ("T", "N")):
+        call(other_mode, ta, tb)
+        torch.cuda.synchronize()
+        errs[ta + tb][other] = rows_error(Cm, refs[ta + tb], rs)
+
+    # ---- dgemm 4096^3 NN: plain FP64 vs Ozaki ----
+    dg = {}
+    if not args.skip_dgemm:
+        Ad = col_major(torch, N_D, N_D, g, "f64", "cuda")
+        Bd = col_major(torch, N_D, N_D, g, "f64", "cuda")
+        Cd = torch.empty((N_D, N_D), dtype=torch.float64, device="cuda")
+        rsd = np.random.default_rng(8).choice(N_D, SAMPLE_ROWS, replace=False)
+        refd = ref_rows("N", "N", Ad, Bd, rsd)
+
+        def dcall(md, s):
+            st = lib.mbg_dgemm_ex(md, s, b"N", b"N", N_D, N_D, N_D, 1.0, Ad.data_ptr(), N_D, Bd.data_ptr(), N_D,
+                                  0.0, Cd.data_ptr(), N_D)
+            if st:
+                raise RuntimeError(f"mbg_dgemm_ex failed: {st} {L.last_error()}")
+
+        for label, md, s in (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s7", L.MODE_OZAKI, 7),
+                             ("ozaki_s8", L.MODE_OZAKI, 8)):
+            for _ in range(2):
+                dcall(md, s)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 3
+            e0.record(stream)
+            for _ in range(reps):
+                dcall(md, s)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            dms = e0.elapsed_time(e1) / reps
+            dg[label] = {"tflops": round(FLOPS_D / (dms * 1e-3) / 1e12, 2), "ms": round(dms, 3),
+                         "fp64_err": rows_error(Cd, refd, rsd)}
+        del Ad, Bd, Cd
+
+    # ---- e2e through the C ABI with pinned host buffers ----
+    hA = A.cpu().pin_memory()
+    hB = B.cpu().pin_memory()
+    hC = torch.empty((N_S, N_S), dtype=torch.float32).pin_memory()
+    lib.mbg_set_sync(1)
+
+    def e2e_step():
+        for ta, tb in (("N", "T"), ("T", "N")):
+            st = lib.mbg_sgemm_ex(mode, ta.encode(), tb.encode(), n, n, n, 1.0, hA.data_ptr(), n, hB.data_ptr(), n,
+                                  0.0, hC.data_ptr(), n)
+            if st:
+                raise RuntimeError(f"e2e call failed: {st} {L.last_error()}")
+        return float(hC[0, 0])  # host read of the result
+
+    e2e_step()
+    if dist:
+        dist.barrier()
+    e2e_steps = max(2, args.steps // 4)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    lib.mbg_set_sync(0)
+    e2e_value = world * 2 * FLOPS_S / (e2e_ms * 1e-3) / 1e12
+    bytes_in = 2 * 2 * N_S * N_S * 4  # A and B per call, two calls
+    bytes_out = 2 * N_S * N_S * 4
+
+    pk = peaks()
+    achieved_tensor = nprod * FLOPS_S / (k_ms * 1e-3) / 1e12
+    out = {
+        "metric": "TFLOP/s at fixed FP64-oracle error (split-precision tensor-core sgemm vs plain FP32)",
+        "value": round(value, 2),
+        "unit": "TFLOP/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (bf16 split terms, fp32 accumulation)",
+        "data": "synthetic: uniform[-1,1) seeded (torch.Generator 1234+rank)",
+        "config": {"workload": "large_gemm: sgemm NT + TN, M=N=K=8192, alpha=1, beta=0",
+                   "mode": args.mode, "l2": "inputs larger than L2 (256 MiB each)",
+                   "parallelism": f"replicas x{world}"},
+        "plain_fp32_tflops": round(plain_tflops, 2),
+        "speedup_vs_plain": round(value / plain_tflops, 2),
+        f"{other}_tflops": round(world * 2 * FLOPS_S / (ms_other * 1e-3) / 1e12, 2),
+        "fp64_oracle_error": errs,
+        "error_metric": f"max|C-C64|/max|C64| over {SAMPLE_ROWS} sampled rows, C64 = float64 numpy",
+        "dgemm_4096": dg,
+        "e2e": {"value": round(e2e_value, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_in,
+                "d2h_bytes_per_step": bytes_out, "ms_per_step": round(e2e_ms, 2)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "tensor", "kernel": kname.decode(),
+                     "achieved": round(achieved_tensor, 1), "peak": pk["bf16"], "unit": "TFLOP/s",
+                     "frac": round(achieved_tensor / pk["bf16"], 3), "traffic": None,
+                     "note": f"bf16 tensor flops = {nprod} products x 2MNK per launch / mean launch time "
+                             f"({k_ms:.3f} ms); peak = {pk['source']} bf16 burst",
+                     "split_prepass_ms": round(split_ms, 3)},
+        "clocks": clocks.summary(),
+    }
+    return out
+
+
+def run_cpu_baseline(args, threads=None, budget_s=None):
+    """Reference algorithm (oracle restatement of _gemm_naive NT/TN) on host cores,
+    over a bounded sample of columns of each 8192^3 call."""
+    import oracle as orc
+    nth = threads or os.cpu_count() or 1
+    orc.set_threads(nth)
+    rng = np.random.default_rng(1234)
+    n = N_S
+    a = np.asfortranarray(rng.uniform(-1, 1, (n, n)).astype(np.float32))
+    b = np.asfortranarray(rng.uniform(-1, 1, (n, n)).astype(np.float32))
+    cols = max(nth, 8)
+    c = np.zeros((n, cols), np.float32, order="F")
+    # NT: op(B)[l, j] = B[j + l*ldb]  -> columns j0.. of C use b + j0
+    # TN: op(B)[l, j] = B[l + j*ldb]  -> columns j0.. use b + j0*ldb
+    def sample(ta, tb):
+        t0 = time.perf_counter()
+        orc.gemm_naive(ta, tb, n, cols, n, 1.0, a, n, b, n, 0.0, c, n)
+        return time.perf_counter() - t0
+    t_nt = sample("N", "T")
+    t_tn = sample("T", "N")
+    flops = 2.0 * n * n * cols * 2
+    return {"value": flops / (t_nt + t_tn) / 1e12, "unit": "TFLOP/s", "cores": nth, "kind": "port",
+            "sample": f"columns 0..{cols - 1} of C for NT and TN 8192^3 (2*8192*8192*{cols} flop each), "
+                      f"float32, mojoBLAS _gemm_naive restated (oracle/ref_level3.cpp), OpenMP {nth} threads",
+            "seconds": round(t_nt + t_tn, 2)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="bf16x6", choices=["bf16x3", "bf16x6"])
+    ap.add_argument("--skip-dgemm", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = max(1, min(args.steps, 3))
+        vals = []
+        info = None
+        for _ in range(steps):
+            info = run_cpu_baseline(args)
+            vals.append(info["value"])
+        v = float(np.mean(vals))
+        line = {"impl": "reference", "metric": "TFLOP/s at fixed FP64-oracle error (split-precision tensor-core "
+                "sgemm vs plain FP32)", "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": steps,
+                "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic: uniform[-1,1) seeded",
+                "config": {"workload": "large_gemm: sgemm NT + TN, M=N=K=8192, alpha=1, beta=0"},
+                "cpu_baseline": {**info, "value": v},
+                "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    out = run_ours(args, rank, world, dist)
+    if rank == 0 and not args.skip_cpu:
+        cb = run_cpu_baseline(args)
+        out["cpu_baseline"] = cb
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

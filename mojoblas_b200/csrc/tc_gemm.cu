@@ -1,17 +1,760 @@
-// Tensor-core (tcgen05) GEMM paths — placeholder until the kernels land.
+// Tensor-core GEMMs on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Two precision forms share one warp-specialised kernel:
+//
+//  * Split-precision sgemm (BF16x3 / BF16x6).  A pre-pass splits each fp32
+//    operand element x into bf16 terms x = x1 + x2 (+ x3) + residual, with
+//    x1 = bf16(x), x2 = bf16(x - x1), x3 = bf16(x - x1 - x2) (each difference is
+//    exact in fp32).  The kernel forms sum_{p+q<T} A_p B_q with
+//    tcgen05.mma.kind::f16 (bf16 inputs, fp32 accumulation in TMEM):
+//    3 products for T=2 (BF16x3), 6 for T=3 (BF16x6).
+//
+//  * Ozaki-scheme dgemm (int8 slices).  A pre-pass scales each row of op(A) and
+//    each column of op(B) by a power of two so that |x'| < 1 and cuts x' into
+//    s slices of 7 bits, x' = sum_p d_p 2^(-7(p+1)), d_p in [-127, 127] (exact in
+//    fp64: multiply by 128, truncate, subtract).  The kernel forms, for each
+//    diagonal t = p+q < s, D_t = sum_{p+q=t} A_p B_q exactly with
+//    tcgen05.mma.kind::i8 (int32 accumulation, one TMEM accumulator per t), and
+//    the epilogue sums 2^(-7(t+2)) D_t from the smallest term up in fp64 and
+//    applies the row and column scales (Ootomo, Ozaki, Yokota, "DGEMM on integer
+//    matrix multiplication unit", IJHPCA 2024; Ozaki, Ogita, Oishi, Rump, 2012).
+//
+// Both pre-passes also transpose as needed, so the kernel always sees
+// K-contiguous ("K-major") operands: planes[term][row][k], rows padded to the
+// tile, k padded to the k-slab, zero-filled.
+//
+// Kernel roles (one CTA per 128 x BN output tile):
+//   warp 0      allocates TMEM; lane 0 issues TMA loads (cp.async.bulk.tensor,
+//               one 3-D box per operand per stage covering every term plane)
+//   warp 1      lane 0 issues the tcgen05.mma instructions and commits each
+//               stage back to the producer, then the accumulators to the epilogue
+//   warps 2..   epilogue (8 warps split, 4 Ozaki): tcgen05.ld from TMEM (warp w
+//               reads lanes 32*(w%4)..), accumulate / scale, add beta*C, store
+//               column-major C with coalesced warps
+// Every mbarrier wait is bounded (about 2 s of globaltimer); on expiry the
+// thread records an error code in the library's mapped error flag and the CTA
+// proceeds to teardown (TMEM is always freed).
 #include "mbg_internal.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <mutex>
 
 namespace mbg {
 
-int sgemm_split_tc(int, char, char, i64, i64, i64, float, const float*, i64, const float*, i64,
-                   float, float*, i64, char) {
-    set_error_msg("split-precision sgemm is not built yet");
-    return MBG_ERR_UNSUPPORTED;
+namespace tc {
+
+constexpr int BM = 128;
+constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-int dgemm_ozaki_tc(int, char, char, i64, i64, i64, double, const double*, i64, const double*, i64,
-                   double, double*, i64) {
-    set_error_msg("Ozaki dgemm is not built yet");
-    return MBG_ERR_UNSUPPORTED;
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int site) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    while (true) {
+#pragma unroll 1
+        for (int i = 0; i < 256; ++i)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+            if (err) {
+                atomicExch(err, 1);
+                atomicExch(err + 1, site);
+            }
+            return false;
+        }
+    }
+}
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0,
+                                            int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+template <bool INT8>
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                     uint32_t accumulate) {
+    if (INT8)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_wait() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor (tcgen05), K-major operand with swizzle:
+// start address and stride-dimension byte offset (between 8-row groups) in
+// 16-byte units, descriptor version 1 (bits 46-47), layout type in bits 61-63
+// (2 = 128-byte swizzle, 4 = 64-byte, 6 = 32-byte).  Tiles are 1024-byte
+// aligned so the base-offset field stays 0.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t sbo_bytes, uint32_t layout) {
+    uint64_t d = 0;
+    d |= uint64_t((saddr >> 4) & 0x3FFFu);
+    d |= uint64_t(1) << 16;  // leading byte offset: unused for swizzled K-major tiles
+    d |= uint64_t((sbo_bytes >> 4) & 0x3FFFu) << 32;
+    d |= uint64_t(1) << 46;
+    d |= uint64_t(layout & 7u) << 61;
+    return d;
+}
+
+// Instruction descriptor: D format (bits 4-5: 1 = f32, 2 = s32), A/B formats
+// (bits 7-9 / 10-12: bf16 = 1 for kind::f16, signed = 1 for kind::i8), both
+// operands K-major (bits 15/16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t instr_desc(bool int8, int M, int N) {
+    return (uint32_t(int8 ? 2 : 1) << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) |
+           (uint32_t(M >> 4) << 24);
+}
+
+// ---------------------------------------------------------------------------
+// Kernel configuration
+// ---------------------------------------------------------------------------
+// TERMS planes per operand; products (p, q) with p + q < TERMS.
+//   split:  every product accumulates into one fp32 accumulator.  The tensor
+//           core's fp32 accumulation truncates, so its error grows linearly in
+//           k; the accumulator is therefore restarted every CHUNK slabs and the
+//           epilogue warps add each chunk into fp32 registers with
+//           round-to-nearest ("promotion").  Two TMEM buffers alternate so the
+//           MMA issuer never waits for a drain.
+//   ozaki:  product (p, q) accumulates into int32 accumulator p + q (exact, so
+//           one chunk covers the whole k range).
+template <bool OZAKI_, int TERMS_, int BN_, int BKB_, int STAGES_, int EPI_WARPS_, int CHUNK_>
+struct Cfg {
+    static constexpr bool OZAKI = OZAKI_;
+    static constexpr int TERMS = TERMS_;
+    static constexpr int BN = BN_;
+    static constexpr int BKB = BKB_;  // k-slab bytes per row (= swizzle width)
+    static constexpr int STAGES = STAGES_;
+    static constexpr int EPI_WARPS = EPI_WARPS_;
+    static constexpr int CHUNK = CHUNK_;  // slabs per TMEM accumulation chunk (split only)
+    static constexpr int THREADS = 64 + 32 * EPI_WARPS;
+    static constexpr int ELEM = OZAKI ? 1 : 2;
+    static constexpr int BK = BKB / ELEM;    // k elements per slab
+    static constexpr int KSTEPS = BKB / 32;  // one MMA consumes 32 bytes of k
+    static constexpr int NPROD = TERMS * (TERMS + 1) / 2;
+    static constexpr int NACC = OZAKI ? TERMS : 2;  // ozaki: one per diagonal; split: two buffers
+    static constexpr int A_PLANE = BM * BKB;
+    static constexpr int B_PLANE = BN * BKB;
+    static constexpr int STAGE_BYTES = TERMS * (A_PLANE + B_PLANE);
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr uint32_t LAYOUT = BKB == 128 ? 2 : (BKB == 64 ? 4 : 6);
+    static constexpr uint32_t SBO = 8 * BKB;
+    static constexpr int TMEM_NEED = NACC * BN;
+    static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
+                                        : TMEM_NEED <= 256 ? 256 : 512;
+    static constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // columns per epilogue thread
+    static constexpr uint32_t IDESC = instr_desc(OZAKI, BM, BN);
+    static_assert(TMEM_NEED <= 512, "accumulators exceed TMEM");
+    static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+    static_assert(A_PLANE % 1024 == 0 && B_PLANE % 1024 == 0, "plane alignment");
+    static_assert(EPI_WARPS % 4 == 0 && EPI_COLS % 16 == 0, "epilogue shape");
+};
+
+using CfgBF16x3 = Cfg<false, 2, 256, 64, 4, 8, 4>;
+using CfgBF16x6 = Cfg<false, 3, 256, 64, 3, 8, 4>;
+template <int S> using CfgOzaki = Cfg<true, S, 64, 32, 4, 4, 0>;
+
+struct Params {
+    i64 m, n;
+    int num_kb;            // k slabs
+    int tiles_m, tiles_n;  // output tiles
+    int tri;               // 0 full, 1 lower, 2 upper (element mask + tile skip)
+    void* c;
+    i64 ldc;
+    double alpha, beta;
+    const int* ea;  // ozaki row exponents (op(A) rows)
+    const int* eb;  // ozaki column exponents (op(B) columns)
+    int* err;
+};
+
+// product table: index -> (p, q); ordered by descending p+q so that small
+// contributions enter each fp32 accumulator first
+template <int TERMS>
+__device__ __forceinline__ void product(int idx, int& p, int& q) {
+    int t = 0;
+    for (int d = TERMS - 1; d >= 0; --d) {
+        for (int pp = 0; pp <= d; ++pp) {
+            if (t == idx) { p = pp; q = d - pp; return; }
+            ++t;
+        }
+    }
+    p = q = 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, 1)
+tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+    uint64_t* empty = full + C::STAGES;
+    uint64_t* tfull = empty + C::STAGES;  // [2]: accumulator buffer ready for the epilogue
+    uint64_t* tempty = tfull + 2;         // [2]: epilogue finished reading a buffer
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+
+    // tile coordinates: groups of 16 m-tiles walk the n-tiles together (L2 reuse)
+    const int tile = blockIdx.x;
+    const int group = 16;
+    const int per_group = group * P.tiles_n;
+    const int g = tile / per_group;
+    const int first_m = g * group;
+    const int gsize = min(group, P.tiles_m - first_m);
+    const int in_g = tile - g * per_group;
+    const int tm = first_m + in_g % gsize;
+    const int tn = in_g / gsize;
+    const i64 m0 = i64(tm) * BM, n0 = i64(tn) * C::BN;
+    if (P.tri == 1 && m0 + BM <= n0) return;        // tile strictly above the diagonal
+    if (P.tri == 2 && m0 > n0 + C::BN - 1) return;  // tile strictly below the diagonal
+
+    const int chunk_slabs = C::OZAKI ? P.num_kb : C::CHUNK;
+    const int nchunks = (P.num_kb + chunk_slabs - 1) / chunk_slabs;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], C::EPI_WARPS);
+        }
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, C::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            prefetch_tmap(&tmA);
+            prefetch_tmap(&tmB);
+            for (int kb = 0; kb < P.num_kb; ++kb) {
+                const int s = kb % C::STAGES;
+                const uint32_t ph = (kb / C::STAGES) & 1;
+                if (!mbar_wait(&empty[s], ph ^ 1, P.err, 1)) break;
+                uint8_t* sa = smem + s * C::STAGE_BYTES;
+                uint8_t* sb = sa + C::TERMS * C::A_PLANE;
+                mbar_expect_tx(&full[s], C::STAGE_BYTES);
+                tma_load_3d(sa, &tmA, &full[s], kb * C::BK, int(m0), 0);
+                tma_load_3d(sb, &tmB, &full[s], kb * C::BK, int(n0), 0);
+            }
+            // all issued loads must land before the CTA can exit: the last
+            // STAGES slabs are the only ones possibly still in flight
+            for (int kb = max(0, P.num_kb - C::STAGES); kb < P.num_kb; ++kb)
+                mbar_wait(&full[kb % C::STAGES], (kb / C::STAGES) & 1, P.err, 2);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            int chunk = 0;
+            for (int kb = 0; kb < P.num_kb; ++kb) {
+                const int kin = kb % chunk_slabs;  // slab index within the chunk
+                const int buf = chunk & 1;
+                if (!C::OZAKI && kin == 0 && chunk >= 2) {
+                    // the epilogue must have drained this buffer's previous chunk
+                    if (!mbar_wait(&tempty[buf], ((chunk >> 1) - 1) & 1, P.err, 5)) break;
+                    tc_fence_after();
+                }
+                const int s = kb % C::STAGES;
+                const uint32_t ph = (kb / C::STAGES) & 1;
+                if (!mbar_wait(&full[s], ph, P.err, 3)) break;
+                tc_fence_after();
+                const uint32_t sa = smem_u32(smem + s * C::STAGE_BYTES);
+                const uint32_t sb = sa + C::TERMS * C::A_PLANE;
+#pragma unroll
+                for (int ks = 0; ks < C::KSTEPS; ++ks) {
+#pragma unroll
+                    for (int pi = 0; pi < C::NPROD; ++pi) {
+                        int p, q;
+                        product<C::TERMS>(pi, p, q);
+                        // the first product into an accumulator in a chunk overwrites it
+                        const bool first = C::OZAKI ? (p == 0) : (pi == 0);
+                        const uint32_t accumulate = (kin > 0 || ks > 0 || !first) ? 1u : 0u;
+                        const uint32_t col = C::OZAKI ? uint32_t((p + q) * C::BN) : uint32_t(buf * C::BN);
+                        const uint64_t ad = smem_desc(sa + p * C::A_PLANE + ks * 32, C::SBO, C::LAYOUT);
+                        const uint64_t bd = smem_desc(sb + q * C::B_PLANE + ks * 32, C::SBO, C::LAYOUT);
+                        umma<C::OZAKI>(tmem + col, ad, bd, C::IDESC, accumulate);
+                    }
+                }
+                umma_commit(&empty[s]);  // slot s is free once these MMAs have read it
+                if (kin == chunk_slabs - 1 || kb == P.num_kb - 1) {
+                    umma_commit(&tfull[buf]);  // chunk complete
+                    ++chunk;
+                }
+            }
+        }
+    } else {
+        // ---------------- epilogue warps ----------------
+        const int e = warp - 2;
+        const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
+        const int part = e >> 2;       // which EPI_COLS-wide column range
+        const i64 row = m0 + quarter * 32 + lane;
+        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16);
+        if constexpr (!C::OZAKI) {
+            float acc[C::EPI_COLS];
+#pragma unroll
+            for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0f;
+            bool ok = true;
+            for (int ch = 0; ch < nchunks; ++ch) {
+                const int buf = ch & 1;
+                if (!mbar_wait(&tfull[buf], (ch >> 1) & 1, P.err, 4)) { ok = false; break; }
+                tc_fence_after();
+#pragma unroll
+                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(lane_base + uint32_t(buf * C::BN + part * C::EPI_COLS + c0), r);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[c0 + j] += __uint_as_float(r[j]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[buf]);
+            }
+            if (ok && row < P.m) {
+                float* Cm = static_cast<float*>(P.c);
+                const float alpha = float(P.alpha), beta = float(P.beta);
+                const i64 cbase = n0 + part * C::EPI_COLS;
+#pragma unroll
+                for (int j = 0; j < C::EPI_COLS; ++j) {
+                    const i64 col = cbase + j;
+                    if (col >= P.n) break;
+                    if (P.tri == 1 && row < col) continue;
+                    if (P.tri == 2 && row > col) continue;
+                    float* cp = Cm + row + col * P.ldc;
+                    const float v = alpha * acc[j];
+                    *cp = (beta == 0.0f) ? v : fmaf(beta, *cp, v);
+                }
+            }
+        } else {
+            if (mbar_wait(&tfull[0], 0, P.err, 4)) {
+                tc_fence_after();
+                double acc[C::BN];
+#pragma unroll
+                for (int j = 0; j < C::BN; ++j) acc[j] = 0.0;
+                // smallest diagonal weight first: t = TERMS-1 .. 0, weight 2^(-7(t+2))
+#pragma unroll 1
+                for (int t = C::NACC - 1; t >= 0; --t) {
+                    const double w = ldexp(1.0, -7 * (t + 2));
+#pragma unroll
+                    for (int c0 = 0; c0 < C::BN; c0 += 16) {
+                        uint32_t r[16];
+                        tmem_ld16(lane_base + uint32_t(t * C::BN + c0), r);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
+                    }
+                }
+                if (row < P.m) {
+                    double* Cm = static_cast<double*>(P.c);
+                    const int er = P.ea[row];
+#pragma unroll
+                    for (int j = 0; j < C::BN; ++j) {
+                        const i64 col = n0 + j;
+                        if (col >= P.n) break;
+                        double* cp = Cm + row + col * P.ldc;
+                        const double v = P.alpha * ldexp(acc[j], er + P.eb[col]);
+                        *cp = (P.beta == 0.0) ? v : fma(P.beta, *cp, v);
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, C::TMEM_COLS);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pre-pass kernels
+// ---------------------------------------------------------------------------
+constexpr int PT_R = 64, PT_K = 32;  // pre-pass tile: 64 rows x 32 k
+
+// value(r, l) of the logical rows x K operand: K-major source src[l + r*ld],
+// otherwise src[r + l*ld]; outside rows x K it is zero (padding).
+template <typename T, bool KMAJOR>
+__device__ __forceinline__ void load_tile(const T* __restrict__ src, i64 ld, i64 rows, i64 K, i64 r0,
+                                          i64 l0, T (&tile)[PT_R][PT_K + 1]) {
+    for (int e = threadIdx.x; e < PT_R * PT_K; e += blockDim.x) {
+        int rr, ll;
+        if (KMAJOR) { rr = e / PT_K; ll = e % PT_K; } else { rr = e % PT_R; ll = e / PT_R; }
+        const i64 r = r0 + rr, l = l0 + ll;
+        T v = T(0);
+        if (r < rows && l < K) v = KMAJOR ? src[l + r * ld] : src[r + l * ld];
+        tile[rr][ll] = v;
+    }
+}
+
+template <int TERMS, bool KMAJOR>
+__global__ void __launch_bounds__(256)
+split_bf16_kernel(const float* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp,
+                  __nv_bfloat16* __restrict__ planes) {
+    __shared__ float tile[PT_R][PT_K + 1];
+    const i64 r0 = i64(blockIdx.y) * PT_R, l0 = i64(blockIdx.x) * PT_K;
+    load_tile<float, KMAJOR>(src, ld, rows, K, r0, l0, tile);
+    __syncthreads();
+    const size_t plane = size_t(Rp) * size_t(Kp);
+    for (int e = threadIdx.x; e < PT_R * (PT_K / 2); e += blockDim.x) {
+        const int rr = e / (PT_K / 2), lp = (e % (PT_K / 2)) * 2;
+        float x0 = tile[rr][lp], x1 = tile[rr][lp + 1];
+        __nv_bfloat162* out = reinterpret_cast<__nv_bfloat162*>(planes + size_t(r0 + rr) * Kp + l0 + lp);
+#pragma unroll
+        for (int t = 0; t < TERMS; ++t) {
+            const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+            out[(plane / 2) * t] = __halves2bfloat162(h0, h1);
+            x0 -= __bfloat162float(h0);  // exact: x0 and h0 agree in their leading bits
+            x1 -= __bfloat162float(h1);
+        }
+    }
+}
+
+// Row exponents for the Ozaki scaling: e(r) with max_l |value(r,l)| < 2^e(r).
+// Partial maxima are combined with atomicMax on the exponent (initialised by
+// the host to 0x80808080, below any double exponent); an all-zero row keeps
+// that value and is mapped to 0.
+template <bool KMAJOR>
+__global__ void row_exponent_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, int* __restrict__ e) {
+    if (KMAJOR) {  // warp per row, lanes stride along k
+        const i64 r = i64(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+        if (r >= rows) return;
+        double mx = 0.0;
+        for (i64 l = (threadIdx.x & 31) + i64(blockIdx.y) * 32; l < K; l += 32 * i64(gridDim.y))
+            mx = fmax(mx, fabs(src[l + r * ld]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((threadIdx.x & 31) == 0 && mx > 0.0) {
+            int ex;
+            frexp(mx, &ex);
+            atomicMax(e + r, ex);
+        }
+    } else {  // thread per row, blocks along k chunks
+        const i64 r = i64(blockIdx.x) * blockDim.x + threadIdx.x;
+        if (r >= rows) return;
+        const i64 chunk = (K + gridDim.y - 1) / gridDim.y;
+        const i64 l0 = i64(blockIdx.y) * chunk, l1 = min(K, l0 + chunk);
+        double mx = 0.0;
+        for (i64 l = l0; l < l1; ++l) mx = fmax(mx, fabs(src[r + l * ld]));
+        if (mx > 0.0) {
+            int ex;
+            frexp(mx, &ex);
+            atomicMax(e + r, ex);
+        }
+    }
+}
+
+__global__ void fix_exponents_kernel(int* e, i64 n) {
+    const i64 i = i64(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n && e[i] < -4096) e[i] = 0;
+}
+
+template <bool KMAJOR>
+__global__ void __launch_bounds__(256)
+slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
+                const int* __restrict__ e, int8_t* __restrict__ planes) {
+    __shared__ double tile[PT_R][PT_K + 1];
+    const i64 r0 = i64(blockIdx.y) * PT_R, l0 = i64(blockIdx.x) * PT_K;
+    load_tile<double, KMAJOR>(src, ld, rows, K, r0, l0, tile);
+    __syncthreads();
+    const size_t plane = size_t(Rp) * size_t(Kp);
+    for (int q = threadIdx.x; q < PT_R * (PT_K / 4); q += blockDim.x) {
+        const int rr = q / (PT_K / 4), lq = (q % (PT_K / 4)) * 4;
+        const i64 r = r0 + rr;
+        const int er = (r < rows) ? e[r] : 0;
+        double x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = ldexp(tile[rr][lq + u], -er);  // |x| < 1
+        char4* out = reinterpret_cast<char4*>(planes + size_t(r) * Kp + l0 + lq);
+        for (int p = 0; p < slices; ++p) {
+            int d[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const double y = x[u] * 128.0;
+                const double t = trunc(y);
+                d[u] = int(t);
+                x[u] = y - t;  // exact
+            }
+            out[(plane / 4) * p] = make_char4((signed char)d[0], (signed char)d[1], (signed char)d[2],
+                                              (signed char)d[3]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// 3-D map over planes[term][row][k]; box = {bkb/elem, box_rows, terms}.
+int make_map(CUtensorMap* map, const void* base, bool int8, i64 Kp, i64 Rp, int terms, int bkb,
+             int box_rows) {
+    auto fn = encode_fn();
+    if (!fn) {
+        set_error_msg("cuTensorMapEncodeTiled is unavailable from the driver");
+        return MBG_ERR_CUDA;
+    }
+    const int elem = int8 ? 1 : 2;
+    cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(Rp), cuuint64_t(terms)};
+    cuuint64_t strides[2] = {cuuint64_t(Kp) * elem, cuuint64_t(Kp) * cuuint64_t(Rp) * elem};
+    cuuint32_t box[3] = {cuuint32_t(bkb / elem), cuuint32_t(box_rows), cuuint32_t(terms)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const CUtensorMapSwizzle sw = bkb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                 : bkb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+    CUresult r = fn(map, int8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
+                    const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error_msg("cuTensorMapEncodeTiled failed (code " + std::to_string(int(r)) + ")");
+        return MBG_ERR_CUDA;
+    }
+    return MBG_OK;
+}
+
+template <class C>
+int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, Params& P, const char* name) {
+    static bool configured = false;  // per instantiation
+    if (!configured) {
+        MBG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      C::SMEM_BYTES));
+        configured = true;
+    }
+    P.err = device_error_flag();
+    const i64 tiles = i64(P.tiles_m) * P.tiles_n;
+    if (tiles > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    ProfScope prof(name);
+    tc_gemm_kernel<C><<<unsigned(tiles), C::THREADS, C::SMEM_BYTES, stream()>>>(ma, mb, P);
+    return check_launch(name);
+}
+
+template <int TERMS>
+int launch_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, __nv_bfloat16* planes) {
+    ProfScope prof("split_bf16");
+    dim3 g(unsigned(Kp / PT_K), unsigned(Rp / PT_R));
+    if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
+    if (kmajor) split_bf16_kernel<TERMS, true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
+    else split_bf16_kernel<TERMS, false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
+    return check_launch("split_bf16");
+}
+
+int launch_slices(const double* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
+                  int* e, int8_t* planes) {
+    {
+        ProfScope prof("ozaki_exponent");
+        MBG_CUDA(cudaMemsetAsync(e, 0x80, sizeof(int) * size_t(rows), stream()));  // 0x80808080 < any exponent
+        if (kmajor) {
+            dim3 g(unsigned(cdiv(rows, 8)), unsigned(imin(cdiv(K, 4096), 16)));
+            row_exponent_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, e);
+        } else {
+            dim3 g(unsigned(cdiv(rows, 256)), unsigned(imin(cdiv(K, 64), 64)));
+            row_exponent_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, e);
+        }
+        MBG_TRY(check_launch("ozaki_exponent"));
+        fix_exponents_kernel<<<unsigned(cdiv(rows, 256)), 256, 0, stream()>>>(e, rows);
+        MBG_TRY(check_launch("ozaki_exponent"));
+    }
+    ProfScope prof("ozaki_slice");
+    dim3 g(unsigned(Kp / PT_K), unsigned(Rp / PT_R));
+    if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
+    if (kmajor) slice_i8_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes);
+    else slice_i8_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes);
+    return check_launch("ozaki_slice");
+}
+
+inline i64 roundup(i64 x, i64 m) { return cdiv(x, m) * m; }
+
+}  // namespace tc
+
+// ---- split-precision sgemm ------------------------------------------------------
+int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a,
+                   i64 lda, const float* b, i64 ldb, float beta, float* c, i64 ldc, char tri_uplo) {
+    using namespace tc;
+    if (m == 0 || n == 0) return MBG_OK;
+    if (terms != 2 && terms != 3) return MBG_ERR_INVALID_MODE;
+    const int BN = 256;
+    const i64 Kp = roundup(k, 32);
+    const bool tri = tri_uplo != 0;
+    // syrk shares one set of planes for both operands (rows padded to BN)
+    const bool shared_planes = tri && a == b && lda == ldb && (is_n(ta) != is_n(tb));
+    const i64 Mp = shared_planes ? roundup(m, BN) : roundup(m, BM);
+    const i64 Np = roundup(n, BN);
+    if (Kp > 0x7fffffff || Mp > 0x7fffffff || Np > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    const size_t a_bytes = size_t(terms) * Mp * Kp * 2, b_bytes = shared_planes ? 0 : size_t(terms) * Np * Kp * 2;
+    Workspace ws;
+    MBG_TRY(ws.reserve(a_bytes + b_bytes));
+    __nv_bfloat16* pa = ws.as<__nv_bfloat16>();
+    __nv_bfloat16* pb = shared_planes ? pa : reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + a_bytes);
+    // op(A) rows are K-contiguous when A is transposed; op(B)^T rows when B is not
+    if (terms == 2) {
+        MBG_TRY(launch_split<2>(a, lda, is_t(ta), m, k, Mp, Kp, pa));
+        if (!shared_planes) MBG_TRY(launch_split<2>(b, ldb, is_n(tb), n, k, Np, Kp, pb));
+    } else {
+        MBG_TRY(launch_split<3>(a, lda, is_t(ta), m, k, Mp, Kp, pa));
+        if (!shared_planes) MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, k, Np, Kp, pb));
+    }
+    CUtensorMap ma, mb;
+    MBG_TRY(make_map(&ma, pa, false, Kp, Mp, terms, 64, BM));
+    MBG_TRY(make_map(&mb, pb, false, Kp, shared_planes ? Mp : Np, terms, 64, BN));
+    Params P{};
+    P.m = m; P.n = n; P.num_kb = int(Kp / 32);
+    P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
+    P.tri = tri ? (is_l(tri_uplo) ? 1 : 2) : 0;
+    P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
+    if (terms == 2) return launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
+    return launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
+}
+
+// ---- Ozaki dgemm ----------------------------------------------------------------
+int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a,
+                   i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+    using namespace tc;
+    if (m == 0 || n == 0) return MBG_OK;
+    if (slices < 2 || slices > 8) return MBG_ERR_INVALID_MODE;
+    const int BN = 64;
+    // int32 accumulators hold at most `slices` products of K terms of 127^2 each
+    const i64 kchunk_max = (i64(0x7fffffff) / (i64(slices) * 127 * 127)) / 32 * 32;
+    const i64 Mp = roundup(m, BM), Np = roundup(n, BN);
+    const i64 kc = imin(k, kchunk_max);
+    const i64 Kp = roundup(kc, 32);
+    const size_t a_bytes = size_t(slices) * Mp * Kp, b_bytes = size_t(slices) * Np * Kp;
+    Workspace ws;
+    MBG_TRY(ws.reserve(a_bytes + b_bytes + sizeof(int) * size_t(Mp + Np) + 1024));
+    int8_t* pa = ws.as<int8_t>();
+    int8_t* pb = pa + a_bytes;
+    int* ea = reinterpret_cast<int*>(pb + b_bytes + (1024 - ((a_bytes + b_bytes) & 1023)) % 1024);
+    int* eb = ea + Mp;
+    for (i64 k0 = 0; k0 < k; k0 += kc) {
+        const i64 klen = imin(kc, k - k0);
+        const i64 Kpc = roundup(klen, 32);
+        // op(A)[:, k0:k0+klen] and op(B)[k0:k0+klen, :]
+        const double* ak = is_n(ta) ? a + k0 * lda : a + k0;
+        const double* bk = is_n(tb) ? b + k0 : b + k0 * ldb;
+        MBG_TRY(launch_slices(ak, lda, is_t(ta), m, klen, Mp, Kpc, slices, ea, pa));
+        MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb));
+        CUtensorMap ma, mb;
+        MBG_TRY(make_map(&ma, pa, true, Kpc, Mp, slices, 32, BM));
+        MBG_TRY(make_map(&mb, pb, true, Kpc, Np, slices, 32, BN));
+        Params P{};
+        P.m = m; P.n = n; P.num_kb = int(Kpc / 32);
+        P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
+        P.tri = 0; P.c = c; P.ldc = ldc; P.alpha = alpha;
+        P.beta = (k0 == 0) ? beta : 1.0;
+        P.ea = ea; P.eb = eb;
+        int st;
+        switch (slices) {
+            case 2: st = launch_tc<CfgOzaki<2>>(ma, mb, P, "tc_gemm_ozaki"); break;
+            case 3: st = launch_tc<CfgOzaki<3>>(ma, mb, P, "tc_gemm_ozaki"); break;
+            case 4: st = launch_tc<CfgOzaki<4>>(ma, mb, P, "tc_gemm_ozaki"); break;
+            case 5: st = launch_tc<CfgOzaki<5>>(ma, mb, P, "tc_gemm_ozaki"); break;
+            case 6: st = launch_tc<CfgOzaki<6>>(ma, mb, P, "tc_gemm_ozaki"); break;
+            case 7: st = launch_tc<CfgOzaki<7>>(ma, mb, P, "tc_gemm_ozaki"); break;
+            default: st = launch_tc<CfgOzaki<8>>(ma, mb, P, "tc_gemm_ozaki"); break;
+        }
+        if (st) return st;
+    }
+    return MBG_OK;
 }
 
 }  // namespace mbg
