@@ -39,6 +39,7 @@ extern "C" {
 #define MBG_ERR_NO_DEVICE     -4  /* no usable CUDA device / driver                   */
 #define MBG_ERR_TIMEOUT       -5  /* a kernel's bounded wait expired (error flag set)  */
 #define MBG_ERR_INVALID_MODE  -6  /* unknown precision mode or slice count            */
+#define MBG_ERR_SCRATCH_LIMIT -7  /* problem exceeds mbg_sgemm_ex_noalloc's fixed scratch */
 
 /* ---- precision modes ---------------------------------------------------- */
 #define MBG_MODE_PLAIN   0  /* FP32 / FP64 FMA on the CUDA cores (the drop-in)           */
@@ -98,6 +99,29 @@ int mbg_strsm_ex(int mode, int refine, char side, char uplo, char trans_a, char 
 int mbg_dtrsm_ex(int mode, int slices, int refine, char side, char uplo, char trans_a,
                  char diag, int64_t m, int64_t n, double alpha, const double* a,
                  int64_t lda, double* b, int64_t ldb);
+
+/* ---- split-precision sgemm that allocates nothing -------------------------
+ * No counterpart in the reference (mojoBLAS allocates host memory freely).
+ * For callers that must not have a library allocate device memory: a host
+ * framework that owns a fixed device-memory budget, a latency-critical loop
+ * where cudaMalloc / cudaFree may synchronise the device, or code inside an
+ * allocator's out-of-memory handling.  Same arguments, numbering and result as
+ * mbg_sgemm_ex with mode MBG_MODE_BF16X3 or MBG_MODE_BF16X6, but:
+ *   - a, b and c must be device pointers (host data would need staging
+ *     buffers); otherwise MBG_ERR_UNSUPPORTED;
+ *   - the bf16 split planes live in a fixed 32 MiB device array owned by the
+ *     library (resident on every GPU that loads it, until the process exits):
+ *     terms * (roundup(m,128) + roundup(n,256)) * roundup(k,32) * 2 bytes must
+ *     fit (terms = 2 for BF16X3, 3 for BF16X6; e.g. m = n = k = 2048 with
+ *     BF16X3), else MBG_ERR_SCRATCH_LIMIT before any device work;
+ *   - the first call on a device resolves that array's device address and sets
+ *     the kernels' shared-memory limit, so make it before any stream capture;
+ *   - every call reuses the same array: calls that overlap on the GPU (other
+ *     streams, other host threads) race and must be serialised by the caller.
+ * No cudaMalloc, cudaFree or other allocating routine is called. */
+int mbg_sgemm_ex_noalloc(int mode, char trans_a, char trans_b, int64_t m, int64_t n, int64_t k,
+                         float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
+                         float beta, float* c, int64_t ldc);
 
 /* ---- runtime ------------------------------------------------------------ */
 /* Stream for subsequent calls from any thread (a cudaStream_t; NULL = legacy

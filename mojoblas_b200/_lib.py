@@ -17,6 +17,7 @@ MBG_ERR_UNSUPPORTED = -3
 MBG_ERR_NO_DEVICE = -4
 MBG_ERR_TIMEOUT = -5
 MBG_ERR_INVALID_MODE = -6
+MBG_ERR_SCRATCH_LIMIT = -7
 
 MODE_PLAIN = 0
 MODE_BF16X3 = 1
@@ -41,6 +42,7 @@ SIGNATURES = {
     "mbg_dtrsm": [_ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
     "mbg_strsm_ex": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],
     "mbg_dtrsm_ex": [_i, _i, _i, _ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
+    "mbg_sgemm_ex_noalloc": [_i, _ch, _ch, i64, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
     "mbg_set_stream": [_vp],
     "mbg_get_stream": [],
     "mbg_set_sync": [_i],

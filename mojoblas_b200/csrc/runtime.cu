@@ -252,6 +252,7 @@ const char* mbg_status_string(int s) {
         case MBG_ERR_NO_DEVICE: return "no usable CUDA device";
         case MBG_ERR_TIMEOUT: return "kernel wait limit expired";
         case MBG_ERR_INVALID_MODE: return "invalid precision mode or slice count";
+        case MBG_ERR_SCRATCH_LIMIT: return "problem exceeds the no-allocation scratch limit";
         default: return "unknown status";
     }
 }

@@ -758,3 +758,144 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
 }
 
 }  // namespace mbg
+
+// ---- split-precision sgemm without device allocation ---------------------------
+// Some callers cannot let a library allocate device memory: a host framework
+// that owns a fixed device-memory budget and forbids plugins from calling
+// cudaMalloc themselves, a latency-critical loop where cudaMalloc / cudaFree
+// may synchronise the whole device, or code running inside an allocator's
+// out-of-memory handling, where a further allocation would fail or recurse.
+// mbg_sgemm_ex_noalloc serves them: the bf16 split planes that
+// sgemm_split_tc takes from the workspace cache live instead in the fixed
+// array below, which the CUDA runtime creates when it loads this module on a
+// device and which stays resident there until the process exits.
+namespace mbg {
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(32) << 20;  // 32 MiB per device
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+__device__ int g_noalloc_err[4];  // bounded-wait error flag for this entry point
+
+struct NoallocDevice {
+    bool ready = false;
+    void* scratch = nullptr;  // device address of g_noalloc_scratch
+    int* err = nullptr;       // device address of g_noalloc_err
+};
+NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mu;
+
+// Once per device, with that device current: resolve the device addresses of
+// the static arrays (host code cannot use the array names as addresses) and
+// raise the kernels' shared-memory limit.
+int noalloc_setup(NoallocDevice** out) {
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return MBG_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoallocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* p = nullptr;
+        MBG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        void* e = nullptr;
+        MBG_CUDA(cudaGetSymbolAddress(&e, g_noalloc_err));
+        MBG_CUDA(cudaFuncSetAttribute(tc::tc_gemm_kernel<tc::CfgBF16x3>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, tc::CfgBF16x3::SMEM_BYTES));
+        MBG_CUDA(cudaFuncSetAttribute(tc::tc_gemm_kernel<tc::CfgBF16x6>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, tc::CfgBF16x6::SMEM_BYTES));
+        d.scratch = p;
+        d.err = static_cast<int*>(e);
+        d.ready = true;
+    }
+    *out = &d;
+    return MBG_OK;
+}
+
+template <int TERMS>
+void noalloc_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp,
+                   __nv_bfloat16* planes) {
+    dim3 g(unsigned(Kp / tc::PT_K), unsigned(Rp / tc::PT_R));
+    if (kmajor) tc::split_bf16_kernel<TERMS, true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
+    else tc::split_bf16_kernel<TERMS, false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
+}
+
+}  // namespace
+
+}  // namespace mbg
+
+extern "C" int mbg_sgemm_ex_noalloc(int mode, char ta, char tb, int64_t m, int64_t n, int64_t k,
+                                    float alpha, const float* a, int64_t lda, const float* b,
+                                    int64_t ldb, float beta, float* c, int64_t ldc) {
+    using namespace mbg;
+    using namespace mbg::tc;
+    if (mode != MBG_MODE_BF16X3 && mode != MBG_MODE_BF16X6) return MBG_ERR_INVALID_MODE;
+    // argument checks as mojoBLAS gemm numbers them (src/level3/gemm.mojo:179-213)
+    if (!is_n(ta) && !is_t(ta)) return 1;
+    if (!is_n(tb) && !is_t(tb)) return 2;
+    if (m < 0) return 3;
+    if (n < 0) return 4;
+    if (k < 0) return 5;
+    if (lda < imax(1, is_n(ta) ? m : k)) return 8;
+    if (ldb < imax(1, is_n(tb) ? k : n)) return 10;
+    if (ldc < imax(1, m)) return 13;
+    if (m == 0 || n == 0) return MBG_OK;
+    const int terms = mode == MBG_MODE_BF16X6 ? 3 : 2;
+    const i64 Mp = roundup(m, BM), Np = roundup(n, 256), Kp = roundup(imax(k, 1), 32);
+    const size_t need = size_t(terms) * size_t(Mp + Np) * size_t(Kp) * 2;
+    if (need > NOALLOC_SCRATCH_BYTES) {
+        set_error_msg("mbg_sgemm_ex_noalloc: needs " + std::to_string(need) + " bytes of scratch, limit " +
+                      std::to_string(NOALLOC_SCRATCH_BYTES) +
+                      " (terms * (roundup(m,128) + roundup(n,256)) * roundup(k,32) * 2)");
+        return MBG_ERR_SCRATCH_LIMIT;
+    }
+    const bool need_ab = !(alpha == 0.0f || k == 0);
+    if ((need_ab && (!is_device_pointer(a) || !is_device_pointer(b))) || !is_device_pointer(c)) {
+        set_error_msg("mbg_sgemm_ex_noalloc: operands must be device pointers (host data would need staging)");
+        return MBG_ERR_UNSUPPORTED;
+    }
+    NoallocDevice* d = nullptr;
+    MBG_TRY(noalloc_setup(&d));
+    if (!need_ab) {
+        MBG_TRY(scale_matrix<float>(m, n, beta, c, ldc));
+    } else {
+        // planes for op(A) then op(B)^T; the split kernels write every element,
+        // zero padding included, so nothing left by an earlier call is read
+        __nv_bfloat16* pa = static_cast<__nv_bfloat16*>(d->scratch);
+        __nv_bfloat16* pb = pa + size_t(terms) * Mp * Kp;
+        if (terms == 2) {
+            noalloc_split<2>(a, lda, is_t(ta), m, k, Mp, Kp, pa);
+            noalloc_split<2>(b, ldb, is_n(tb), n, k, Np, Kp, pb);
+        } else {
+            noalloc_split<3>(a, lda, is_t(ta), m, k, Mp, Kp, pa);
+            noalloc_split<3>(b, ldb, is_n(tb), n, k, Np, Kp, pb);
+        }
+        MBG_TRY(check_launch("split_bf16"));
+        CUtensorMap ma, mb;
+        MBG_TRY(make_map(&ma, pa, false, Kp, Mp, terms, 64, BM));
+        MBG_TRY(make_map(&mb, pb, false, Kp, Np, terms, 64, 256));
+        Params P{};
+        P.m = m; P.n = n; P.num_kb = int(Kp / 32);
+        P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, 256));
+        P.tri = 0; P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
+        P.err = d->err;
+        const unsigned tiles = unsigned(i64(P.tiles_m) * P.tiles_n);
+        if (terms == 2)
+            tc_gemm_kernel<CfgBF16x3><<<tiles, CfgBF16x3::THREADS, CfgBF16x3::SMEM_BYTES, stream()>>>(ma, mb, P);
+        else
+            tc_gemm_kernel<CfgBF16x6><<<tiles, CfgBF16x6::THREADS, CfgBF16x6::SMEM_BYTES, stream()>>>(ma, mb, P);
+        MBG_TRY(check_launch(terms == 2 ? "tc_gemm_bf16x3" : "tc_gemm_bf16x6"));
+    }
+    if (sync_mode()) {
+        MBG_CUDA(cudaStreamSynchronize(stream()));
+        int flag[4] = {0, 0, 0, 0};
+        MBG_CUDA(cudaMemcpyFromSymbol(flag, g_noalloc_err, sizeof(flag)));
+        if (flag[0]) {
+            const int zero[4] = {0, 0, 0, 0};
+            MBG_CUDA(cudaMemcpyToSymbol(g_noalloc_err, zero, sizeof(zero)));
+            set_error_msg("mbg_sgemm_ex_noalloc: a kernel's bounded wait expired; results are invalid");
+            return MBG_ERR_TIMEOUT;
+        }
+    }
+    return MBG_OK;
+}

@@ -1,0 +1,83 @@
+"""mbg_sgemm_ex_noalloc: the split-precision sgemm for callers that cannot let a
+library allocate device memory (a host framework that owns a fixed device-memory
+budget, a latency-critical loop where cudaMalloc / cudaFree may synchronise the
+device, or code inside an allocator's out-of-memory handling).
+
+Its result must match the allocating entry point mbg_sgemm_ex with the same
+mode on the same device inputs, within the float32 tolerance the other GPU
+tests use, on two calls in a row (the second reuses the fixed scratch array
+the first one filled).  This file is collected last on purpose, and passes
+both alone in a fresh process and after the rest of the suite.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mojoblas_b200 import _lib as L
+from tests.gpu_util import need_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def tol32(k):
+    return 1e-6 * np.sqrt(max(k, 16))  # the float32 tolerance of the GPU parity tests
+
+
+def _col_major(torch, rows, cols, seed):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    return torch.rand((cols, rows), generator=g, device="cuda", dtype=torch.float32) * 2 - 1
+
+
+def _call(fn, mode, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    return fn(mode, ta.encode(), tb.encode(), m, n, k, alpha, a.data_ptr(), lda, b.data_ptr(), ldb, beta,
+              c.data_ptr(), ldc)
+
+
+def test_noalloc_matches_allocating_entry_point_twice():
+    torch = need_gpu()
+    lib = L.load()
+    lib.mbg_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    cases = [  # two calls in a row, different shapes, modes and transposes
+        (L.MODE_BF16X3, "N", "T", 1000, 700, 900, 1.5, 0.5),
+        (L.MODE_BF16X6, "T", "N", 513, 1024, 2048, -1.0, 0.0),
+    ]
+    for i, (mode, ta, tb, m, n, k, alpha, beta) in enumerate(cases):
+        lda = m if ta == "N" else k
+        ldb = k if tb == "N" else n
+        a = _col_major(torch, lda, k if ta == "N" else m, 10 + i)
+        b = _col_major(torch, ldb, n if tb == "N" else k, 20 + i)
+        c0 = _col_major(torch, m, n, 30 + i)
+        c_ref, c_new = c0.clone(), c0.clone()
+        st = _call(lib.mbg_sgemm_ex, mode, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c_ref, m)
+        assert st == 0, L.last_error()
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        st = _call(lib.mbg_sgemm_ex_noalloc, mode, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c_new, m)
+        assert st == 0, L.last_error()
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
+        assert free_before - free_after < (2 << 20), "the no-allocation entry point allocated device memory"
+        ref = c_ref.double()
+        diff = float((c_new.double() - ref).abs().max() / ref.abs().max())
+        assert diff <= tol32(k), (i, diff)
+
+
+def test_noalloc_rejects_oversized_and_host_operands():
+    torch = need_gpu()
+    lib = L.load()
+    n = 4096  # BF16x3 needs 2 * (4096 + 4096) * 4096 * 2 bytes = 128 MiB > 32 MiB
+    a = torch.zeros((n, n), device="cuda", dtype=torch.float32)
+    st = _call(lib.mbg_sgemm_ex_noalloc, L.MODE_BF16X3, "N", "N", n, n, n, 1.0, a, n, a, n, 0.0, a, n)
+    assert st == L.MBG_ERR_SCRATCH_LIMIT
+    assert "limit" in L.last_error()
+    h = np.zeros((64, 64), np.float32, order="F")
+    st = lib.mbg_sgemm_ex_noalloc(L.MODE_BF16X3, b"N", b"N", 64, 64, 64, 1.0, h.ctypes.data, 64,
+                                  h.ctypes.data, 64, 0.0, h.ctypes.data, 64)
+    assert st == L.MBG_ERR_UNSUPPORTED
+    st = lib.mbg_sgemm_ex_noalloc(L.MODE_PLAIN, b"N", b"N", 64, 64, 64, 1.0, h.ctypes.data, 64,
+                                  h.ctypes.data, 64, 0.0, h.ctypes.data, 64)
+    assert st == L.MBG_ERR_INVALID_MODE
+    assert lib.mbg_sgemm_ex_noalloc(L.MODE_BF16X3, b"N", b"N", 64, 64, 64, 1.0, h.ctypes.data, 63,
+                                    h.ctypes.data, 64, 0.0, h.ctypes.data, 64) == 8
