@@ -1,0 +1,94 @@
+"""Run one library routine on cuda:0 a few times — the command profilers wrap.
+
+    python mojoblas_b200/profile_case.py --op sgemm --mode bf16x6 --m 4096 --n 4096 --k 8192
+    python mojoblas_b200/profile_case.py --op dgemm --mode ozaki --slices 8 --m 2048 --n 2048 --k 4096
+    python mojoblas_b200/profile_case.py --op dtrsm --mode ozaki --m 4096 --n 4096
+
+Inputs are uniform[-1, 1) (trsm: diagonally dominant lower triangle), device
+resident; each rep is one call through the C ABI.  Prints the mean CUDA-event
+time per call.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import sys
+from pathlib import Path
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--op", choices=["sgemm", "dgemm", "ssyrk", "dtrsm", "strsm"], default="sgemm")
+    ap.add_argument("--mode", choices=["plain", "bf16x3", "bf16x6", "ozaki"], default="bf16x6")
+    ap.add_argument("--slices", type=int, default=8)
+    ap.add_argument("--refine", type=int, default=0)
+    ap.add_argument("--ta", default="N")
+    ap.add_argument("--tb", default="T")
+    ap.add_argument("--m", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--k", type=int, default=8192)
+    ap.add_argument("--reps", type=int, default=2)
+    a = ap.parse_args()
+
+    import torch
+    from mojoblas_b200 import _lib as L
+    lib = L.load()
+    torch.cuda.set_device(0)
+    lib.mbg_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    lib.mbg_set_sync(0)
+    mode = {"plain": L.MODE_PLAIN, "bf16x3": L.MODE_BF16X3, "bf16x6": L.MODE_BF16X6, "ozaki": L.MODE_OZAKI}[a.mode]
+    dt = torch.float64 if a.op[0] == "d" else torch.float32
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+
+    def cm(rows, cols):  # column-major rows x cols
+        return torch.rand((cols, rows), generator=g, device="cuda", dtype=dt) * 2 - 1
+
+    if a.op in ("sgemm", "dgemm"):
+        lda = a.m if a.ta == "N" else a.k
+        ldb = a.k if a.tb == "N" else a.n
+        A, B, Cm = cm(lda, a.k if a.ta == "N" else a.m), cm(ldb, a.n if a.tb == "N" else a.k), cm(a.m, a.n)
+
+        def call():
+            if a.op == "sgemm":
+                return lib.mbg_sgemm_ex(mode, a.ta.encode(), a.tb.encode(), a.m, a.n, a.k, 1.0, A.data_ptr(), lda,
+                                        B.data_ptr(), ldb, 0.0, Cm.data_ptr(), a.m)
+            return lib.mbg_dgemm_ex(mode, a.slices, a.ta.encode(), a.tb.encode(), a.m, a.n, a.k, 1.0, A.data_ptr(),
+                                    lda, B.data_ptr(), ldb, 0.0, Cm.data_ptr(), a.m)
+    elif a.op == "ssyrk":
+        A, Cm = cm(a.n, a.k), cm(a.n, a.n)
+
+        def call():
+            return lib.mbg_ssyrk_ex(mode, b"L", b"N", a.n, a.k, 1.0, A.data_ptr(), a.n, 0.0, Cm.data_ptr(), a.n)
+    else:
+        m = a.m
+        A = torch.randn((m, m), generator=g, device="cuda", dtype=dt) / m ** 0.5
+        A.diagonal().copy_(m + torch.rand(m, generator=g, device="cuda", dtype=dt))
+        B0 = torch.randn((a.n, m), generator=g, device="cuda", dtype=dt)
+        X = B0.clone()
+
+        def call():
+            X.copy_(B0)
+            if a.op == "dtrsm":
+                return lib.mbg_dtrsm_ex(mode, a.slices, a.refine, b"L", b"L", b"N", b"N", m, a.n, 1.0, A.data_ptr(),
+                                        m, X.data_ptr(), m)
+            return lib.mbg_strsm_ex(mode, a.refine, b"L", b"L", b"N", b"N", m, a.n, 1.0, A.data_ptr(), m,
+                                    X.data_ptr(), m)
+
+    st = call()
+    assert st == 0, L.last_error()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        st = call()
+        assert st == 0, L.last_error()
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"{a.op} {a.mode} m={a.m} n={a.n} k={a.k}: {e0.elapsed_time(e1) / a.reps:.3f} ms per call")
+
+
+if __name__ == "__main__":
+    main()
