@@ -1,6 +1,7 @@
 // Tensor-core GEMMs on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// Two precision forms share one warp-specialised kernel:
+// Two precision forms, each a warp-specialised kernel sharing the PTX helpers
+// and the pre-pass design:
 //
 //  * Split-precision sgemm (BF16x3 / BF16x6).  A pre-pass splits each fp32
 //    operand element x into bf16 terms x = x1 + x2 (+ x3) + residual, with
@@ -14,7 +15,8 @@
 //    s slices of 7 bits, x' = sum_p d_p 2^(-7(p+1)), d_p in [-127, 127] (exact in
 //    fp64: multiply by 128, truncate, subtract).  The kernel forms, for each
 //    diagonal t = p+q < s, D_t = sum_{p+q=t} A_p B_q exactly with
-//    tcgen05.mma.kind::i8 (int32 accumulation, one TMEM accumulator per t), and
+//    tcgen05.mma.kind::i8 (int32 accumulation, one TMEM accumulator per t, at
+//    most four at a time: more than four slices run two passes over k), and
 //    the epilogue sums 2^(-7(t+2)) D_t from the smallest term up in fp64 and
 //    applies the row and column scales (Ootomo, Ozaki, Yokota, "DGEMM on integer
 //    matrix multiplication unit", IJHPCA 2024; Ozaki, Ogita, Oishi, Rump, 2012).
@@ -23,12 +25,12 @@
 // K-contiguous ("K-major") operands: planes[term][row][k], rows padded to the
 // tile, k padded to the k-slab, zero-filled.
 //
-// Kernel roles (one CTA per 128 x BN output tile):
+// Kernel roles (one CTA per 128 x BN output tile; BN = 256 split, 128 Ozaki):
 //   warp 0      allocates TMEM; lane 0 issues TMA loads (cp.async.bulk.tensor,
 //               one 3-D box per operand per stage covering every term plane)
 //   warp 1      lane 0 issues the tcgen05.mma instructions and commits each
 //               stage back to the producer, then the accumulators to the epilogue
-//   warps 2..   epilogue (8 warps split, 4 Ozaki): tcgen05.ld from TMEM (warp w
+//   warps 2..9  epilogue, two warps per TMEM lane quarter: tcgen05.ld (warp w
 //               reads lanes 32*(w%4)..), accumulate / scale, add beta*C, store
 //               column-major C with coalesced warps
 // Every mbarrier wait is bounded (about 2 s of globaltimer); on expiry the
@@ -125,22 +127,27 @@ __device__ __forceinline__ void tc_fence_before() {
 __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
+// COLLECTOR: 0 = read A from shared memory only, 1 = fill the tensor core's A
+// collector buffer, 2 = reuse it, 3 = reuse it for the last time.  Consecutive
+// MMAs with the same A tile (Ozaki products A_p B_q for one p) read A once.
+#define MBG_UMMA(KIND, COL)                                                        \
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"                \
+                 "tcgen05.mma.cta_group::1.kind::" KIND COL " [%0], %1, %2, %3, p;\n\t}" \
+                 ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)  \
+                 : "memory")
 template <bool INT8>
 __device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                     uint32_t accumulate) {
-    if (INT8)
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-            : "memory");
-    else
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-            : "memory");
+                                     uint32_t accumulate, int collector = 0) {
+    if (INT8) {
+        if (collector == 1) MBG_UMMA("i8", ".collector::a::fill");
+        else if (collector == 2) MBG_UMMA("i8", ".collector::a::use");
+        else if (collector == 3) MBG_UMMA("i8", ".collector::a::lastuse");
+        else MBG_UMMA("i8", "");
+    } else {
+        MBG_UMMA("f16", "");
+    }
 }
+#undef MBG_UMMA
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                      smem_u32(bar))
@@ -180,6 +187,13 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t sbo_bytes
 __host__ __device__ constexpr uint32_t instr_desc(bool int8, int M, int N) {
     return (uint32_t(int8 ? 2 : 1) << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) |
            (uint32_t(M >> 4) << 24);
+}
+
+// 2^e as a double: built from the exponent bits in the normal range (exact, no
+// libm call), ldexp outside it.
+__device__ __forceinline__ double pow2_exact(int e) {
+    if (e >= -1022 && e <= 1023) return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+    return ldexp(1.0, e);
 }
 
 // ---------------------------------------------------------------------------
@@ -228,7 +242,6 @@ struct Cfg {
 
 using CfgBF16x3 = Cfg<false, 2, 256, 64, 4, 8, 4>;
 using CfgBF16x6 = Cfg<false, 3, 256, 64, 3, 8, 4>;
-template <int S> using CfgOzaki = Cfg<true, S, 64, 32, 4, 4, 0>;
 
 struct Params {
     i64 m, n;
@@ -243,10 +256,30 @@ struct Params {
     int* err;
 };
 
-// product table: index -> (p, q); ordered by descending p+q so that small
-// contributions enter each fp32 accumulator first
-template <int TERMS>
-__device__ __forceinline__ void product(int idx, int& p, int& q) {
+// Product table, index -> (p, q) and collector use.
+//   split: ordered by descending p+q so small contributions enter the fp32
+//          accumulator first;
+//   ozaki: ordered by p (A slice), q ascending, so the products that share A_p
+//          run back to back and reuse it from the collector buffer; the first
+//          product into diagonal d is then (0, d).
+template <int TERMS, bool OZAKI>
+__device__ __forceinline__ void product(int idx, int& p, int& q, int& collector) {
+    collector = 0;
+    if (OZAKI) {
+        int t = 0;
+        for (int pp = 0; pp < TERMS; ++pp) {
+            const int cnt = TERMS - pp;  // q = 0 .. TERMS-1-pp
+            if (idx < t + cnt) {
+                p = pp;
+                q = idx - t;
+                if (cnt > 1) collector = (q == 0) ? 1 : (q == cnt - 1 ? 3 : 2);
+                return;
+            }
+            t += cnt;
+        }
+        p = q = 0;
+        return;
+    }
     int t = 0;
     for (int d = TERMS - 1; d >= 0; --d) {
         for (int pp = 0; pp <= d; ++pp) {
@@ -352,15 +385,15 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 for (int ks = 0; ks < C::KSTEPS; ++ks) {
 #pragma unroll
                     for (int pi = 0; pi < C::NPROD; ++pi) {
-                        int p, q;
-                        product<C::TERMS>(pi, p, q);
+                        int p, q, collector;
+                        product<C::TERMS, C::OZAKI>(pi, p, q, collector);
                         // the first product into an accumulator in a chunk overwrites it
                         const bool first = C::OZAKI ? (p == 0) : (pi == 0);
                         const uint32_t accumulate = (kin > 0 || ks > 0 || !first) ? 1u : 0u;
                         const uint32_t col = C::OZAKI ? uint32_t((p + q) * C::BN) : uint32_t(buf * C::BN);
                         const uint64_t ad = smem_desc(sa + p * C::A_PLANE + ks * 32, C::SBO, C::LAYOUT);
                         const uint64_t bd = smem_desc(sb + q * C::B_PLANE + ks * 32, C::SBO, C::LAYOUT);
-                        umma<C::OZAKI>(tmem + col, ad, bd, C::IDESC, accumulate);
+                        umma<C::OZAKI>(tmem + col, ad, bd, C::IDESC, accumulate, collector);
                     }
                 }
                 umma_commit(&empty[s]);  // slot s is free once these MMAs have read it
@@ -413,38 +446,6 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                     *cp = (beta == 0.0f) ? v : fmaf(beta, *cp, v);
                 }
             }
-        } else {
-            if (mbar_wait(&tfull[0], 0, P.err, 4)) {
-                tc_fence_after();
-                double acc[C::BN];
-#pragma unroll
-                for (int j = 0; j < C::BN; ++j) acc[j] = 0.0;
-                // smallest diagonal weight first: t = TERMS-1 .. 0, weight 2^(-7(t+2))
-#pragma unroll 1
-                for (int t = C::NACC - 1; t >= 0; --t) {
-                    const double w = ldexp(1.0, -7 * (t + 2));
-#pragma unroll
-                    for (int c0 = 0; c0 < C::BN; c0 += 16) {
-                        uint32_t r[16];
-                        tmem_ld16(lane_base + uint32_t(t * C::BN + c0), r);
-                        tmem_ld_wait();
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
-                    }
-                }
-                if (row < P.m) {
-                    double* Cm = static_cast<double*>(P.c);
-                    const int er = P.ea[row];
-#pragma unroll
-                    for (int j = 0; j < C::BN; ++j) {
-                        const i64 col = n0 + j;
-                        if (col >= P.n) break;
-                        double* cp = Cm + row + col * P.ldc;
-                        const double v = P.alpha * ldexp(acc[j], er + P.eb[col]);
-                        *cp = (P.beta == 0.0) ? v : fma(P.beta, *cp, v);
-                    }
-                }
-            }
         }
     }
     tc_fence_before();
@@ -453,6 +454,236 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         __syncwarp();
         tc_fence_after();
         tmem_dealloc(tmem, C::TMEM_COLS);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ozaki kernel: 128 x 128 tiles, diagonals in up to two passes over k
+// ---------------------------------------------------------------------------
+// An MMA of N = 128 columns reads its A tile once per 128 outputs; N = 64 left
+// the int8 pipe half idle.  Four int32 accumulators of 128 columns fill TMEM, so
+// with more than four slices the diagonals are split: pass 0 accumulates the
+// high diagonals 4 .. S-1 (the smallest weights, needing every slice), pass 1
+// the low diagonals 0 .. 3 (needing slices 0 .. 3 only).  After each pass the
+// epilogue warps add w_d * D_d into fp64 registers, smallest weights first, and
+// release TMEM for the next pass.
+template <int S_>
+struct OzCfg {
+    static constexpr int S = S_;
+    static constexpr int BN = 128;
+    static constexpr int BKB = 32;                    // k slab: 32 int8 per row (32-byte swizzle)
+    static constexpr int EPI_WARPS = 8;
+    static constexpr int THREADS = 64 + 32 * EPI_WARPS;
+    static constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // 64
+    static constexpr int NPASS = S <= 4 ? 1 : 2;
+    static constexpr int SPLIT = S <= 4 ? 0 : 4;      // pass 0: [SPLIT, S), pass 1: [0, SPLIT)
+    static constexpr int PLANE = BM * BKB;            // A and B tiles are both 128 x 32 bytes
+    static constexpr int STAGE_BYTES = 2 * S * PLANE;
+    static constexpr int STAGES = (196608 / STAGE_BYTES) > 6 ? 6 : (196608 / STAGE_BYTES);
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr uint32_t IDESC = instr_desc(true, BM, BN);
+    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 6;
+    static_assert(STAGES >= 2, "pipeline depth");
+};
+
+// pass -> diagonal range [lo, hi) and the slices whose tiles it loads
+template <class C>
+__device__ __forceinline__ void pass_range(int pass, int& lo, int& hi, int& planes) {
+    if (C::NPASS == 1) { lo = 0; hi = C::S; planes = C::S; return; }
+    if (pass == 0) { lo = C::SPLIT; hi = C::S; planes = C::S; }
+    else { lo = 0; hi = C::SPLIT; planes = C::SPLIT; }
+}
+
+// product index within a pass -> (p, q, collector use); ordered by p so that
+// consecutive products share A_p (collector buffer), q ascending
+template <int S>
+__device__ __forceinline__ bool oz_product(int lo, int hi, int idx, int& p, int& q, int& collector) {
+    int t = 0;
+    for (int pp = 0; pp < S; ++pp) {
+        const int q0 = lo - pp > 0 ? lo - pp : 0;
+        const int q1 = (hi - 1 - pp) < (S - 1) ? (hi - 1 - pp) : (S - 1);
+        const int cnt = q1 >= q0 ? q1 - q0 + 1 : 0;
+        if (idx < t + cnt) {
+            p = pp;
+            q = q0 + (idx - t);
+            collector = cnt > 1 ? (q == q0 ? 1 : (q == q1 ? 3 : 2)) : 0;
+            return true;
+        }
+        t += cnt;
+    }
+    return false;
+}
+
+struct OzParams {
+    i64 m, n;
+    int num_kb, tiles_m, tiles_n;
+    double* c;
+    i64 ldc;
+    double alpha, beta;
+    const int* ea;
+    const int* eb;
+    int* err;
+};
+
+template <int S, int PASS> struct OzPass {
+    static constexpr int NP = S <= 4 ? 1 : 2;
+    static constexpr int LO = (NP == 1) ? 0 : (PASS == 0 ? 4 : 0);
+    static constexpr int HI = (NP == 1) ? S : (PASS == 0 ? S : 4);
+};
+
+// Issues one pass: every k slab, the products of diagonals [LO, HI), then
+// commits the accumulators to the epilogue.  Returns false if a wait expired.
+template <class C, int PASS>
+__device__ __forceinline__ bool oz_mma_pass(const OzParams& P, uint8_t* smem, uint64_t* full, uint64_t* empty,
+                                            uint64_t* tfull, uint64_t* tempty, uint32_t tmem) {
+    constexpr int LO = OzPass<C::S, PASS>::LO, HI = OzPass<C::S, PASS>::HI;
+    if (PASS > 0) {  // the epilogue must have read the previous pass's accumulators
+        if (!mbar_wait(tempty, (PASS - 1) & 1, P.err, 13)) return false;
+        tc_fence_after();
+    }
+    for (int kb = 0; kb < P.num_kb; ++kb) {
+        const int it = PASS * P.num_kb + kb;
+        const int s = it % C::STAGES;
+        if (!mbar_wait(&full[s], (it / C::STAGES) & 1, P.err, 14)) return false;
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * C::STAGE_BYTES);
+        const uint32_t sb = sa + C::S * C::PLANE;
+#pragma unroll
+        for (int pi = 0; pi < C::S * C::S; ++pi) {
+            int p = 0, q = 0, collector = 0;
+            if (!oz_product<C::S>(LO, HI, pi, p, q, collector)) break;
+            // (0, d) is the first product of diagonal d in p-major order
+            const uint32_t accumulate = (kb > 0 || p > 0) ? 1u : 0u;
+            const uint64_t ad = smem_desc(sa + p * C::PLANE, C::SBO, C::LAYOUT);
+            const uint64_t bd = smem_desc(sb + q * C::PLANE, C::SBO, C::LAYOUT);
+            umma<true>(tmem + uint32_t((p + q - LO) * C::BN), ad, bd, C::IDESC, accumulate, collector);
+        }
+        umma_commit(&empty[s]);
+    }
+    umma_commit(tfull);  // this pass's accumulators are complete
+    return true;
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, 1)
+ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+             const __grid_constant__ CUtensorMap tmAlo, const __grid_constant__ CUtensorMap tmBlo, OzParams P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+    uint64_t* empty = full + C::STAGES;
+    uint64_t* tfull = empty + C::STAGES;
+    uint64_t* tempty = tfull + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
+
+    const int tile = blockIdx.x;
+    const int group = 16;
+    const int per_group = group * P.tiles_n;
+    const int g = tile / per_group;
+    const int first_m = g * group;
+    const int gsize = min(group, P.tiles_m - first_m);
+    const int in_g = tile - g * per_group;
+    const i64 m0 = i64(first_m + in_g % gsize) * BM, n0 = i64(in_g / gsize) * C::BN;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(tfull, 1);
+        mbar_init(tempty, C::EPI_WARPS);
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, 512);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int total = C::NPASS * P.num_kb;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            prefetch_tmap(&tmA);
+            prefetch_tmap(&tmB);
+            for (int it = 0; it < total; ++it) {
+                const int pass = it / P.num_kb, kb = it - pass * P.num_kb;
+                int lo, hi, planes;
+                pass_range<C>(pass, lo, hi, planes);
+                const int s = it % C::STAGES;
+                const uint32_t ph = (it / C::STAGES) & 1;
+                if (!mbar_wait(&empty[s], ph ^ 1, P.err, 11)) break;
+                uint8_t* sa = smem + s * C::STAGE_BYTES;
+                uint8_t* sb = sa + C::S * C::PLANE;
+                mbar_expect_tx(&full[s], uint32_t(2 * planes * C::PLANE));
+                const bool all = planes == C::S;
+                tma_load_3d(sa, all ? &tmA : &tmAlo, &full[s], kb * C::BKB, int(m0), 0);
+                tma_load_3d(sb, all ? &tmB : &tmBlo, &full[s], kb * C::BKB, int(n0), 0);
+            }
+            for (int it = max(0, total - C::STAGES); it < total; ++it)
+                mbar_wait(&full[it % C::STAGES], (it / C::STAGES) & 1, P.err, 12);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            if (oz_mma_pass<C, 0>(P, smem, full, empty, tfull, tempty, tmem) && C::NPASS > 1)
+                oz_mma_pass<C, 1>(P, smem, full, empty, tfull, tempty, tmem);
+        }
+    } else {
+        // ---------------- epilogue warps ----------------
+        const int e = warp - 2;
+        const int quarter = warp & 3;
+        const int part = e >> 2;
+        const i64 row = m0 + quarter * 32 + lane;
+        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(part * C::EPI_COLS);
+        double acc[C::EPI_COLS];
+#pragma unroll
+        for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0;
+        bool ok = true;
+        for (int pass = 0; pass < C::NPASS; ++pass) {
+            int lo, hi, planes;
+            pass_range<C>(pass, lo, hi, planes);
+            if (!mbar_wait(tfull, pass & 1, P.err, 15)) { ok = false; break; }
+            tc_fence_after();
+#pragma unroll 1
+            for (int d = hi - 1; d >= lo; --d) {  // smallest weight first
+                const double w = pow2_exact(-7 * (d + 2));
+#pragma unroll
+                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(lane_base + uint32_t((d - lo) * C::BN + c0), r);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty);
+        }
+        if (ok && row < P.m) {
+            const int er = P.ea[row];
+            const i64 cbase = n0 + part * C::EPI_COLS;
+#pragma unroll
+            for (int j = 0; j < C::EPI_COLS; ++j) {
+                const i64 col = cbase + j;
+                if (col >= P.n) break;
+                double* cp = P.c + row + col * P.ldc;
+                const double v = P.alpha * (acc[j] * pow2_exact(er + P.eb[col]));
+                *cp = (P.beta == 0.0) ? v : fma(P.beta, *cp, v);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, 512);
     }
 }
 
@@ -707,12 +938,30 @@ int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha
 }
 
 // ---- Ozaki dgemm ----------------------------------------------------------------
+namespace tc {
+template <class C>
+int launch_ozaki(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mal, const CUtensorMap& mbl,
+                 OzParams& P) {
+    static bool configured = false;  // per instantiation
+    if (!configured) {
+        MBG_CUDA(cudaFuncSetAttribute(ozaki_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
+        configured = true;
+    }
+    P.err = device_error_flag();
+    const i64 tiles = i64(P.tiles_m) * P.tiles_n;
+    if (tiles > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    ProfScope prof("tc_gemm_ozaki");
+    ozaki_kernel<C><<<unsigned(tiles), C::THREADS, C::SMEM_BYTES, stream()>>>(ma, mb, mal, mbl, P);
+    return check_launch("tc_gemm_ozaki");
+}
+}  // namespace tc
+
 int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a,
                    i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc) {
     using namespace tc;
     if (m == 0 || n == 0) return MBG_OK;
     if (slices < 2 || slices > 8) return MBG_ERR_INVALID_MODE;
-    const int BN = 64;
+    const int BN = 128;
     // int32 accumulators hold at most `slices` products of K terms of 127^2 each
     const i64 kchunk_max = (i64(0x7fffffff) / (i64(slices) * 127 * 127)) / 32 * 32;
     const i64 Mp = roundup(m, BM), Np = roundup(n, BN);
@@ -725,6 +974,7 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
     int8_t* pb = pa + a_bytes;
     int* ea = reinterpret_cast<int*>(pb + b_bytes + (1024 - ((a_bytes + b_bytes) & 1023)) % 1024);
     int* eb = ea + Mp;
+    const int lo_planes = slices <= 4 ? slices : 4;
     for (i64 k0 = 0; k0 < k; k0 += kc) {
         const i64 klen = imin(kc, k - k0);
         const i64 Kpc = roundup(klen, 32);
@@ -733,24 +983,26 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
         const double* bk = is_n(tb) ? b + k0 : b + k0 * ldb;
         MBG_TRY(launch_slices(ak, lda, is_t(ta), m, klen, Mp, Kpc, slices, ea, pa));
         MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb));
-        CUtensorMap ma, mb;
+        CUtensorMap ma, mb, mal, mbl;
         MBG_TRY(make_map(&ma, pa, true, Kpc, Mp, slices, 32, BM));
         MBG_TRY(make_map(&mb, pb, true, Kpc, Np, slices, 32, BN));
-        Params P{};
+        MBG_TRY(make_map(&mal, pa, true, Kpc, Mp, lo_planes, 32, BM));
+        MBG_TRY(make_map(&mbl, pb, true, Kpc, Np, lo_planes, 32, BN));
+        OzParams P{};
         P.m = m; P.n = n; P.num_kb = int(Kpc / 32);
         P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
-        P.tri = 0; P.c = c; P.ldc = ldc; P.alpha = alpha;
+        P.c = c; P.ldc = ldc; P.alpha = alpha;
         P.beta = (k0 == 0) ? beta : 1.0;
         P.ea = ea; P.eb = eb;
         int st;
         switch (slices) {
-            case 2: st = launch_tc<CfgOzaki<2>>(ma, mb, P, "tc_gemm_ozaki"); break;
-            case 3: st = launch_tc<CfgOzaki<3>>(ma, mb, P, "tc_gemm_ozaki"); break;
-            case 4: st = launch_tc<CfgOzaki<4>>(ma, mb, P, "tc_gemm_ozaki"); break;
-            case 5: st = launch_tc<CfgOzaki<5>>(ma, mb, P, "tc_gemm_ozaki"); break;
-            case 6: st = launch_tc<CfgOzaki<6>>(ma, mb, P, "tc_gemm_ozaki"); break;
-            case 7: st = launch_tc<CfgOzaki<7>>(ma, mb, P, "tc_gemm_ozaki"); break;
-            default: st = launch_tc<CfgOzaki<8>>(ma, mb, P, "tc_gemm_ozaki"); break;
+            case 2: st = launch_ozaki<OzCfg<2>>(ma, mb, mal, mbl, P); break;
+            case 3: st = launch_ozaki<OzCfg<3>>(ma, mb, mal, mbl, P); break;
+            case 4: st = launch_ozaki<OzCfg<4>>(ma, mb, mal, mbl, P); break;
+            case 5: st = launch_ozaki<OzCfg<5>>(ma, mb, mal, mbl, P); break;
+            case 6: st = launch_ozaki<OzCfg<6>>(ma, mb, mal, mbl, P); break;
+            case 7: st = launch_ozaki<OzCfg<7>>(ma, mb, mal, mbl, P); break;
+            default: st = launch_ozaki<OzCfg<8>>(ma, mb, mal, mbl, P); break;
         }
         if (st) return st;
     }
