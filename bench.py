@@ -55,18 +55,19 @@ def peaks():
 
 class Clocks:
     """nvidia-smi sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.dev = device
         self.proc = None
+        self.window = None  # (t0, t1) host wall-clock of the timed region
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -84,23 +85,25 @@ class Clocks:
             self.lines = [ln for ln in out.splitlines() if ln.strip()]
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        import datetime
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for ln in getattr(self, "lines", []):
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(f[1]), float(f[2]), f[5:9]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+        inside = [r for r in rows if self.window and self.window[0] <= r[0] <= self.window[1]]
+        use = inside or rows
+        if not use:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        reasons = sorted({nm for r in use for nm, v in zip(names, r[3]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[1] for r in use])), "sm_max_mhz": use[-1][2], "reasons": reasons,
+                "samples": len(use), "samples_in_timed_region": len(inside)}
 
 
 def col_major(torch, rows, cols, gen, dtype, device):
@@ -123,6 +126,83 @@ def rows_error(c, ref, rows):
     """max|C - C64| / max|C64| on the sampled rows."""
     got = c.double().cpu().numpy().T[rows, :]
     return float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+
+
+def run_cfg3(torch, lib, L, stream):
+    """Blocked trsm (Left/Lower/NoTrans/NonUnit, 4096^2 float64, A off-diagonal
+    N(0,1)/sqrt(4096), diagonal 4096 + |N(0,1)|, B N(0,1)) and syrk (Lower/NoTrans,
+    N = 8192, K = 2048, float32, A uniform[-1,1)), plain vs split / Ozaki, with the
+    float64-oracle error on sampled columns (trsm) / rows (syrk)."""
+    import scipy.linalg as sl
+    out = {}
+    g = torch.Generator(device="cuda")
+    g.manual_seed(99)
+    n = 4096
+    A = torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64) / np.sqrt(n)
+    A.diagonal().copy_(n + torch.randn(n, generator=g, device="cuda", dtype=torch.float64).abs())
+    B0 = torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64)
+    X = torch.empty_like(B0)
+    cols = np.random.default_rng(5).choice(n, 128, replace=False)
+    An = A.cpu().numpy().T  # column-major view: An[i, l]
+    L_ = np.tril(An)
+    Bn = B0.cpu().numpy().T
+    Xref = sl.solve_triangular(L_, Bn[:, cols], lower=True)
+
+    def tcall(md, s_, r_):
+        X.copy_(B0)
+        st = lib.mbg_dtrsm_ex(md, s_, r_, b"L", b"L", b"N", b"N", n, n, 1.0, A.data_ptr(), n, X.data_ptr(), n)
+        if st:
+            raise RuntimeError(f"dtrsm failed {st}: {L.last_error()}")
+
+    tr = {}
+    for label, md, s_, r_ in (("plain_fp64", L.MODE_PLAIN, 0, 0), ("ozaki_s8", L.MODE_OZAKI, 8, 0),
+                              ("ozaki_s6_ir1", L.MODE_OZAKI, 6, 1)):
+        tcall(md, s_, r_)
+        torch.cuda.synchronize()
+        got = X.cpu().numpy().T[:, cols]
+        err = float(np.max(np.abs(got - Xref)) / np.max(np.abs(Xref)))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        e0.record(stream)
+        for _ in range(reps):
+            tcall(md, s_, r_)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tr[label] = {"tflops": round(n ** 3 / (ms * 1e-3) / 1e12, 2), "ms": round(ms, 3), "fp64_err": err}
+    out["dtrsm_LLNN_4096"] = tr
+    out["dtrsm_note"] = "flops m^2 n; each timed call includes a 128 MiB device copy restoring B"
+    del A, B0, X
+
+    nn, kk = 8192, 2048
+    As = torch.rand((kk, nn), generator=g, device="cuda", dtype=torch.float32) * 2 - 1  # column-major n x k
+    Cs = torch.zeros((nn, nn), device="cuda", dtype=torch.float32)
+    rows = np.sort(np.random.default_rng(6).choice(nn, 128, replace=False))
+    Ah = As.double().cpu().numpy().T  # n x k
+    ref = Ah[rows, :] @ Ah.T  # rows of A A^T
+    mask = np.arange(nn)[None, :] <= rows[:, None]  # lower triangle of those rows
+    sy = {}
+    for label, md in (("plain_fp32", L.MODE_PLAIN), ("bf16x3", L.MODE_BF16X3), ("bf16x6", L.MODE_BF16X6)):
+        def scall():
+            st = lib.mbg_ssyrk_ex(md, b"L", b"N", nn, kk, 1.0, As.data_ptr(), nn, 0.0, Cs.data_ptr(), nn)
+            if st:
+                raise RuntimeError(f"ssyrk failed {st}: {L.last_error()}")
+        scall()
+        torch.cuda.synchronize()
+        got = Cs.double().cpu().numpy().T[rows, :]
+        err = float(np.max(np.abs((got - ref)[mask])) / np.max(np.abs(ref[mask])))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            scall()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        sy[label] = {"tflops": round(nn * (nn + 1) * kk / (ms * 1e-3) / 1e12, 2), "ms": round(ms, 3),
+                     "fp64_err": err}
+    out["ssyrk_LN_8192x2048"] = sy
+    out["ssyrk_note"] = "flops n(n+1)k (the reference plot uses n^3 at n = k)"
+    return out
 
 
 def run_ours(args, rank, world, dist):
@@ -156,6 +236,8 @@ def run_ours(args, rank, world, dist):
         call(md, "N", "T")
         call(md, "T", "N")
 
+    window = [None, None]
+
     def timed(md, steps, warmup):
         for _ in range(warmup):
             step(md)
@@ -165,11 +247,13 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize()
         lib.mbg_prof_reset()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        window[0] = time.time()
         e0.record(stream)
         for _ in range(steps):
             step(md)
         e1.record(stream)
         torch.cuda.synchronize()
+        window[1] = time.time()
         launches = int(lib.mbg_launch_count())
         ms = e0.elapsed_time(e1) / steps
         if dist:
@@ -181,7 +265,9 @@ def run_ours(args, rank, world, dist):
     # ---- headline: split-precision sgemm ----
     clocks = Clocks(dev)
     with clocks:
+        time.sleep(0.3)  # let the sampler start before the timed region
         ms, launches = timed(mode, args.steps, args.warmup)
+    clocks.window = tuple(window)
     value = world * 2 * FLOPS_S / (ms * 1e-3) / 1e12
 
     # per-kernel timing of the dominant kernel (CUDA events around each launch)
@@ -256,6 +342,9 @@ def run_ours(args, rank, world, dist):
                          "fp64_err": rows_error(Cd, refd, rsd)}
         del Ad, Bd, Cd
 
+    # ---- configuration 3: blocked dtrsm 4096^2 and ssyrk 8192 x 2048 ----
+    cfg3 = {} if args.skip_cfg3 else run_cfg3(torch, lib, L, stream)
+
     # ---- e2e through the C ABI with pinned host buffers ----
     hA = A.cpu().pin_memory()
     hB = B.cpu().pin_memory()
@@ -311,6 +400,7 @@ def run_ours(args, rank, world, dist):
         "fp64_oracle_error": errs,
         "error_metric": f"max|C-C64|/max|C64| over {SAMPLE_ROWS} sampled rows, C64 = float64 numpy",
         "dgemm_4096": dg,
+        "cfg3": cfg3,
         "e2e": {"value": round(e2e_value, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_out, "ms_per_step": round(e2e_ms, 2)},
         "gpu_launches": launches,
@@ -355,12 +445,13 @@ def run_cpu_baseline(args, threads=None, budget_s=None):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="bf16x6", choices=["bf16x3", "bf16x6"])
     ap.add_argument("--skip-dgemm", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-cfg3", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

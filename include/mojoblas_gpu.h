@@ -139,6 +139,13 @@ int   mbg_version(void);
 /* Release cached device workspace. */
 int   mbg_release_workspace(void);
 
+/* ---- tuning table -------------------------------------------------------
+ * Keys: "trsm_tc_min_k" — trsm off-diagonal updates with a shorter reduction
+ * run on the plain kernel instead of the split / Ozaki forms (default 256).
+ * mbg_get_tuning returns -1 for an unknown key. */
+int     mbg_set_tuning(const char* key, int64_t value);
+int64_t mbg_get_tuning(const char* key);
+
 /* ---- kernel timing (CUDA events around each library kernel launch) ------ */
 int mbg_prof_enable(int on);
 int mbg_prof_reset(void);

@@ -56,12 +56,15 @@ SIGNATURES = {
     "mbg_prof_query": [C.c_char_p, C.POINTER(_d), C.POINTER(i64)],
     "mbg_launch_count": [],
     "mbg_debug_fail_alloc": [_i],
+    "mbg_set_tuning": [C.c_char_p, i64],
+    "mbg_get_tuning": [C.c_char_p],
 }
 _RESTYPES = {
     "mbg_get_stream": _vp,
     "mbg_status_string": C.c_char_p,
     "mbg_last_error": C.c_char_p,
     "mbg_launch_count": i64,
+    "mbg_get_tuning": i64,
 }
 
 _lib = None

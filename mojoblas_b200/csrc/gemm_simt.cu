@@ -10,13 +10,16 @@
 // 64+tx*4+{0..3}, columns likewise from ty) with one FMA per product.  Each
 // element's sum runs over k in ascending order, like the reference's per-column
 // axpy loops; beta is applied once in the epilogue (beta == 0 does not read C).
+// Launches that would fill fewer than two waves of 128 x 128 tiles (the
+// tall-skinny updates inside trsm, small problems) use 64 x 64 tiles with a
+// 4 x 4 register block instead, for four times as many CTAs.
 #include "mbg_internal.cuh"
 
 namespace mbg {
 
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 8, NT = 256;
+constexpr int BK = 8, NT = 256;
 
 template <typename T> struct Pad;
 template <> struct Pad<float> { static constexpr int v = 4; };
@@ -45,10 +48,16 @@ __device__ __forceinline__ void tri_tile(i64 t, i64& ti, i64& tj) {
     tj = t - r * (r + 1) / 2;
 }
 
-template <typename T, bool TA, bool TB, int TRI>
-__global__ void __launch_bounds__(NT, 1)
+// TILE = 128: 128 x 128 tile, 8 x 8 per thread (rows tx*4+{0..3} and
+// 64+tx*4+{0..3}); TILE = 64: 64 x 64 tile, 4 x 4 per thread (rows tx*4+{0..3}),
+// four times as many CTAs for launches that would not fill the GPU.
+template <typename T, bool TA, bool TB, int TRI, int TILE>
+__global__ void __launch_bounds__(NT, TILE == 128 ? 1 : 2)
 gemm_simt_kernel(i64 m, i64 n, i64 k, T alpha, const T* __restrict__ A, i64 lda,
                  const T* __restrict__ B, i64 ldb, T beta, T* __restrict__ C, i64 ldc) {
+    constexpr int BM = TILE, BN = TILE;
+    constexpr int TM = TILE / 16;        // 8 or 4 rows (and columns) per thread
+    constexpr int LPT = BM * BK / NT;    // elements of each operand a thread loads per slab
     constexpr int P = Pad<T>::v;
     __shared__ __align__(16) T As[2][BK][BM + P];
     __shared__ __align__(16) T Bs[2][BK][BN + P];
@@ -62,14 +71,14 @@ gemm_simt_kernel(i64 m, i64 n, i64 k, T alpha, const T* __restrict__ A, i64 lda,
         tri_tile(blockIdx.x, ti, tj);
         if (TRI == 1) { tm = ti; tn = tj; } else { tm = tj; tn = ti; }
     }
-    const i64 m0 = tm * BM, n0 = tn * BN;
+    const i64 m0 = tm * BM, n0 = tn * BN;  // tile origin
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
 
-    T ra[4], rb[4];
+    T ra[LPT], rb[LPT];
     auto load_global = [&](i64 k0) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < LPT; ++r) {
             const int e = tid + r * NT;
             int i, l;
             if (!TA) { i = e % BM; l = e / BM; } else { i = e / BK; l = e % BK; }
@@ -79,7 +88,7 @@ gemm_simt_kernel(i64 m, i64 n, i64 k, T alpha, const T* __restrict__ A, i64 lda,
             ra[r] = v;
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < LPT; ++r) {
             const int e = tid + r * NT;
             int j, l;
             if (!TB) { j = e / BK; l = e % BK; } else { j = e % BN; l = e / BN; }
@@ -91,14 +100,14 @@ gemm_simt_kernel(i64 m, i64 n, i64 k, T alpha, const T* __restrict__ A, i64 lda,
     };
     auto store_shared = [&](int buf) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < LPT; ++r) {
             const int e = tid + r * NT;
             int i, l;
             if (!TA) { i = e % BM; l = e / BM; } else { i = e / BK; l = e % BK; }
             As[buf][l][i] = ra[r];
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < LPT; ++r) {
             const int e = tid + r * NT;
             int j, l;
             if (!TB) { j = e / BK; l = e % BK; } else { j = e % BN; l = e / BN; }
@@ -106,11 +115,11 @@ gemm_simt_kernel(i64 m, i64 n, i64 k, T alpha, const T* __restrict__ A, i64 lda,
         }
     };
 
-    T acc[8][8];
+    T acc[TM][TM];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+        for (int j = 0; j < TM; ++j) acc[i][j] = T(0);
 
     const i64 nk = (k + BK - 1) / BK;
     load_global(0);
@@ -121,35 +130,37 @@ gemm_simt_kernel(i64 m, i64 n, i64 k, T alpha, const T* __restrict__ A, i64 lda,
         if (kt + 1 < nk) load_global((kt + 1) * BK);
 #pragma unroll
         for (int l = 0; l < BK; ++l) {
-            T a[8], b[8];
+            T a[TM], b[TM];
             T t4[4];
             lds4<T>(&As[buf][l][tx * 4], t4);
 #pragma unroll
             for (int q = 0; q < 4; ++q) a[q] = t4[q];
-            lds4<T>(&As[buf][l][64 + tx * 4], t4);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) a[4 + q] = t4[q];
             lds4<T>(&Bs[buf][l][ty * 4], t4);
 #pragma unroll
             for (int q = 0; q < 4; ++q) b[q] = t4[q];
-            lds4<T>(&Bs[buf][l][64 + ty * 4], t4);
+            if (TM == 8) {
+                lds4<T>(&As[buf][l][64 + tx * 4], t4);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) b[4 + q] = t4[q];
+                for (int q = 0; q < 4; ++q) a[(4 + q) % TM] = t4[q];
+                lds4<T>(&Bs[buf][l][64 + ty * 4], t4);
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+                for (int q = 0; q < 4; ++q) b[(4 + q) % TM] = t4[q];
+            }
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            for (int i = 0; i < TM; ++i)
+#pragma unroll
+                for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
         }
         if (kt + 1 < nk) store_shared(buf ^ 1);
         __syncthreads();
     }
 
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < TM; ++j) {
         const i64 gj = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
         if (gj >= n) continue;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < TM; ++i) {
             const i64 gi = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
             if (gi >= m) continue;
             if (TRI == 1 && gi < gj) continue;
@@ -175,15 +186,15 @@ __global__ void scale_kernel(i64 m, i64 n, T beta, T* __restrict__ C, i64 ldc) {
     }
 }
 
-template <typename T, int TRI>
+template <typename T, int TRI, int TILE>
 int launch_gemm(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, T alpha, const T* a, i64 lda,
                 const T* b, i64 ldb, T beta, T* c, i64 ldc) {
     ProfScope prof(sizeof(T) == 4 ? "gemm_simt_f32" : "gemm_simt_f64");
     cudaStream_t s = stream();
-    if (!ta && !tb) gemm_simt_kernel<T, false, false, TRI><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    else if (!ta && tb) gemm_simt_kernel<T, false, true, TRI><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    else if (ta && !tb) gemm_simt_kernel<T, true, false, TRI><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    else gemm_simt_kernel<T, true, true, TRI><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (!ta && !tb) gemm_simt_kernel<T, false, false, TRI, TILE><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    else if (!ta && tb) gemm_simt_kernel<T, false, true, TRI, TILE><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    else if (ta && !tb) gemm_simt_kernel<T, true, false, TRI, TILE><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    else gemm_simt_kernel<T, true, true, TRI, TILE><<<grid, NT, 0, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     return check_launch(sizeof(T) == 4 ? "gemm_simt_f32" : "gemm_simt_f64");
 }
 
@@ -213,10 +224,16 @@ int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 l
                const T* b, i64 ldb, T beta, T* c, i64 ldc) {
     if (m == 0 || n == 0) return MBG_OK;
     if (alpha == T(0) || k == 0) return scale_matrix<T>(m, n, beta, c, ldc);
-    const i64 gm = cdiv(m, BM), gn = cdiv(n, BN);
+    const i64 gm = cdiv(m, 128), gn = cdiv(n, 128);
+    if (gm * gn < 2 * 148) {  // under two waves of 128 x 128 tiles: use 64 x 64 tiles
+        const i64 sm = cdiv(m, 64), sn = cdiv(n, 64);
+        if (sn > 65535 || sm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+        return launch_gemm<T, 0, 64>(is_t(ta), is_t(tb), dim3((unsigned)sm, (unsigned)sn), m, n, k, alpha,
+                                     a, lda, b, ldb, beta, c, ldc);
+    }
     if (gn > 65535 || gm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
-    return launch_gemm<T, 0>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha,
-                             a, lda, b, ldb, beta, c, ldc);
+    return launch_gemm<T, 0, 128>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha,
+                                  a, lda, b, ldb, beta, c, ldc);
 }
 
 template <typename T>
@@ -224,14 +241,14 @@ int gemmt_plain(char uplo, char ta, char tb, i64 n, i64 k, T alpha, const T* a, 
                 const T* b, i64 ldb, T beta, T* c, i64 ldc) {
     if (n == 0) return MBG_OK;
     if (alpha == T(0) || k == 0) return scale_triangle<T>(uplo, n, beta, c, ldc);
-    const i64 t = cdiv(n, BM);
+    const i64 t = cdiv(n, 128);
     const i64 tiles = t * (t + 1) / 2;
     if (tiles > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
     if (is_l(uplo))
-        return launch_gemm<T, 1>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda,
-                                 b, ldb, beta, c, ldc);
-    return launch_gemm<T, 2>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b,
-                             ldb, beta, c, ldc);
+        return launch_gemm<T, 1, 128>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda,
+                                      b, ldb, beta, c, ldc);
+    return launch_gemm<T, 2, 128>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b,
+                                  ldb, beta, c, ldc);
 }
 
 template int gemm_plain<float>(char, char, i64, i64, i64, float, const float*, i64, const float*, i64, float, float*, i64);

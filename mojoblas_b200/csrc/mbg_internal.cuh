@@ -95,6 +95,12 @@ int* device_error_flag();
 int read_and_clear_device_error();
 int finish_call(bool any_staged);  // synchronises when required, checks flag
 
+// ---- tuning table (defaults; mbg_set_tuning / mbg_load_tuning override) ------
+struct Tuning {
+    i64 trsm_tc_min_k = 256;   // trsm off-diagonal updates with shorter k use the plain kernel
+};
+Tuning& tuning();
+
 // ---- kernels (implemented in the other translation units) --------------------
 template <typename T>
 int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 lda,

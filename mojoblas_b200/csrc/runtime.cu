@@ -52,6 +52,11 @@ int current_device() {
 }
 }  // namespace
 
+Tuning& tuning() {
+    static Tuning t;
+    return t;
+}
+
 cudaStream_t stream() { return g_stream; }
 bool sync_mode() { return g_sync.load(); }
 
@@ -303,6 +308,20 @@ int mbg_prof_query(const char* sub, double* total_ms, int64_t* launches) {
 }
 
 int64_t mbg_launch_count(void) { return g_launches.load(); }
+
+int mbg_set_tuning(const char* key, int64_t value) {
+    if (!key) return MBG_ERR_INVALID_MODE;
+    const std::string k(key);
+    if (k == "trsm_tc_min_k") { tuning().trsm_tc_min_k = value; return MBG_OK; }
+    set_error_msg("unknown tuning key: " + k);
+    return MBG_ERR_INVALID_MODE;
+}
+
+int64_t mbg_get_tuning(const char* key) {
+    const std::string k(key ? key : "");
+    if (k == "trsm_tc_min_k") return tuning().trsm_tc_min_k;
+    return -1;
+}
 
 int mbg_debug_fail_alloc(int nth) { g_fail_alloc_countdown = nth > 0 ? nth : 0; return MBG_OK; }
 

@@ -31,13 +31,20 @@ namespace {
 constexpr int NB = 64;        // diagonal block (leaf) size
 constexpr int DS_WARPS = 8;   // columns per CTA in flight
 
-// Solves op(A)[r0:r0+nb, r0:r0+nb] X = B[r0:r0+nb, :] in place.
+// Solves op(A)[0:nb, 0:nb] X = B[0:nb, :] in place for nb <= 64.
 // LOWER: effective op(A) lower triangular (forward), else upper (backward).
+// The block is staged once per CTA in shared memory (column-major, padded)
+// with the reciprocals of its diagonal.  Each warp owns one right-hand-side
+// column, two rows per lane, and runs the reference's column-axpy substitution
+// (src/level3/trsm.mojo:111-148): the pivot x_l is broadcast from its lane by a
+// warp shuffle, scaled by 1/a_ll (a multiply: a division would put a long
+// software sequence on every step's dependency chain), and every lane updates
+// its rows below (above) it; zero pivots are skipped as in the reference.
 template <typename T, bool LOWER, bool TRANS, bool UNIT>
 __global__ void __launch_bounds__(DS_WARPS * 32)
 diag_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __restrict__ B, i64 ldb) {
     __shared__ T Ls[NB * (NB + 1)];
-    // stage op(A) block, column-major with a padded leading dimension
+    __shared__ T inv[NB];
     for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
         int i, l;
         if (TRANS) { l = e % nb; i = e / nb; } else { i = e % nb; l = e / nb; }  // coalesced reads
@@ -48,6 +55,8 @@ diag_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __rest
         Ls[l * (NB + 1) + i] = v;
     }
     __syncthreads();
+    for (int l = threadIdx.x; l < nb; l += blockDim.x) inv[l] = UNIT ? T(1) : T(1) / Ls[l * (NB + 1) + l];
+    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (i64 j = (i64)blockIdx.x * DS_WARPS + warp; j < ncols; j += (i64)gridDim.x * DS_WARPS) {
         T* bj = B + j * ldb;
@@ -55,18 +64,19 @@ diag_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __rest
         T x1 = lane + 32 < nb ? bj[lane + 32] : T(0);
         for (int s = 0; s < nb; ++s) {
             const int l = LOWER ? s : nb - 1 - s;
+            const T* col = Ls + l * (NB + 1);
+            const T c0 = col[lane], c1 = col[lane + 32], il = inv[l];  // independent of the chain
             const T src = (l < 32) ? x0 : x1;
             T xl = __shfl_sync(0xffffffffu, src, l & 31);
-            if (xl == T(0)) continue;  // the reference skips zero pivots (:133, :115)
-            if (!UNIT) xl = xl / Ls[l * (NB + 1) + l];
+            if (xl == T(0)) continue;  // the reference skips zero pivots (:115, :133)
+            if (!UNIT) xl *= il;
             if (lane == (l & 31)) { if (l < 32) x0 = xl; else x1 = xl; }
-            const T* col = Ls + l * (NB + 1);
             if (LOWER) {
-                if (lane > l) x0 -= xl * col[lane];
-                if (lane + 32 > l && lane + 32 < nb) x1 -= xl * col[lane + 32];
+                if (lane > l) x0 -= xl * c0;
+                if (lane + 32 > l && lane + 32 < nb) x1 -= xl * c1;
             } else {
-                if (lane < l) x0 -= xl * col[lane];
-                if (lane + 32 < l) x1 -= xl * col[lane + 32];
+                if (lane < l) x0 -= xl * c0;
+                if (lane + 32 < l) x1 -= xl * c1;
             }
         }
         if (lane < nb) bj[lane] = x0;
@@ -174,14 +184,19 @@ int launch_diag_residual(bool lower, bool trans, bool unit, int nb, i64 n, const
     return check_launch("trsm_diag_residual");
 }
 
-// gemm in a precision mode, device operands
+// gemm in a precision mode, device operands.  Updates with a short reduction
+// (k below the tuning table's trsm_tc_min_k) carry few flops and would pay the
+// split/slice pre-pass for little work: they run on the plain kernel, which is
+// as accurate as the split / Ozaki forms.
 inline int gemm_in_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, float alpha,
                         const float* a, i64 lda, const float* b, i64 ldb, float beta, float* c, i64 ldc) {
     (void)slices;
+    if (k < tuning().trsm_tc_min_k) mode = MBG_MODE_PLAIN;
     return sgemm_mode(mode, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
 }
 inline int gemm_in_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
                         const double* a, i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+    if (k < tuning().trsm_tc_min_k) mode = MBG_MODE_PLAIN;
     return dgemm_mode(mode, slices, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
 }
 
