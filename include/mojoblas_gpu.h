@@ -123,6 +123,45 @@ int mbg_sgemm_ex_noalloc(int mode, char trans_a, char trans_b, int64_t m, int64_
                          float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
                          float beta, float* c, int64_t ldc);
 
+/* ---- batched: many independent problems in one persistent launch ----------
+ * No counterpart in the reference, whose callers loop over gemm / trsm.
+ * A plan validates the problems (Netlib numbering per problem; the first
+ * invalid problem's info is returned and described by mbg_last_error), copies
+ * the problem table to the device once and records [reset; persistent kernel]
+ * into a CUDA graph; mbg_plan_execute replays it on the library stream.  All
+ * matrix pointers must be device pointers and stay valid for the plan's life.
+ *   sgemm: any transposes, any sizes; tiles of 64 or 128 (tuning key
+ *          "grouped_gemm_tile"), largest problems first, atomic tile counter.
+ *   strsm: side 'L' only, m <= 256 (the triangle order), any uplo/trans/diag;
+ *          one warp per right-hand-side column.
+ * mode: MBG_MODE_PLAIN. */
+typedef struct {
+    char trans_a, trans_b;
+    int64_t m, n, k;
+    float alpha, beta;
+    const float* a; int64_t lda;
+    const float* b; int64_t ldb;
+    float* c; int64_t ldc;
+} mbg_sgemm_problem;
+
+typedef struct {
+    char side, uplo, trans_a, diag;
+    int64_t m, n;
+    float alpha;
+    const float* a; int64_t lda;
+    float* b; int64_t ldb;
+} mbg_strsm_problem;
+
+typedef struct mbg_plan mbg_plan;
+
+int mbg_sgemm_grouped_plan(int mode, int count, const mbg_sgemm_problem* problems, mbg_plan** plan);
+int mbg_strsm_grouped_plan(int mode, int count, const mbg_strsm_problem* problems, mbg_plan** plan);
+int mbg_plan_execute(mbg_plan* plan);
+int mbg_plan_destroy(mbg_plan* plan);
+/* one-shot forms: plan, execute, destroy */
+int mbg_sgemm_grouped(int mode, int count, const mbg_sgemm_problem* problems);
+int mbg_strsm_grouped(int mode, int count, const mbg_strsm_problem* problems);
+
 /* ---- runtime ------------------------------------------------------------ */
 /* Stream for subsequent calls from any thread (a cudaStream_t; NULL = legacy
  * default stream, the initial value). */
@@ -141,10 +180,14 @@ int   mbg_release_workspace(void);
 
 /* ---- tuning table -------------------------------------------------------
  * Keys: "trsm_tc_min_k" — trsm off-diagonal updates with a shorter reduction
- * run on the plain kernel instead of the split / Ozaki forms (default 256).
+ * run on the plain kernel instead of the split / Ozaki forms (default 256);
+ * "grouped_gemm_tile" — 64 or 128, tile edge of grouped sgemm plans (default 64).
+ * mbg_load_tuning reads "key value" lines (or a flat JSON object of them) as
+ * written by the autotuner (mojoblas_b200/autotune.py).
  * mbg_get_tuning returns -1 for an unknown key. */
 int     mbg_set_tuning(const char* key, int64_t value);
 int64_t mbg_get_tuning(const char* key);
+int     mbg_load_tuning(const char* path);
 
 /* ---- kernel timing (CUDA events around each library kernel launch) ------ */
 int mbg_prof_enable(int on);

@@ -9,6 +9,7 @@ import ctypes as C
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "libmojoblas_gpu.so"
+TUNING_PATH = Path(__file__).resolve().parent / "tuning_b200.json"
 
 MBG_OK = 0
 MBG_ERR_CUDA = -1
@@ -58,6 +59,13 @@ SIGNATURES = {
     "mbg_debug_fail_alloc": [_i],
     "mbg_set_tuning": [C.c_char_p, i64],
     "mbg_get_tuning": [C.c_char_p],
+    "mbg_load_tuning": [C.c_char_p],
+    "mbg_sgemm_grouped_plan": [_i, _i, _vp, C.POINTER(_vp)],
+    "mbg_strsm_grouped_plan": [_i, _i, _vp, C.POINTER(_vp)],
+    "mbg_plan_execute": [_vp],
+    "mbg_plan_destroy": [_vp],
+    "mbg_sgemm_grouped": [_i, _i, _vp],
+    "mbg_strsm_grouped": [_i, _i, _vp],
 }
 _RESTYPES = {
     "mbg_get_stream": _vp,
@@ -66,6 +74,20 @@ _RESTYPES = {
     "mbg_launch_count": i64,
     "mbg_get_tuning": i64,
 }
+
+class SgemmProblem(C.Structure):
+    """mbg_sgemm_problem (include/mojoblas_gpu.h)."""
+    _fields_ = [("trans_a", C.c_char), ("trans_b", C.c_char), ("m", i64), ("n", i64), ("k", i64),
+                ("alpha", C.c_float), ("beta", C.c_float), ("a", C.c_void_p), ("lda", i64),
+                ("b", C.c_void_p), ("ldb", i64), ("c", C.c_void_p), ("ldc", i64)]
+
+
+class StrsmProblem(C.Structure):
+    """mbg_strsm_problem (include/mojoblas_gpu.h)."""
+    _fields_ = [("side", C.c_char), ("uplo", C.c_char), ("trans_a", C.c_char), ("diag", C.c_char),
+                ("m", i64), ("n", i64), ("alpha", C.c_float), ("a", C.c_void_p), ("lda", i64),
+                ("b", C.c_void_p), ("ldb", i64)]
+
 
 _lib = None
 
@@ -84,6 +106,8 @@ def load() -> C.CDLL:
             fn.argtypes = argtypes
             fn.restype = _RESTYPES.get(name, _i)
         _lib = lib
+        if TUNING_PATH.exists():  # the autotuner's table for B200 (mojoblas_b200/autotune.py)
+            lib.mbg_load_tuning(str(TUNING_PATH).encode())
     return _lib
 
 

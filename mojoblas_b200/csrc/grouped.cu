@@ -1,0 +1,523 @@
+// Grouped (batched) gemm and trsm: thousands of independent problems of uneven
+// sizes in one persistent launch per problem type.
+//
+// The reference has no batched interface; a mojoBLAS caller loops over its
+// gemm (src/level3/gemm.mojo:56) / trsm (src/level3/trsm.mojo:20) calls.  Here
+// a host-side plan uploads a problem table once, and each execution is a CUDA
+// graph of [reset the tile counter; one persistent kernel]:
+//
+//  * sgemm: problems are ordered by k * m * n descending and cut into square
+//    tiles (64 or 128, from the tuning table); persistent CTAs take tiles from
+//    an atomic counter (largest first, so the tail is short), locate the problem
+//    by binary search over the tile prefix sums, and run the plain FP32 tile
+//    code of gemm_simt.cu with that problem's transposes, alpha and beta.
+//  * strsm (left side, any uplo / trans / diag, n <= 256): one warp per
+//    (problem, right-hand-side column); the column lives in registers, eight
+//    rows per lane, and the reference's column substitution
+//    (src/level3/trsm.mojo:111-168) runs with the pivot broadcast by a warp
+//    shuffle and multiplied by a precomputed reciprocal of the diagonal.
+#include "mbg_internal.cuh"
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+namespace mbg {
+
+namespace {
+
+struct GemmDesc {  // device copy of one problem
+    i64 m, n, k, lda, ldb, ldc;
+    const float* a;
+    const float* b;
+    float* c;
+    float alpha, beta;
+    int ta, tb;
+    i64 tile0;   // first tile index of this problem
+    int tiles_m;  // tiles along m
+};
+
+constexpr int GT_NT = 256, GT_BK = 8;
+
+template <int TILE, bool TA, bool TB>
+__device__ __forceinline__ void gemm_tile(const GemmDesc& d, i64 tm, i64 tn, float* As_, float* Bs_) {
+    constexpr int BM = TILE, BN = TILE, TM = TILE / 16, LPT = BM * GT_BK / GT_NT, P = 4;
+    float(*As)[GT_BK][BM + P] = reinterpret_cast<float(*)[GT_BK][BM + P]>(As_);
+    float(*Bs)[GT_BK][BN + P] = reinterpret_cast<float(*)[GT_BK][BN + P]>(Bs_);
+    const i64 m0 = tm * BM, n0 = tn * BN;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const i64 m = d.m, n = d.n, k = d.k;
+    float ra[LPT], rb[LPT];
+    auto load_global = [&](i64 k0) {
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) {
+            const int e = tid + r * GT_NT;
+            int i, l;
+            if (!TA) { i = e % BM; l = e / BM; } else { i = e / GT_BK; l = e % GT_BK; }
+            const i64 gi = m0 + i, gl = k0 + l;
+            ra[r] = (gi < m && gl < k) ? (TA ? d.a[gl + gi * d.lda] : d.a[gi + gl * d.lda]) : 0.0f;
+        }
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) {
+            const int e = tid + r * GT_NT;
+            int j, l;
+            if (!TB) { j = e / GT_BK; l = e % GT_BK; } else { j = e % BN; l = e / BN; }
+            const i64 gj = n0 + j, gl = k0 + l;
+            rb[r] = (gj < n && gl < k) ? (TB ? d.b[gj + gl * d.ldb] : d.b[gl + gj * d.ldb]) : 0.0f;
+        }
+    };
+    auto store_shared = [&](int buf) {
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) {
+            const int e = tid + r * GT_NT;
+            int i, l;
+            if (!TA) { i = e % BM; l = e / BM; } else { i = e / GT_BK; l = e % GT_BK; }
+            As[buf][l][i] = ra[r];
+        }
+#pragma unroll
+        for (int r = 0; r < LPT; ++r) {
+            const int e = tid + r * GT_NT;
+            int j, l;
+            if (!TB) { j = e / GT_BK; l = e % GT_BK; } else { j = e % BN; l = e / BN; }
+            Bs[buf][l][j] = rb[r];
+        }
+    };
+    float acc[TM][TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TM; ++j) acc[i][j] = 0.0f;
+    const i64 nk = (k + GT_BK - 1) / GT_BK;
+    load_global(0);
+    store_shared(0);
+    __syncthreads();
+    for (i64 kt = 0; kt < nk; ++kt) {
+        const int buf = int(kt & 1);
+        if (kt + 1 < nk) load_global((kt + 1) * GT_BK);
+#pragma unroll
+        for (int l = 0; l < GT_BK; ++l) {
+            float a[TM], b[TM];
+            const float4 va = *reinterpret_cast<const float4*>(&As[buf][l][tx * 4]);
+            const float4 vb = *reinterpret_cast<const float4*>(&Bs[buf][l][ty * 4]);
+            a[0] = va.x; a[1] = va.y; a[2] = va.z; a[3] = va.w;
+            b[0] = vb.x; b[1] = vb.y; b[2] = vb.z; b[3] = vb.w;
+            if (TM == 8) {
+                const float4 wa = *reinterpret_cast<const float4*>(&As[buf][l][64 + tx * 4]);
+                const float4 wb = *reinterpret_cast<const float4*>(&Bs[buf][l][64 + ty * 4]);
+                a[4 % TM] = wa.x; a[5 % TM] = wa.y; a[6 % TM] = wa.z; a[7 % TM] = wa.w;
+                b[4 % TM] = wb.x; b[5 % TM] = wb.y; b[6 % TM] = wb.z; b[7 % TM] = wb.w;
+            }
+#pragma unroll
+            for (int i = 0; i < TM; ++i)
+#pragma unroll
+                for (int j = 0; j < TM; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        if (kt + 1 < nk) store_shared(buf ^ 1);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < TM; ++j) {
+        const i64 gj = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+        if (gj >= n) continue;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const i64 gi = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+            if (gi >= m) continue;
+            float* cp = d.c + gi + gj * d.ldc;
+            const float v = d.alpha * acc[i][j];
+            *cp = (d.beta == 0.0f) ? v : fmaf(d.beta, *cp, v);
+        }
+    }
+}
+
+template <int TILE>
+__global__ void __launch_bounds__(GT_NT, TILE == 128 ? 1 : 2)
+grouped_sgemm_kernel(const GemmDesc* __restrict__ probs, int count, i64 total_tiles,
+                     unsigned long long* __restrict__ counter) {
+    constexpr int P = 4;
+    __shared__ __align__(16) float As[2 * GT_BK * (TILE + P)];
+    __shared__ __align__(16) float Bs[2 * GT_BK * (TILE + P)];
+    __shared__ long long s_tile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const i64 t = s_tile;
+        __syncthreads();  // every thread has read s_tile before it is overwritten
+        if (t >= total_tiles) return;
+        // problem owning tile t: the last with tile0 <= t
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (probs[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+        }
+        const GemmDesc d = probs[lo];  // registers
+        const i64 local = t - d.tile0;
+        const i64 tm = local % d.tiles_m, tn = local / d.tiles_m;
+        if (d.k == 0 || d.alpha == 0.0f) {  // C := beta*C on this tile
+            for (int e = threadIdx.x; e < TILE * TILE; e += GT_NT) {
+                const i64 gi = tm * TILE + e % TILE, gj = tn * TILE + e / TILE;
+                if (gi < d.m && gj < d.n) {
+                    float* cp = d.c + gi + gj * d.ldc;
+                    *cp = (d.beta == 0.0f) ? 0.0f : d.beta * *cp;
+                }
+            }
+        } else if (!d.ta && !d.tb) gemm_tile<TILE, false, false>(d, tm, tn, As, Bs);
+        else if (!d.ta && d.tb) gemm_tile<TILE, false, true>(d, tm, tn, As, Bs);
+        else if (d.ta && !d.tb) gemm_tile<TILE, true, false>(d, tm, tn, As, Bs);
+        else gemm_tile<TILE, true, true>(d, tm, tn, As, Bs);
+        __syncthreads();  // shared tiles are reused by the next tile
+    }
+}
+
+struct TrsmDesc {
+    i64 n, nrhs, lda, ldb;
+    const float* a;
+    float* b;
+    float alpha;
+    int lower, trans, unit;  // lower: effective op(A) lower triangular
+    i64 col0;                // first global column index of this problem
+};
+
+constexpr int TR_MAXN = 256, TR_SLOTS = TR_MAXN / 32;
+
+// One warp solves op(A) x = alpha * b for one column of one problem.
+__global__ void __launch_bounds__(256)
+grouped_strsm_kernel(const TrsmDesc* __restrict__ probs, int count, i64 total_cols) {
+    const int lane = threadIdx.x & 31;
+    const i64 wid = (i64(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const i64 nwarps = (i64(gridDim.x) * blockDim.x) >> 5;
+    for (i64 c = wid; c < total_cols; c += nwarps) {
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (probs[mid].col0 <= c) lo = mid; else hi = mid - 1;
+        }
+        const TrsmDesc d = probs[lo];  // registers
+        const int n = int(d.n);
+        float* bj = d.b + (c - d.col0) * d.ldb;
+        auto aval = [&](int r, int l) -> float { return d.trans ? d.a[l + i64(r) * d.lda] : d.a[r + i64(l) * d.lda]; };
+        float x[TR_SLOTS], inv[TR_SLOTS];
+#pragma unroll
+        for (int s = 0; s < TR_SLOTS; ++s) {
+            const int r = s * 32 + lane;
+            x[s] = r < n ? d.alpha * bj[r] : 0.0f;
+            inv[s] = (r < n && !d.unit) ? 1.0f / aval(r, r) : 1.0f;  // off the dependency chain
+        }
+        if (d.lower) {
+#pragma unroll
+            for (int s = 0; s < TR_SLOTS; ++s) {
+                if (s * 32 >= n) break;
+                for (int t = 0; t < 32; ++t) {
+                    const int l = s * 32 + t;
+                    if (l >= n) break;
+                    float xl = __shfl_sync(0xffffffffu, x[s], t);
+                    if (xl == 0.0f) continue;  // zero pivot: skipped as in the reference
+                    xl *= __shfl_sync(0xffffffffu, inv[s], t);
+                    if (lane == t) x[s] = xl;
+#pragma unroll
+                    for (int s2 = s; s2 < TR_SLOTS; ++s2) {
+                        const int r = s2 * 32 + lane;
+                        if (r > l && r < n) x[s2] -= xl * aval(r, l);
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int s = TR_SLOTS - 1; s >= 0; --s) {
+                if (s * 32 >= n) continue;
+                for (int t = 31; t >= 0; --t) {
+                    const int l = s * 32 + t;
+                    if (l >= n) continue;
+                    float xl = __shfl_sync(0xffffffffu, x[s], t);
+                    if (xl == 0.0f) continue;
+                    xl *= __shfl_sync(0xffffffffu, inv[s], t);
+                    if (lane == t) x[s] = xl;
+#pragma unroll
+                    for (int s2 = 0; s2 <= s; ++s2) {
+                        const int r = s2 * 32 + lane;
+                        if (r < l) x[s2] -= xl * aval(r, l);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < TR_SLOTS; ++s) {
+            const int r = s * 32 + lane;
+            if (r < n) bj[r] = x[s];
+        }
+    }
+}
+
+int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+            cudaGetLastError();
+            sms = 148;
+        }
+    }
+    return sms;
+}
+
+}  // namespace
+
+}  // namespace mbg
+
+// ---- plans ------------------------------------------------------------------------
+struct mbg_plan {
+    int kind = 0;  // 1 sgemm, 2 strsm
+    void* table = nullptr;                 // device problem table
+    unsigned long long* counter = nullptr;  // device tile counter (sgemm)
+    int count = 0;
+    i64 total = 0;       // tiles (sgemm) or columns (strsm)
+    int tile = 64;
+    int grid = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;  // stream the graph was captured on
+};
+
+namespace mbg {
+namespace {
+
+int enqueue_plan(mbg_plan* p) {
+    cudaStream_t s = stream();
+    if (p->kind == 1) {
+        MBG_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
+        if (p->tile == 128)
+            grouped_sgemm_kernel<128><<<p->grid, GT_NT, 0, s>>>(static_cast<const GemmDesc*>(p->table), p->count,
+                                                                p->total, p->counter);
+        else
+            grouped_sgemm_kernel<64><<<p->grid, GT_NT, 0, s>>>(static_cast<const GemmDesc*>(p->table), p->count,
+                                                               p->total, p->counter);
+        return check_launch("grouped_sgemm");
+    }
+    grouped_strsm_kernel<<<p->grid, 256, 0, s>>>(static_cast<const TrsmDesc*>(p->table), p->count, p->total);
+    return check_launch("grouped_strsm");
+}
+
+// Records the plan's work into a CUDA graph on a private capture stream.
+int capture_plan(mbg_plan* p) {
+    cudaStream_t cap = nullptr;
+    MBG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaStream_t saved = stream();
+    mbg_set_stream(cap);
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    int st = MBG_OK;
+    if (e == cudaSuccess) {
+        st = enqueue_plan(p);
+        e = cudaStreamEndCapture(cap, &p->graph);
+    }
+    mbg_set_stream(saved);
+    cudaStreamDestroy(cap);
+    if (e != cudaSuccess) {
+        set_error("graph capture of a grouped plan", e);
+        return MBG_ERR_CUDA;
+    }
+    if (st) return st;
+    MBG_CUDA(cudaGraphInstantiate(&p->exec, p->graph, 0));
+    return MBG_OK;
+}
+
+template <typename D>
+int upload(mbg_plan* p, const std::vector<D>& v) {
+    MBG_CUDA(cudaMalloc(&p->table, sizeof(D) * v.size()));
+    MBG_CUDA(cudaMemcpy(p->table, v.data(), sizeof(D) * v.size(), cudaMemcpyHostToDevice));
+    return MBG_OK;
+}
+
+}  // namespace
+}  // namespace mbg
+
+using namespace mbg;
+
+extern "C" {
+
+int mbg_sgemm_grouped_plan(int mode, int count, const mbg_sgemm_problem* probs, mbg_plan** out) {
+    if (!out) return MBG_ERR_INVALID_MODE;
+    *out = nullptr;
+    if (mode != MBG_MODE_PLAIN) {
+        set_error_msg("grouped sgemm: only MBG_MODE_PLAIN is implemented");
+        return MBG_ERR_UNSUPPORTED;
+    }
+    if (count < 0 || (count > 0 && !probs)) return MBG_ERR_INVALID_MODE;
+    for (int i = 0; i < count; ++i) {  // argument checks per problem, numbered as gemm numbers them
+        const mbg_sgemm_problem& q = probs[i];
+        const char ta = q.trans_a, tb = q.trans_b;
+        int info = 0;
+        if (!is_n(ta) && !is_t(ta)) info = 1;
+        else if (!is_n(tb) && !is_t(tb)) info = 2;
+        else if (q.m < 0) info = 3;
+        else if (q.n < 0) info = 4;
+        else if (q.k < 0) info = 5;
+        else if (q.lda < imax(1, is_n(ta) ? q.m : q.k)) info = 8;
+        else if (q.ldb < imax(1, is_n(tb) ? q.k : q.n)) info = 10;
+        else if (q.ldc < imax(1, q.m)) info = 13;
+        if (info) {
+            set_error_msg("grouped sgemm: problem " + std::to_string(i) + " has invalid argument " +
+                          std::to_string(info));
+            return info;
+        }
+        if (q.m > 0 && q.n > 0 && (!is_device_pointer(q.c) ||
+                                    (q.k > 0 && (!is_device_pointer(q.a) || !is_device_pointer(q.b))))) {
+            set_error_msg("grouped sgemm: problem " + std::to_string(i) + " has a host pointer (device only)");
+            return MBG_ERR_UNSUPPORTED;
+        }
+    }
+    const int tile = tuning().grouped_gemm_tile == 128 ? 128 : 64;
+    std::vector<int> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const double cx = double(probs[x].m) * probs[x].n * imax(probs[x].k, 1);
+        const double cy = double(probs[y].m) * probs[y].n * imax(probs[y].k, 1);
+        return cx > cy;  // largest first: the tail of the schedule is short tiles
+    });
+    std::vector<GemmDesc> v;
+    v.reserve(count);
+    i64 tiles = 0;
+    for (int idx : order) {
+        const mbg_sgemm_problem& q = probs[idx];
+        if (q.m == 0 || q.n == 0) continue;
+        GemmDesc d{};
+        d.m = q.m; d.n = q.n; d.k = q.k; d.lda = q.lda; d.ldb = q.ldb; d.ldc = q.ldc;
+        d.a = q.a; d.b = q.b; d.c = q.c; d.alpha = q.alpha; d.beta = q.beta;
+        d.ta = is_t(q.trans_a); d.tb = is_t(q.trans_b);
+        d.tiles_m = int(cdiv(q.m, tile));
+        d.tile0 = tiles;
+        tiles += i64(d.tiles_m) * cdiv(q.n, tile);
+        v.push_back(d);
+    }
+    mbg_plan* p = new mbg_plan();
+    p->kind = 1;
+    p->count = int(v.size());
+    p->total = tiles;
+    p->tile = tile;
+    int per_sm = 1;
+    if (tile == 128)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<128>, GT_NT, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<64>, GT_NT, 0);
+    cudaGetLastError();
+    p->grid = int(imax(1, imin(tiles, i64(num_sms()) * imax(per_sm, 1))));
+    int st = MBG_OK;
+    if (p->count > 0) {
+        st = upload(p, v);
+        if (!st) {
+            if (cudaMalloc(&p->counter, sizeof(unsigned long long)) != cudaSuccess) {
+                set_error("cudaMalloc(grouped counter)", cudaGetLastError());
+                st = MBG_ERR_ALLOC;
+            }
+        }
+        if (!st) st = capture_plan(p);
+    }
+    if (st) {
+        mbg_plan_destroy(p);
+        return st;
+    }
+    *out = p;
+    return MBG_OK;
+}
+
+int mbg_strsm_grouped_plan(int mode, int count, const mbg_strsm_problem* probs, mbg_plan** out) {
+    if (!out) return MBG_ERR_INVALID_MODE;
+    *out = nullptr;
+    if (mode != MBG_MODE_PLAIN) {
+        set_error_msg("grouped strsm: only MBG_MODE_PLAIN is implemented");
+        return MBG_ERR_UNSUPPORTED;
+    }
+    if (count < 0 || (count > 0 && !probs)) return MBG_ERR_INVALID_MODE;
+    std::vector<TrsmDesc> v;
+    v.reserve(count);
+    i64 cols = 0;
+    for (int i = 0; i < count; ++i) {
+        const mbg_strsm_problem& q = probs[i];
+        int info = 0;  // numbered as trsm numbers them (src/level3/trsm.mojo:62-89)
+        if (!is_l(q.side) && !is_r(q.side)) info = 1;
+        else if (!is_u(q.uplo) && !is_l(q.uplo)) info = 2;
+        else if (!is_n(q.trans_a) && !is_t(q.trans_a)) info = 3;
+        else if (!is_u(q.diag) && !is_n(q.diag)) info = 4;
+        else if (q.m < 0) info = 5;
+        else if (q.n < 0) info = 6;
+        else if (q.lda < imax(1, is_l(q.side) ? q.m : q.n)) info = 9;
+        else if (q.ldb < imax(1, q.m)) info = 11;
+        if (info) {
+            set_error_msg("grouped strsm: problem " + std::to_string(i) + " has invalid argument " +
+                          std::to_string(info));
+            return info;
+        }
+        if (q.m > 0 && q.n > 0 && (!is_device_pointer(q.a) || !is_device_pointer(q.b))) {
+            set_error_msg("grouped strsm: problem " + std::to_string(i) + " has a host pointer (device only)");
+            return MBG_ERR_UNSUPPORTED;
+        }
+        if (is_r(q.side) || q.m > TR_MAXN) {
+            set_error_msg("grouped strsm: left side with m <= 256 only (problem " + std::to_string(i) + ")");
+            return MBG_ERR_UNSUPPORTED;
+        }
+        if (q.m == 0 || q.n == 0) continue;
+        TrsmDesc d{};
+        d.n = q.m; d.nrhs = q.n; d.lda = q.lda; d.ldb = q.ldb; d.a = q.a; d.b = q.b; d.alpha = q.alpha;
+        d.trans = is_t(q.trans_a);
+        d.lower = (!is_u(q.uplo)) != (d.trans != 0);
+        d.unit = is_u(q.diag);
+        d.col0 = cols;
+        cols += q.n;
+        v.push_back(d);
+    }
+    mbg_plan* p = new mbg_plan();
+    p->kind = 2;
+    p->count = int(v.size());
+    p->total = cols;
+    p->grid = int(imax(1, imin(cdiv(cols, 8), i64(num_sms()) * 8)));
+    int st = MBG_OK;
+    if (p->count > 0) {
+        st = upload(p, v);
+        if (!st) st = capture_plan(p);
+    }
+    if (st) {
+        mbg_plan_destroy(p);
+        return st;
+    }
+    *out = p;
+    return MBG_OK;
+}
+
+int mbg_plan_execute(mbg_plan* p) {
+    if (!p) return MBG_ERR_INVALID_MODE;
+    if (p->count == 0) return MBG_OK;
+    ProfScope prof(p->kind == 1 ? "grouped_sgemm" : "grouped_strsm");
+    MBG_CUDA(cudaGraphLaunch(p->exec, stream()));
+    count_launch(1);
+    return finish_call(false);
+}
+
+int mbg_plan_destroy(mbg_plan* p) {
+    if (!p) return MBG_OK;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->table) cudaFree(p->table);
+    if (p->counter) cudaFree(p->counter);
+    delete p;
+    return MBG_OK;
+}
+
+int mbg_sgemm_grouped(int mode, int count, const mbg_sgemm_problem* probs) {
+    mbg_plan* p = nullptr;
+    MBG_TRY(mbg_sgemm_grouped_plan(mode, count, probs, &p));
+    int st = mbg_plan_execute(p);
+    if (!st) st = finish_call(true);  // the plan's table is freed below
+    mbg_plan_destroy(p);
+    return st;
+}
+
+int mbg_strsm_grouped(int mode, int count, const mbg_strsm_problem* probs) {
+    mbg_plan* p = nullptr;
+    MBG_TRY(mbg_strsm_grouped_plan(mode, count, probs, &p));
+    int st = mbg_plan_execute(p);
+    if (!st) st = finish_call(true);
+    mbg_plan_destroy(p);
+    return st;
+}
+
+}  // extern "C"

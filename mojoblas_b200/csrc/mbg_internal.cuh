@@ -98,6 +98,7 @@ int finish_call(bool any_staged);  // synchronises when required, checks flag
 // ---- tuning table (defaults; mbg_set_tuning / mbg_load_tuning override) ------
 struct Tuning {
     i64 trsm_tc_min_k = 256;   // trsm off-diagonal updates with shorter k use the plain kernel
+    i64 grouped_gemm_tile = 64;  // tile edge of grouped sgemm plans (64 or 128)
 };
 Tuning& tuning();
 

@@ -7,6 +7,7 @@
 #include <mutex>
 #include <vector>
 #include <cstring>
+#include <cstdlib>
 
 namespace mbg {
 
@@ -312,15 +313,50 @@ int64_t mbg_launch_count(void) { return g_launches.load(); }
 int mbg_set_tuning(const char* key, int64_t value) {
     if (!key) return MBG_ERR_INVALID_MODE;
     const std::string k(key);
-    if (k == "trsm_tc_min_k") { tuning().trsm_tc_min_k = value; return MBG_OK; }
-    set_error_msg("unknown tuning key: " + k);
+    if (k == "trsm_tc_min_k" && value >= 0) { tuning().trsm_tc_min_k = value; return MBG_OK; }
+    if (k == "grouped_gemm_tile" && (value == 64 || value == 128)) { tuning().grouped_gemm_tile = value; return MBG_OK; }
+    set_error_msg("unknown tuning key or value: " + k + " = " + std::to_string(value));
     return MBG_ERR_INVALID_MODE;
 }
 
 int64_t mbg_get_tuning(const char* key) {
     const std::string k(key ? key : "");
     if (k == "trsm_tc_min_k") return tuning().trsm_tc_min_k;
+    if (k == "grouped_gemm_tile") return tuning().grouped_gemm_tile;
     return -1;
+}
+
+// Reads "key value" pairs: plain lines, or a flat JSON object {"key": value, ...}.
+int mbg_load_tuning(const char* path) {
+    FILE* f = path ? std::fopen(path, "r") : nullptr;
+    if (!f) {
+        set_error_msg(std::string("cannot open tuning file ") + (path ? path : "(null)"));
+        return MBG_ERR_INVALID_MODE;
+    }
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+    std::fclose(f);
+    for (char& ch : text)
+        if (ch == '{' || ch == '}' || ch == ',' || ch == ':' || ch == '"' || ch == '\n' || ch == '\r' || ch == '\t')
+            ch = ' ';
+    size_t pos = 0;
+    int applied = 0;
+    auto next = [&](std::string& tok) {
+        while (pos < text.size() && text[pos] == ' ') ++pos;
+        size_t st = pos;
+        while (pos < text.size() && text[pos] != ' ') ++pos;
+        tok = text.substr(st, pos - st);
+        return !tok.empty();
+    };
+    std::string key, val;
+    while (next(key) && next(val)) {
+        char* end = nullptr;
+        const long long v = std::strtoll(val.c_str(), &end, 10);
+        if (end && *end == '\0' && mbg_set_tuning(key.c_str(), v) == MBG_OK) ++applied;
+    }
+    return applied > 0 ? MBG_OK : MBG_ERR_INVALID_MODE;
 }
 
 int mbg_debug_fail_alloc(int nth) { g_fail_alloc_countdown = nth > 0 ? nth : 0; return MBG_OK; }
