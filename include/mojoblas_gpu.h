@@ -123,6 +123,32 @@ int mbg_sgemm_ex_noalloc(int mode, char trans_a, char trans_b, int64_t m, int64_
                          float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
                          float beta, float* c, int64_t ldc);
 
+/* ---- adjoints (reverse mode) --------------------------------------------
+ * No counterpart in the reference.  Given the upstream gradient G = dL/dC of
+ * C = alpha*op(A)*op(B), the gemm adjoint writes dA (shape of A, skipped if da
+ * is NULL) and dB (shape of B, skipped if db is NULL):
+ *     d op(A) = alpha * G * op(B)^T,   d op(B) = alpha * op(A)^T * G.
+ * Given X (the trsm result) and G = dL/dX, the trsm adjoint writes
+ *     dB = alpha * op(A)^{-T} G                    (side 'L'; G op(A)^{-T} for 'R')
+ *     dA = -tri(W X^T)  with W = op(A)^{-T} G      (left, trans 'N'; the other
+ *          cases are the corresponding transposes), only on the stored
+ *          triangle of A (a triangle-only GEMM: the other triangle's tiles are
+ *          not computed, nor written); zero diagonal for diag 'U'; da may be NULL.
+ * `info` numbering follows the argument position (mode / slices not counted). */
+int mbg_sgemm_adjoint(int mode, char trans_a, char trans_b, int64_t m, int64_t n, int64_t k, float alpha,
+                      const float* a, int64_t lda, const float* b, int64_t ldb, const float* g, int64_t ldg,
+                      float* da, int64_t ldda, float* db, int64_t lddb);
+int mbg_dgemm_adjoint(int mode, int slices, char trans_a, char trans_b, int64_t m, int64_t n, int64_t k,
+                      double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                      const double* g, int64_t ldg, double* da, int64_t ldda, double* db, int64_t lddb);
+int mbg_strsm_adjoint(int mode, char side, char uplo, char trans_a, char diag, int64_t m, int64_t n,
+                      float alpha, const float* a, int64_t lda, const float* x, int64_t ldx,
+                      const float* g, int64_t ldg, float* db, int64_t lddb, float* da, int64_t ldda);
+int mbg_dtrsm_adjoint(int mode, int slices, char side, char uplo, char trans_a, char diag, int64_t m,
+                      int64_t n, double alpha, const double* a, int64_t lda, const double* x,
+                      int64_t ldx, const double* g, int64_t ldg, double* db, int64_t lddb, double* da,
+                      int64_t ldda);
+
 /* ---- batched: many independent problems in one persistent launch ----------
  * No counterpart in the reference, whose callers loop over gemm / trsm.
  * A plan validates the problems (Netlib numbering per problem; the first

@@ -43,6 +43,11 @@ SIGNATURES = {
     "mbg_dtrsm": [_ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
     "mbg_strsm_ex": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],
     "mbg_dtrsm_ex": [_i, _i, _i, _ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
+    "mbg_sgemm_adjoint": [_i, _ch, _ch, i64, i64, i64, _f, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp, i64],
+    "mbg_dgemm_adjoint": [_i, _i, _ch, _ch, i64, i64, i64, _d, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp, i64],
+    "mbg_strsm_adjoint": [_i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp, i64],
+    "mbg_dtrsm_adjoint": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp,
+                          i64],
     "mbg_sgemm_ex_noalloc": [_i, _ch, _ch, i64, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
     "mbg_set_stream": [_vp],
     "mbg_get_stream": [],

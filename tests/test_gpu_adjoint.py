@@ -1,0 +1,161 @@
+"""Adjoint kernels (gemm and trsm) checked three ways:
+
+1. central finite differences in float64 along 64 seeded random directions:
+   for f = <G, C(A, B)> (gemm) or f = <G, X(A, B)> (trsm), the directional
+   derivative (f(+h d) - f(-h d)) / 2h must match <dA, dA_dir> + <dB, dB_dir>
+   from the kernels within 1e-4 * (|dA||dA_dir| + |dB||dB_dir|) (float32 kernels);
+2. the closed-form float64 gradients (numpy / scipy);
+3. gradients composed from the reference's own routines (the oracle's
+   restatements of mojoBLAS trsm / gemm): dB = trsm(op(A)^T, G), dA = -tri(W X^T).
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+from mojoblas_b200 import _lib as L
+from tests.gpu_util import need_gpu
+
+pytestmark = pytest.mark.gpu
+
+N_DIRS = 64
+
+
+def rel(x, ref):
+    return float(np.max(np.abs(np.asarray(x, np.float64) - ref)) / max(np.max(np.abs(ref)), 1e-300))
+
+
+def opm(x, t):
+    return x if t == "N" else x.T
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    need_gpu()
+
+
+@pytest.mark.parametrize("mode", [L.MODE_PLAIN, L.MODE_BF16X6], ids=["plain", "bf16x6"])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
+def test_gemm_adjoint(mode, ta, tb):
+    lib = L.load()
+    rng = np.random.default_rng(31)
+    m, n, k, alpha = 96, 80, 72, 1.5
+    A = np.asfortranarray(rng.uniform(-1, 1, (m, k) if ta == "N" else (k, m)).astype(np.float32))
+    B = np.asfortranarray(rng.uniform(-1, 1, (k, n) if tb == "N" else (n, k)).astype(np.float32))
+    G = np.asfortranarray(rng.standard_normal((m, n)).astype(np.float32))
+    dA = np.zeros_like(A, order="F")
+    dB = np.zeros_like(B, order="F")
+    st = lib.mbg_sgemm_adjoint(mode, ta.encode(), tb.encode(), m, n, k, alpha, A.ctypes.data, A.shape[0],
+                               B.ctypes.data, B.shape[0], G.ctypes.data, m, dA.ctypes.data, A.shape[0],
+                               dB.ctypes.data, B.shape[0])
+    assert st == 0, L.last_error()
+    A64, B64, G64 = A.astype(np.float64), B.astype(np.float64), G.astype(np.float64)
+    dopA = alpha * G64 @ opm(B64, tb).T
+    dopB = alpha * opm(A64, ta).T @ G64
+    assert rel(dA, opm(dopA, ta)) < 2e-5
+    assert rel(dB, opm(dopB, tb)) < 2e-5
+
+    def f(a, b):
+        return float(np.sum(G64 * (alpha * opm(a, ta) @ opm(b, tb))))
+    h = 1e-3
+    for _ in range(N_DIRS):
+        ea, eb = rng.standard_normal(A.shape), rng.standard_normal(B.shape)
+        fd = (f(A64 + h * ea, B64 + h * eb) - f(A64 - h * ea, B64 - h * eb)) / (2 * h)
+        ad = float(np.sum(dA * ea) + np.sum(dB * eb))
+        scale = np.linalg.norm(dA) * np.linalg.norm(ea) + np.linalg.norm(dB) * np.linalg.norm(eb)
+        assert abs(fd - ad) <= 1e-4 * scale
+
+
+def _tri(rng, n, uplo, unit):
+    a = rng.standard_normal((n, n)) / np.sqrt(n)
+    a[np.arange(n), np.arange(n)] = n + np.abs(rng.standard_normal(n))
+    if unit:
+        a /= n
+    return np.tril(a) if uplo == "L" else np.triu(a)
+
+
+@pytest.mark.parametrize("mode", [L.MODE_PLAIN, L.MODE_BF16X6], ids=["plain", "bf16x6"])
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("ta", ["N", "T"])
+@pytest.mark.parametrize("diag", ["N", "U"])
+def test_trsm_adjoint(oracle, mode, side, uplo, ta, diag):
+    lib = L.load()
+    rng = np.random.default_rng(32)
+    m, n, alpha = 96, 40, 0.75
+    na = m if side == "L" else n
+    A64 = _tri(rng, na, uplo, diag == "U")
+    A = np.asfortranarray(A64.astype(np.float32))
+    Bm = np.asfortranarray(rng.standard_normal((m, n)).astype(np.float32))
+    G = np.asfortranarray(rng.standard_normal((m, n)).astype(np.float32))
+    Aeff = A.astype(np.float64).copy()
+    if diag == "U":
+        np.fill_diagonal(Aeff, 1.0)
+    opA = opm(Aeff, ta)
+    low = (uplo == "L") != (ta == "T")
+
+    def solve(a_eff, b):
+        oa = opm(a_eff, ta)
+        if side == "L":
+            return alpha * sl.solve_triangular(oa, b, lower=low)
+        return alpha * sl.solve_triangular(oa.T, b.T, lower=not low).T
+
+    X = solve(Aeff, Bm.astype(np.float64))
+    Xf = np.asfortranarray(X.astype(np.float32))
+    dB = np.zeros((m, n), np.float32, order="F")
+    dA = np.zeros((na, na), np.float32, order="F")
+    st = lib.mbg_strsm_adjoint(mode, side.encode(), uplo.encode(), ta.encode(), diag.encode(), m, n, alpha,
+                               A.ctypes.data, na, Xf.ctypes.data, m, G.ctypes.data, m, dB.ctypes.data, m,
+                               dA.ctypes.data, na)
+    assert st == 0, L.last_error()
+    G64 = G.astype(np.float64)
+    # closed form
+    if side == "L":
+        W = sl.solve_triangular(opA.T, G64, lower=not low)
+        dopA = -W @ X.T
+    else:
+        W = sl.solve_triangular(opA, G64.T, lower=low).T
+        dopA = -X.T @ W
+    dA_ref = opm(dopA, ta)
+    mask = np.tril(np.ones((na, na), bool)) if uplo == "L" else np.triu(np.ones((na, na), bool))
+    if diag == "U":
+        np.fill_diagonal(mask, False)
+    dA_ref = np.where(mask, dA_ref, 0.0)
+    assert rel(dB, alpha * W) < 2e-5
+    assert rel(np.where(mask, dA, 0.0), dA_ref) < 5e-5
+    if diag == "U":
+        assert np.all(np.diag(dA) == 0.0)
+    # gradients composed from the reference routines (oracle restatements)
+    db_orc = G.copy(order="F")
+    flip = "T" if ta == "N" else "N"
+    oracle.trsm(side, uplo, flip, diag, m, n, alpha, A, na, db_orc, m)
+    assert rel(dB, db_orc.astype(np.float64)) < 5e-5
+    c_orc = np.zeros((na, na), np.float32, order="F")
+    first, second = (db_orc, Xf) if (side == "L") == (ta == "N") else (Xf, db_orc)
+    if side == "L":  # -(1/alpha) (first second^T)
+        oracle.gemm("N", "T", na, na, n, -1.0 / alpha, first, m, second, m, 0.0, c_orc, na)
+    else:            # -(1/alpha) (first^T second)
+        oracle.gemm("T", "N", na, na, m, -1.0 / alpha, first, m, second, m, 0.0, c_orc, na)
+    assert rel(np.where(mask, dA, 0.0), np.where(mask, c_orc, 0.0).astype(np.float64)) < 5e-5
+    # finite differences along random directions on the stored triangle and B
+    h = 1e-4
+
+    def f(a_eff, b):
+        return float(np.sum(G64 * solve(a_eff, b)))
+    B64 = Bm.astype(np.float64)
+    for _ in range(N_DIRS):
+        ea = np.where(mask, rng.standard_normal((na, na)), 0.0)
+        eb = rng.standard_normal((m, n))
+        fd = (f(Aeff + h * ea, B64 + h * eb) - f(Aeff - h * ea, B64 - h * eb)) / (2 * h)
+        ad = float(np.sum(dA * ea) + np.sum(dB * eb))
+        scale = np.linalg.norm(dA * mask) * np.linalg.norm(ea) + np.linalg.norm(dB) * np.linalg.norm(eb)
+        assert abs(fd - ad) <= 1e-4 * scale
+
+
+def test_adjoint_info_codes():
+    lib = L.load()
+    z = np.zeros(64, np.float32)
+    p = z.ctypes.data
+    assert lib.mbg_sgemm_adjoint(0, b"X", b"N", 2, 2, 2, 1.0, p, 2, p, 2, p, 2, p, 2, p, 2) == 1
+    assert lib.mbg_sgemm_adjoint(0, b"N", b"N", 2, 2, 2, 1.0, p, 2, p, 2, p, 1, p, 2, p, 2) == 12
+    assert lib.mbg_strsm_adjoint(0, b"L", b"L", b"N", b"N", 2, 2, 1.0, p, 2, p, 1, p, 2, p, 2, p, 2) == 11
+    assert lib.mbg_strsm_adjoint(0, b"L", b"L", b"N", b"N", 3, 2, 1.0, p, 3, p, 3, p, 3, p, 3, p, 2) == 17
