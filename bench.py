@@ -311,6 +311,121 @@ def run_cfg4(torch, lib, L, stream):
     return out
 
 
+def run_cfg5(torch, lib, L, stream):
+    """Adjoints at the configuration-5 sizes, float32 kernels: trsm with L 2048^2
+    lower and diagonally dominant, B 2048 x 512 N(0,1), X = L^-1 B, G N(0,1)
+    (dB = L^-T G, dL = -tril(dB X^T)); gemm C = A B, A 3072 x 1024, B 1024 x 2048
+    uniform[-1,1) (dA = G B^T, dB = A^T G).  Checked by central finite differences
+    in float64 along 64 random directions, the function evaluated with the
+    library's plain FP64 kernels."""
+    out = {}
+    g = torch.Generator(device="cuda")
+    g.manual_seed(55)
+    n, r = 2048, 512
+    Ld = torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64) / np.sqrt(n)
+    Ld.diagonal().copy_(n + torch.randn(n, generator=g, device="cuda", dtype=torch.float64).abs())
+    Ld = torch.tril(Ld.T).T.contiguous()  # column-major lower triangle (row-major upper storage)
+    Bd = torch.randn((r, n), generator=g, device="cuda", dtype=torch.float64)
+    Gd = torch.randn((r, n), generator=g, device="cuda", dtype=torch.float64)
+    Lf, Bf, Gf = Ld.float(), Bd.float(), Gd.float()
+    Xd = Bd.clone()
+    lib.mbg_dtrsm(b"L", b"L", b"N", b"N", n, r, 1.0, Ld.data_ptr(), n, Xd.data_ptr(), n)
+    Xf = Xd.float()
+
+    def f(Lp, Bp):  # <G, L^-1 B> in float64 with the plain FP64 trsm
+        Y = Bp.clone()
+        lib.mbg_dtrsm(b"L", b"L", b"N", b"N", n, r, 1.0, Lp.data_ptr(), n, Y.data_ptr(), n)
+        return float((Gd * Y).sum())
+
+    lower = torch.tril(torch.ones((n, n), device="cuda", dtype=torch.float64)).T  # storage mask
+    res = {}
+    for label, md in (("plain", L.MODE_PLAIN), ("bf16x6", L.MODE_BF16X6)):
+        dB = torch.zeros_like(Bf)
+        dL = torch.zeros_like(Lf)
+
+        def call():
+            st = lib.mbg_strsm_adjoint(md, b"L", b"L", b"N", b"N", n, r, 1.0, Lf.data_ptr(), n, Xf.data_ptr(), n,
+                                       Gf.data_ptr(), n, dB.data_ptr(), n, dL.data_ptr(), n)
+            if st:
+                raise RuntimeError(f"strsm_adjoint {st}: {L.last_error()}")
+        call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(5):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        gg = torch.Generator(device="cuda")
+        gg.manual_seed(7)
+        worst = worst_fd = 0.0
+        h = 1e-4
+        for _ in range(64):
+            eL = torch.randn((n, n), generator=gg, device="cuda", dtype=torch.float64) * lower
+            eB = torch.randn((r, n), generator=gg, device="cuda", dtype=torch.float64)
+            fd = (f(Ld + h * eL, Bd + h * eB) - f(Ld - h * eL, Bd - h * eB)) / (2 * h)
+            ad = float((dL.double() * eL).sum() + (dB.double() * eB).sum())
+            scale = float((dL.double() * lower).norm() * eL.norm() + dB.double().norm() * eB.norm())
+            worst = max(worst, abs(fd - ad) / scale)
+            worst_fd = max(worst_fd, abs(fd - ad) / max(abs(fd), 1e-300))
+        flops = 2.0 * n * n * r  # dB: n^2 r, masked dL: n^2 r
+        res[label] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2),
+                      "fd_max_rel_discrepancy_64_dirs": worst, "fd_max_rel_to_fd_64_dirs": worst_fd}
+    out["strsm_adjoint_2048x512"] = res
+    del Ld, Bd, Gd, Lf, Bf, Gf, Xd, Xf, lower
+
+    m, k, nn = 3072, 1024, 2048
+    Ad = torch.rand((k, m), generator=g, device="cuda", dtype=torch.float64) * 2 - 1  # column-major m x k
+    Bd = torch.rand((nn, k), generator=g, device="cuda", dtype=torch.float64) * 2 - 1  # column-major k x nn
+    Gd = torch.randn((nn, m), generator=g, device="cuda", dtype=torch.float64)
+    Af, Bf, Gf = Ad.float(), Bd.float(), Gd.float()
+    Cd = torch.empty_like(Gd)
+
+    def fg(Ap, Bp):
+        lib.mbg_dgemm(b"N", b"N", m, nn, k, 1.0, Ap.data_ptr(), m, Bp.data_ptr(), k, 0.0, Cd.data_ptr(), m)
+        return float((Gd * Cd).sum())
+
+    res = {}
+    for label, md in (("plain", L.MODE_PLAIN), ("bf16x6", L.MODE_BF16X6)):
+        dA = torch.zeros_like(Af)
+        dB = torch.zeros_like(Bf)
+
+        def call():
+            st = lib.mbg_sgemm_adjoint(md, b"N", b"N", m, nn, k, 1.0, Af.data_ptr(), m, Bf.data_ptr(), k,
+                                       Gf.data_ptr(), m, dA.data_ptr(), m, dB.data_ptr(), k)
+            if st:
+                raise RuntimeError(f"sgemm_adjoint {st}: {L.last_error()}")
+        call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(5):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        gg = torch.Generator(device="cuda")
+        gg.manual_seed(8)
+        worst = worst_fd = 0.0
+        h = 1e-3
+        for _ in range(64):
+            eA = torch.randn(Ad.shape, generator=gg, device="cuda", dtype=torch.float64)
+            eB = torch.randn(Bd.shape, generator=gg, device="cuda", dtype=torch.float64)
+            fd = (fg(Ad + h * eA, Bd + h * eB) - fg(Ad - h * eA, Bd - h * eB)) / (2 * h)
+            ad = float((dA.double() * eA).sum() + (dB.double() * eB).sum())
+            scale = float(dA.double().norm() * eA.norm() + dB.double().norm() * eB.norm())
+            worst = max(worst, abs(fd - ad) / scale)
+            worst_fd = max(worst_fd, abs(fd - ad) / max(abs(fd), 1e-300))
+        flops = 2.0 * (2.0 * m * nn * k)
+        res[label] = {"ms": round(ms, 3), "tflops": round(flops / ms / 1e9, 2),
+                      "fd_max_rel_discrepancy_64_dirs": worst, "fd_max_rel_to_fd_64_dirs": worst_fd}
+    out["sgemm_adjoint_3072x1024x2048"] = res
+    out["note"] = ("discrepancy = |FD - <grad, dir>| / (|grad| |dir|), FD in float64 with the plain FP64 kernels; "
+                   "trsm flops 2 n^2 nrhs (dB + triangle-only dL), gemm 2 x 2mnk")
+    return out
+
+
 def run_ours(args, rank, world, dist):
     import torch
     import mojoblas_b200 as mb
@@ -448,9 +563,33 @@ def run_ours(args, rank, world, dist):
                          "fp64_err": rows_error(Cd, refd, rsd)}
         del Ad, Bd, Cd
 
+    # ---- context: the vendor library's plain FP32 / FP64 GEMM on the same sizes ----
+    ctx = {}
+    if not args.skip_context:
+        prev = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = False  # true FP32 arithmetic
+        for label, dtype, nn, flops in (("torch_matmul_fp32_8192", torch.float32, N_S, FLOPS_S),
+                                        ("torch_matmul_fp64_4096", torch.float64, N_D, FLOPS_D)):
+            xa = torch.rand((nn, nn), device="cuda", dtype=dtype)
+            xb = torch.rand((nn, nn), device="cuda", dtype=dtype)
+            for _ in range(2):
+                torch.matmul(xa, xb)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(3):
+                torch.matmul(xa, xb)
+            e1.record()
+            torch.cuda.synchronize()
+            tms = e0.elapsed_time(e1) / 3
+            ctx[label] = {"tflops": round(flops / (tms * 1e-3) / 1e12, 2), "ms": round(tms, 3)}
+            del xa, xb
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
     # ---- configuration 3: blocked dtrsm 4096^2 and ssyrk 8192 x 2048 ----
     cfg3 = {} if args.skip_cfg3 else run_cfg3(torch, lib, L, stream)
     cfg4 = {} if args.skip_cfg4 else run_cfg4(torch, lib, L, stream)
+    cfg5 = {} if args.skip_cfg5 else run_cfg5(torch, lib, L, stream)
 
     # ---- e2e through the C ABI with pinned host buffers ----
     hA = A.cpu().pin_memory()
@@ -507,8 +646,10 @@ def run_ours(args, rank, world, dist):
         "fp64_oracle_error": errs,
         "error_metric": f"max|C-C64|/max|C64| over {SAMPLE_ROWS} sampled rows, C64 = float64 numpy",
         "dgemm_4096": dg,
+        "context_vendor_plain_gemm": ctx,
         "cfg3": cfg3,
         "cfg4_batched": cfg4,
+        "cfg5_adjoints": cfg5,
         "e2e": {"value": round(e2e_value, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_out, "ms_per_step": round(e2e_ms, 2)},
         "gpu_launches": launches,
@@ -561,6 +702,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-cfg3", action="store_true")
     ap.add_argument("--skip-cfg4", action="store_true")
+    ap.add_argument("--skip-cfg5", action="store_true")
+    ap.add_argument("--skip-context", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

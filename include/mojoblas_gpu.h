@@ -207,7 +207,8 @@ int   mbg_release_workspace(void);
 /* ---- tuning table -------------------------------------------------------
  * Keys: "trsm_tc_min_k" — trsm off-diagonal updates with a shorter reduction
  * run on the plain kernel instead of the split / Ozaki forms (default 256);
- * "grouped_gemm_tile" — 64 or 128, tile edge of grouped sgemm plans (default 64).
+ * "grouped_gemm_tile" — 64 or 128, tile edge of grouped sgemm plans (default 64);
+ * "trsm_leaf_ctas" — CTA cap of the trsm diagonal-block solve (0 = 8 per SM).
  * mbg_load_tuning reads "key value" lines (or a flat JSON object of them) as
  * written by the autotuner (mojoblas_b200/autotune.py).
  * mbg_get_tuning returns -1 for an unknown key. */
@@ -227,6 +228,10 @@ int64_t mbg_launch_count(void);
 /* ---- test hooks ----------------------------------------------------------- */
 /* Make the n-th device allocation from now on fail (n >= 1); 0 disables. */
 int mbg_debug_fail_alloc(int nth);
+/* Launch one kernel whose bounded mbarrier wait can never be satisfied and
+ * gives up after limit_ns (at most 5 s): returns MBG_ERR_TIMEOUT with the
+ * context still usable — the failure path of every tcgen05 kernel's waits. */
+int mbg_debug_wait_probe(int64_t limit_ns);
 
 #ifdef __cplusplus
 }

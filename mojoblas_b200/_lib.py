@@ -62,6 +62,7 @@ SIGNATURES = {
     "mbg_prof_query": [C.c_char_p, C.POINTER(_d), C.POINTER(i64)],
     "mbg_launch_count": [],
     "mbg_debug_fail_alloc": [_i],
+    "mbg_debug_wait_probe": [i64],
     "mbg_set_tuning": [C.c_char_p, i64],
     "mbg_get_tuning": [C.c_char_p],
     "mbg_load_tuning": [C.c_char_p],

@@ -21,9 +21,16 @@ namespace {
 
 constexpr int BK = 8, NT = 256;
 
+// Shared-tile row padding: with 8-byte elements a pad of 4 spreads the k-major
+// stores of eight consecutive k rows over distinct bank pairs.
 template <typename T> struct Pad;
 template <> struct Pad<float> { static constexpr int v = 4; };
-template <> struct Pad<double> { static constexpr int v = 2; };
+template <> struct Pad<double> { static constexpr int v = 4; };
+
+// Resident CTAs per SM the register budget is sized for: the fp32 128-tile
+// fits two (128 registers), the fp64 one needs 240+ registers and keeps one.
+template <typename T, int TILE> struct MinBlocks { static constexpr int v = TILE == 128 ? 1 : 2; };
+template <> struct MinBlocks<float, 128> { static constexpr int v = 2; };
 
 template <typename T>
 __device__ __forceinline__ void lds4(const T* p, T (&o)[4]);
@@ -52,7 +59,7 @@ __device__ __forceinline__ void tri_tile(i64 t, i64& ti, i64& tj) {
 // 64+tx*4+{0..3}); TILE = 64: 64 x 64 tile, 4 x 4 per thread (rows tx*4+{0..3}),
 // four times as many CTAs for launches that would not fill the GPU.
 template <typename T, bool TA, bool TB, int TRI, int TILE>
-__global__ void __launch_bounds__(NT, TILE == 128 ? 1 : 2)
+__global__ void __launch_bounds__(NT, MinBlocks<T, TILE>::v)
 gemm_simt_kernel(i64 m, i64 n, i64 k, T alpha, const T* __restrict__ A, i64 lda,
                  const T* __restrict__ B, i64 ldb, T beta, T* __restrict__ C, i64 ldc) {
     constexpr int BM = TILE, BN = TILE;

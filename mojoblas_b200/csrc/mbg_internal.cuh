@@ -99,6 +99,7 @@ int finish_call(bool any_staged);  // synchronises when required, checks flag
 struct Tuning {
     i64 trsm_tc_min_k = 256;   // trsm off-diagonal updates with shorter k use the plain kernel
     i64 grouped_gemm_tile = 64;  // tile edge of grouped sgemm plans (64 or 128)
+    i64 trsm_leaf_ctas = 0;      // CTA cap of the trsm diagonal-block solve (0: 8 per SM)
 };
 Tuning& tuning();
 

@@ -315,6 +315,7 @@ int mbg_set_tuning(const char* key, int64_t value) {
     const std::string k(key);
     if (k == "trsm_tc_min_k" && value >= 0) { tuning().trsm_tc_min_k = value; return MBG_OK; }
     if (k == "grouped_gemm_tile" && (value == 64 || value == 128)) { tuning().grouped_gemm_tile = value; return MBG_OK; }
+    if (k == "trsm_leaf_ctas" && value >= 0) { tuning().trsm_leaf_ctas = value; return MBG_OK; }
     set_error_msg("unknown tuning key or value: " + k + " = " + std::to_string(value));
     return MBG_ERR_INVALID_MODE;
 }
@@ -323,6 +324,7 @@ int64_t mbg_get_tuning(const char* key) {
     const std::string k(key ? key : "");
     if (k == "trsm_tc_min_k") return tuning().trsm_tc_min_k;
     if (k == "grouped_gemm_tile") return tuning().grouped_gemm_tile;
+    if (k == "trsm_leaf_ctas") return tuning().trsm_leaf_ctas;
     return -1;
 }
 

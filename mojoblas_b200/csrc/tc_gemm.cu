@@ -80,14 +80,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int site) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int site,
+                                          uint64_t limit_ns = WAIT_LIMIT_NS) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     while (true) {
 #pragma unroll 1
         for (int i = 0; i < 256; ++i)
             if (mbar_try_wait(bar, parity)) return true;
-        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+        if (globaltimer() - t0 > limit_ns) {
             if (err) {
                 atomicExch(err, 1);
                 atomicExch(err + 1, site);
@@ -1150,4 +1151,32 @@ extern "C" int mbg_sgemm_ex_noalloc(int mode, char ta, char tb, int64_t m, int64
         }
     }
     return MBG_OK;
+}
+
+// ---- bounded-wait probe ---------------------------------------------------------
+// Exercises the failure path of the kernels' bounded waits without faulting the
+// GPU: one thread waits on an mbarrier phase that nothing completes, gives up
+// after limit_ns, records the error code and returns.
+namespace mbg {
+namespace tc {
+__global__ void wait_probe_kernel(int* err, unsigned long long limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+        mbar_wait(&bar, 0, err, 99, limit_ns);  // no arrival ever comes
+    }
+}
+}  // namespace tc
+}  // namespace mbg
+
+extern "C" int mbg_debug_wait_probe(int64_t limit_ns) {
+    using namespace mbg;
+    if (limit_ns <= 0 || limit_ns > 5000000000LL) return MBG_ERR_INVALID_MODE;
+    int* err = device_error_flag();
+    if (!err) return MBG_ERR_CUDA;
+    tc::wait_probe_kernel<<<1, 32, 0, stream()>>>(err, (unsigned long long)limit_ns);
+    MBG_TRY(check_launch("wait_probe"));
+    MBG_CUDA(cudaStreamSynchronize(stream()));
+    return read_and_clear_device_error() ? MBG_ERR_TIMEOUT : MBG_OK;
 }

@@ -45,14 +45,14 @@ __global__ void __launch_bounds__(DS_WARPS * 32)
 diag_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __restrict__ B, i64 ldb) {
     __shared__ T Ls[NB * (NB + 1)];
     __shared__ T inv[NB];
-    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-        int i, l;
-        if (TRANS) { l = e % nb; i = e / nb; } else { i = e % nb; l = e / nb; }  // coalesced reads
-        const bool in_tri = LOWER ? (i >= l) : (i <= l);
-        T v = T(0);
-        if (in_tri && !(UNIT && i == l)) v = TRANS ? A[l + (i64)i * lda] : A[i + (i64)l * lda];
-        if (UNIT && i == l) v = T(1);
-        Ls[l * (NB + 1) + i] = v;
+    // stage the whole nb x nb block (compile-time 64 x 64 indexing, coalesced,
+    // no per-element branches): entries of the other triangle are copied but
+    // never read, since the substitution only touches i > l (i < l) below
+#pragma unroll 4
+    for (int e = threadIdx.x; e < NB * NB; e += DS_WARPS * 32) {
+        const int fast = e & (NB - 1), slow = e >> 6;  // fast index runs along contiguous memory
+        const int i = TRANS ? slow : fast, l = TRANS ? fast : slow;
+        if (i < nb && l < nb) Ls[l * (NB + 1) + i] = TRANS ? A[l + (i64)i * lda] : A[i + (i64)l * lda];
     }
     __syncthreads();
     for (int l = threadIdx.x; l < nb; l += blockDim.x) inv[l] = UNIT ? T(1) : T(1) / Ls[l * (NB + 1) + l];
@@ -147,7 +147,10 @@ __global__ void copy_scale_kernel(i64 m, i64 n, T alpha, const T* __restrict__ x
             y[i + j * ldy] = alpha * x[i + j * ldx];
 }
 
-unsigned ds_grid(i64 ncols) { return (unsigned)imin(cdiv(ncols, DS_WARPS), 148 * 8); }
+unsigned ds_grid(i64 ncols) {
+    const i64 cap = tuning().trsm_leaf_ctas > 0 ? tuning().trsm_leaf_ctas : 148 * 8;
+    return (unsigned)imax(1, imin(cdiv(ncols, DS_WARPS), cap));
+}
 
 template <typename T>
 int launch_diag_solve(bool lower, bool trans, bool unit, int nb, i64 n, const T* a, i64 lda, T* b, i64 ldb) {

@@ -20,7 +20,8 @@ sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--op", choices=["sgemm", "dgemm", "ssyrk", "dtrsm", "strsm"], default="sgemm")
+    ap.add_argument("--op", choices=["sgemm", "dgemm", "ssyrk", "dtrsm", "strsm", "grouped_sgemm", "grouped_strsm"],
+                    default="sgemm")
     ap.add_argument("--mode", choices=["plain", "bf16x3", "bf16x6", "ozaki"], default="bf16x6")
     ap.add_argument("--slices", type=int, default=8)
     ap.add_argument("--refine", type=int, default=0)
@@ -46,7 +47,39 @@ def main():
     def cm(rows, cols):  # column-major rows x cols
         return torch.rand((cols, rows), generator=g, device="cuda", dtype=dt) * 2 - 1
 
-    if a.op in ("sgemm", "dgemm"):
+    if a.op == "grouped_sgemm":  # 4096 problems, m, n, k log-uniform 16..512
+        from mojoblas_b200.autotune import sgemm_batch
+        buf, probs, _, _ = sgemm_batch(torch, L, 4096, seed=41)
+        plan = C.c_void_p()
+        assert lib.mbg_sgemm_grouped_plan(L.MODE_PLAIN, len(probs), probs, C.byref(plan)) == 0, L.last_error()
+
+        def call():
+            return lib.mbg_plan_execute(plan)
+    elif a.op == "grouped_strsm":  # 2048 lower solves, n log-uniform 8..256, nrhs 1..64
+        import numpy as np
+        from mojoblas_b200.autotune import log_uniform
+        rng = np.random.default_rng(42)
+        ns, rh = log_uniform(rng, 8, 256, 2048), rng.integers(1, 65, 2048)
+        sizes = [int(x * x) for x in ns] + [int(x * y) for x, y in zip(ns, rh)]
+        tot = sum((v + 63) // 64 * 64 for v in sizes)
+        buf = torch.randn(tot, generator=g, device="cuda") * 0.01
+        probs = (L.StrsmProblem * 2048)()
+        off = 0
+        base = buf.data_ptr()
+        for i in range(2048):
+            ai = off
+            off += (int(ns[i] * ns[i]) + 63) // 64 * 64
+            bi = off
+            off += (int(ns[i] * rh[i]) + 63) // 64 * 64
+            buf[ai:ai + int(ns[i] * ns[i]):int(ns[i]) + 1] = float(ns[i])  # dominant diagonal
+            probs[i] = L.StrsmProblem(b"L", b"L", b"N", b"N", int(ns[i]), int(rh[i]), 1.0, base + 4 * ai,
+                                      int(ns[i]), base + 4 * bi, int(ns[i]))
+        plan = C.c_void_p()
+        assert lib.mbg_strsm_grouped_plan(L.MODE_PLAIN, 2048, probs, C.byref(plan)) == 0, L.last_error()
+
+        def call():
+            return lib.mbg_plan_execute(plan)
+    elif a.op in ("sgemm", "dgemm"):
         lda = a.m if a.ta == "N" else a.k
         ldb = a.k if a.tb == "N" else a.n
         A, B, Cm = cm(lda, a.k if a.ta == "N" else a.m), cm(ldb, a.n if a.tb == "N" else a.k), cm(a.m, a.n)

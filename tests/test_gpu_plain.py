@@ -223,3 +223,16 @@ def test_workspace_allocation_failure_is_reported():
         lib.mbg_debug_fail_alloc(0)
     assert mb.gemm("N", "N", 64, 64, 64, 1.0, a, 64, a, 64, 0.0, c, 64) == 0
     assert np.all(c == 64.0)
+
+
+def test_bounded_wait_expires_and_context_survives():
+    """A kernel wait that can never be satisfied gives up after its limit (50 ms
+    here), reports MBG_ERR_TIMEOUT, and the library keeps working afterwards."""
+    from mojoblas_b200 import _lib as L
+    lib = L.load()
+    assert lib.mbg_debug_wait_probe(50_000_000) == L.MBG_ERR_TIMEOUT
+    assert "bounded wait expired" in L.last_error()
+    a = np.ones((32, 32), np.float32, order="F")
+    c = np.zeros((32, 32), np.float32, order="F")
+    assert mb.gemm("N", "N", 32, 32, 32, 1.0, a, 32, a, 32, 0.0, c, 32, mode=mb.BF16X6) == 0
+    assert np.all(c == 32.0)
