@@ -113,6 +113,17 @@ def col_major(torch, rows, cols, gen, dtype, device):
     return t.mul_(2).sub_(1)
 
 
+def max_over_ranks(value: float, dist, device="cpu") -> float:
+    """The slowest rank's time: every rank contributes its own measurement and all
+    receive the maximum (all_reduce MAX; NCCL on GPUs, gloo in the CPU tests)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def ref_rows(ta, tb, a, b, rows):
     """float64 oracle rows of C = op(A) op(B) (a, b: column-major torch tensors)."""
     A = a.double().cpu().numpy().T  # A[i, l]
@@ -476,11 +487,7 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize()
         window[1] = time.time()
         launches = int(lib.mbg_launch_count())
-        ms = e0.elapsed_time(e1) / steps
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, dist, "cuda")
         return ms, launches
 
     # ---- headline: split-precision sgemm ----
@@ -561,7 +568,28 @@ def run_ours(args, rank, world, dist):
             dms = e0.elapsed_time(e1) / reps
             dg[label] = {"tflops": round(FLOPS_D / (dms * 1e-3) / 1e12, 2), "ms": round(dms, 3),
                          "fp64_err": rows_error(Cd, refd, rsd)}
+            if md == L.MODE_OZAKI:  # kernel-only time (CUDA events around the tcgen05 launch)
+                lib.mbg_prof_enable(1)
+                lib.mbg_prof_reset()
+                dcall(md, s)
+                torch.cuda.synchronize()
+                tot, cnt = C.c_double(), C.c_int64()
+                lib.mbg_prof_query(b"tc_gemm_ozaki", C.byref(tot), C.byref(cnt))
+                lib.mbg_prof_enable(0)
+                dg[label]["kernel_ms"] = round(tot.value / max(cnt.value, 1), 3)
         del Ad, Bd, Cd
+
+    # ---- own peak probes (FMA loops, back-to-back tcgen05.mma) ----
+    pv = [C.c_double() for _ in range(4)]
+    probes = {}
+    if lib.mbg_probe_peaks(*[C.byref(x) for x in pv]) == 0:
+        probes = {"fp32_fma_tflops": round(pv[0].value, 1), "fp64_fma_tflops": round(pv[1].value, 1),
+                  "bf16_mma_tflops": round(pv[2].value, 1), "int8_mma_tops": round(pv[3].value, 1)}
+        probes["plain_fp32_frac"] = round(plain_tflops / pv[0].value, 3)
+        if dg:
+            probes["plain_fp64_frac"] = round(dg["plain_fp64"]["tflops"] / pv[1].value, 3)
+            probes["ozaki_s8_int8_frac"] = round(36 * FLOPS_D / (dg["ozaki_s8"]["kernel_ms"] * 1e-3) / 1e12
+                                                 / pv[3].value, 3) if dg["ozaki_s8"].get("kernel_ms") else None
 
     # ---- context: the vendor library's plain FP32 / FP64 GEMM on the same sizes ----
     ctx = {}
@@ -612,11 +640,7 @@ def run_ours(args, rank, world, dist):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, dist, "cuda")
     lib.mbg_set_sync(0)
     e2e_value = world * 2 * FLOPS_S / (e2e_ms * 1e-3) / 1e12
     bytes_in = 2 * 2 * N_S * N_S * 4  # A and B per call, two calls
@@ -647,6 +671,7 @@ def run_ours(args, rank, world, dist):
         "error_metric": f"max|C-C64|/max|C64| over {SAMPLE_ROWS} sampled rows, C64 = float64 numpy",
         "dgemm_4096": dg,
         "context_vendor_plain_gemm": ctx,
+        "probe_peaks": probes,
         "cfg3": cfg3,
         "cfg4_batched": cfg4,
         "cfg5_adjoints": cfg5,

@@ -216,6 +216,13 @@ int     mbg_set_tuning(const char* key, int64_t value);
 int64_t mbg_get_tuning(const char* key);
 int     mbg_load_tuning(const char* path);
 
+/* ---- peak probes ----------------------------------------------------------
+ * Measured throughput (TFLOP/s, dense, 2 ops per multiply-add) of fp32 and fp64
+ * FMA loops on the CUDA cores and of back-to-back tcgen05.mma kind::f16 (bf16)
+ * and kind::i8 on one CTA per SM: the roofline denominators of the plain and
+ * Ozaki kernels.  Any output pointer may be NULL. */
+int mbg_probe_peaks(double* fp32_tflops, double* fp64_tflops, double* bf16_tflops, double* int8_tops);
+
 /* ---- kernel timing (CUDA events around each library kernel launch) ------ */
 int mbg_prof_enable(int on);
 int mbg_prof_reset(void);

@@ -63,6 +63,7 @@ SIGNATURES = {
     "mbg_launch_count": [],
     "mbg_debug_fail_alloc": [_i],
     "mbg_debug_wait_probe": [i64],
+    "mbg_probe_peaks": [C.POINTER(_d)] * 4,
     "mbg_set_tuning": [C.c_char_p, i64],
     "mbg_get_tuning": [C.c_char_p],
     "mbg_load_tuning": [C.c_char_p],

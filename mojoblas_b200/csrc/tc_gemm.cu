@@ -1180,3 +1180,127 @@ extern "C" int mbg_debug_wait_probe(int64_t limit_ns) {
     MBG_CUDA(cudaStreamSynchronize(stream()));
     return read_and_clear_device_error() ? MBG_ERR_TIMEOUT : MBG_OK;
 }
+
+// ---- peak probes ------------------------------------------------------------------
+// Throughput probes for the roofline denominators that are not in the driver's
+// measured peaks: fp32 and fp64 FMA on the CUDA cores, and back-to-back
+// tcgen05.mma (kind::f16 bf16 and kind::i8) on fixed shared-memory operands.
+// Operand values are irrelevant: the probes time instruction throughput.
+namespace mbg {
+namespace tc {
+
+template <typename T>
+__global__ void __launch_bounds__(256) fma_probe_kernel(int iters, T seed, T* out) {
+    T a0 = seed + T(threadIdx.x), a1 = a0 + T(1), a2 = a0 + T(2), a3 = a0 + T(3);
+    T a4 = a0 + T(4), a5 = a0 + T(5), a6 = a0 + T(6), a7 = a0 + T(7);
+    const T m = T(0.999), c = T(1e-3);
+#pragma unroll 1
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+            a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+        }
+    }
+    const T s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == T(-12345)) out[threadIdx.x] = s;  // keeps the chains alive
+}
+
+// One CTA per SM: lane 0 of warp 1 issues `iters` MMAs of 128 x 256 x (32 bytes of k)
+// into one TMEM accumulator, commits, and waits (bounded) for them to complete.
+template <bool INT8>
+__global__ void __launch_bounds__(128, 1) mma_probe_kernel(int iters, int* err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* done = reinterpret_cast<uint64_t*>(smem + 3 * 16384);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(done + 1);
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        mbar_init(done, 1);
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(slot, 256);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    if (threadIdx.x == 32) {
+        const uint32_t sa = smem_u32(smem), sb = sa + 16384;  // A: 128 rows x 128 B, B: 256 rows x 128 B
+        const uint64_t ad = smem_desc(sa, 1024, 2), bd = smem_desc(sb, 1024, 2);
+        const uint32_t idesc = instr_desc(INT8, 128, 256);
+#pragma unroll 1
+        for (int i = 0; i < iters; ++i) umma<INT8>(tmem, ad, bd, idesc, i > 0 ? 1u : 0u);
+        umma_commit(done);
+        mbar_wait(done, 0, err, 98);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, 256);
+    }
+}
+
+}  // namespace tc
+}  // namespace mbg
+
+// Measured throughputs in TFLOP/s (tensor probes: dense ops, 2 per multiply-add).
+extern "C" int mbg_probe_peaks(double* fp32_tflops, double* fp64_tflops, double* bf16_tflops, double* int8_tops) {
+    using namespace mbg;
+    using namespace mbg::tc;
+    int dev = 0, sms = 148;
+    MBG_CUDA(cudaGetDevice(&dev));
+    MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t s = stream();
+    cudaEvent_t e0, e1;
+    MBG_CUDA(cudaEventCreate(&e0));
+    MBG_CUDA(cudaEventCreate(&e1));
+    float* f32 = nullptr;
+    double* f64 = nullptr;
+    Workspace ws;
+    MBG_TRY(ws.reserve(4096));
+    f32 = ws.as<float>();
+    f64 = ws.as<double>();
+    auto time_ms = [&](auto launch) -> float {
+        launch();  // warm-up
+        cudaEventRecord(e0, s);
+        launch();
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+    };
+    const int blocks = sms * 8, iters = 4096;
+    const double fma_flops = 2.0 * blocks * 256.0 * iters * 64.0;
+    if (fp32_tflops) {
+        const float ms = time_ms([&] { fma_probe_kernel<float><<<blocks, 256, 0, s>>>(iters, 1.0f, f32); });
+        *fp32_tflops = fma_flops / (ms * 1e-3) / 1e12;
+    }
+    if (fp64_tflops) {
+        const float ms = time_ms([&] { fma_probe_kernel<double><<<blocks, 256, 0, s>>>(iters / 4, 1.0, f64); });
+        *fp64_tflops = fma_flops / 4 / (ms * 1e-3) / 1e12;
+    }
+    int* err = device_error_flag();
+    const int smem = 3 * 16384 + 1024 + 64;
+    const int mma_iters = 8192;
+    if (bf16_tflops) {
+        MBG_CUDA(cudaFuncSetAttribute(mma_probe_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        const float ms = time_ms([&] { mma_probe_kernel<false><<<sms, 128, smem, s>>>(mma_iters, err); });
+        *bf16_tflops = 2.0 * sms * double(mma_iters) * 128 * 256 * 16 / (ms * 1e-3) / 1e12;
+    }
+    if (int8_tops) {
+        MBG_CUDA(cudaFuncSetAttribute(mma_probe_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        const float ms = time_ms([&] { mma_probe_kernel<true><<<sms, 128, smem, s>>>(mma_iters, err); });
+        *int8_tops = 2.0 * sms * double(mma_iters) * 128 * 256 * 32 / (ms * 1e-3) / 1e12;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MBG_TRY(check_launch("peak_probes"));
+    MBG_CUDA(cudaStreamSynchronize(s));
+    return read_and_clear_device_error() ? MBG_ERR_TIMEOUT : MBG_OK;
+}

@@ -8,10 +8,10 @@
 // The off-diagonal updates are gemm calls in the caller's precision mode (plain
 // FP32/FP64, BF16x3/x6 split, or Ozaki int8 slices), so almost all flops run in
 // large GEMMs.  Diagonal blocks are solved by `diag_solve_kernel`: the block is
-// staged once per CTA in shared memory in canonical column-major form, and
-// each warp owns one right-hand-side column, two rows per lane, broadcasting the
-// pivot with a warp shuffle — the reference's column-axpy substitution
-// (:130-148), divide by the diagonal included, with the same skip of zero pivots.
+// staged once per CTA in shared memory, and each group of eight lanes owns one
+// right-hand-side column, eight rows per lane, broadcasting the pivot with a
+// shuffle — the reference's column-axpy substitution (:130-148), scaled by the
+// reciprocal of the diagonal, with the same skip of zero pivots.
 //
 // Right side: X op(A) = alpha B  <=>  op(A)^T X^T = alpha B^T.  B is transposed
 // into a workspace (alpha folded in), solved from the left with the transpose
@@ -33,54 +33,74 @@ constexpr int DS_WARPS = 8;   // columns per CTA in flight
 
 // Solves op(A)[0:nb, 0:nb] X = B[0:nb, :] in place for nb <= 64.
 // LOWER: effective op(A) lower triangular (forward), else upper (backward).
-// The block is staged once per CTA in shared memory (column-major, padded)
-// with the reciprocals of its diagonal.  Each warp owns one right-hand-side
-// column, two rows per lane, and runs the reference's column-axpy substitution
-// (src/level3/trsm.mojo:111-148): the pivot x_l is broadcast from its lane by a
-// warp shuffle, scaled by 1/a_ll (a multiply: a division would put a long
+// The block is staged once per CTA in shared memory with the reciprocals of its
+// diagonal; its rows are stored interleaved (row q*8+j at position j*8+q of the
+// column) so that the eight lanes serving one right-hand side read eight
+// consecutive words.  Each group of eight lanes owns one column, eight rows per
+// lane in registers, and runs the reference's column-axpy substitution
+// (src/level3/trsm.mojo:111-148): the pivot x_l is broadcast within the group
+// by a shuffle, scaled by 1/a_ll (a multiply: a division would put a long
 // software sequence on every step's dependency chain), and every lane updates
-// its rows below (above) it; zero pivots are skipped as in the reference.
+// its rows below (above) it.  Zero pivots are skipped as in the reference, by
+// predication so the four columns of a warp do not diverge.
 template <typename T, bool LOWER, bool TRANS, bool UNIT>
 __global__ void __launch_bounds__(DS_WARPS * 32)
 diag_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __restrict__ B, i64 ldb) {
-    __shared__ T Ls[NB * (NB + 1)];
+    constexpr int LD = NB + 1;
+    __shared__ T Ls[NB * LD];
     __shared__ T inv[NB];
-    // stage the whole nb x nb block (compile-time 64 x 64 indexing, coalesced,
-    // no per-element branches): entries of the other triangle are copied but
-    // never read, since the substitution only touches i > l (i < l) below
+    // stage the whole nb x nb block (compile-time 64 x 64 indexing, coalesced);
+    // entries of the other triangle are copied but never read
 #pragma unroll 4
     for (int e = threadIdx.x; e < NB * NB; e += DS_WARPS * 32) {
         const int fast = e & (NB - 1), slow = e >> 6;  // fast index runs along contiguous memory
         const int i = TRANS ? slow : fast, l = TRANS ? fast : slow;
-        if (i < nb && l < nb) Ls[l * (NB + 1) + i] = TRANS ? A[l + (i64)i * lda] : A[i + (i64)l * lda];
+        if (i < nb && l < nb)
+            Ls[l * LD + (i & 7) * 8 + (i >> 3)] = TRANS ? A[l + (i64)i * lda] : A[i + (i64)l * lda];
     }
     __syncthreads();
-    for (int l = threadIdx.x; l < nb; l += blockDim.x) inv[l] = UNIT ? T(1) : T(1) / Ls[l * (NB + 1) + l];
+    for (int l = threadIdx.x; l < nb; l += blockDim.x)
+        inv[l] = UNIT ? T(1) : T(1) / Ls[l * LD + (l & 7) * 8 + (l >> 3)];
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (i64 j = (i64)blockIdx.x * DS_WARPS + warp; j < ncols; j += (i64)gridDim.x * DS_WARPS) {
-        T* bj = B + j * ldb;
-        T x0 = lane < nb ? bj[lane] : T(0);
-        T x1 = lane + 32 < nb ? bj[lane + 32] : T(0);
-        for (int s = 0; s < nb; ++s) {
-            const int l = LOWER ? s : nb - 1 - s;
-            const T* col = Ls + l * (NB + 1);
-            const T c0 = col[lane], c1 = col[lane + 32], il = inv[l];  // independent of the chain
-            const T src = (l < 32) ? x0 : x1;
-            T xl = __shfl_sync(0xffffffffu, src, l & 31);
-            if (xl == T(0)) continue;  // the reference skips zero pivots (:115, :133)
-            if (!UNIT) xl *= il;
-            if (lane == (l & 31)) { if (l < 32) x0 = xl; else x1 = xl; }
-            if (LOWER) {
-                if (lane > l) x0 -= xl * c0;
-                if (lane + 32 > l && lane + 32 < nb) x1 -= xl * c1;
-            } else {
-                if (lane < l) x0 -= xl * c0;
-                if (lane + 32 < l) x1 -= xl * c1;
+    const int lane = threadIdx.x & 31;
+    const int q = lane & 7;      // rows q*8 .. q*8+7 of the column
+    const int grp = lane >> 3;   // which of the warp's four columns
+    const i64 cols_per_cta = DS_WARPS * 4;
+    for (i64 j0 = (i64)blockIdx.x * cols_per_cta; j0 < ncols; j0 += (i64)gridDim.x * cols_per_cta) {
+        const i64 j = j0 + (threadIdx.x >> 5) * 4 + grp;
+        const bool active = j < ncols;
+        T* bj = B + (active ? j : 0) * ldb;
+        T x[8];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            const int r = q * 8 + s;
+            x[s] = (active && r < nb) ? bj[r] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < NB; ++u) {
+            const int l = LOWER ? u : NB - 1 - u;
+            if (l >= nb) continue;  // uniform: nb is the same for every thread
+            const int owner = l >> 3, slot = l & 7;
+            T xl = __shfl_sync(0xffffffffu, x[slot], owner, 8);
+            const bool live = xl != T(0);  // the reference skips zero pivots
+            if (!UNIT) xl *= inv[l];
+            if (q == owner && live) x[slot] = xl;
+            const T* col = Ls + l * LD;
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                const int r = q * 8 + s;
+                const bool below = LOWER ? (r > l) : (r < l);
+                const T a = col[s * 8 + q];
+                if (live && below) x[s] -= xl * a;
             }
         }
-        if (lane < nb) bj[lane] = x0;
-        if (lane + 32 < nb) bj[lane + 32] = x1;
+        if (active) {
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                const int r = q * 8 + s;
+                if (r < nb) bj[r] = x[s];
+            }
+        }
     }
 }
 
@@ -147,15 +167,18 @@ __global__ void copy_scale_kernel(i64 m, i64 n, T alpha, const T* __restrict__ x
             y[i + j * ldy] = alpha * x[i + j * ldx];
 }
 
-unsigned ds_grid(i64 ncols) {
+unsigned ds_grid(i64 ncols) {  // residual leaf: one warp per column
+    return (unsigned)imax(1, imin(cdiv(ncols, DS_WARPS), 148 * 8));
+}
+unsigned ds_solve_grid(i64 ncols) {  // solve leaf: four columns per warp
     const i64 cap = tuning().trsm_leaf_ctas > 0 ? tuning().trsm_leaf_ctas : 148 * 8;
-    return (unsigned)imax(1, imin(cdiv(ncols, DS_WARPS), cap));
+    return (unsigned)imax(1, imin(cdiv(ncols, DS_WARPS * 4), cap));
 }
 
 template <typename T>
 int launch_diag_solve(bool lower, bool trans, bool unit, int nb, i64 n, const T* a, i64 lda, T* b, i64 ldb) {
     ProfScope prof("trsm_diag_solve");
-    const dim3 g(ds_grid(n)), blk(DS_WARPS * 32);
+    const dim3 g(ds_solve_grid(n)), blk(DS_WARPS * 32);
     cudaStream_t s = stream();
 #define DS(L, TR, U) diag_solve_kernel<T, L, TR, U><<<g, blk, 0, s>>>(nb, n, a, lda, b, ldb)
     if (lower) {

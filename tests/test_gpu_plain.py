@@ -236,3 +236,14 @@ def test_bounded_wait_expires_and_context_survives():
     c = np.zeros((32, 32), np.float32, order="F")
     assert mb.gemm("N", "N", 32, 32, 32, 1.0, a, 32, a, 32, 0.0, c, 32, mode=mb.BF16X6) == 0
     assert np.all(c == 32.0)
+
+
+def test_peak_probes_are_plausible():
+    """The probe kernels run and report throughputs in a plausible range for a B200."""
+    import ctypes as C
+    from mojoblas_b200 import _lib as L
+    lib = L.load()
+    v = [C.c_double() for _ in range(4)]
+    assert lib.mbg_probe_peaks(*[C.byref(x) for x in v]) == 0, L.last_error()
+    fp32, fp64, bf16, int8 = (x.value for x in v)
+    assert 20 < fp32 < 200 and 5 < fp64 < 100 and 300 < bf16 < 5000 and 600 < int8 < 10000, (fp32, fp64, bf16, int8)
