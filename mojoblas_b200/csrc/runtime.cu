@@ -316,6 +316,8 @@ int mbg_set_tuning(const char* key, int64_t value) {
     if (k == "trsm_tc_min_k" && value >= 0) { tuning().trsm_tc_min_k = value; return MBG_OK; }
     if (k == "grouped_gemm_tile" && (value == 64 || value == 128)) { tuning().grouped_gemm_tile = value; return MBG_OK; }
     if (k == "trsm_leaf_ctas" && value >= 0) { tuning().trsm_leaf_ctas = value; return MBG_OK; }
+    if (k == "trsm_block_rows" && value >= 0 && value <= 1024) { tuning().trsm_block_rows = value; return MBG_OK; }
+    if (k == "trsm_block_min_cols" && value >= 0) { tuning().trsm_block_min_cols = value; return MBG_OK; }
     set_error_msg("unknown tuning key or value: " + k + " = " + std::to_string(value));
     return MBG_ERR_INVALID_MODE;
 }
@@ -325,6 +327,8 @@ int64_t mbg_get_tuning(const char* key) {
     if (k == "trsm_tc_min_k") return tuning().trsm_tc_min_k;
     if (k == "grouped_gemm_tile") return tuning().grouped_gemm_tile;
     if (k == "trsm_leaf_ctas") return tuning().trsm_leaf_ctas;
+    if (k == "trsm_block_rows") return tuning().trsm_block_rows;
+    if (k == "trsm_block_min_cols") return tuning().trsm_block_min_cols;
     return -1;
 }
 
