@@ -110,7 +110,7 @@ template <> struct Pair<float> { using type = float2; };
 
 constexpr int BS_COLS = 32;                       // right-hand sides per CTA of block_solve_kernel
 constexpr int BS_THREADS = 8 * BS_COLS;           // eight lanes per column in the substitution
-constexpr int BS_TILE = NB * (NB + 1) + NB;       // diagonal block + reciprocals; also holds a 64 x 66 tile
+constexpr int BS_TILE = NB * 72;                  // diagonal block + reciprocals (64 x 65 + 64), or a 64 x 72 tile
 
 inline int bs_strip_ld(int nb) { return (int)(cdiv(nb, NB) * NB) + 2; }
 template <typename T>
@@ -152,13 +152,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // past nb stay zero in the strip and staged items are zero outside op(A)'s
 // block, so ragged edges need no special case in the inner loops.
 template <typename T, bool LOWER, bool TRANS, bool UNIT, int W>
-__global__ void __launch_bounds__(8 * W)
+__global__ void __launch_bounds__(8 * W, 1)
 block_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __restrict__ B, i64 ldb) {
     using P2 = typename Pair<T>::type;
     static_assert(W == 32, "the tile update maps 256 threads onto 64 rows x 32 columns x 2 halves");
     constexpr int NT = 8 * W;
     constexpr int LDL = NB + 1;               // diagonal block, interleaved rows
-    constexpr int LT = TRANS ? NB + 2 : NB;   // update tile: [l][r] (plain) or [r][l] (transposed)
+    constexpr int LT = TRANS ? NB + 2 : NB + 8;  // update tile: [l][r] (plain) or [r][l] (transposed)
     extern __shared__ __align__(16) unsigned char bs_smem_raw[];
     const int nsub = (nb + NB - 1) / NB, nbr = nsub * NB, ldbs = nbr + 2;
     T* Bs = reinterpret_cast<T*>(bs_smem_raw);
@@ -251,10 +251,55 @@ block_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __res
                     if (q * 8 + s < nbb) bc[q * 8 + s] = x[s];
             } else {
                 // ---- trailing tile: B_t -= op(A)[t, b] X_b ----
-                // Thread (h, rg, cp): reduction half h (l in [32h, 32h + 32)), rows
-                // {2rg, 2rg+1, 2rg+32, 2rg+33} (plain) or {rg + 16i} (transposed),
-                // columns cp + 8j.  One warp covers 8 row groups x 4 column groups,
-                // so each 16-byte load of the tile or of X_b is one wavefront.
+                if constexpr (sizeof(T) == 8) {
+                    // FP64 tensor-core MMA (m8n8k4): warp w owns rows 16 (w % 4) .. +16
+                    // and columns 16 (w / 4) .. +16 of the 64 x 32 product, 2 x 2
+                    // fragments, the full 64-long reduction in registers.  Fragment
+                    // loads: A[row = lane / 4][k = lane % 4], X[k = lane % 4][col =
+                    // lane / 4]; with the tile's leading dimension (72 or 66) and the
+                    // strip's (2 mod 16) each is two wavefronts, the minimum for 256 B.
+                    const int rt0 = (LOWER ? b + 1 + tt : tt) * NB;
+                    const int lane = tid & 31, w = tid >> 5;
+                    const int m0 = 16 * (w & 3), n0 = 16 * (w >> 2);
+                    const int lr = lane >> 2, lk = lane & 3;
+                    double d[2][2][2];
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                        for (int nj = 0; nj < 2; ++nj) d[mi][nj][0] = d[mi][nj][1] = 0.0;
+                    const double* tile = reinterpret_cast<const double*>(cur);
+                    const double* xs = reinterpret_cast<const double*>(Bs) + r0;
+#pragma unroll 4
+                    for (int k0 = 0; k0 < NB; k0 += 4) {
+                        double af[2], bf[2];
+#pragma unroll
+                        for (int mi = 0; mi < 2; ++mi) {
+                            const int r = m0 + 8 * mi + lr, k = k0 + lk;
+                            af[mi] = TRANS ? tile[r * LT + k] : tile[k * LT + r];
+                        }
+#pragma unroll
+                        for (int nj = 0; nj < 2; ++nj) bf[nj] = xs[(n0 + 8 * nj + lr) * ldbs + k0 + lk];
+#pragma unroll
+                        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                            for (int nj = 0; nj < 2; ++nj)
+                                asm volatile(
+                                    "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                                    : "+d"(d[mi][nj][0]), "+d"(d[mi][nj][1])
+                                    : "d"(af[mi]), "d"(bf[nj]));
+                    }
+                    double* bs = reinterpret_cast<double*>(Bs);
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi) {
+                        const int r = rt0 + m0 + 8 * mi + lr;  // D fragment: row lane / 4, columns 2 (lane % 4) + {0, 1}
+                        if (r < nb) {
+#pragma unroll
+                            for (int nj = 0; nj < 2; ++nj)
+#pragma unroll
+                                for (int e = 0; e < 2; ++e) bs[(n0 + 8 * nj + 2 * lk + e) * ldbs + r] -= d[mi][nj][e];
+                        }
+                    }
+                } else {
                 const int rt0 = (LOWER ? b + 1 + tt : tt) * NB;
                 const int lane = tid & 31, wq = (tid >> 5) & 3, h = tid >> 7;
                 const int rg = (lane >> 2) + 8 * (wq & 1), cp = (lane & 3) + 4 * (wq >> 1);
@@ -309,6 +354,7 @@ block_solve_kernel(int nb, i64 ncols, const T* __restrict__ A, i64 lda, T* __res
                         }
                     }
                     if (half == 0) __syncthreads();
+                }
                 }
             }
             step = ns;
