@@ -436,15 +436,25 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 float* Cm = static_cast<float*>(P.c);
                 const float alpha = float(P.alpha), beta = float(P.beta);
                 const i64 cbase = n0 + part * C::EPI_COLS;
+                // 8 columns at a time: all loads of C are issued before the
+                // first is used, so the read-modify-write of a beta != 0 call
+                // waits for memory once per 8 columns, not once per column
 #pragma unroll
-                for (int j = 0; j < C::EPI_COLS; ++j) {
-                    const i64 col = cbase + j;
-                    if (col >= P.n) break;
-                    if (P.tri == 1 && row < col) continue;
-                    if (P.tri == 2 && row > col) continue;
-                    float* cp = Cm + row + col * P.ldc;
-                    const float v = alpha * acc[j];
-                    *cp = (beta == 0.0f) ? v : fmaf(beta, *cp, v);
+                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 8) {
+                    float cv[8];
+                    bool live[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const i64 col = cbase + c0 + j;
+                        live[j] = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
+                        cv[j] = (live[j] && beta != 0.0f) ? Cm[row + col * P.ldc] : 0.0f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        if (!live[j]) continue;
+                        const float v = alpha * acc[c0 + j];
+                        Cm[row + (cbase + c0 + j) * P.ldc] = (beta == 0.0f) ? v : fmaf(beta, cv[j], v);
+                    }
                 }
             }
         }
@@ -669,13 +679,26 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
         if (ok && row < P.m) {
             const int er = P.ea[row];
             const i64 cbase = n0 + part * C::EPI_COLS;
+            // 4 columns at a time, loads first (see the split kernel's epilogue;
+            // the 64 fp64 accumulators leave room for no more)
 #pragma unroll
-            for (int j = 0; j < C::EPI_COLS; ++j) {
-                const i64 col = cbase + j;
-                if (col >= P.n) break;
-                double* cp = P.c + row + col * P.ldc;
-                const double v = P.alpha * (acc[j] * pow2_exact(er + P.eb[col]));
-                *cp = (P.beta == 0.0) ? v : fma(P.beta, *cp, v);
+            for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+                double cv[4];
+                int ec[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const i64 col = cbase + c0 + j;
+                    const bool live = col < P.n;
+                    ec[j] = live ? P.eb[col] : 0;
+                    cv[j] = (live && P.beta != 0.0) ? P.c[row + col * P.ldc] : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const i64 col = cbase + c0 + j;
+                    if (col >= P.n) continue;
+                    const double v = P.alpha * (acc[c0 + j] * pow2_exact(er + ec[j]));
+                    P.c[row + col * P.ldc] = (P.beta == 0.0) ? v : fma(P.beta, cv[j], v);
+                }
             }
         }
     }
