@@ -439,6 +439,16 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 // 8 columns at a time: all loads of C are issued before the
                 // first is used, so the read-modify-write of a beta != 0 call
                 // waits for memory once per 8 columns, not once per column
+                // beta == 1 (the trsm updates): C += v as a reduction in L2 — one
+                // add per element, rounded as c + v, with no read in the thread
+                if (beta == 1.0f) {
+#pragma unroll
+                    for (int j = 0; j < C::EPI_COLS; ++j) {
+                        const i64 col = cbase + j;
+                        if (col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col))
+                            atomicAdd(Cm + row + col * P.ldc, alpha * acc[j]);
+                    }
+                } else
 #pragma unroll
                 for (int c0 = 0; c0 < C::EPI_COLS; c0 += 8) {
                     float cv[8];
@@ -679,8 +689,16 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
         if (ok && row < P.m) {
             const int er = P.ea[row];
             const i64 cbase = n0 + part * C::EPI_COLS;
-            // 4 columns at a time, loads first (see the split kernel's epilogue;
-            // the 64 fp64 accumulators leave room for no more)
+            // beta == 1: reductions in L2, as in the split kernel's epilogue; else
+            // 4 columns at a time, loads first (the 64 fp64 accumulators leave
+            // room for no more)
+            if (P.beta == 1.0) {
+#pragma unroll
+                for (int j = 0; j < C::EPI_COLS; ++j) {
+                    const i64 col = cbase + j;
+                    if (col < P.n) atomicAdd(P.c + row + col * P.ldc, P.alpha * (acc[j] * pow2_exact(er + P.eb[col])));
+                }
+            } else
 #pragma unroll
             for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
                 double cv[4];
