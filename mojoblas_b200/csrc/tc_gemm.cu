@@ -773,48 +773,75 @@ split_bf16_kernel(const float* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp
 }
 
 // Row exponents for the Ozaki scaling: e(r) with max_l |value(r,l)| < 2^e(r).
-// Partial maxima are combined with atomicMax on the exponent (initialised by
-// the host to 0x80808080, below any double exponent); an all-zero row keeps
-// that value and is mapped to 0.
+// Partial maxima over k chunks are combined with atomicMax on the exponent
+// (initialised by the host to 0x80808080, below any double exponent); an
+// all-zero row keeps that value, which the slicing kernel maps to 0.
+constexpr int OZ_EXP_KCHUNK = 64;    // k columns per CTA row block, rows contiguous in memory
+constexpr int OZ_EXP_KWARP = 1024;   // k per warp, k contiguous in memory
+
+__device__ __forceinline__ void oz_exponent_max(int* e, i64 r, double mx) {
+    if (mx > 0.0) {
+        int ex;
+        frexp(mx, &ex);
+        atomicMax(e + r, ex);
+    }
+}
+
 template <bool KMAJOR>
-__global__ void row_exponent_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, int* __restrict__ e) {
-    if (KMAJOR) {  // warp per row, lanes stride along k
-        const i64 r = i64(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(256)
+row_exponent_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, int* __restrict__ e) {
+    if (KMAJOR) {  // warp per row and k chunk, lanes along k (coalesced)
+        const i64 r = i64(blockIdx.x) * 8 + (threadIdx.x >> 5);
         if (r >= rows) return;
+        const i64 l0 = i64(blockIdx.y) * OZ_EXP_KWARP, l1 = min(K, l0 + OZ_EXP_KWARP);
+        const double* row = src + r * ld;
         double mx = 0.0;
-        for (i64 l = (threadIdx.x & 31) + i64(blockIdx.y) * 32; l < K; l += 32 * i64(gridDim.y))
-            mx = fmax(mx, fabs(src[l + r * ld]));
+#pragma unroll 8
+        for (i64 l = l0 + (threadIdx.x & 31); l < l1; l += 32) mx = fmax(mx, fabs(row[l]));
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if ((threadIdx.x & 31) == 0 && mx > 0.0) {
-            int ex;
-            frexp(mx, &ex);
-            atomicMax(e + r, ex);
-        }
-    } else {  // thread per row, blocks along k chunks
-        const i64 r = i64(blockIdx.x) * blockDim.x + threadIdx.x;
-        if (r >= rows) return;
-        const i64 chunk = (K + gridDim.y - 1) / gridDim.y;
-        const i64 l0 = i64(blockIdx.y) * chunk, l1 = min(K, l0 + chunk);
+        if ((threadIdx.x & 31) == 0) oz_exponent_max(e, r, mx);
+    } else {  // 32 rows (lanes, coalesced) x 8 k lanes per CTA, OZ_EXP_KCHUNK columns per CTA
+        __shared__ double part[8][33];
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+        const i64 r = i64(blockIdx.x) * 32 + tx;
+        const i64 l0 = i64(blockIdx.y) * OZ_EXP_KCHUNK;
         double mx = 0.0;
-        for (i64 l = l0; l < l1; ++l) mx = fmax(mx, fabs(src[r + l * ld]));
-        if (mx > 0.0) {
-            int ex;
-            frexp(mx, &ex);
-            atomicMax(e + r, ex);
+        if (r < rows) {
+#pragma unroll
+            for (int j = 0; j < OZ_EXP_KCHUNK / 8; ++j) {
+                const i64 l = l0 + ty + 8 * j;
+                if (l < K) mx = fmax(mx, fabs(src[r + l * ld]));
+            }
+        }
+        part[ty][tx] = mx;
+        __syncthreads();
+        if (ty == 0 && r < rows) {
+#pragma unroll
+            for (int y = 1; y < 8; ++y) mx = fmax(mx, part[y][tx]);
+            oz_exponent_max(e, r, mx);
         }
     }
 }
 
-__global__ void fix_exponents_kernel(int* e, i64 n) {
-    const i64 i = i64(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n && e[i] < -4096) e[i] = 0;
+// floor(|v| / 2^er * 2^56) from the bits of v: |v| = M 2^(max(E,1) - 1075) with the
+// 53-bit significand M.  Every step of the truncation loop (y = 128 x, digit =
+// trunc(y), x = y - digit) is exact, so its digits are the 7-bit fields of this
+// integer, most significant first; integer shifts keep the FP64 pipe free.
+__device__ __forceinline__ unsigned long long oz_fixed56(double v, int er, bool& neg) {
+    const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(v));
+    neg = (b >> 63) != 0;
+    const int E = int((b >> 52) & 0x7ff);
+    const unsigned long long M = (b & 0xfffffffffffffULL) | (E ? (1ULL << 52) : 0ULL);
+    const int sh = (E ? E : 1) - 1075 - er + 56;
+    if (sh >= 0) return sh < 64 ? M << sh : 0ULL;  // |v| < 2^er keeps a live result below 2^56
+    return sh > -64 ? M >> -sh : 0ULL;
 }
 
 template <bool KMAJOR>
 __global__ void __launch_bounds__(256)
 slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
-                const int* __restrict__ e, int8_t* __restrict__ planes) {
+                int* __restrict__ e, int8_t* __restrict__ planes) {
     __shared__ double tile[PT_R][PT_K + 1];
     const i64 r0 = i64(blockIdx.y) * PT_R, l0 = i64(blockIdx.x) * PT_K;
     load_tile<double, KMAJOR>(src, ld, rows, K, r0, l0, tile);
@@ -823,19 +850,22 @@ slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp,
     for (int q = threadIdx.x; q < PT_R * (PT_K / 4); q += blockDim.x) {
         const int rr = q / (PT_K / 4), lq = (q % (PT_K / 4)) * 4;
         const i64 r = r0 + rr;
-        const int er = (r < rows) ? e[r] : 0;
-        double x[4];
+        int er = (r < rows) ? e[r] : 0;
+        if (er < -4096) {  // all-zero row: exponent 0; the k-chunk-0 CTA stores it for the gemm kernel
+            er = 0;
+            if (blockIdx.x == 0 && lq == 0) e[r] = 0;
+        }
+        unsigned long long F[4];
+        bool neg[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = ldexp(tile[rr][lq + u], -er);  // |x| < 1
+        for (int u = 0; u < 4; ++u) F[u] = oz_fixed56(tile[rr][lq + u], er, neg[u]);
         char4* out = reinterpret_cast<char4*>(planes + size_t(r) * Kp + l0 + lq);
         for (int p = 0; p < slices; ++p) {
             int d[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const double y = x[u] * 128.0;
-                const double t = trunc(y);
-                d[u] = int(t);
-                x[u] = y - t;  // exact
+                const int dig = int((F[u] >> (49 - 7 * p)) & 127);
+                d[u] = neg[u] ? -dig : dig;
             }
             out[(plane / 4) * p] = make_char4((signed char)d[0], (signed char)d[1], (signed char)d[2],
                                               (signed char)d[3]);
@@ -918,14 +948,14 @@ int launch_slices(const double* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 R
         ProfScope prof("ozaki_exponent");
         MBG_CUDA(cudaMemsetAsync(e, 0x80, sizeof(int) * size_t(rows), stream()));  // 0x80808080 < any exponent
         if (kmajor) {
-            dim3 g(unsigned(cdiv(rows, 8)), unsigned(imin(cdiv(K, 4096), 16)));
+            dim3 g(unsigned(cdiv(rows, 8)), unsigned(cdiv(K, OZ_EXP_KWARP)));
+            if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
             row_exponent_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, e);
         } else {
-            dim3 g(unsigned(cdiv(rows, 256)), unsigned(imin(cdiv(K, 64), 64)));
+            dim3 g(unsigned(cdiv(rows, 32)), unsigned(cdiv(K, OZ_EXP_KCHUNK)));
+            if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
             row_exponent_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, e);
         }
-        MBG_TRY(check_launch("ozaki_exponent"));
-        fix_exponents_kernel<<<unsigned(cdiv(rows, 256)), 256, 0, stream()>>>(e, rows);
         MBG_TRY(check_launch("ozaki_exponent"));
     }
     ProfScope prof("ozaki_slice");
