@@ -206,14 +206,14 @@ int   mbg_release_workspace(void);
 
 /* ---- tuning table -------------------------------------------------------
  * Keys: "trsm_tc_min_k" — trsm off-diagonal updates with a shorter reduction
- * run on the plain kernel instead of the split / Ozaki forms (default 256);
+ * run on the plain kernel instead of the split / Ozaki forms (default 512);
  * "grouped_gemm_tile" — 64 or 128, tile edge of grouped sgemm plans (default 64);
  * "trsm_leaf_ctas" — CTA cap of the trsm 64-row diagonal-block solve (0 = 8 per SM);
  * "trsm_block_rows" — diagonal blocks up to this many rows (capped at 512 for
  * double, 1024 for float) are solved in one fused launch, sub-block updates
  * included (default 512; 64 or less: 64-row leaves with gemm updates between them);
  * "trsm_block_min_cols" — the fused launch is used only with at least this
- * many right-hand sides (default 1024).
+ * many right-hand sides (default 64).
  * mbg_load_tuning reads "key value" lines (or a flat JSON object of them) as
  * written by the autotuner (mojoblas_b200/autotune.py).
  * mbg_get_tuning returns -1 for an unknown key. */

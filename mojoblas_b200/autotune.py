@@ -8,9 +8,15 @@ Keys swept:
   grouped_gemm_tile  64 or 128 — tile edge of grouped sgemm plans, timed on a
                      batch of 4096 problems with m, n, k log-uniform in 16..512
                      (the batched configuration's distribution);
-  trsm_tc_min_k      128 .. 1024 — the reduction length below which the
-                     blocked trsm's off-diagonal updates stay on the plain
-                     kernel, timed on dtrsm 4096^2 with 8-slice Ozaki updates.
+  trsm_block_rows    0 (64-row leaves), 256, 512 — diagonal blocks solved in
+  trsm_tc_min_k      one fused launch, and the reduction length below which
+                     the blocked trsm's off-diagonal updates stay on the plain
+                     kernel; swept jointly on dtrsm 4096^2 with 8-slice Ozaki
+                     updates (the blocked-trsm configuration);
+  trsm_block_min_cols  the fewest right-hand sides for which the fused launch
+                     beats the 64-row leaves, timed on dtrsm 4096 x nrhs.
+Labels in the measurement log avoid the key names, since the library's loader
+reads the table as "key value" pairs.
 """
 from __future__ import annotations
 
@@ -83,7 +89,7 @@ def tune(out: Path) -> dict:
             raise RuntimeError(L.last_error())
         ms = time_plan(torch, lib, plan)
         lib.mbg_plan_destroy(plan)
-        log[f"grouped_gemm_tile={tile}"] = {"ms": round(ms, 4), "tflops": round(flops / ms / 1e9, 2)}
+        log[f"grouped sgemm tile {tile}"] = {"ms": round(ms, 4), "tflops": round(flops / ms / 1e9, 2)}
         if best is None or ms < best[1]:
             best = (tile, ms)
     table["grouped_gemm_tile"] = best[0]
@@ -95,13 +101,11 @@ def tune(out: Path) -> dict:
     A.diagonal().copy_(n + torch.rand(n, dtype=torch.float64, device="cuda"))
     B0 = torch.randn(n, n, dtype=torch.float64, device="cuda")
     X = B0.clone()
-    best = None
-    for thr in (128, 256, 512, 1024):
-        lib.mbg_set_tuning(b"trsm_tc_min_k", thr)
 
+    def time_trsm(mode, nrhs, reps=3):
         def call():
-            X.copy_(B0)
-            st = lib.mbg_dtrsm_ex(L.MODE_OZAKI, 8, 0, b"L", b"L", b"N", b"N", n, n, 1.0, A.data_ptr(), n,
+            X[:, :nrhs].copy_(B0[:, :nrhs])
+            st = lib.mbg_dtrsm_ex(mode, 8, 0, b"L", b"L", b"N", b"N", n, nrhs, 1.0, A.data_ptr(), n,
                                   X.data_ptr(), n)
             if st:
                 raise RuntimeError(L.last_error())
@@ -109,16 +113,42 @@ def tune(out: Path) -> dict:
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(3):
+        for _ in range(reps):
             call()
         e1.record()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / 3
-        log[f"trsm_tc_min_k={thr}"] = {"ms": round(ms, 3)}
-        if best is None or ms < best[1]:
-            best = (thr, ms)
-    table["trsm_tc_min_k"] = best[0]
-    lib.mbg_set_tuning(b"trsm_tc_min_k", best[0])
+        return e0.elapsed_time(e1) / reps
+
+    lib.mbg_set_tuning(b"trsm_block_min_cols", 1)
+    best = None
+    for rows in (0, 256, 512):
+        for thr in (256, 512, 1024):
+            lib.mbg_set_tuning(b"trsm_block_rows", rows)
+            lib.mbg_set_tuning(b"trsm_tc_min_k", thr)
+            ms = time_trsm(L.MODE_OZAKI, n)
+            log[f"ozaki dtrsm 4096^2, fused rows {rows}, split from k {thr}"] = {"ms": round(ms, 3)}
+            if best is None or ms < best[2]:
+                best = (rows, thr, ms)
+    table["trsm_block_rows"], table["trsm_tc_min_k"] = best[0], best[1]
+    lib.mbg_set_tuning(b"trsm_block_rows", best[0])
+    lib.mbg_set_tuning(b"trsm_tc_min_k", best[1])
+
+    # smallest right-hand-side count from which the fused blocks win (plain dtrsm 4096 x nrhs)
+    min_cols = n  # fused blocks won at n right-hand sides in the sweep above
+    if best[0] > 64:
+        for nrhs in (2048, 1024, 512, 256, 128, 64):
+            lib.mbg_set_tuning(b"trsm_block_rows", best[0])
+            fused = time_trsm(L.MODE_PLAIN, nrhs)
+            lib.mbg_set_tuning(b"trsm_block_rows", 0)
+            leaves = time_trsm(L.MODE_PLAIN, nrhs)
+            log[f"plain dtrsm 4096 x {nrhs}: fused vs leaves"] = {"ms": [round(fused, 3), round(leaves, 3)]}
+            if fused <= leaves:
+                min_cols = nrhs
+            else:
+                break
+        lib.mbg_set_tuning(b"trsm_block_rows", best[0])
+    table["trsm_block_min_cols"] = min_cols
+    lib.mbg_set_tuning(b"trsm_block_min_cols", min_cols)
 
     doc = {**table, "_measurements": log, "_device": torch.cuda.get_device_name(0)}
     out.write_text(json.dumps(doc, indent=1) + "\n")

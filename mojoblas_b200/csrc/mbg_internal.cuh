@@ -97,11 +97,11 @@ int finish_call(bool any_staged);  // synchronises when required, checks flag
 
 // ---- tuning table (defaults; mbg_set_tuning / mbg_load_tuning override) ------
 struct Tuning {
-    i64 trsm_tc_min_k = 256;   // trsm off-diagonal updates with shorter k use the plain kernel
+    i64 trsm_tc_min_k = 512;   // trsm off-diagonal updates with shorter k use the plain kernel
     i64 grouped_gemm_tile = 64;  // tile edge of grouped sgemm plans (64 or 128)
     i64 trsm_leaf_ctas = 0;      // CTA cap of the trsm diagonal-block solve (0: 8 per SM)
     i64 trsm_block_rows = 512;   // diagonal blocks solved in one fused launch (<= 64: leaves + gemm)
-    i64 trsm_block_min_cols = 1024;  // ... when there are at least this many right-hand sides
+    i64 trsm_block_min_cols = 64;    // ... when there are at least this many right-hand sides
 };
 Tuning& tuning();
 
