@@ -231,6 +231,9 @@ int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 l
                const T* b, i64 ldb, T beta, T* c, i64 ldc) {
     if (m == 0 || n == 0) return MBG_OK;
     if (alpha == T(0) || k == 0) return scale_matrix<T>(m, n, beta, c, ldc);
+    if constexpr (sizeof(T) == 8)
+        if (!tuning().plain_fp64_simt)
+            return dgemm_dmma(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     const i64 gm = cdiv(m, 128), gn = cdiv(n, 128);
     if (gm * gn < 2 * 148) {  // under two waves of 128 x 128 tiles: use 64 x 64 tiles
         const i64 sm = cdiv(m, 64), sn = cdiv(n, 64);
@@ -248,6 +251,9 @@ int gemmt_plain(char uplo, char ta, char tb, i64 n, i64 k, T alpha, const T* a, 
                 const T* b, i64 ldb, T beta, T* c, i64 ldc) {
     if (n == 0) return MBG_OK;
     if (alpha == T(0) || k == 0) return scale_triangle<T>(uplo, n, beta, c, ldc);
+    if constexpr (sizeof(T) == 8)
+        if (!tuning().plain_fp64_simt)
+            return dgemmt_dmma(uplo, ta, tb, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     const i64 t = cdiv(n, 128);
     const i64 tiles = t * (t + 1) / 2;
     if (tiles > 0x7fffffff) return MBG_ERR_UNSUPPORTED;

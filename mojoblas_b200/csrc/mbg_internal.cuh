@@ -102,6 +102,7 @@ struct Tuning {
     i64 trsm_leaf_ctas = 0;      // CTA cap of the trsm diagonal-block solve (0: 8 per SM)
     i64 trsm_block_rows = 512;   // diagonal blocks solved in one fused launch (<= 64: leaves + gemm)
     i64 trsm_block_min_cols = 64;    // ... when there are at least this many right-hand sides
+    i64 plain_fp64_simt = 0;     // 1: plain FP64 gemm/syrk on the CUDA cores instead of the FP64 tensor pipe
 };
 Tuning& tuning();
 
@@ -109,6 +110,11 @@ Tuning& tuning();
 template <typename T>
 int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 lda,
                const T* b, i64 ldb, T beta, T* c, i64 ldc);
+// FP64 tensor-pipe GEMM (gemm_dmma.cu): alpha != 0, k > 0
+int dgemm_dmma(char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
+               const double* b, i64 ldb, double beta, double* c, i64 ldc);
+int dgemmt_dmma(char uplo, char ta, char tb, i64 n, i64 k, double alpha, const double* a, i64 lda,
+                const double* b, i64 ldb, double beta, double* c, i64 ldc);
 // lower (uplo 'L') or upper triangle of C := alpha*op(A)*op(B) + beta*C
 template <typename T>
 int gemmt_plain(char uplo, char ta, char tb, i64 n, i64 k, T alpha, const T* a, i64 lda,
