@@ -10,25 +10,33 @@
 // element from shared memory once per warp instead of once per thread.
 //
 // CTA tile BM x BN with (BM / WM) x (BN / WN) warps, warp tile WM x WN made of
-// (WM / 8) x (WN / 8) MMA fragments.  K advances in slabs of 16 through a
+// (WM / 8) x (WN / 8) MMA fragments.  K advances in slabs of 32 through a
 // 3-stage cp.async pipeline: every element is copied global -> shared on its
 // own (8 bytes), so any transpose, leading dimension and ragged edge is served
-// by the same code (elements outside the matrix are zero-filled).  Shared tiles
-// are k-major ([k][m], [k][n]) with rows padded to BM + 8 (= 8 mod 16), so the
-// fragment loads A[row = lane / 4][k = lane % 4] and B[k = lane % 4][col =
-// lane / 4] are two wavefronts each, the minimum for 256 bytes.
+// by the same code (elements outside the matrix are zero-filled).  Each operand
+// keeps in shared memory the orientation it has in global memory, so a warp's
+// copies land in consecutive words: [k][m] rows of BM + 8 doubles for an
+// m-contiguous operand, [m][k] rows of 36 doubles for a k-contiguous one.  Both
+// paddings make the fragment loads A[row = lane / 4][k = lane % 4] and
+// B[k = lane % 4][col = lane / 4] two wavefronts each, the minimum for 256 bytes.
 #include "mbg_internal.cuh"
 
 namespace mbg {
 
 namespace {
 
-constexpr int DK = 16, DSTAGES = 3;
+constexpr int DK = 32, DSTAGES = 3;
+constexpr int DKP = DK + 4;  // row of a k-contiguous tile: 36 doubles = 72 words = 8 mod 32
 
 __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0)
                  : "memory");
+}
+// 16 bytes (two doubles) of which the first `bytes` are read (16, 8 or 0), the rest zero-filled
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -53,18 +61,25 @@ template <int BM, int BN, int WM, int WN>
 struct DmmaCfg {
     static constexpr int WARPS = (BM / WM) * (BN / WN);
     static constexpr int THREADS = 32 * WARPS;
-    static constexpr int LDA = BM + 8, LDB = BN + 8;
     static constexpr int MI = WM / 8, NJ = WN / 8;
-    static constexpr size_t SMEM = sizeof(double) * size_t(DSTAGES) * DK * (LDA + LDB);
+    // a stage holds each operand in the orientation it is contiguous in: [k][m] rows of
+    // BM + 8 doubles, or [m][k] rows of DKP doubles; both sizes are reserved
+    static constexpr int A_ELEMS = (DK * (BM + 8) > BM * DKP) ? DK * (BM + 8) : BM * DKP;
+    static constexpr int B_ELEMS = (DK * (BN + 8) > BN * DKP) ? DK * (BN + 8) : BN * DKP;
+    static constexpr size_t SMEM = sizeof(double) * size_t(DSTAGES) * (A_ELEMS + B_ELEMS);
 };
 
-template <class C, bool TA, bool TB, int TRI, int BM, int BN>
+// VEC = 2: both operands 16-byte aligned with even leading dimensions, so pairs
+// of elements along the contiguous index are copied 16 bytes at a time.
+template <class C, bool TA, bool TB, int TRI, int BM, int BN, int VEC>
 __global__ void __launch_bounds__(C::THREADS, 1)
 gemm_dmma_kernel(i64 m, i64 n, i64 k, double alpha, const double* __restrict__ A, i64 lda,
                  const double* __restrict__ B, i64 ldb, double beta, double* __restrict__ Cm, i64 ldc) {
     extern __shared__ __align__(16) double dsm[];
-    double* As = dsm;                                   // [stage][k][LDA]
-    double* Bs = dsm + size_t(DSTAGES) * DK * C::LDA;  // [stage][k][LDB]
+    // A: TA (k contiguous in memory) -> [m][DKP], else [k][BM + 8]; B: !TB -> [n][DKP], else [k][BN + 8]
+    constexpr int LA = TA ? DKP : BM + 8, LB = TB ? BN + 8 : DKP;
+    double* As = dsm;
+    double* Bs = dsm + size_t(DSTAGES) * C::A_ELEMS;
 
     i64 tm, tn;
     if (TRI == 0) {
@@ -83,23 +98,41 @@ gemm_dmma_kernel(i64 m, i64 n, i64 k, double alpha, const double* __restrict__ A
 
     auto issue = [&](i64 kt, int st) {
         const i64 k0 = kt * DK;
-        double* as = As + size_t(st) * DK * C::LDA;
-        double* bs = Bs + size_t(st) * DK * C::LDB;
+        double* as = As + size_t(st) * C::A_ELEMS;
+        double* bs = Bs + size_t(st) * C::B_ELEMS;
 #pragma unroll
-        for (int e = tid; e < BM * DK; e += C::THREADS) {
+        for (int e0 = tid; e0 < BM * DK / VEC; e0 += C::THREADS) {
+            const int e = e0 * VEC;
             int i, l;
             if (!TA) { i = e % BM; l = e / BM; } else { l = e % DK; i = e / DK; }  // contiguous index first
             const i64 gi = m0 + i, gl = k0 + l;
-            const bool v = gi < m && gl < k;
-            cp_async8(as + l * C::LDA + i, v ? (TA ? A + gl + gi * lda : A + gi + gl * lda) : A, v);
+            double* dst = as + (TA ? i * LA + l : l * LA + i);
+            if (VEC == 1) {
+                const bool v = gi < m && gl < k;
+                cp_async8(dst, v ? (TA ? A + gl + gi * lda : A + gi + gl * lda) : A, v);
+            } else {  // the pair runs along the contiguous index; the second may fall off the edge
+                const i64 c0 = TA ? gl : gi, cend = TA ? k : m;
+                const bool v = TA ? gi < m : gl < k;
+                const int bytes = (!v || c0 >= cend) ? 0 : (c0 + 1 < cend ? 16 : 8);
+                cp_async16(dst, bytes ? (TA ? A + gl + gi * lda : A + gi + gl * lda) : A, bytes);
+            }
         }
 #pragma unroll
-        for (int e = tid; e < BN * DK; e += C::THREADS) {
+        for (int e0 = tid; e0 < BN * DK / VEC; e0 += C::THREADS) {
+            const int e = e0 * VEC;
             int j, l;
             if (!TB) { l = e % DK; j = e / DK; } else { j = e % BN; l = e / BN; }
             const i64 gj = n0 + j, gl = k0 + l;
-            const bool v = gj < n && gl < k;
-            cp_async8(bs + l * C::LDB + j, v ? (TB ? B + gj + gl * ldb : B + gl + gj * ldb) : B, v);
+            double* dst = bs + (TB ? l * LB + j : j * LB + l);
+            if (VEC == 1) {
+                const bool v = gj < n && gl < k;
+                cp_async8(dst, v ? (TB ? B + gj + gl * ldb : B + gl + gj * ldb) : B, v);
+            } else {
+                const i64 c0 = TB ? gj : gl, cend = TB ? n : k;
+                const bool v = TB ? gl < k : gj < n;
+                const int bytes = (!v || c0 >= cend) ? 0 : (c0 + 1 < cend ? 16 : 8);
+                cp_async16(dst, bytes ? (TB ? B + gj + gl * ldb : B + gl + gj * ldb) : B, bytes);
+            }
         }
     };
 
@@ -121,15 +154,16 @@ gemm_dmma_kernel(i64 m, i64 n, i64 k, double alpha, const double* __restrict__ A
         if (kt + DSTAGES - 1 < nk) issue(kt + DSTAGES - 1, int((kt + DSTAGES - 1) % DSTAGES));
         cp_commit();
         const int st = int(kt % DSTAGES);
-        const double* as = As + size_t(st) * DK * C::LDA + wm0 + lr;
-        const double* bs = Bs + size_t(st) * DK * C::LDB + wn0 + lr;
+        // fragment element (row wm0 + 8i + lr, k kk + lk) and (k kk + lk, column wn0 + 8j + lr)
+        const double* as = As + size_t(st) * C::A_ELEMS + (TA ? (wm0 + lr) * LA + lk : lk * LA + wm0 + lr);
+        const double* bs = Bs + size_t(st) * C::B_ELEMS + (TB ? lk * LB + wn0 + lr : (wn0 + lr) * LB + lk);
 #pragma unroll
         for (int kk = 0; kk < DK; kk += 4) {
             double af[C::MI], bf[C::NJ];
 #pragma unroll
-            for (int i = 0; i < C::MI; ++i) af[i] = as[(kk + lk) * C::LDA + 8 * i];
+            for (int i = 0; i < C::MI; ++i) af[i] = TA ? as[8 * i * LA + kk] : as[kk * LA + 8 * i];
 #pragma unroll
-            for (int j = 0; j < C::NJ; ++j) bf[j] = bs[(kk + lk) * C::LDB + 8 * j];
+            for (int j = 0; j < C::NJ; ++j) bf[j] = TB ? bs[kk * LB + 8 * j] : bs[8 * j * LB + kk];
 #pragma unroll
             for (int i = 0; i < C::MI; ++i)
 #pragma unroll
@@ -170,32 +204,41 @@ gemm_dmma_kernel(i64 m, i64 n, i64 k, double alpha, const double* __restrict__ A
 using Big = DmmaCfg<128, 128, 64, 32>;   // 8 warps
 using Small = DmmaCfg<64, 64, 32, 32>;   // 4 warps
 
-template <class C, int TRI, int BM, int BN>
-int launch_dmma(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
-                const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+template <class C, int TRI, int BM, int BN, int VEC>
+int launch_dmma_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
+                  const double* b, i64 ldb, double beta, double* c, i64 ldc) {
     static unsigned configured = 0;  // one bit per device
     int dev = 0;
     MBG_CUDA(cudaGetDevice(&dev));
     if (dev >= 32 || !(configured & (1u << dev))) {  // all four transposes, on a device's first call
-        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, false, false, TRI, BM, BN>,
+        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, false, false, TRI, BM, BN, VEC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, false, true, TRI, BM, BN>,
+        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, false, true, TRI, BM, BN, VEC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, true, false, TRI, BM, BN>,
+        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, true, false, TRI, BM, BN, VEC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, true, true, TRI, BM, BN>,
+        MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, true, true, TRI, BM, BN, VEC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
         if (dev < 32) configured |= 1u << dev;
     }
     cudaStream_t s = stream();
 #define DM(TA_, TB_) \
-    gemm_dmma_kernel<C, TA_, TB_, TRI, BM, BN><<<grid, C::THREADS, C::SMEM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    gemm_dmma_kernel<C, TA_, TB_, TRI, BM, BN, VEC><<<grid, C::THREADS, C::SMEM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
     if (!ta && !tb) DM(false, false);
     else if (!ta && tb) DM(false, true);
     else if (ta && !tb) DM(true, false);
     else DM(true, true);
 #undef DM
     return check_launch("gemm_dmma_f64");
+}
+
+template <class C, int TRI, int BM, int BN>
+int launch_dmma(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
+                const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+    const bool vec = (reinterpret_cast<uintptr_t>(a) % 16 == 0) && (reinterpret_cast<uintptr_t>(b) % 16 == 0) &&
+                     lda % 2 == 0 && ldb % 2 == 0;
+    if (vec) return launch_dmma_v<C, TRI, BM, BN, 2>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    return launch_dmma_v<C, TRI, BM, BN, 1>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
 }
 
 }  // namespace
