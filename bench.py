@@ -44,6 +44,13 @@ FLOPS_D = 2.0 * N_D ** 3
 SAMPLE_ROWS = 256  # rows of C checked against the float64 oracle
 
 
+# DRAM bytes of one tc_gemm_bf16x6 launch at M = N = K = 8192 (NT), measured with
+# ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum (one pass, full size):
+# 3.43 GB read + 0.267 GB written.  Algorithmic: 3 bf16 planes of A and of B
+# (2 x 3 x 8192^2 x 2 B) read once, C (8192^2 x 4 B) written once.
+TRAFFIC_BF16X6_8192 = 3.43e9 + 0.267e9
+PLANES_BF16X6_8192 = 2 * 3 * 8192 * 8192 * 2 + 8192 * 8192 * 4
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -714,9 +721,15 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": launches,
         "roofline": {"bound": "tensor", "kernel": kname.decode(),
                      "achieved": round(achieved_tensor, 1), "peak": pk["bf16"], "unit": "TFLOP/s",
-                     "frac": round(achieved_tensor / pk["bf16"], 3), "traffic": None,
+                     "frac": round(achieved_tensor / pk["bf16"], 3),
+                     # dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch (8192^3 NT, bf16x6),
+                     # single-pass ncu capture summarised in profiles/tc_gemm_bf16x6_dram_traffic_8192.md
+                     "traffic": TRAFFIC_BF16X6_8192 if args.mode == "bf16x6" else None,
+                     "traffic_unit": "bytes per launch",
                      "note": f"bf16 tensor flops = {nprod} products x 2MNK per launch / mean launch time "
-                             f"({k_ms:.3f} ms); peak = {pk['source']} bf16 burst",
+                             f"({k_ms:.3f} ms); peak = {pk['source']} bf16 burst; traffic = "
+                             f"{TRAFFIC_BF16X6_8192 / 1e9:.2f} GB against {PLANES_BF16X6_8192 / 1e9:.2f} GB of bf16 "
+                             f"planes + C: the planes are re-read across output tiles",
                      "split_prepass_ms": round(split_ms, 3)},
         "clocks": clocks.summary(),
     }
