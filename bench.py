@@ -51,6 +51,7 @@ SAMPLE_ROWS = 256  # rows of C checked against the float64 oracle
 TRAFFIC_BF16X6_8192 = 3.43e9 + 0.267e9
 PLANES_BF16X6_8192 = 2 * 3 * 8192 * 8192 * 2 + 8192 * 8192 * 4
 
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -722,8 +723,8 @@ def run_ours(args, rank, world, dist):
         "roofline": {"bound": "tensor", "kernel": kname.decode(),
                      "achieved": round(achieved_tensor, 1), "peak": pk["bf16"], "unit": "TFLOP/s",
                      "frac": round(achieved_tensor / pk["bf16"], 3),
-                     # dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch (8192^3 NT, bf16x6),
-                     # single-pass ncu capture summarised in profiles/tc_gemm_bf16x6_dram_traffic_8192.md
+                     # dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch (8192^3 NT, bf16x6)
+                     # from a single-pass ncu capture
                      "traffic": TRAFFIC_BF16X6_8192 if args.mode == "bf16x6" else None,
                      "traffic_unit": "bytes per launch",
                      "note": f"bf16 tensor flops = {nprod} products x 2MNK per launch / mean launch time "
