@@ -19,8 +19,11 @@
  * mbg_set_sync(0) is in effect and every operand is a device pointer.
  *
  * Quick returns, argument checks and the alpha == 0 / k == 0 paths follow the
- * reference; the arithmetic follows Netlib where the reference departs from it
- * (gemm_v7 alpha, right-side transposed trsm).
+ * reference; the arithmetic follows Netlib where the reference departs from it:
+ * alpha is applied in float64 NN gemm for n >= 512 (the reference's gemm_v7,
+ * src/level3/gemm.mojo:817-1132, never applies it), and side 'R' with trans 'T'
+ * solves X op(A)^T = alpha B (the reference's right-side transposed branches run
+ * the NoTrans loops, src/level3/trsm.mojo:224-273).
  */
 #ifndef MOJOBLAS_GPU_H
 #define MOJOBLAS_GPU_H
