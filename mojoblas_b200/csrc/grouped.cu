@@ -11,12 +11,16 @@
 //    an atomic counter (largest first, so the tail is short), locate the problem
 //    by binary search over the tile prefix sums, and run the plain FP32 tile
 //    code of gemm_simt.cu with that problem's transposes, alpha and beta.
-//  * strsm (left side, any uplo / trans / diag, n <= 256): one warp per
-//    (problem, right-hand-side column); the column lives in registers, eight
-//    rows per lane, and the reference's column substitution
-//    (src/level3/trsm.mojo:111-168) runs with the pivot broadcast by a warp
-//    shuffle and multiplied by a precomputed reciprocal of the diagonal.
+//  * strsm (left side, any uplo / trans / diag, n <= 256): problems are cut
+//    into strips of 32 right-hand sides, ordered largest problem first;
+//    persistent CTAs take strips from an atomic counter and solve each with
+//    the blocked trsm's fused diagonal-block routine (block_solve.cuh): the
+//    strip in shared memory, the reference's column substitution
+//    (src/level3/trsm.mojo:111-168) on 64-row sub-blocks with the pivot
+//    broadcast by a shuffle and multiplied by a precomputed reciprocal, and the
+//    updates between sub-blocks from cp.async-staged tiles of op(A).
 #include "mbg_internal.cuh"
+#include "block_solve.cuh"
 
 #include <algorithm>
 #include <numeric>
@@ -178,73 +182,48 @@ struct TrsmDesc {
     i64 col0;                // first global column index of this problem
 };
 
-constexpr int TR_MAXN = 256, TR_SLOTS = TR_MAXN / 32;
+constexpr int TR_MAXN = 256;  // largest problem order a grouped strsm plan takes
 
-// One warp solves op(A) x = alpha * b for one column of one problem.
-__global__ void __launch_bounds__(256)
-grouped_strsm_kernel(const TrsmDesc* __restrict__ probs, int count, i64 total_cols) {
-    const int lane = threadIdx.x & 31;
-    const i64 wid = (i64(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const i64 nwarps = (i64(gridDim.x) * blockDim.x) >> 5;
-    for (i64 c = wid; c < total_cols; c += nwarps) {
-        int lo = 0, hi = count - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (probs[mid].col0 <= c) lo = mid; else hi = mid - 1;
+// One unit of grouped-strsm work: a strip of up to bs::BS_COLS right-hand sides of one problem.
+struct TrsmItem {
+    int prob;
+    int pad_;
+    i64 c0;
+};
+
+// Persistent grouped strsm: each CTA takes (problem, strip) items from an atomic
+// counter — the plan orders them largest problem first, so the long solves start
+// early and the small ones fill in behind them — and solves each with the fused
+// diagonal-block routine of the blocked trsm: the strip in shared memory, 64-row
+// substitution sub-blocks, cp.async-staged tiles of op(A), alpha applied to the
+// strip as it lands.
+__global__ void __launch_bounds__(bs::BS_THREADS, 2)
+grouped_block_strsm_kernel(const TrsmDesc* __restrict__ probs, const TrsmItem* __restrict__ items, int nitems,
+                           unsigned long long* __restrict__ counter) {
+    extern __shared__ __align__(16) unsigned char gs_smem[];
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = int(atomicAdd(counter, 1ULL));
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();  // every thread has read s_item before thread 0 writes the next one
+        if (it >= nitems) break;
+        const TrsmItem w = items[it];
+        const TrsmDesc d = probs[w.prob];
+        const int nb = int(d.n);
+#define GS(L, TR, U)                                                                                  \
+    bs::block_solve_strip<float, L, TR, U, bs::BS_COLS>(nb, d.nrhs, d.a, d.lda, d.b, d.ldb, w.c0, d.alpha, gs_smem)
+        switch ((d.lower ? 4 : 0) | (d.trans ? 2 : 0) | (d.unit ? 1 : 0)) {
+            case 0: GS(false, false, false); break;
+            case 1: GS(false, false, true); break;
+            case 2: GS(false, true, false); break;
+            case 3: GS(false, true, true); break;
+            case 4: GS(true, false, false); break;
+            case 5: GS(true, false, true); break;
+            case 6: GS(true, true, false); break;
+            default: GS(true, true, true); break;
         }
-        const TrsmDesc d = probs[lo];  // registers
-        const int n = int(d.n);
-        float* bj = d.b + (c - d.col0) * d.ldb;
-        auto aval = [&](int r, int l) -> float { return d.trans ? d.a[l + i64(r) * d.lda] : d.a[r + i64(l) * d.lda]; };
-        float x[TR_SLOTS], inv[TR_SLOTS];
-#pragma unroll
-        for (int s = 0; s < TR_SLOTS; ++s) {
-            const int r = s * 32 + lane;
-            x[s] = r < n ? d.alpha * bj[r] : 0.0f;
-            inv[s] = (r < n && !d.unit) ? 1.0f / aval(r, r) : 1.0f;  // off the dependency chain
-        }
-        if (d.lower) {
-#pragma unroll
-            for (int s = 0; s < TR_SLOTS; ++s) {
-                if (s * 32 >= n) break;
-                for (int t = 0; t < 32; ++t) {
-                    const int l = s * 32 + t;
-                    if (l >= n) break;
-                    float xl = __shfl_sync(0xffffffffu, x[s], t);
-                    if (xl == 0.0f) continue;  // zero pivot: skipped as in the reference
-                    xl *= __shfl_sync(0xffffffffu, inv[s], t);
-                    if (lane == t) x[s] = xl;
-#pragma unroll
-                    for (int s2 = s; s2 < TR_SLOTS; ++s2) {
-                        const int r = s2 * 32 + lane;
-                        if (r > l && r < n) x[s2] -= xl * aval(r, l);
-                    }
-                }
-            }
-        } else {
-#pragma unroll
-            for (int s = TR_SLOTS - 1; s >= 0; --s) {
-                if (s * 32 >= n) continue;
-                for (int t = 31; t >= 0; --t) {
-                    const int l = s * 32 + t;
-                    if (l >= n) continue;
-                    float xl = __shfl_sync(0xffffffffu, x[s], t);
-                    if (xl == 0.0f) continue;
-                    xl *= __shfl_sync(0xffffffffu, inv[s], t);
-                    if (lane == t) x[s] = xl;
-#pragma unroll
-                    for (int s2 = 0; s2 <= s; ++s2) {
-                        const int r = s2 * 32 + lane;
-                        if (r < l) x[s2] -= xl * aval(r, l);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int s = 0; s < TR_SLOTS; ++s) {
-            const int r = s * 32 + lane;
-            if (r < n) bj[r] = x[s];
-        }
+#undef GS
     }
 }
 
@@ -274,6 +253,9 @@ struct mbg_plan {
     i64 total = 0;       // tiles (sgemm) or columns (strsm)
     int tile = 64;
     int grid = 0;
+    void* items = nullptr;  // strsm: (problem, strip) work items, inside the table allocation
+    int nitems = 0;
+    size_t smem = 0;        // strsm: dynamic shared memory per CTA
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;  // stream the graph was captured on
@@ -294,7 +276,9 @@ int enqueue_plan(mbg_plan* p) {
                                                                p->total, p->counter);
         return check_launch("grouped_sgemm");
     }
-    grouped_strsm_kernel<<<p->grid, 256, 0, s>>>(static_cast<const TrsmDesc*>(p->table), p->count, p->total);
+    MBG_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
+    grouped_block_strsm_kernel<<<p->grid, bs::BS_THREADS, p->smem, s>>>(
+        static_cast<const TrsmDesc*>(p->table), static_cast<const TrsmItem*>(p->items), p->nitems, p->counter);
     return check_launch("grouped_strsm");
 }
 
@@ -465,14 +449,45 @@ int mbg_strsm_grouped_plan(int mode, int count, const mbg_strsm_problem* probs, 
         cols += q.n;
         v.push_back(d);
     }
+    // work items: 32-column strips, largest problem first (ties keep the caller's order)
+    std::vector<TrsmItem> items;
+    for (int i = 0; i < int(v.size()); ++i)
+        for (i64 c0 = 0; c0 < v[size_t(i)].nrhs; c0 += bs::BS_COLS) items.push_back(TrsmItem{i, 0, c0});
+    std::stable_sort(items.begin(), items.end(),
+                     [&](const TrsmItem& x, const TrsmItem& y) { return v[size_t(x.prob)].n > v[size_t(y.prob)].n; });
     mbg_plan* p = new mbg_plan();
     p->kind = 2;
     p->count = int(v.size());
     p->total = cols;
-    p->grid = int(imax(1, imin(cdiv(cols, 8), i64(num_sms()) * 8)));
+    p->nitems = int(items.size());
+    p->smem = bs::bs_smem_bytes<float>(TR_MAXN);
     int st = MBG_OK;
     if (p->count > 0) {
-        st = upload(p, v);
+        int per_sm = 0;
+        cudaError_t e = cudaFuncSetAttribute(grouped_block_strsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(p->smem));
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_block_strsm_kernel, bs::BS_THREADS,
+                                                              p->smem);
+        if (e != cudaSuccess) {
+            set_error("grouped strsm kernel set-up", e);
+            st = MBG_ERR_CUDA;
+        } else {
+            p->grid = int(imax(1, imin(i64(items.size()), i64(num_sms()) * imax(per_sm, 1))));
+            const size_t dbytes = (sizeof(TrsmDesc) * v.size() + 255) / 256 * 256;
+            const size_t ibytes = sizeof(TrsmItem) * items.size();
+            e = cudaMalloc(&p->table, dbytes + ibytes);
+            if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&p->counter), sizeof(unsigned long long));
+            if (e == cudaSuccess) {
+                p->items = static_cast<char*>(p->table) + dbytes;
+                e = cudaMemcpy(p->table, v.data(), sizeof(TrsmDesc) * v.size(), cudaMemcpyHostToDevice);
+            }
+            if (e == cudaSuccess) e = cudaMemcpy(p->items, items.data(), ibytes, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                set_error("grouped strsm plan upload", e);
+                st = MBG_ERR_CUDA;
+            }
+        }
         if (!st) st = capture_plan(p);
     }
     if (st) {
