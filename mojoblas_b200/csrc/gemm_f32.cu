@@ -1,0 +1,227 @@
+// Plain FP32 GEMM on the CUDA cores, 128 x 128 tiles — the single-precision
+// drop-in arithmetic for mojoBLAS gemm (src/level3/gemm.mojo:56-377, v11
+// :2092-2436) and, with a triangular tile schedule, ssyrk
+// (src/level3/syrk.mojo:20-200).
+//
+// One 256-thread CTA computes a 128 x 128 tile; every thread accumulates an
+// 8 x 8 register block (rows tx*4+{0..3} and 64+tx*4+{0..3}, columns likewise
+// from ty) with one FMA per product, each element's sum running over k in
+// ascending order as in the reference's column loops.  K advances in slabs of 16
+// through a 3-stage cp.async pipeline straight into shared memory (no register
+// round trip, so global latency overlaps two slabs of arithmetic): an operand
+// that is contiguous along m (n) and 16-byte aligned with a leading dimension
+// divisible by 4 is copied 16 bytes at a time, any other operand element by
+// element into the same k-major tiles.  Rows of the tiles are padded to 132
+// floats.  beta == 0 writes C without reading it, beta == 1 adds with an L2
+// reduction (one add per element, the same rounding as fma(1, c, v)).
+#include "mbg_internal.cuh"
+
+namespace mbg {
+
+namespace {
+
+constexpr int FK = 16, FSTAGES = 3, FT = 128, FLD = FT + 4, FNT = 256;
+
+__device__ __forceinline__ void cpa4(void* dst, const void* src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+// 16 bytes of which the first `bytes` are read, the rest zero-filled
+__device__ __forceinline__ void cpa16(void* dst, const void* src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void f32_tri_tile(i64 t, i64& ti, i64& tj) {
+    i64 r = (i64)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((r + 1) * (r + 2) / 2 <= t) ++r;
+    while (r * (r + 1) / 2 > t) --r;
+    ti = r;
+    tj = t - r * (r + 1) / 2;
+}
+
+// Copies one FK-deep slab of an operand into a [k][FLD] tile.  MAJ: the operand
+// is contiguous along the tile's row index (m or n) in memory; else along k.
+// VEC: 16-byte copies along the contiguous index.
+template <bool MAJ, bool VEC>
+__device__ __forceinline__ void f32_stage(float* tile, const float* __restrict__ P, i64 ld, i64 r0, i64 rows,
+                                          i64 k0, i64 k, int tid) {
+    if (MAJ && VEC) {  // 4 consecutive rows of one k per copy
+#pragma unroll
+        for (int e0 = tid; e0 < FT * FK / 4; e0 += FNT) {
+            const int e = e0 * 4, i = e % FT, l = e / FT;
+            const i64 gi = r0 + i, gl = k0 + l;
+            const i64 left = (gl < k) ? rows - gi : 0;
+            const int bytes = left >= 4 ? 16 : (left > 0 ? int(left) * 4 : 0);
+            cpa16(tile + l * FLD + i, bytes ? P + gi + gl * ld : P, bytes);
+        }
+    } else {
+#pragma unroll
+        for (int e = tid; e < FT * FK; e += FNT) {
+            int i, l;
+            if (MAJ) { i = e % FT; l = e / FT; } else { l = e % FK; i = e / FK; }  // contiguous index first
+            const i64 gi = r0 + i, gl = k0 + l;
+            const bool v = gi < rows && gl < k;
+            cpa4(tile + l * FLD + i, v ? (MAJ ? P + gi + gl * ld : P + gl + gi * ld) : P, v);
+        }
+    }
+}
+
+template <bool TA, bool TB, int TRI, bool VA, bool VB>
+__global__ void __launch_bounds__(FNT, 2)
+gemm_f32_kernel(i64 m, i64 n, i64 k, float alpha, const float* __restrict__ A, i64 lda,
+                const float* __restrict__ B, i64 ldb, float beta, float* __restrict__ C, i64 ldc) {
+    extern __shared__ __align__(16) float fsm[];
+    float* As = fsm;                               // [stage][k][FLD]
+    float* Bs = fsm + size_t(FSTAGES) * FK * FLD;  // [stage][k][FLD]
+    i64 tm, tn;
+    if (TRI == 0) {
+        tm = blockIdx.x;
+        tn = blockIdx.y;
+    } else {
+        i64 ti, tj;
+        f32_tri_tile(blockIdx.x, ti, tj);
+        if (TRI == 1) { tm = ti; tn = tj; } else { tm = tj; tn = ti; }
+    }
+    const i64 m0 = tm * FT, n0 = tn * FT;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+
+    // op(A) is m-contiguous when A is not transposed; op(B) is n-contiguous when B is
+    auto issue = [&](i64 kt, int st) {
+        f32_stage<!TA, VA>(As + size_t(st) * FK * FLD, A, lda, m0, m, kt * FK, k, tid);
+        f32_stage<TB, VB>(Bs + size_t(st) * FK * FLD, B, ldb, n0, n, kt * FK, k, tid);
+    };
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+
+    const i64 nk = (k + FK - 1) / FK;
+#pragma unroll
+    for (int s = 0; s < FSTAGES - 1; ++s) {
+        if (s < nk) issue(s, s);
+        cpa_commit();
+    }
+    for (i64 kt = 0; kt < nk; ++kt) {
+        cpa_wait<FSTAGES - 2>();
+        __syncthreads();  // slab kt has landed; the buffer of slab kt - 1 is free
+        if (kt + FSTAGES - 1 < nk) issue(kt + FSTAGES - 1, int((kt + FSTAGES - 1) % FSTAGES));
+        cpa_commit();
+        const float* as = As + size_t(kt % FSTAGES) * FK * FLD;
+        const float* bs = Bs + size_t(kt % FSTAGES) * FK * FLD;
+#pragma unroll
+        for (int l = 0; l < FK; ++l) {
+            const float4 a0 = *reinterpret_cast<const float4*>(as + l * FLD + tx * 4);
+            const float4 a1 = *reinterpret_cast<const float4*>(as + l * FLD + 64 + tx * 4);
+            const float4 b0 = *reinterpret_cast<const float4*>(bs + l * FLD + ty * 4);
+            const float4 b1 = *reinterpret_cast<const float4*>(bs + l * FLD + 64 + ty * 4);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+    }
+    cpa_wait<0>();
+
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const i64 gj = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
+        if (gj >= n) continue;
+        float cv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const i64 gi = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+            cv[i] = (gi < m && beta != 0.0f && beta != 1.0f) ? C[gi + gj * ldc] : 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const i64 gi = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
+            if (gi >= m) continue;
+            if (TRI == 1 && gi < gj) continue;
+            if (TRI == 2 && gi > gj) continue;
+            float* cp = C + gi + gj * ldc;
+            const float v = alpha * acc[i][j];
+            if (beta == 0.0f) *cp = v;
+            else if (beta == 1.0f) atomicAdd(cp, v);
+            else *cp = fmaf(beta, cv[i], v);
+        }
+    }
+}
+
+constexpr size_t F32_SMEM = sizeof(float) * size_t(FSTAGES) * FK * FLD * 2;
+
+template <int TRI, bool VA, bool VB>
+int launch_f32_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
+                 const float* b, i64 ldb, float beta, float* c, i64 ldc) {
+    static unsigned configured = 0;  // one bit per device: the 50 KB of shared memory needs an opt-in
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    if (dev >= 32 || !(configured & (1u << dev))) {
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<false, false, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<false, true, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<true, false, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<true, true, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
+        if (dev < 32) configured |= 1u << dev;
+    }
+    cudaStream_t s = stream();
+#define F32(TA_, TB_) \
+    gemm_f32_kernel<TA_, TB_, TRI, VA, VB><<<grid, FNT, F32_SMEM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    if (!ta && !tb) F32(false, false);
+    else if (!ta && tb) F32(false, true);
+    else if (ta && !tb) F32(true, false);
+    else F32(true, true);
+#undef F32
+    return check_launch("gemm_f32");
+}
+
+// 16-byte copies need the operand contiguous along m (n), a 16-byte aligned base and ld % 4 == 0
+inline bool f32_vec(bool contiguous_rows, const float* p, i64 ld) {
+    return contiguous_rows && reinterpret_cast<uintptr_t>(p) % 16 == 0 && ld % 4 == 0;
+}
+
+template <int TRI>
+int launch_f32(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
+               const float* b, i64 ldb, float beta, float* c, i64 ldc) {
+    const bool va = f32_vec(!ta, a, lda), vb = f32_vec(tb, b, ldb);
+    if (va && vb) return launch_f32_v<TRI, true, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (va) return launch_f32_v<TRI, true, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (vb) return launch_f32_v<TRI, false, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    return launch_f32_v<TRI, false, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+}  // namespace
+
+// C := alpha op(A) op(B) + beta C, 128 x 128 tiles (alpha != 0, k > 0).
+int sgemm_f32(char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda, const float* b,
+              i64 ldb, float beta, float* c, i64 ldc) {
+    ProfScope prof("gemm_f32");
+    const i64 gm = cdiv(m, FT), gn = cdiv(n, FT);
+    if (gn > 65535 || gm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    return launch_f32<0>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha, a, lda, b, ldb,
+                         beta, c, ldc);
+}
+
+// Lower ('L') or upper triangle of C := alpha op(A) op(B) + beta C (ssyrk).
+int sgemmt_f32(char uplo, char ta, char tb, i64 n, i64 k, float alpha, const float* a, i64 lda,
+               const float* b, i64 ldb, float beta, float* c, i64 ldc) {
+    ProfScope prof("gemm_f32");
+    const i64 t = cdiv(n, FT);
+    const i64 tiles = t * (t + 1) / 2;
+    if (tiles > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    if (is_l(uplo))
+        return launch_f32<1>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    return launch_f32<2>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+}  // namespace mbg

@@ -242,6 +242,8 @@ int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 l
                                      a, lda, b, ldb, beta, c, ldc);
     }
     if (gn > 65535 || gm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    if constexpr (sizeof(T) == 4)
+        if (!tuning().plain_fp32_staged) return sgemm_f32(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     return launch_gemm<T, 0, 128>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha,
                                   a, lda, b, ldb, beta, c, ldc);
 }
@@ -254,6 +256,8 @@ int gemmt_plain(char uplo, char ta, char tb, i64 n, i64 k, T alpha, const T* a, 
     if constexpr (sizeof(T) == 8)
         if (!tuning().plain_fp64_simt)
             return dgemmt_dmma(uplo, ta, tb, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if constexpr (sizeof(T) == 4)
+        if (!tuning().plain_fp32_staged) return sgemmt_f32(uplo, ta, tb, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     const i64 t = cdiv(n, 128);
     const i64 tiles = t * (t + 1) / 2;
     if (tiles > 0x7fffffff) return MBG_ERR_UNSUPPORTED;

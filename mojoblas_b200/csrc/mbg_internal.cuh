@@ -103,6 +103,7 @@ struct Tuning {
     i64 trsm_block_rows = 512;   // diagonal blocks solved in one fused launch (<= 64: leaves + gemm)
     i64 trsm_block_min_cols = 64;    // ... when there are at least this many right-hand sides
     i64 plain_fp64_simt = 0;     // 1: plain FP64 gemm/syrk on the CUDA cores instead of the FP64 tensor pipe
+    i64 plain_fp32_staged = 0;   // 1: plain FP32 128-tiles staged through registers (the earlier kernel)
 };
 Tuning& tuning();
 
@@ -110,6 +111,11 @@ Tuning& tuning();
 template <typename T>
 int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 lda,
                const T* b, i64 ldb, T beta, T* c, i64 ldc);
+// FP32 CUDA-core GEMM, 128 x 128 tiles, cp.async pipeline (gemm_f32.cu): alpha != 0, k > 0
+int sgemm_f32(char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda, const float* b,
+              i64 ldb, float beta, float* c, i64 ldc);
+int sgemmt_f32(char uplo, char ta, char tb, i64 n, i64 k, float alpha, const float* a, i64 lda,
+               const float* b, i64 ldb, float beta, float* c, i64 ldc);
 // FP64 tensor-pipe GEMM (gemm_dmma.cu): alpha != 0, k > 0
 int dgemm_dmma(char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
                const double* b, i64 ldb, double beta, double* c, i64 ldc);
