@@ -2,6 +2,8 @@
 // routines), quick returns, host-operand staging and precision-mode dispatch.
 #include "mbg_internal.cuh"
 
+#include <vector>
+
 namespace mbg {
 
 // ---- argument checks ----------------------------------------------------------
@@ -74,12 +76,102 @@ int dgemm_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, doub
 
 // ---- staged drivers ------------------------------------------------------------
 template <typename T>
+static int gemm_compute(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 lda,
+                        const T* b, i64 ldb, T beta, T* c, i64 ldc) {
+    if (sizeof(T) == 4)
+        return sgemm_mode(mode, ta, tb, m, n, k, (float)alpha, (const float*)a, lda, (const float*)b, ldb,
+                          (float)beta, (float*)c, ldc);
+    return dgemm_mode(mode, slices, ta, tb, m, n, k, (double)alpha, (const double*)a, lda, (const double*)b, ldb,
+                      (double)beta, (double*)c, ldc);
+}
+
+// Large gemm with host operands: the host <-> device copies overlap the
+// arithmetic.  C is cut into GEMM_PIPE_BLOCKS column blocks.  A copy stream
+// brings op(A) over first and then, block by block, the columns of op(B) (and
+// of C when beta != 0); the library's stream computes each block as soon as its
+// operands have landed; a second copy stream returns each finished block of C,
+// so the two directions of the PCIe link run at the same time.  The device
+// buffers are the same full-size copies the sequential path uses.
+constexpr int GEMM_PIPE_BLOCKS = 4;
+
+template <typename T>
+static bool gemm_pipeline_pays(const T* a, const T* b, const T* c, i64 m, i64 n, i64 k) {
+    if (n < 4096 || double(m) * double(n) * double(k) < double(1ll << 34)) return false;
+    return !is_device_pointer(a) || !is_device_pointer(b) || !is_device_pointer(c);
+}
+
+template <typename T>
+static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, T alpha,
+                               const T* a, i64 lda, const T* b, i64 ldb, T beta, T* c, i64 ldc) {
+    cudaStream_t s = stream(), sin = nullptr, sout = nullptr;
+    MBG_TRY(copy_streams(&sin, &sout));
+    const bool ha = !is_device_pointer(a), hb = !is_device_pointer(b), hc = !is_device_pointer(c);
+    const i64 ar = is_n(ta) ? m : k, ac = is_n(ta) ? k : m;  // stored shape of A
+    const i64 br = is_n(tb) ? k : n, bc = is_n(tb) ? n : k;  // stored shape of B
+    const size_t e = sizeof(T);
+    Workspace wa, wb, wc;
+    const T* da = a;
+    const T* db = b;
+    T* dc = c;
+    i64 dlda = lda, dldb = ldb, dldc = ldc;
+    if (ha) { MBG_TRY(wa.reserve(e * size_t(ar) * size_t(ac))); da = wa.as<T>(); dlda = ar; }
+    if (hb) { MBG_TRY(wb.reserve(e * size_t(br) * size_t(bc))); db = wb.as<T>(); dldb = br; }
+    if (hc) { MBG_TRY(wc.reserve(e * size_t(m) * size_t(n))); dc = wc.as<T>(); dldc = m; }
+
+    std::vector<cudaEvent_t> ev(2 * GEMM_PIPE_BLOCKS + 2);
+    for (auto& x : ev) MBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    cudaEvent_t ev_start = ev[0], ev_end = ev[1];
+    MBG_CUDA(cudaEventRecord(ev_start, s));  // earlier work on the library stream (workspace reuse) first
+    MBG_CUDA(cudaStreamWaitEvent(sin, ev_start, 0));
+    MBG_CUDA(cudaStreamWaitEvent(sout, ev_start, 0));
+    if (ha)
+        MBG_CUDA(cudaMemcpy2DAsync(const_cast<T*>(da), size_t(ar) * e, a, size_t(lda) * e, size_t(ar) * e,
+                                   size_t(ac), cudaMemcpyHostToDevice, sin));
+    const i64 nb = cdiv(cdiv(n, GEMM_PIPE_BLOCKS), 256) * 256;
+    int st = MBG_OK;
+    int used = 0;
+    for (i64 j0 = 0; j0 < n && !st; j0 += nb, ++used) {
+        const i64 w = imin(nb, n - j0);
+        cudaEvent_t ev_in = ev[2 + 2 * used], ev_done = ev[3 + 2 * used];
+        // op(B)[:, j0 : j0 + w] is columns j0.. of B ('N') or rows j0.. of B ('T')
+        if (hb) {
+            if (is_n(tb))
+                MBG_CUDA(cudaMemcpy2DAsync(const_cast<T*>(db) + j0 * dldb, size_t(dldb) * e, b + j0 * ldb,
+                                           size_t(ldb) * e, size_t(k) * e, size_t(w), cudaMemcpyHostToDevice, sin));
+            else
+                MBG_CUDA(cudaMemcpy2DAsync(const_cast<T*>(db) + j0, size_t(dldb) * e, b + j0, size_t(ldb) * e,
+                                           size_t(w) * e, size_t(k), cudaMemcpyHostToDevice, sin));
+        }
+        if (hc && beta != T(0))
+            MBG_CUDA(cudaMemcpy2DAsync(dc + j0 * dldc, size_t(dldc) * e, c + j0 * ldc, size_t(ldc) * e,
+                                       size_t(m) * e, size_t(w), cudaMemcpyHostToDevice, sin));
+        MBG_CUDA(cudaEventRecord(ev_in, sin));
+        MBG_CUDA(cudaStreamWaitEvent(s, ev_in, 0));
+        const T* bj = is_n(tb) ? db + j0 * dldb : db + j0;
+        st = gemm_compute<T>(mode, slices, ta, tb, m, w, k, alpha, da, dlda, bj, dldb, beta, dc + j0 * dldc, dldc);
+        MBG_CUDA(cudaEventRecord(ev_done, s));
+        if (hc) {
+            MBG_CUDA(cudaStreamWaitEvent(sout, ev_done, 0));
+            MBG_CUDA(cudaMemcpy2DAsync(c + j0 * ldc, size_t(ldc) * e, dc + j0 * dldc, size_t(dldc) * e,
+                                       size_t(m) * e, size_t(w), cudaMemcpyDeviceToHost, sout));
+        }
+    }
+    MBG_CUDA(cudaEventRecord(ev_end, sout));
+    MBG_CUDA(cudaStreamWaitEvent(s, ev_end, 0));  // the library stream completes after the last copy back
+    const int fin = finish_call(true);
+    for (auto& x : ev) cudaEventDestroy(x);
+    return st ? st : fin;
+}
+
+template <typename T>
 static int gemm_entry(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, T alpha,
                       const T* a, i64 lda, const T* b, i64 ldb, T beta, T* c, i64 ldc) {
     int info = gemm_info(ta, tb, m, n, k, lda, ldb, ldc);
     if (info) return info;
     if (m == 0 || n == 0) return MBG_OK;
     const bool need_ab = !(alpha == T(0) || k == 0);
+    if (need_ab && gemm_pipeline_pays<T>(a, b, c, m, n, k))
+        return gemm_host_pipelined<T>(mode, slices, ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     Operand A, B, Cc;
     if (need_ab) {
         MBG_TRY(A.prepare(a, is_n(ta) ? m : k, is_n(ta) ? k : m, lda, sizeof(T), true, false));

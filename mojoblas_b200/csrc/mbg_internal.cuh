@@ -49,6 +49,10 @@ void set_error_msg(const std::string& msg);
 // Checks the launch that was just enqueued (configuration errors only).
 int check_launch(const char* name);
 
+// Two non-blocking streams of the current device (host->device and device->host
+// copies of the pipelined host path), created on first use and kept.
+int copy_streams(cudaStream_t* in, cudaStream_t* out);
+
 // ---- device workspace: a per-device cache of blocks, stream-ordered reuse ---
 // Blocks are handed out for the duration of one library call and returned to
 // the cache when the call finishes enqueueing; all library work runs on one

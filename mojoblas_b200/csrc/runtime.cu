@@ -24,6 +24,7 @@ struct DeviceCache {
     std::map<void*, size_t> sizes;
     int* err_host = nullptr;                    // mapped pinned flag
     int* err_dev = nullptr;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;  // pipelined host path
 };
 std::map<int, DeviceCache> g_cache;
 
@@ -164,6 +165,17 @@ int Operand::finish() {
     if (staged && copy_out)
         MBG_CUDA(cudaMemcpy2DAsync(const_cast<void*>(user), size_t(ld) * elem, dev, size_t(rows) * elem,
                                    size_t(rows) * elem, size_t(cols), cudaMemcpyDeviceToHost, stream()));
+    return MBG_OK;
+}
+
+// ---- copy streams of the pipelined host path ---------------------------------------
+int copy_streams(cudaStream_t* in, cudaStream_t* out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    DeviceCache& dc = g_cache[current_device()];
+    if (!dc.copy_in) MBG_CUDA(cudaStreamCreateWithFlags(&dc.copy_in, cudaStreamNonBlocking));
+    if (!dc.copy_out) MBG_CUDA(cudaStreamCreateWithFlags(&dc.copy_out, cudaStreamNonBlocking));
+    *in = dc.copy_in;
+    *out = dc.copy_out;
     return MBG_OK;
 }
 
