@@ -1,11 +1,12 @@
-// Plain FP32 GEMM on the CUDA cores, 128 x 128 tiles — the single-precision
+// Plain FP32 GEMM on the CUDA cores, 128 x 128 or 64 x 64 tiles — the single-precision
 // drop-in arithmetic for mojoBLAS gemm (src/level3/gemm.mojo:56-377, v11
 // :2092-2436) and, with a triangular tile schedule, ssyrk
 // (src/level3/syrk.mojo:20-200).
 //
-// One 256-thread CTA computes a 128 x 128 tile; every thread accumulates an
+// One 256-thread CTA computes a 128 x 128 tile, every thread accumulating an
 // 8 x 8 register block (rows tx*4+{0..3} and 64+tx*4+{0..3}, columns likewise
-// from ty) with one FMA per product, each element's sum running over k in
+// from ty), or — for launches under two waves of those — a 64 x 64 tile with a
+// 4 x 4 block per thread; one FMA per product, each element's sum running over k in
 // ascending order as in the reference's column loops.  K advances in slabs of 16
 // through a 3-stage cp.async pipeline straight into shared memory (no register
 // round trip, so global latency overlaps two slabs of arithmetic): an operand
@@ -20,7 +21,11 @@ namespace mbg {
 
 namespace {
 
-constexpr int FK = 16, FSTAGES = 3, FT = 128, FLD = FT + 4, FNT = 256;
+constexpr int FK = 16, FSTAGES = 3, FNT = 256;
+template <int FT> struct FTile {
+    static constexpr int LD = FT + 4;     // tile row (floats)
+    static constexpr int TM = FT / 16;    // rows (and columns) per thread: 8 or 4
+};
 
 __device__ __forceinline__ void cpa4(void* dst, const void* src, bool valid) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -46,9 +51,10 @@ __device__ __forceinline__ void f32_tri_tile(i64 t, i64& ti, i64& tj) {
 // Copies one FK-deep slab of an operand into a [k][FLD] tile.  MAJ: the operand
 // is contiguous along the tile's row index (m or n) in memory; else along k.
 // VEC: 16-byte copies along the contiguous index.
-template <bool MAJ, bool VEC>
+template <int FT, bool MAJ, bool VEC>
 __device__ __forceinline__ void f32_stage(float* tile, const float* __restrict__ P, i64 ld, i64 r0, i64 rows,
                                           i64 k0, i64 k, int tid) {
+    constexpr int FLD = FTile<FT>::LD;
     if (MAJ && VEC) {  // 4 consecutive rows of one k per copy
 #pragma unroll
         for (int e0 = tid; e0 < FT * FK / 4; e0 += FNT) {
@@ -70,10 +76,11 @@ __device__ __forceinline__ void f32_stage(float* tile, const float* __restrict__
     }
 }
 
-template <bool TA, bool TB, int TRI, bool VA, bool VB>
-__global__ void __launch_bounds__(FNT, 2)
+template <int FT, bool TA, bool TB, int TRI, bool VA, bool VB>
+__global__ void __launch_bounds__(FNT, FT == 128 ? 2 : 4)
 gemm_f32_kernel(i64 m, i64 n, i64 k, float alpha, const float* __restrict__ A, i64 lda,
                 const float* __restrict__ B, i64 ldb, float beta, float* __restrict__ C, i64 ldc) {
+    constexpr int FLD = FTile<FT>::LD, TM = FTile<FT>::TM;
     extern __shared__ __align__(16) float fsm[];
     float* As = fsm;                               // [stage][k][FLD]
     float* Bs = fsm + size_t(FSTAGES) * FK * FLD;  // [stage][k][FLD]
@@ -91,15 +98,15 @@ gemm_f32_kernel(i64 m, i64 n, i64 k, float alpha, const float* __restrict__ A, i
 
     // op(A) is m-contiguous when A is not transposed; op(B) is n-contiguous when B is
     auto issue = [&](i64 kt, int st) {
-        f32_stage<!TA, VA>(As + size_t(st) * FK * FLD, A, lda, m0, m, kt * FK, k, tid);
-        f32_stage<TB, VB>(Bs + size_t(st) * FK * FLD, B, ldb, n0, n, kt * FK, k, tid);
+        f32_stage<FT, !TA, VA>(As + size_t(st) * FK * FLD, A, lda, m0, m, kt * FK, k, tid);
+        f32_stage<FT, TB, VB>(Bs + size_t(st) * FK * FLD, B, ldb, n0, n, kt * FK, k, tid);
     };
 
-    float acc[8][8];
+    float acc[TM][TM];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < TM; ++j) acc[i][j] = 0.0f;
 
     const i64 nk = (k + FK - 1) / FK;
 #pragma unroll
@@ -116,32 +123,37 @@ gemm_f32_kernel(i64 m, i64 n, i64 k, float alpha, const float* __restrict__ A, i
         const float* bs = Bs + size_t(kt % FSTAGES) * FK * FLD;
 #pragma unroll
         for (int l = 0; l < FK; ++l) {
+            float a[TM], b[TM];
             const float4 a0 = *reinterpret_cast<const float4*>(as + l * FLD + tx * 4);
-            const float4 a1 = *reinterpret_cast<const float4*>(as + l * FLD + 64 + tx * 4);
             const float4 b0 = *reinterpret_cast<const float4*>(bs + l * FLD + ty * 4);
-            const float4 b1 = *reinterpret_cast<const float4*>(bs + l * FLD + 64 + ty * 4);
-            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
+            b[0] = b0.x; b[1] = b0.y; b[2] = b0.z; b[3] = b0.w;
+            if constexpr (TM == 8) {
+                const float4 a1 = *reinterpret_cast<const float4*>(as + l * FLD + 64 + tx * 4);
+                const float4 b1 = *reinterpret_cast<const float4*>(bs + l * FLD + 64 + ty * 4);
+                a[TM - 4] = a1.x; a[TM - 3] = a1.y; a[TM - 2] = a1.z; a[TM - 1] = a1.w;
+                b[TM - 4] = b1.x; b[TM - 3] = b1.y; b[TM - 2] = b1.z; b[TM - 1] = b1.w;
+            }
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < TM; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
         }
     }
     cpa_wait<0>();
 
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < TM; ++j) {
         const i64 gj = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
         if (gj >= n) continue;
-        float cv[8];
+        float cv[TM];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < TM; ++i) {
             const i64 gi = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
             cv[i] = (gi < m && beta != 0.0f && beta != 1.0f) ? C[gi + gj * ldc] : 0.0f;
         }
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < TM; ++i) {
             const i64 gi = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
             if (gi >= m) continue;
             if (TRI == 1 && gi < gj) continue;
@@ -155,28 +167,30 @@ gemm_f32_kernel(i64 m, i64 n, i64 k, float alpha, const float* __restrict__ A, i
     }
 }
 
-constexpr size_t F32_SMEM = sizeof(float) * size_t(FSTAGES) * FK * FLD * 2;
+template <int FT>
+constexpr size_t f32_smem() { return sizeof(float) * size_t(FSTAGES) * FK * FTile<FT>::LD * 2; }
 
-template <int TRI, bool VA, bool VB>
+template <int FT, int TRI, bool VA, bool VB>
 int launch_f32_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
                  const float* b, i64 ldb, float beta, float* c, i64 ldc) {
-    static unsigned configured = 0;  // one bit per device: the 50 KB of shared memory needs an opt-in
+    constexpr size_t SM = f32_smem<FT>();
+    static unsigned configured = 0;  // one bit per device: more than 48 KB of shared memory needs an opt-in
     int dev = 0;
     MBG_CUDA(cudaGetDevice(&dev));
     if (dev >= 32 || !(configured & (1u << dev))) {
-        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<false, false, TRI, VA, VB>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
-        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<false, true, TRI, VA, VB>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
-        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<true, false, TRI, VA, VB>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
-        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<true, true, TRI, VA, VB>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F32_SMEM));
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<FT, false, false, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<FT, false, true, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<FT, true, false, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
+        MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<FT, true, true, TRI, VA, VB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
         if (dev < 32) configured |= 1u << dev;
     }
     cudaStream_t s = stream();
 #define F32(TA_, TB_) \
-    gemm_f32_kernel<TA_, TB_, TRI, VA, VB><<<grid, FNT, F32_SMEM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    gemm_f32_kernel<FT, TA_, TB_, TRI, VA, VB><<<grid, FNT, SM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
     if (!ta && !tb) F32(false, false);
     else if (!ta && tb) F32(false, true);
     else if (ta && !tb) F32(true, false);
@@ -190,38 +204,45 @@ inline bool f32_vec(bool contiguous_rows, const float* p, i64 ld) {
     return contiguous_rows && reinterpret_cast<uintptr_t>(p) % 16 == 0 && ld % 4 == 0;
 }
 
-template <int TRI>
+template <int FT, int TRI>
 int launch_f32(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
                const float* b, i64 ldb, float beta, float* c, i64 ldc) {
     const bool va = f32_vec(!ta, a, lda), vb = f32_vec(tb, b, ldb);
-    if (va && vb) return launch_f32_v<TRI, true, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    if (va) return launch_f32_v<TRI, true, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    if (vb) return launch_f32_v<TRI, false, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    return launch_f32_v<TRI, false, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (va && vb) return launch_f32_v<FT, TRI, true, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (va) return launch_f32_v<FT, TRI, true, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (vb) return launch_f32_v<FT, TRI, false, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    return launch_f32_v<FT, TRI, false, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
 }
 
 }  // namespace
 
-// C := alpha op(A) op(B) + beta C, 128 x 128 tiles (alpha != 0, k > 0).
+// C := alpha op(A) op(B) + beta C (alpha != 0, k > 0): 128 x 128 tiles, or 64 x 64
+// tiles (4 x 4 per thread) when 128-tiles would fill fewer than two waves.
 int sgemm_f32(char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda, const float* b,
               i64 ldb, float beta, float* c, i64 ldc) {
     ProfScope prof("gemm_f32");
-    const i64 gm = cdiv(m, FT), gn = cdiv(n, FT);
+    const i64 gm = cdiv(m, 128), gn = cdiv(n, 128);
+    if (gm * gn < 2 * 148) {
+        const i64 sm = cdiv(m, 64), sn = cdiv(n, 64);
+        if (sn > 65535 || sm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+        return launch_f32<64, 0>(is_t(ta), is_t(tb), dim3((unsigned)sm, (unsigned)sn), m, n, k, alpha, a, lda, b,
+                                 ldb, beta, c, ldc);
+    }
     if (gn > 65535 || gm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
-    return launch_f32<0>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha, a, lda, b, ldb,
-                         beta, c, ldc);
+    return launch_f32<128, 0>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha, a, lda, b,
+                              ldb, beta, c, ldc);
 }
 
 // Lower ('L') or upper triangle of C := alpha op(A) op(B) + beta C (ssyrk).
 int sgemmt_f32(char uplo, char ta, char tb, i64 n, i64 k, float alpha, const float* a, i64 lda,
                const float* b, i64 ldb, float beta, float* c, i64 ldc) {
     ProfScope prof("gemm_f32");
-    const i64 t = cdiv(n, FT);
+    const i64 t = cdiv(n, 128);
     const i64 tiles = t * (t + 1) / 2;
     if (tiles > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
     if (is_l(uplo))
-        return launch_f32<1>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    return launch_f32<2>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+        return launch_f32<128, 1>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    return launch_f32<128, 2>(is_t(ta), is_t(tb), dim3((unsigned)tiles), n, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
 }
 
 }  // namespace mbg

@@ -234,6 +234,8 @@ int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 l
     if constexpr (sizeof(T) == 8)
         if (!tuning().plain_fp64_simt)
             return dgemm_dmma(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if constexpr (sizeof(T) == 4)
+        if (!tuning().plain_fp32_staged) return sgemm_f32(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     const i64 gm = cdiv(m, 128), gn = cdiv(n, 128);
     if (gm * gn < 2 * 148) {  // under two waves of 128 x 128 tiles: use 64 x 64 tiles
         const i64 sm = cdiv(m, 64), sn = cdiv(n, 64);
@@ -242,8 +244,6 @@ int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 l
                                      a, lda, b, ldb, beta, c, ldc);
     }
     if (gn > 65535 || gm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
-    if constexpr (sizeof(T) == 4)
-        if (!tuning().plain_fp32_staged) return sgemm_f32(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
     return launch_gemm<T, 0, 128>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha,
                                   a, lda, b, ldb, beta, c, ldc);
 }

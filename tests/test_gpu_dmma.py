@@ -88,14 +88,14 @@ def test_dsyrk_tensor_pipe_triangle(env):
 
 
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")])
-@pytest.mark.parametrize("m,n,k", [(2200, 2180, 33), (2304, 2304, 64), (2177, 2201, 130)])
+@pytest.mark.parametrize("m,n,k", [(2200, 2180, 33), (2304, 2304, 64), (2177, 2201, 130), (300, 521, 257)])
 @pytest.mark.parametrize("path", ["vec16", "odd_ld", "offset"])
 @pytest.mark.parametrize("beta", [0.0, 1.0, 0.5])
 def test_sgemm_pipelined_copy_paths(env, ta, tb, m, n, k, path, beta):
     """Plain FP32 128-tiles (cp.async pipeline): 16-byte copies need an operand contiguous along
     m (n), a 16-byte aligned base and ld % 4 == 0; every other operand is copied element-wise.
-    The sizes give at least two waves of 128 x 128 tiles (smaller launches use 64 x 64 tiles),
-    with ragged edges in m, n and k; tolerance 1e-6 sqrt(k)."""
+    Three sizes give at least two waves of 128 x 128 tiles, the last one the 64 x 64 tiles of
+    smaller launches, all with ragged edges in m, n and k; tolerance 1e-6 sqrt(k)."""
     torch, lib = env
     rng = np.random.default_rng(m + 5 * n + 11 * k)
     ar, ac = (m, k) if ta == "N" else (k, m)
