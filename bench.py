@@ -175,7 +175,7 @@ def run_cfg3(torch, lib, L, stream):
 
     tr = {}
     for label, md, s_, r_ in (("plain_fp64", L.MODE_PLAIN, 0, 0), ("ozaki_s8", L.MODE_OZAKI, 8, 0),
-                              ("ozaki_s6_ir1", L.MODE_OZAKI, 6, 1)):
+                              ("ozaki_s4_ir1", L.MODE_OZAKI, 4, 1)):
         tcall(md, s_, r_)
         torch.cuda.synchronize()
         got = X.cpu().numpy().T[:, cols]

@@ -308,10 +308,38 @@ int solve_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i
     return solve_left<T>(mode, slices, lower, trans, unit, m1, n, a11, lda, b, ldb);
 }
 
-// R -= tri(op(A)) X, left side.
+// W[0:m, 0:m] = tri(op(A)) as a dense column-major block: the effective triangle
+// (unit diagonal when UNIT), zeros elsewhere; the other triangle of A is not read.
+template <typename T>
+__global__ void tri_dense_kernel(i64 m, const T* __restrict__ A, i64 lda, bool lower, bool trans, bool unit,
+                                 T* __restrict__ W) {
+    for (i64 l = blockIdx.y; l < m; l += gridDim.y)
+        for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x) {
+            const bool in = lower ? i > l : i < l;
+            T v = T(0);
+            if (i == l) v = unit ? T(1) : (trans ? A[l + i * lda] : A[i + l * lda]);
+            else if (in) v = trans ? A[l + i * lda] : A[i + l * lda];
+            W[i + l * m] = v;
+        }
+}
+
+// R -= tri(op(A)) X, left side.  Diagonal blocks up to the fused solve's size
+// are one plain GEMM with a dense copy of the triangle (input precision, all of
+// R's rows in parallel); larger ones recurse with the accurate products between.
 template <typename T>
 int residual_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, const T* a,
                   i64 lda, const T* x, i64 ldx, T* r, i64 ldr) {
+    if (m > NB && m <= block_rows<T>(n)) {
+        Workspace ww;
+        MBG_TRY(ww.reserve(sizeof(T) * size_t(m) * size_t(m)));
+        {
+            ProfScope prof("trsm_tri_dense");
+            dim3 g((unsigned)imin(cdiv(m, 256), 64), (unsigned)imin(m, 65535));
+            tri_dense_kernel<T><<<g, 256, 0, stream()>>>(m, a, lda, lower, trans, unit, ww.as<T>());
+            MBG_TRY(check_launch("trsm_tri_dense"));
+        }
+        return gemm_plain<T>('N', 'N', m, n, m, T(-1), ww.as<T>(), m, x, ldx, T(1), r, ldr);
+    }
     if (m <= NB) return launch_diag_residual<T>(lower, trans, unit, (int)m, n, a, lda, x, ldx, r, ldr);
     const i64 m1 = split_point(m), m2 = m - m1;
     const char tc = trans ? 'T' : 'N';
