@@ -9,8 +9,9 @@
 //  * sgemm: problems are ordered by k * m * n descending and cut into square
 //    tiles (64 or 128, from the tuning table); persistent CTAs take tiles from
 //    an atomic counter (largest first, so the tail is short), locate the problem
-//    by binary search over the tile prefix sums, and run the plain FP32 tile
-//    code of gemm_simt.cu with that problem's transposes, alpha and beta.
+//    by binary search over the tile prefix sums, and run the pipelined FP32
+//    tile code of gemm_f32_tile.cuh with that problem's transposes, alpha and
+//    beta (16-byte copies where that problem's operands allow them).
 //  * strsm (left side, any uplo / trans / diag, n <= 256): problems are cut
 //    into strips of 32 right-hand sides, ordered largest problem first;
 //    persistent CTAs take strips from an atomic counter and solve each with
@@ -21,6 +22,7 @@
 //    updates between sub-blocks from cp.async-staged tiles of op(A).
 #include "mbg_internal.cuh"
 #include "block_solve.cuh"
+#include "gemm_f32_tile.cuh"
 
 #include <algorithm>
 #include <numeric>
@@ -41,106 +43,27 @@ struct GemmDesc {  // device copy of one problem
     int tiles_m;  // tiles along m
 };
 
-constexpr int GT_NT = 256, GT_BK = 8;
+constexpr int GT_NT = f32t::FNT;
 
+// Runs one tile of problem d with the pipelined FP32 tile code; the 16-byte copy
+// path is chosen per problem (operand contiguity, alignment and leading dimension).
 template <int TILE, bool TA, bool TB>
-__device__ __forceinline__ void gemm_tile(const GemmDesc& d, i64 tm, i64 tn, float* As_, float* Bs_) {
-    constexpr int BM = TILE, BN = TILE, TM = TILE / 16, LPT = BM * GT_BK / GT_NT, P = 4;
-    float(*As)[GT_BK][BM + P] = reinterpret_cast<float(*)[GT_BK][BM + P]>(As_);
-    float(*Bs)[GT_BK][BN + P] = reinterpret_cast<float(*)[GT_BK][BN + P]>(Bs_);
-    const i64 m0 = tm * BM, n0 = tn * BN;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const i64 m = d.m, n = d.n, k = d.k;
-    float ra[LPT], rb[LPT];
-    auto load_global = [&](i64 k0) {
-#pragma unroll
-        for (int r = 0; r < LPT; ++r) {
-            const int e = tid + r * GT_NT;
-            int i, l;
-            if (!TA) { i = e % BM; l = e / BM; } else { i = e / GT_BK; l = e % GT_BK; }
-            const i64 gi = m0 + i, gl = k0 + l;
-            ra[r] = (gi < m && gl < k) ? (TA ? d.a[gl + gi * d.lda] : d.a[gi + gl * d.lda]) : 0.0f;
-        }
-#pragma unroll
-        for (int r = 0; r < LPT; ++r) {
-            const int e = tid + r * GT_NT;
-            int j, l;
-            if (!TB) { j = e / GT_BK; l = e % GT_BK; } else { j = e % BN; l = e / BN; }
-            const i64 gj = n0 + j, gl = k0 + l;
-            rb[r] = (gj < n && gl < k) ? (TB ? d.b[gj + gl * d.ldb] : d.b[gl + gj * d.ldb]) : 0.0f;
-        }
-    };
-    auto store_shared = [&](int buf) {
-#pragma unroll
-        for (int r = 0; r < LPT; ++r) {
-            const int e = tid + r * GT_NT;
-            int i, l;
-            if (!TA) { i = e % BM; l = e / BM; } else { i = e / GT_BK; l = e % GT_BK; }
-            As[buf][l][i] = ra[r];
-        }
-#pragma unroll
-        for (int r = 0; r < LPT; ++r) {
-            const int e = tid + r * GT_NT;
-            int j, l;
-            if (!TB) { j = e / GT_BK; l = e % GT_BK; } else { j = e % BN; l = e / BN; }
-            Bs[buf][l][j] = rb[r];
-        }
-    };
-    float acc[TM][TM];
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-        for (int j = 0; j < TM; ++j) acc[i][j] = 0.0f;
-    const i64 nk = (k + GT_BK - 1) / GT_BK;
-    load_global(0);
-    store_shared(0);
-    __syncthreads();
-    for (i64 kt = 0; kt < nk; ++kt) {
-        const int buf = int(kt & 1);
-        if (kt + 1 < nk) load_global((kt + 1) * GT_BK);
-#pragma unroll
-        for (int l = 0; l < GT_BK; ++l) {
-            float a[TM], b[TM];
-            const float4 va = *reinterpret_cast<const float4*>(&As[buf][l][tx * 4]);
-            const float4 vb = *reinterpret_cast<const float4*>(&Bs[buf][l][ty * 4]);
-            a[0] = va.x; a[1] = va.y; a[2] = va.z; a[3] = va.w;
-            b[0] = vb.x; b[1] = vb.y; b[2] = vb.z; b[3] = vb.w;
-            if (TM == 8) {
-                const float4 wa = *reinterpret_cast<const float4*>(&As[buf][l][64 + tx * 4]);
-                const float4 wb = *reinterpret_cast<const float4*>(&Bs[buf][l][64 + ty * 4]);
-                a[4 % TM] = wa.x; a[5 % TM] = wa.y; a[6 % TM] = wa.z; a[7 % TM] = wa.w;
-                b[4 % TM] = wb.x; b[5 % TM] = wb.y; b[6 % TM] = wb.z; b[7 % TM] = wb.w;
-            }
-#pragma unroll
-            for (int i = 0; i < TM; ++i)
-#pragma unroll
-                for (int j = 0; j < TM; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-        }
-        if (kt + 1 < nk) store_shared(buf ^ 1);
-        __syncthreads();
-    }
-#pragma unroll
-    for (int j = 0; j < TM; ++j) {
-        const i64 gj = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
-        if (gj >= n) continue;
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-            const i64 gi = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-            if (gi >= m) continue;
-            float* cp = d.c + gi + gj * d.ldc;
-            const float v = d.alpha * acc[i][j];
-            *cp = (d.beta == 0.0f) ? v : fmaf(d.beta, *cp, v);
-        }
-    }
+__device__ __forceinline__ void grouped_tile(const GemmDesc& d, i64 tm, i64 tn, float* gsm) {
+    const bool va = f32t::f32_vec(!TA, d.a, d.lda), vb = f32t::f32_vec(TB, d.b, d.ldb);
+#define GT(VA, VB) \
+    f32t::f32_tile<TILE, TA, TB, 0, VA, VB>(d.m, d.n, d.k, d.alpha, d.a, d.lda, d.b, d.ldb, d.beta, d.c, d.ldc, tm, tn, gsm)
+    if (va && vb) GT(true, true);
+    else if (va) GT(true, false);
+    else if (vb) GT(false, true);
+    else GT(false, false);
+#undef GT
 }
 
 template <int TILE>
-__global__ void __launch_bounds__(GT_NT, TILE == 128 ? 1 : 2)
+__global__ void __launch_bounds__(GT_NT, TILE == 128 ? 1 : 3)
 grouped_sgemm_kernel(const GemmDesc* __restrict__ probs, int count, i64 total_tiles,
                      unsigned long long* __restrict__ counter) {
-    constexpr int P = 4;
-    __shared__ __align__(16) float As[2 * GT_BK * (TILE + P)];
-    __shared__ __align__(16) float Bs[2 * GT_BK * (TILE + P)];
+    extern __shared__ __align__(16) float gsm[];  // f32t::f32_smem<TILE>() bytes
     __shared__ long long s_tile;
     for (;;) {
         if (threadIdx.x == 0) s_tile = (long long)atomicAdd(counter, 1ull);
@@ -165,10 +88,10 @@ grouped_sgemm_kernel(const GemmDesc* __restrict__ probs, int count, i64 total_ti
                     *cp = (d.beta == 0.0f) ? 0.0f : d.beta * *cp;
                 }
             }
-        } else if (!d.ta && !d.tb) gemm_tile<TILE, false, false>(d, tm, tn, As, Bs);
-        else if (!d.ta && d.tb) gemm_tile<TILE, false, true>(d, tm, tn, As, Bs);
-        else if (d.ta && !d.tb) gemm_tile<TILE, true, false>(d, tm, tn, As, Bs);
-        else gemm_tile<TILE, true, true>(d, tm, tn, As, Bs);
+        } else if (!d.ta && !d.tb) grouped_tile<TILE, false, false>(d, tm, tn, gsm);
+        else if (!d.ta && d.tb) grouped_tile<TILE, false, true>(d, tm, tn, gsm);
+        else if (d.ta && !d.tb) grouped_tile<TILE, true, false>(d, tm, tn, gsm);
+        else grouped_tile<TILE, true, true>(d, tm, tn, gsm);
         __syncthreads();  // shared tiles are reused by the next tile
     }
 }
@@ -269,10 +192,10 @@ int enqueue_plan(mbg_plan* p) {
     if (p->kind == 1) {
         MBG_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
         if (p->tile == 128)
-            grouped_sgemm_kernel<128><<<p->grid, GT_NT, 0, s>>>(static_cast<const GemmDesc*>(p->table), p->count,
+            grouped_sgemm_kernel<128><<<p->grid, GT_NT, f32t::f32_smem<128>(), s>>>(static_cast<const GemmDesc*>(p->table), p->count,
                                                                 p->total, p->counter);
         else
-            grouped_sgemm_kernel<64><<<p->grid, GT_NT, 0, s>>>(static_cast<const GemmDesc*>(p->table), p->count,
+            grouped_sgemm_kernel<64><<<p->grid, GT_NT, f32t::f32_smem<64>(), s>>>(static_cast<const GemmDesc*>(p->table), p->count,
                                                                p->total, p->counter);
         return check_launch("grouped_sgemm");
     }
@@ -379,10 +302,18 @@ int mbg_sgemm_grouped_plan(int mode, int count, const mbg_sgemm_problem* probs, 
     p->total = tiles;
     p->tile = tile;
     int per_sm = 1;
-    if (tile == 128)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<128>, GT_NT, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<64>, GT_NT, 0);
+    // dynamic shared memory above 48 KB needs the opt-in before the occupancy query and the launch
+    if (tile == 128) {
+        cudaFuncSetAttribute(grouped_sgemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(f32t::f32_smem<128>()));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<128>, GT_NT,
+                                                      f32t::f32_smem<128>());
+    } else {
+        cudaFuncSetAttribute(grouped_sgemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(f32t::f32_smem<64>()));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<64>, GT_NT,
+                                                      f32t::f32_smem<64>());
+    }
     cudaGetLastError();
     p->grid = int(imax(1, imin(tiles, i64(num_sms()) * imax(per_sm, 1))));
     int st = MBG_OK;
