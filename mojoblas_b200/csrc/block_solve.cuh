@@ -46,9 +46,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //       (eight lanes per column, pivot broadcast by shuffle, reciprocal
 //       multiply, zero pivots skipped — src/level3/trsm.mojo:130-148);
 //     - subtract op(A)[t, b] X_b from every sub-block t still to be solved,
-//       one 64 x 64 tile of op(A) at a time, each thread keeping 4 rows x 4
-//       columns of the product over half of the 64-long reduction in
-//       registers and reading the tile and X_b as 8/16-byte pairs.
+//       one 64 x 64 tile of op(A) at a time: on the FP64 tensor pipe for
+//       double (mma.sync m8n8k4, each warp a 16 x 16 part of the 64 x 32
+//       product), on the CUDA cores for float (each thread 4 rows x 4 columns
+//       over half of the 64-long reduction, tile and X_b read as 8-byte pairs).
 // The diagonal blocks and tiles form one sequence per strip that is staged
 // with cp.async into two alternating buffers: the next item is in flight while
 // the current one is computed, so the L2 latency of A (shared by every CTA)
