@@ -96,6 +96,10 @@ int mbg_dgemm_ex(int mode, int slices, char trans_a, char trans_b, int64_t m, in
                  int64_t ldb, double beta, double* c, int64_t ldc);
 int mbg_ssyrk_ex(int mode, char uplo, char trans, int64_t n, int64_t k, float alpha,
                  const float* a, int64_t lda, float beta, float* c, int64_t ldc);
+/* dsyrk in MBG_MODE_PLAIN or MBG_MODE_OZAKI (slices as for mbg_dgemm_ex; one set of
+ * int8 slices serves both operands, only the uplo triangle is computed). */
+int mbg_dsyrk_ex(int mode, int slices, char uplo, char trans, int64_t n, int64_t k, double alpha,
+                 const double* a, int64_t lda, double beta, double* c, int64_t ldc);
 int mbg_strsm_ex(int mode, int refine, char side, char uplo, char trans_a, char diag,
                  int64_t m, int64_t n, float alpha, const float* a, int64_t lda,
                  float* b, int64_t ldb);

@@ -39,6 +39,7 @@ SIGNATURES = {
     "mbg_ssyrk": [_ch, _ch, i64, i64, _f, _vp, i64, _f, _vp, i64],
     "mbg_dsyrk": [_ch, _ch, i64, i64, _d, _vp, i64, _d, _vp, i64],
     "mbg_ssyrk_ex": [_i, _ch, _ch, i64, i64, _f, _vp, i64, _f, _vp, i64],
+    "mbg_dsyrk_ex": [_i, _i, _ch, _ch, i64, i64, _d, _vp, i64, _d, _vp, i64],
     "mbg_strsm": [_ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],
     "mbg_dtrsm": [_ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
     "mbg_strsm_ex": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],

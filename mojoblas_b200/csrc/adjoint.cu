@@ -43,8 +43,10 @@ int gemmt_any(int mode, int, char uplo, char ta, char tb, i64 n, i64 k, float al
                               is_l(uplo) ? 'L' : 'U');
     return gemmt_plain<float>(uplo, ta, tb, n, k, alpha, a, lda, b, ldb, 0.0f, c, ldc);
 }
-int gemmt_any(int, int, char uplo, char ta, char tb, i64 n, i64 k, double alpha, const double* a, i64 lda,
-              const double* b, i64 ldb, double* c, i64 ldc) {
+int gemmt_any(int mode, int slices, char uplo, char ta, char tb, i64 n, i64 k, double alpha, const double* a,
+              i64 lda, const double* b, i64 ldb, double* c, i64 ldc) {
+    if (mode == MBG_MODE_OZAKI)
+        return dgemm_ozaki_tc(slices, ta, tb, n, n, k, alpha, a, lda, b, ldb, 0.0, c, ldc, is_l(uplo) ? 'L' : 'U');
     return gemmt_plain<double>(uplo, ta, tb, n, k, alpha, a, lda, b, ldb, 0.0, c, ldc);
 }
 

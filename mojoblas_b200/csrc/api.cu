@@ -192,7 +192,7 @@ static int gemm_entry(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 
 
 template <typename T>
 static int syrk_entry(int mode, char uplo, char trans, i64 n, i64 k, T alpha, const T* a, i64 lda,
-                      T beta, T* c, i64 ldc) {
+                      T beta, T* c, i64 ldc, int slices = 8) {
     int info = syrk_info(uplo, trans, n, k, lda, ldc);
     if (info) return info;
     if (n == 0 || (alpha == T(0) && beta == T(1))) return MBG_OK;  // syrk.mojo:85-86
@@ -207,8 +207,11 @@ static int syrk_entry(int mode, char uplo, char trans, i64 n, i64 k, T alpha, co
     const char tb = is_n(trans) ? 'T' : 'N';
     int st;
     if (!need_a) st = scale_triangle<T>(uplo, n, beta, cd, Cc.dev_ld);
-    else if (mode == MBG_MODE_PLAIN || sizeof(T) == 8)
+    else if (mode == MBG_MODE_PLAIN)
         st = gemmt_plain<T>(uplo, ta, tb, n, k, alpha, ad, A.dev_ld, ad, A.dev_ld, beta, cd, Cc.dev_ld);
+    else if (sizeof(T) == 8)  // Ozaki int8 slices, one set of slices for both operands
+        st = dgemm_ozaki_tc(slices, ta, tb, n, n, k, (double)alpha, (const double*)ad, A.dev_ld,
+                            (const double*)ad, A.dev_ld, (double)beta, (double*)cd, Cc.dev_ld, is_l(uplo) ? 'L' : 'U');
     else
         st = sgemm_split_tc(mode == MBG_MODE_BF16X6 ? 3 : 2, ta, tb, n, n, k, (float)alpha,
                             (const float*)ad, A.dev_ld, (const float*)ad, A.dev_ld, (float)beta,
@@ -274,6 +277,11 @@ int mbg_ssyrk_ex(int mode, char uplo, char trans, int64_t n, int64_t k, float al
                  const float* a, int64_t lda, float beta, float* c, int64_t ldc) {
     if (!valid_smode(mode)) return MBG_ERR_INVALID_MODE;
     return syrk_entry<float>(mode, uplo, trans, n, k, alpha, a, lda, beta, c, ldc);
+}
+int mbg_dsyrk_ex(int mode, int slices, char uplo, char trans, int64_t n, int64_t k, double alpha,
+                 const double* a, int64_t lda, double beta, double* c, int64_t ldc) {
+    if (!valid_dmode(mode, slices)) return MBG_ERR_INVALID_MODE;
+    return syrk_entry<double>(mode, uplo, trans, n, k, alpha, a, lda, beta, c, ldc, slices);
 }
 
 int mbg_strsm(char side, char uplo, char ta, char diag, int64_t m, int64_t n, float alpha,

@@ -144,9 +144,10 @@ int dgemm_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, doub
 int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha,
                    const float* a, i64 lda, const float* b, i64 ldb, float beta, float* c,
                    i64 ldc, char tri_uplo);
+// tri_uplo 'L' / 'U': only that triangle of C is written (syrk, triangular adjoints)
 int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
                    const double* a, i64 lda, const double* b, i64 ldb, double beta,
-                   double* c, i64 ldc);
+                   double* c, i64 ldc, char tri_uplo = 0);
 
 // trsm on device operands (trsm.cu)
 template <typename T>

@@ -538,6 +538,7 @@ __device__ __forceinline__ bool oz_product(int lo, int hi, int idx, int& p, int&
 struct OzParams {
     i64 m, n;
     int num_kb, tiles_m, tiles_n;
+    int tri;  // 0 full, 1 lower, 2 upper (element mask + tile skip)
     double* c;
     i64 ldc;
     double alpha, beta;
@@ -605,6 +606,8 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
     const int gsize = min(group, P.tiles_m - first_m);
     const int in_g = tile - g * per_group;
     const i64 m0 = i64(first_m + in_g % gsize) * BM, n0 = i64(in_g / gsize) * C::BN;
+    if (P.tri == 1 && m0 + BM <= n0) return;        // tile strictly above the diagonal
+    if (P.tri == 2 && m0 > n0 + C::BN - 1) return;  // tile strictly below the diagonal
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -696,7 +699,8 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
 #pragma unroll
                 for (int j = 0; j < C::EPI_COLS; ++j) {
                     const i64 col = cbase + j;
-                    if (col < P.n) atomicAdd(P.c + row + col * P.ldc, P.alpha * (acc[j] * pow2_exact(er + P.eb[col])));
+                    const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
+                    if (live) atomicAdd(P.c + row + col * P.ldc, P.alpha * (acc[j] * pow2_exact(er + P.eb[col])));
                 }
             } else
 #pragma unroll
@@ -706,14 +710,14 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const i64 col = cbase + c0 + j;
-                    const bool live = col < P.n;
+                    const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
                     ec[j] = live ? P.eb[col] : 0;
                     cv[j] = (live && P.beta != 0.0) ? P.c[row + col * P.ldc] : 0.0;
                 }
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const i64 col = cbase + c0 + j;
-                    if (col >= P.n) continue;
+                    if (col >= P.n || (P.tri == 1 && row < col) || (P.tri == 2 && row > col)) continue;
                     const double v = P.alpha * (acc[c0 + j] * pow2_exact(er + ec[j]));
                     P.c[row + col * P.ldc] = (P.beta == 0.0) ? v : fma(P.beta, cv[j], v);
                 }
@@ -1029,23 +1033,26 @@ int launch_ozaki(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap
 }  // namespace tc
 
 int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a,
-                   i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+                   i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc, char tri_uplo) {
     using namespace tc;
     if (m == 0 || n == 0) return MBG_OK;
     if (slices < 2 || slices > 8) return MBG_ERR_INVALID_MODE;
     const int BN = 128;
     // int32 accumulators hold at most `slices` products of K terms of 127^2 each
     const i64 kchunk_max = (i64(0x7fffffff) / (i64(slices) * 127 * 127)) / 32 * 32;
+    const bool tri = tri_uplo != 0;
+    // syrk shares one set of slices and exponents for both operands (op(B)^T = op(A))
+    const bool shared_planes = tri && a == b && lda == ldb && (is_n(ta) != is_n(tb)) && m == n;
     const i64 Mp = roundup(m, BM), Np = roundup(n, BN);
     const i64 kc = imin(k, kchunk_max);
     const i64 Kp = roundup(kc, 32);
-    const size_t a_bytes = size_t(slices) * Mp * Kp, b_bytes = size_t(slices) * Np * Kp;
+    const size_t a_bytes = size_t(slices) * Mp * Kp, b_bytes = shared_planes ? 0 : size_t(slices) * Np * Kp;
     Workspace ws;
     MBG_TRY(ws.reserve(a_bytes + b_bytes + sizeof(int) * size_t(Mp + Np) + 1024));
     int8_t* pa = ws.as<int8_t>();
-    int8_t* pb = pa + a_bytes;
-    int* ea = reinterpret_cast<int*>(pb + b_bytes + (1024 - ((a_bytes + b_bytes) & 1023)) % 1024);
-    int* eb = ea + Mp;
+    int8_t* pb = shared_planes ? pa : pa + a_bytes;
+    int* ea = reinterpret_cast<int*>(pa + a_bytes + b_bytes + (1024 - ((a_bytes + b_bytes) & 1023)) % 1024);
+    int* eb = shared_planes ? ea : ea + Mp;
     const int lo_planes = slices <= 4 ? slices : 4;
     for (i64 k0 = 0; k0 < k; k0 += kc) {
         const i64 klen = imin(kc, k - k0);
@@ -1054,7 +1061,7 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
         const double* ak = is_n(ta) ? a + k0 * lda : a + k0;
         const double* bk = is_n(tb) ? b + k0 : b + k0 * ldb;
         MBG_TRY(launch_slices(ak, lda, is_t(ta), m, klen, Mp, Kpc, slices, ea, pa));
-        MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb));
+        if (!shared_planes) MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb));
         CUtensorMap ma, mb, mal, mbl;
         MBG_TRY(make_map(&ma, pa, true, Kpc, Mp, slices, 32, BM));
         MBG_TRY(make_map(&mb, pb, true, Kpc, Np, slices, 32, BN));
@@ -1063,6 +1070,7 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
         OzParams P{};
         P.m = m; P.n = n; P.num_kb = int(Kpc / 32);
         P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
+        P.tri = tri ? (is_l(tri_uplo) ? 1 : 2) : 0;
         P.c = c; P.ldc = ldc; P.alpha = alpha;
         P.beta = (k0 == 0) ? beta : 1.0;
         P.ea = ea; P.eb = eb;

@@ -88,7 +88,7 @@ def gemm(trans_a, trans_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode
     return _report("gemm", st)
 
 
-def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, *, mode=PLAIN, dtype=None) -> int:
+def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, *, mode=PLAIN, slices=8, dtype=None) -> int:
     """C := alpha*A*A^T + beta*C or alpha*A^T*A + beta*C on one triangle (syrk.mojo:20-200)."""
     dt = _dtype_of(c, dtype)
     lib = L.load()
@@ -96,9 +96,7 @@ def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, *, mode=PLAIN, dtype=No
     if dt == np.float32:
         st = lib.mbg_ssyrk(*args) if mode == PLAIN else lib.mbg_ssyrk_ex(mode, *args)
     elif dt == np.float64:
-        if mode != PLAIN:
-            raise MbgError("syrk", L.MBG_ERR_INVALID_MODE)
-        st = lib.mbg_dsyrk(*args)
+        st = lib.mbg_dsyrk(*args) if mode == PLAIN else lib.mbg_dsyrk_ex(mode, slices, *args)
     else:
         raise TypeError(f"unsupported dtype {dt}")
     return _report("syrk", st)

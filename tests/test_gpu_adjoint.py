@@ -159,3 +159,67 @@ def test_adjoint_info_codes():
     assert lib.mbg_sgemm_adjoint(0, b"N", b"N", 2, 2, 2, 1.0, p, 2, p, 2, p, 1, p, 2, p, 2) == 12
     assert lib.mbg_strsm_adjoint(0, b"L", b"L", b"N", b"N", 2, 2, 1.0, p, 2, p, 1, p, 2, p, 2, p, 2) == 11
     assert lib.mbg_strsm_adjoint(0, b"L", b"L", b"N", b"N", 3, 2, 1.0, p, 3, p, 3, p, 3, p, 3, p, 2) == 17
+
+
+# ---- double-precision adjoints: plain FP64 and 8-slice Ozaki -------------------------
+@pytest.mark.parametrize("mode", [L.MODE_PLAIN, L.MODE_OZAKI], ids=["plain", "ozaki"])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T")])
+def test_dgemm_adjoint_closed_form(mode, ta, tb):
+    """dA = alpha op^-1(G op(B)^T), dB = alpha op^-1(op(A)^T G) in float64, within the plain FP64
+    (4e-16 sqrt(k)) or 8-slice Ozaki (2^-56 * 16 + that) tolerance of the float64 products."""
+    lib = L.load()
+    rng = np.random.default_rng(41)
+    m, n, k, alpha = 300, 200, 260, 1.5
+    A = np.asfortranarray(rng.uniform(-1, 1, (m, k) if ta == "N" else (k, m)))
+    B = np.asfortranarray(rng.uniform(-1, 1, (k, n) if tb == "N" else (n, k)))
+    G = np.asfortranarray(rng.standard_normal((m, n)))
+    dA = np.zeros_like(A, order="F")
+    dB = np.zeros_like(B, order="F")
+    st = lib.mbg_dgemm_adjoint(mode, 8, ta.encode(), tb.encode(), m, n, k, alpha, A.ctypes.data, A.shape[0],
+                               B.ctypes.data, B.shape[0], G.ctypes.data, m, dA.ctypes.data, A.shape[0],
+                               dB.ctypes.data, B.shape[0])
+    assert st == 0, L.last_error()
+    dopA = alpha * G @ opm(B, tb).T
+    dopB = alpha * opm(A, ta).T @ G
+    tol = 4e-16 * np.sqrt(max(m, n, k)) * 4 + (16 * 2.0 ** -56 if mode == L.MODE_OZAKI else 0.0)
+    assert rel(dA, opm(dopA, ta)) < tol
+    assert rel(dB, opm(dopB, tb)) < tol
+
+
+@pytest.mark.parametrize("mode", [L.MODE_PLAIN, L.MODE_OZAKI], ids=["plain", "ozaki"])
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("ta", ["N", "T"])
+def test_dtrsm_adjoint_closed_form(mode, side, uplo, ta):
+    """dB = alpha op(A)^-T G and the stored triangle of dA = -tri(W X^T) (left) or -tri(X^T W)
+    (right) in float64; the Ozaki mode computes the triangle-only product with int8 slices."""
+    lib = L.load()
+    rng = np.random.default_rng(42)
+    m, n, alpha = 260, 150, 0.75
+    na = m if side == "L" else n
+    A = np.asfortranarray(_tri(rng, na, uplo, False))
+    Bm = rng.standard_normal((m, n))
+    G = np.asfortranarray(rng.standard_normal((m, n)))
+    opA = opm(A, ta)
+    low = (uplo == "L") != (ta == "T")
+    if side == "L":
+        X = alpha * sl.solve_triangular(opA, Bm, lower=low)
+        W = sl.solve_triangular(opA.T, G, lower=not low)
+        dopA = -W @ X.T
+    else:
+        X = alpha * sl.solve_triangular(opA.T, Bm.T, lower=not low).T
+        W = sl.solve_triangular(opA, G.T, lower=low).T
+        dopA = -X.T @ W
+    Xf = np.asfortranarray(X)
+    dB = np.zeros((m, n), order="F")
+    dA = np.full((na, na), 7.0, order="F")  # the other triangle must survive
+    st = lib.mbg_dtrsm_adjoint(mode, 8, side.encode(), uplo.encode(), ta.encode(), b"N", m, n, alpha,
+                               A.ctypes.data, na, Xf.ctypes.data, m, G.ctypes.data, m, dB.ctypes.data, m,
+                               dA.ctypes.data, na)
+    assert st == 0, L.last_error()
+    mask = np.tril(np.ones((na, na), bool)) if uplo == "L" else np.triu(np.ones((na, na), bool))
+    dA_ref = opm(dopA, ta)
+    tol = 4e-16 * np.sqrt(na) * 16 + (16 * 2.0 ** -56 if mode == L.MODE_OZAKI else 0.0)
+    assert rel(dB, alpha * W) < tol
+    assert rel(np.where(mask, dA, 0.0), np.where(mask, dA_ref, 0.0)) < tol
+    assert np.all(dA[~mask] == 7.0)

@@ -123,6 +123,29 @@ def test_split_sgemm_alpha0_k0_beta0_nan(oracle, mode):
     assert np.all(np.isfinite(c))
 
 
+# ---- Ozaki dsyrk (triangle-only int8 product, one set of slices for both operands) ----
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("trans", ["N", "T"])
+def test_ozaki_dsyrk_parity(oracle, uplo, trans):
+    rng = np.random.default_rng(13)
+    n, k, alpha, beta = 600, 333, 1.25, 0.5
+    lda = (n if trans == "N" else k) + 2
+    a = rand(rng, (lda, k if trans == "N" else n), np.float64)
+    c = rand(rng, (n + 1, n), np.float64)
+    c_o, c_g = c.copy(order="F"), c.copy(order="F")
+    assert oracle.syrk(uplo, trans, n, k, alpha, a, lda, beta, c_o, n + 1) == 0
+    assert mb.syrk(uplo, trans, n, k, alpha, a, lda, beta, c_g, n + 1, mode=mb.OZAKI, slices=8) == 0
+    A = oracle.op(oracle.view(a, *((n, k) if trans == "N" else (k, n)), lda), trans)
+    ref = alpha * A @ A.T + beta * oracle.view(c, n, n, n + 1)
+    mask = np.tril(np.ones((n, n), bool)) if uplo == "L" else np.triu(np.ones((n, n), bool))
+    g, o = oracle.view(c_g, n, n, n + 1), oracle.view(c_o, n, n, n + 1)
+    den = np.max(np.abs(ref[mask]))
+    assert np.max(np.abs(g[mask] - ref[mask])) / den < tol_oz(8, k)
+    assert np.max(np.abs(g[mask] - o[mask])) / den < tol_oz(8, k) + tol64(k)
+    np.testing.assert_array_equal(g[~mask], oracle.view(c, n, n, n + 1)[~mask])
+    np.testing.assert_array_equal(c_g[n:], c[n:])
+
+
 # ---- split-precision syrk (triangular tile schedule) ---------------------------------
 @pytest.mark.parametrize("mode", [mb.BF16X3, mb.BF16X6], ids=["bf16x3", "bf16x6"])
 @pytest.mark.parametrize("uplo", ["L", "U"])
