@@ -92,7 +92,7 @@ static int gemm_compute(int mode, int slices, char ta, char tb, i64 m, i64 n, i6
 // operands have landed; a second copy stream returns each finished block of C,
 // so the two directions of the PCIe link run at the same time.  The device
 // buffers are the same full-size copies the sequential path uses.
-constexpr int GEMM_PIPE_BLOCKS = 4;
+constexpr int GEMM_PIPE_BLOCKS = 8;
 
 template <typename T>
 static bool gemm_pipeline_pays(const T* a, const T* b, const T* c, i64 m, i64 n, i64 k) {
