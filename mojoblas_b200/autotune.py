@@ -31,6 +31,7 @@ import numpy as np
 sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 
 DEFAULT_OUT = Path(__file__).resolve().parent / "tuning_b200.json"
+ROUNDS = 5  # interleaved timing rounds per trsm candidate
 
 
 def log_uniform(rng, lo, hi, size):
@@ -120,15 +121,22 @@ def tune(out: Path) -> dict:
         return e0.elapsed_time(e1) / reps
 
     lib.mbg_set_tuning(b"trsm_block_min_cols", 1)
-    best = None
-    for rows in (0, 256, 512):
-        for thr in (256, 512, 1024):
+    # candidates are timed in interleaved rounds and ranked by their median, so that a clock
+    # or power-cap drift during the sweep does not favour whichever ran first
+    cands = [(rows, thr) for rows in (0, 256, 512) for thr in (256, 512, 1024)]
+    samples = {c: [] for c in cands}
+    for _ in range(ROUNDS):
+        for rows, thr in cands:
             lib.mbg_set_tuning(b"trsm_block_rows", rows)
             lib.mbg_set_tuning(b"trsm_tc_min_k", thr)
-            ms = time_trsm(L.MODE_OZAKI, n)
-            log[f"ozaki dtrsm 4096^2, fused rows {rows}, split from k {thr}"] = {"ms": round(ms, 3)}
-            if best is None or ms < best[2]:
-                best = (rows, thr, ms)
+            samples[(rows, thr)].append(time_trsm(L.MODE_OZAKI, n))
+    best = None
+    for (rows, thr), v in samples.items():
+        ms = float(np.median(v))
+        log[f"ozaki dtrsm 4096^2, fused rows {rows}, split from k {thr}"] = {"ms_median": round(ms, 3),
+                                                                            "rounds": len(v)}
+        if best is None or ms < best[2]:
+            best = (rows, thr, ms)
     table["trsm_block_rows"], table["trsm_tc_min_k"] = best[0], best[1]
     lib.mbg_set_tuning(b"trsm_block_rows", best[0])
     lib.mbg_set_tuning(b"trsm_tc_min_k", best[1])
