@@ -445,6 +445,38 @@ def run_cfg5(torch, lib, L, stream):
     return out
 
 
+def leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk):
+    """Each leg's achieved rate over the peak of the pipe that bounds it: the measured
+    bf16 burst for split-precision tensor work (P bf16 products per FP32 product), the
+    run's own probes for the FP32 / FP64 pipes and the int8 tensor pipe (36 int8 products
+    per FP64 product at 8 slices), the measured HBM copy for the batched trsm."""
+    out = {}
+    f32, f64, i8 = probes.get("fp32_fma_tflops"), probes.get("fp64_fma_tflops"), probes.get("int8_mma_tops")
+
+    def put(key, value, peak, note):
+        if value is not None and peak:
+            out[key] = {"frac": round(value / peak, 3), "peak": round(peak, 1), "bound": note}
+    if dg:
+        put("dgemm_plain_fp64", dg["plain_fp64"]["tflops"], f64, "fp64 pipe (probe)")
+        put("dgemm_ozaki_s8_int8", 36 * dg["ozaki_s8"]["tflops"], i8, "int8 tensor pipe (probe), whole call")
+    sy = cfg3.get("ssyrk_LN_8192x2048", {}) if cfg3 else {}
+    if sy:
+        put("ssyrk_plain_fp32", sy["plain_fp32"]["tflops"], f32, "fp32 pipe (probe)")
+        put("ssyrk_bf16x6_tensor", 6 * sy["bf16x6"]["tflops"], pk["bf16"], "bf16 tensor pipe (measured burst)")
+    tr = cfg3.get("dtrsm_LLNN_4096", {}) if cfg3 else {}
+    if tr:
+        put("dtrsm_plain_fp64", tr["plain_fp64"]["tflops"], f64, "fp64 pipe (probe); diagonal blocks latency-bound")
+    if cfg4:
+        put("grouped_sgemm_fp32", cfg4["grouped_sgemm_4096"]["tflops"], f32, "fp32 pipe (probe)")
+        g = cfg4.get("grouped_strsm_2048")
+        if g:
+            put("grouped_strsm_hbm", g["gbs"], pk["hbm_gbs"], "HBM (measured copy); latency-bound")
+    ga = (cfg5 or {}).get("sgemm_adjoint_3072x1024x2048")
+    if ga:
+        put("sgemm_adjoint_bf16x6_tensor", 6 * ga["bf16x6"]["tflops"], pk["bf16"], "bf16 tensor pipe (measured burst)")
+    return out
+
+
 def run_ours(args, rank, world, dist):
     import torch
     import mojoblas_b200 as mb
@@ -717,6 +749,7 @@ def run_ours(args, rank, world, dist):
         "cfg3": cfg3,
         "cfg4_batched": cfg4,
         "cfg5_adjoints": cfg5,
+        "roofline_fractions": leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk),
         "e2e": {"value": round(e2e_value, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_out, "ms_per_step": round(e2e_ms, 2)},
         "gpu_launches": launches,
