@@ -220,7 +220,10 @@ int   mbg_release_workspace(void);
  * double, 1024 for float) are solved in one fused launch, sub-block updates
  * included (default 512; 64 or less: 64-row leaves with gemm updates between them);
  * "trsm_block_min_cols" — the fused launch is used only with at least this
- * many right-hand sides (default 64).
+ * many right-hand sides (default 64);
+ * "plain_fp64_simt" — 1: plain FP64 gemm / syrk on the CUDA cores instead of the
+ * FP64 tensor pipe (default 0); "plain_fp32_staged" — 1: plain FP32 gemm / syrk
+ * with the register-staged tiles instead of the cp.async pipeline (default 0).
  * mbg_load_tuning reads "key value" lines (or a flat JSON object of them) as
  * written by the autotuner (mojoblas_b200/autotune.py).
  * mbg_get_tuning returns -1 for an unknown key. */

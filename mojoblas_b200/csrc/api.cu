@@ -118,7 +118,15 @@ static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i6
     if (hb) { MBG_TRY(wb.reserve(e * size_t(br) * size_t(bc))); db = wb.as<T>(); dldb = br; }
     if (hc) { MBG_TRY(wc.reserve(e * size_t(m) * size_t(n))); dc = wc.as<T>(); dldc = m; }
 
-    std::vector<cudaEvent_t> ev(2 * GEMM_PIPE_BLOCKS + 2);
+    struct Events {  // destroyed on every return path (pending work keeps them alive until done)
+        std::vector<cudaEvent_t> v;
+        ~Events() {
+            for (auto x : v)
+                if (x) cudaEventDestroy(x);
+        }
+    } events;
+    events.v.assign(2 * GEMM_PIPE_BLOCKS + 2, nullptr);
+    auto& ev = events.v;
     for (auto& x : ev) MBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
     cudaEvent_t ev_start = ev[0], ev_end = ev[1];
     MBG_CUDA(cudaEventRecord(ev_start, s));  // earlier work on the library stream (workspace reuse) first
@@ -159,7 +167,6 @@ static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i6
     MBG_CUDA(cudaEventRecord(ev_end, sout));
     MBG_CUDA(cudaStreamWaitEvent(s, ev_end, 0));  // the library stream completes after the last copy back
     const int fin = finish_call(true);
-    for (auto& x : ev) cudaEventDestroy(x);
     return st ? st : fin;
 }
 
