@@ -71,7 +71,7 @@ def _report(routine: str, st: int) -> int:
 
 
 def gemm(trans_a, trans_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN,
-         slices=7, dtype=None) -> int:
+         slices=8, dtype=None) -> int:
     """C := alpha*op(A)*op(B) + beta*C (mojoBLAS gemm, gemm.mojo:56-124)."""
     dt = _dtype_of(c, dtype)
     lib = L.load()
@@ -102,7 +102,7 @@ def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, *, mode=PLAIN, slices=8
     return _report("syrk", st)
 
 
-def trsm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, slices=7,
+def trsm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, slices=8,
          refine=0, dtype=None) -> int:
     """op(A) X = alpha B or X op(A) = alpha B, X overwrites B (trsm.mojo:20-275)."""
     dt = _dtype_of(b, dtype)
