@@ -21,7 +21,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle_level3.so"
-BUG_COMPAT = 1  # reproduce the reference's quirks (v7 alpha, right/trans trsm)
+BUG_COMPAT = 1  # reproduce the reference's quirks (v7 alpha, right/trans trsm, symm zero skip)
 
 _lib = None
 
@@ -51,6 +51,12 @@ def lib():
             "orc_dsyrk": [ch, ch, i64, i64, C.c_double, f64p, i64, C.c_double, f64p, i64],
             "orc_strsm": [ch, ch, ch, ch, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_int],
             "orc_dtrsm": [ch, ch, ch, ch, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_int],
+            "orc_ssymm": [ch, ch, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_float, f32p, i64, C.c_int],
+            "orc_dsymm": [ch, ch, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64, C.c_int],
+            "orc_ssyr2k": [ch, ch, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_float, f32p, i64],
+            "orc_dsyr2k": [ch, ch, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64],
+            "orc_strmm": [ch, ch, ch, ch, i64, i64, C.c_float, f32p, i64, f32p, i64],
+            "orc_dtrmm": [ch, ch, ch, ch, i64, i64, C.c_double, f64p, i64, f64p, i64],
         }
         for name, argtypes in sig.items():
             fn = getattr(_lib, name)
@@ -117,6 +123,27 @@ def trsm(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb, flags=0) -> int:
     return fn(_c(side), _c(uplo), _c(ta), _c(diag), m, n, alpha, _p(a, dt), lda, _p(b, dt), ldb, flags)
 
 
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, flags=0) -> int:
+    """The reference's symm (symm.mojo:20-241), in place on c."""
+    dt = _dt(c)
+    fn = lib().orc_ssymm if dt == np.float32 else lib().orc_dsymm
+    return fn(_c(side), _c(uplo), m, n, alpha, _p(a, dt), lda, _p(b, dt), ldb, beta, _p(c, dt), ldc, flags)
+
+
+def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> int:
+    """The reference's syr2k (syr2k.mojo:20-190), in place on c."""
+    dt = _dt(c)
+    fn = lib().orc_ssyr2k if dt == np.float32 else lib().orc_dsyr2k
+    return fn(_c(uplo), _c(trans), n, k, alpha, _p(a, dt), lda, _p(b, dt), ldb, beta, _p(c, dt), ldc)
+
+
+def trmm(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb) -> int:
+    """The reference's trmm (trmm.mojo:20-305), in place on b."""
+    dt = _dt(b)
+    fn = lib().orc_strmm if dt == np.float32 else lib().orc_dtrmm
+    return fn(_c(side), _c(uplo), _c(ta), _c(diag), m, n, alpha, _p(a, dt), lda, _p(b, dt), ldb)
+
+
 # ---------------------------------------------------------------------------
 # float64 references (Netlib semantics, independent of the reference's code)
 # ---------------------------------------------------------------------------
@@ -164,6 +191,44 @@ def trsm_f64(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb) -> np.ndarray:
         return sl.solve_triangular(opA, B, lower=lower)
     # X opA = B  <=>  opA^T X^T = B^T
     return sl.solve_triangular(opA.T, B.T, lower=not lower).T
+
+
+def sym(x: np.ndarray, uplo) -> np.ndarray:
+    """The symmetric matrix whose `uplo` triangle is stored in x (the other triangle ignored)."""
+    t = np.tril(x) if _c(uplo) in (b"L", b"l") else np.triu(x)
+    return t + t.T - np.diag(np.diag(x))
+
+
+def symm_f64(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc) -> np.ndarray:
+    """float64 Netlib symm result (m x n); c untouched."""
+    na = m if _c(side) in (b"L", b"l") else n
+    A = sym(view(a, na, na, lda).astype(np.float64), uplo)
+    B = view(b, m, n, ldb).astype(np.float64)
+    out = float(alpha) * (A @ B if _c(side) in (b"L", b"l") else B @ A)
+    if beta != 0:
+        out = out + float(beta) * view(c, m, n, ldc).astype(np.float64)
+    return out
+
+
+def syr2k_f64(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc) -> np.ndarray:
+    """float64 Netlib syr2k result as a full n x n array; only its `uplo` triangle is defined."""
+    shape = (n, k) if _c(trans) in (b"N", b"n") else (k, n)
+    A = view(a, *shape, lda).astype(np.float64)
+    B = view(b, *shape, ldb).astype(np.float64)
+    if _c(trans) not in (b"N", b"n"):
+        A, B = A.T, B.T
+    out = float(alpha) * (A @ B.T + B @ A.T)
+    if beta != 0:
+        out = out + float(beta) * view(c, n, n, ldc).astype(np.float64)
+    return out
+
+
+def trmm_f64(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb) -> np.ndarray:
+    """float64 Netlib trmm result (m x n); b untouched."""
+    na = m if _c(side) in (b"L", b"l") else n
+    opA = op(tri(view(a, na, na, lda).astype(np.float64), uplo, diag), ta)
+    B = view(b, m, n, ldb).astype(np.float64)
+    return float(alpha) * (opA @ B if _c(side) in (b"L", b"l") else B @ opA)
 
 
 def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:

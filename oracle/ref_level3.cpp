@@ -1,6 +1,7 @@
 // ORACLE — test infrastructure only.
 //
-// A CPU restatement of mojoBLAS's level-3 hot path (gemm / syrk / trsm), written
+// A CPU restatement of mojoBLAS's level-3 routines (gemm / syrk / trsm, and the
+// neighbours built on the same GEMM core: symm / syr2k / trmm), written
 // from the reference's algorithm so that tests, the smoke check and the CPU
 // baseline leg of the benchmark can compare the CUDA library against what the
 // reference computes on the same inputs.  Nothing in the shipped library links,
@@ -17,7 +18,10 @@
 //   * gemm_v7 (float64 NN, n >= 512) never applies alpha
 //     (src/level3/gemm.mojo:912-1132);
 //   * trsm with side='R' ignores trans_a: the Trans branches are copies of the
-//     NoTrans ones (src/level3/trsm.mojo:224-273 vs :170-222).
+//     NoTrans ones (src/level3/trsm.mojo:224-273 vs :170-222);
+//   * left-side symm skips step l of column j entirely when B(l,j) == 0, which
+//     also drops that step's alpha * sum_i A(i,l) B(i,j) from C(l,j)
+//     (src/level3/symm.mojo:113, :131).
 // Without the flag the oracle computes the Netlib-defined result with the same
 // loop structure, which is what the CUDA library implements.
 //
@@ -429,6 +433,219 @@ static int trsm_ref(char side, char uplo, char ta, char diag, i64 m, i64 n, T al
     return 0;
 }
 
+// symm, src/level3/symm.mojo:20-241.  Info (:69-86); quick return (:88-89);
+// columns of C in parallel when n >= 64 (:152-156, :235-239).  Per column: beta
+// first (:102-110, :163-171).  Left side: for each l (downwards for 'U', :112-129;
+// upwards for 'L', :130-151) C(i,j) += alpha*B(l,j)*A(i,l) over the stored part of
+// column l, and C(l,j) += alpha*B(l,j)*A(l,l) + alpha*sum_i A(i,l)*B(i,j).  Right
+// side (:173-233): C(:,j) += alpha*A(j,j)*B(:,j), then the off-diagonal columns of
+// B with A read from the stored triangle.
+// The reference skips the whole step l when B(l,j) == 0 (:113, :131), which also
+// drops the alpha*sum term of C(l,j); that quirk reproduces only with
+// ORC_BUG_COMPAT, otherwise the sum is always added (Netlib dsymm).
+template <typename T>
+static int symm_ref(char side, char uplo, i64 m, i64 n, T alpha, const T* a, i64 lda, const T* b,
+                    i64 ldb, T beta, T* c, i64 ldc, int flags) {
+    if (!is_l(side) && !is_r(side)) return 1;
+    if (!is_u(uplo) && !is_l(uplo)) return 2;
+    if (m < 0) return 3;
+    if (n < 0) return 4;
+    if (lda < std::max<i64>(1, is_l(side) ? m : n)) return 7;
+    if (ldb < std::max<i64>(1, m)) return 9;
+    if (ldc < std::max<i64>(1, m)) return 12;
+    if (m == 0 || n == 0 || (alpha == T(0) && beta == T(1))) return 0;
+    const bool left = is_l(side), upper = is_u(uplo);
+    const bool skip_zero_pivot = (flags & ORC_BUG_COMPAT) != 0;
+#pragma omp parallel for schedule(dynamic, 1) if (n >= PAR_THRESHOLD)
+    for (i64 j = 0; j < n; ++j) {
+        T* cj = c + j * ldc;
+        const T* bj = b + j * ldb;
+        if (beta == T(0)) {
+            for (i64 i = 0; i < m; ++i) cj[i] = T(0);
+        } else if (beta != T(1)) {
+            for (i64 i = 0; i < m; ++i) cj[i] = beta * cj[i];
+        }
+        if (left) {
+            for (i64 s = 0; s < m; ++s) {
+                const i64 l = upper ? m - 1 - s : s;
+                if (bj[l] == T(0) && skip_zero_pivot) continue;
+                const T temp1 = alpha * bj[l];
+                T temp2 = T(0);
+                const T* al = a + l * lda;
+                const i64 i0 = upper ? 0 : l + 1, i1 = upper ? l : m;
+                for (i64 i = i0; i < i1; ++i) {
+                    cj[i] = cj[i] + temp1 * al[i];
+                    temp2 = temp2 + al[i] * bj[i];
+                }
+                cj[l] = cj[l] + temp1 * al[l] + alpha * temp2;
+            }
+        } else {
+            const T td = alpha * a[j + j * lda];
+            for (i64 i = 0; i < m; ++i) cj[i] = cj[i] + td * bj[i];
+            for (i64 k = 0; k < n; ++k) {
+                if (k == j) continue;
+                // A(k,j) for k < j lives above the diagonal; for k > j below it
+                const bool above = k < j;
+                const T akj = (above == upper) ? a[k + j * lda] : a[j + k * lda];
+                const T temp = alpha * akj;
+                const T* bk = b + k * ldb;
+                for (i64 i = 0; i < m; ++i) cj[i] = cj[i] + temp * bk[i];
+            }
+        }
+    }
+    return 0;
+}
+
+// syr2k, src/level3/syr2k.mojo:20-190.  Info (:69-93); quick return (:95-96);
+// beta on the triangle (:101-118); alpha == 0 returns (:120-121).  NoTrans
+// (:125-167): per column j and each l with A(j,l) or B(j,l) nonzero,
+// C(i,j) += alpha*A(j,l)*B(i,l) + alpha*B(j,l)*A(i,l) over the triangle's rows.
+// Trans (:169-188): two dot products per element, C(i,j) += alpha*(t1 + t2).
+// The reference runs the columns serially; they are independent, so the oracle
+// runs them in parallel, which changes no element's arithmetic.
+template <typename T>
+static int syr2k_ref(char uplo, char trans, i64 n, i64 k, T alpha, const T* a, i64 lda, const T* b,
+                     i64 ldb, T beta, T* c, i64 ldc) {
+    if (!is_u(uplo) && !is_l(uplo)) return 1;
+    if (!is_n(trans) && !is_t(trans)) return 2;
+    if (n < 0) return 3;
+    if (k < 0) return 4;
+    if (lda < std::max<i64>(1, is_n(trans) ? n : k)) return 7;
+    if (ldb < std::max<i64>(1, is_n(trans) ? n : k)) return 9;
+    if (ldc < std::max<i64>(1, n)) return 12;
+    if (n == 0 || (alpha == T(0) && beta == T(1))) return 0;
+    const bool upper = is_u(uplo);
+    for (i64 j = 0; j < n; ++j)
+        for (i64 i = upper ? 0 : j; i < (upper ? j + 1 : n); ++i)
+            c[i + j * ldc] = beta == T(0) ? T(0) : (beta == T(1) ? c[i + j * ldc] : beta * c[i + j * ldc]);
+    if (alpha == T(0)) return 0;
+#pragma omp parallel for schedule(dynamic, 1) if (n >= PAR_THRESHOLD)
+    for (i64 j = 0; j < n; ++j) {
+        T* cj = c + j * ldc;
+        const i64 i0 = upper ? 0 : j, i1 = upper ? j + 1 : n;
+        if (is_n(trans)) {
+            for (i64 l = 0; l < k; ++l) {
+                const T ajl = a[j + l * lda], bjl = b[j + l * ldb];
+                if (ajl == T(0) && bjl == T(0)) continue;
+                const T temp1 = alpha * ajl, temp2 = alpha * bjl;
+                const T* al = a + l * lda;
+                const T* bl = b + l * ldb;
+                for (i64 i = i0; i < i1; ++i) cj[i] = cj[i] + temp1 * bl[i] + temp2 * al[i];
+            }
+        } else {
+            for (i64 i = i0; i < i1; ++i) {
+                T t1 = T(0), t2 = T(0);
+                for (i64 l = 0; l < k; ++l) {
+                    t1 = t1 + a[l + i * lda] * b[l + j * ldb];
+                    t2 = t2 + b[l + i * ldb] * a[l + j * lda];
+                }
+                cj[i] = cj[i] + alpha * (t1 + t2);
+            }
+        }
+    }
+    return 0;
+}
+
+// trmm, src/level3/trmm.mojo:20-305.  Info (:63-89); quick return (:91-92);
+// alpha == 0 sets B to zero (:94-98).  Left side: each column of B is
+// independent (the reference parallelises the Trans branches, :148-185, and runs
+// the NoTrans ones serially, :108-147; the oracle runs all of them in parallel,
+// which changes no element's arithmetic).  Left/NoTrans/Upper walks k upwards,
+// B(0:k,j) += alpha*B(k,j)*A(0:k,k), then B(k,j) = alpha*B(k,j)*A(k,k) (:109-127);
+// Lower walks k downwards (:128-147); both skip B(k,j) == 0.  Left/Trans forms
+// each B(i,j) as a dot product with the not yet updated entries (:150-185).
+// Right/NoTrans runs columns in the order of the dependence (downwards for 'U',
+// :189-218; upwards for 'L', :219-248): scale column j by alpha*A(j,j), then add
+// alpha*A(k,j)*B(:,k) over the stored part, skipping A(k,j) == 0.  Right/Trans
+// (:249-305) adds alpha*A(j,k)*B(:,k) into the columns j before (U) or after (L)
+// k, then scales column k when alpha*A(k,k) != 1.
+template <typename T>
+static int trmm_ref(char side, char uplo, char ta, char diag, i64 m, i64 n, T alpha, const T* a,
+                    i64 lda, T* b, i64 ldb) {
+    if (!is_l(side) && !is_r(side)) return 1;
+    if (!is_u(uplo) && !is_l(uplo)) return 2;
+    if (!is_n(ta) && !is_t(ta)) return 3;
+    if (!is_u(diag) && !is_n(diag)) return 4;
+    if (m < 0) return 5;
+    if (n < 0) return 6;
+    if (lda < std::max<i64>(1, is_l(side) ? m : n)) return 9;
+    if (ldb < std::max<i64>(1, m)) return 11;
+    if (m == 0 || n == 0) return 0;
+    if (alpha == T(0)) {
+        for (i64 j = 0; j < n; ++j)
+            for (i64 i = 0; i < m; ++i) b[i + j * ldb] = T(0);
+        return 0;
+    }
+    const bool upper = is_u(uplo), notrans = is_n(ta), nounit = is_n(diag);
+    if (is_l(side)) {
+#pragma omp parallel for schedule(static) if (n >= PAR_THRESHOLD)
+        for (i64 j = 0; j < n; ++j) {
+            T* bj = b + j * ldb;
+            if (notrans && upper) {
+                for (i64 k = 0; k < m; ++k) {
+                    if (bj[k] == T(0)) continue;
+                    T temp = alpha * bj[k];
+                    const T* ak = a + k * lda;
+                    for (i64 i = 0; i < k; ++i) bj[i] = bj[i] + temp * ak[i];
+                    if (nounit) temp = temp * ak[k];
+                    bj[k] = temp;
+                }
+            } else if (notrans) {
+                for (i64 k = m - 1; k >= 0; --k) {
+                    if (bj[k] == T(0)) continue;
+                    const T temp = alpha * bj[k];
+                    const T* ak = a + k * lda;
+                    bj[k] = nounit ? temp * ak[k] : temp;
+                    for (i64 i = k + 1; i < m; ++i) bj[i] = bj[i] + temp * ak[i];
+                }
+            } else if (upper) {
+                for (i64 i = m - 1; i >= 0; --i) {
+                    T temp = bj[i];
+                    if (nounit) temp = temp * a[i + i * lda];
+                    for (i64 l = 0; l < i; ++l) temp = temp + a[l + i * lda] * bj[l];
+                    bj[i] = alpha * temp;
+                }
+            } else {
+                for (i64 i = 0; i < m; ++i) {
+                    T temp = bj[i];
+                    if (nounit) temp = temp * a[i + i * lda];
+                    for (i64 l = i + 1; l < m; ++l) temp = temp + a[l + i * lda] * bj[l];
+                    bj[i] = alpha * temp;
+                }
+            }
+        }
+        return 0;
+    }
+    auto axpy_col = [&](T temp, i64 src, i64 dst) {
+        const T* bs = b + src * ldb;
+        T* bd = b + dst * ldb;
+        for (i64 i = 0; i < m; ++i) bd[i] = bd[i] + temp * bs[i];
+    };
+    auto scale_col = [&](T temp, i64 j) {
+        T* bj = b + j * ldb;
+        for (i64 i = 0; i < m; ++i) bj[i] = temp * bj[i];
+    };
+    if (notrans) {
+        for (i64 s = 0; s < n; ++s) {
+            const i64 j = upper ? n - 1 - s : s;
+            scale_col(nounit ? alpha * a[j + j * lda] : alpha, j);
+            const i64 k0 = upper ? 0 : j + 1, k1 = upper ? j : n;
+            for (i64 k = k0; k < k1; ++k)
+                if (a[k + j * lda] != T(0)) axpy_col(alpha * a[k + j * lda], k, j);
+        }
+        return 0;
+    }
+    for (i64 s = 0; s < n; ++s) {
+        const i64 k = upper ? s : n - 1 - s;
+        const i64 j0 = upper ? 0 : k + 1, j1 = upper ? k : n;
+        for (i64 j = j0; j < j1; ++j)
+            if (a[j + k * lda] != T(0)) axpy_col(alpha * a[j + k * lda], k, j);
+        const T temp = nounit ? alpha * a[k + k * lda] : alpha;
+        if (temp != T(1)) scale_col(temp, k);
+    }
+    return 0;
+}
+
 extern "C" {
 
 void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
@@ -480,6 +697,30 @@ int orc_strsm(char side, char uplo, char ta, char diag, i64 m, i64 n, float alph
 int orc_dtrsm(char side, char uplo, char ta, char diag, i64 m, i64 n, double alpha, const double* a,
               i64 lda, double* b, i64 ldb, int flags) {
     return trsm_ref<double>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb, flags);
+}
+int orc_ssymm(char side, char uplo, i64 m, i64 n, float alpha, const float* a, i64 lda, const float* b,
+              i64 ldb, float beta, float* c, i64 ldc, int flags) {
+    return symm_ref<float>(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, flags);
+}
+int orc_dsymm(char side, char uplo, i64 m, i64 n, double alpha, const double* a, i64 lda,
+              const double* b, i64 ldb, double beta, double* c, i64 ldc, int flags) {
+    return symm_ref<double>(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, flags);
+}
+int orc_ssyr2k(char uplo, char trans, i64 n, i64 k, float alpha, const float* a, i64 lda, const float* b,
+               i64 ldb, float beta, float* c, i64 ldc) {
+    return syr2k_ref<float>(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int orc_dsyr2k(char uplo, char trans, i64 n, i64 k, double alpha, const double* a, i64 lda,
+               const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+    return syr2k_ref<double>(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int orc_strmm(char side, char uplo, char ta, char diag, i64 m, i64 n, float alpha, const float* a,
+              i64 lda, float* b, i64 ldb) {
+    return trmm_ref<float>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int orc_dtrmm(char side, char uplo, char ta, char diag, i64 m, i64 n, double alpha, const double* a,
+              i64 lda, double* b, i64 ldb) {
+    return trmm_ref<double>(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
 }
 
 }  // extern "C"
