@@ -224,6 +224,96 @@ def run_cfg3(torch, lib, L, stream):
     return out
 
 
+def run_neighbours(torch, lib, L, stream):
+    """symm, syr2k and trmm at the configuration sizes of the hot path: symm (Left, Upper)
+    with A symmetric and B uniform[-1,1) at M = N = 4096 (float32 and float64); syr2k
+    (Lower, NoTrans) at N = 8192, K = 2048 float32; trmm (Left, Lower, NoTrans, NonUnit)
+    at M = N = 4096 with the trsm configuration's triangle (float64 and float32).  Plain
+    vs split / Ozaki, with the float64-oracle error on 128 sampled columns (rows for
+    syr2k).  Flops: symm 2 m^2 n, syr2k 2 n(n+1) k, trmm m^2 n."""
+    out = {}
+    g = torch.Generator(device="cuda")
+    g.manual_seed(77)
+    cols = np.sort(np.random.default_rng(8).choice(4096, 128, replace=False))
+
+    def timed(call, flops):
+        call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        return {"tflops": round(flops / (ms * 1e-3) / 1e12, 2), "ms": round(ms, 3)}
+
+    def check(st, what):
+        if st:
+            raise RuntimeError(f"{what} failed {st}: {L.last_error()}")
+
+    n = 4096
+    for dt, tname, modes in ((torch.float32, "s", (("plain_fp32", L.MODE_PLAIN, 0), ("bf16x6", L.MODE_BF16X6, 0))),
+                             (torch.float64, "d", (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s8", L.MODE_OZAKI, 8)))):
+        A = torch.rand((n, n), generator=g, device="cuda", dtype=dt) * 2 - 1
+        B = torch.rand((n, n), generator=g, device="cuda", dtype=dt) * 2 - 1
+        C = torch.empty_like(B)
+        An = A.double().cpu().numpy().T
+        Asym = np.triu(An) + np.triu(An, 1).T
+        ref = Asym @ B.double().cpu().numpy().T[:, cols]
+        res = {}
+        for label, md, sl in modes:
+            def call():
+                args = (b"L", b"U", n, n, 1.0, A.data_ptr(), n, B.data_ptr(), n, 0.0, C.data_ptr(), n)
+                check(lib.mbg_ssymm_ex(md, *args) if tname == "s" else lib.mbg_dsymm_ex(md, sl, *args), "symm")
+            r = timed(call, 2.0 * n ** 3)
+            got = C.double().cpu().numpy().T[:, cols]
+            r["fp64_err"] = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+            res[label] = r
+        out[f"{tname}symm_LU_4096"] = res
+
+        # trmm with the trsm configuration's triangle: off-diagonal N(0,1)/sqrt(n), diagonal n + |N(0,1)|
+        T = torch.randn((n, n), generator=g, device="cuda", dtype=dt) / np.sqrt(n)
+        T.diagonal().copy_(n + torch.randn(n, generator=g, device="cuda", dtype=dt).abs())
+        B0 = torch.randn((n, n), generator=g, device="cuda", dtype=dt)
+        ref = np.tril(T.double().cpu().numpy().T) @ B0.double().cpu().numpy().T[:, cols]
+        res = {}
+        for label, md, sl in modes:
+            def call():
+                C.copy_(B0)
+                args = (b"L", b"L", b"N", b"N", n, n, 1.0, T.data_ptr(), n, C.data_ptr(), n)
+                check(lib.mbg_strmm_ex(md, *args) if tname == "s" else lib.mbg_dtrmm_ex(md, sl, *args), "trmm")
+            r = timed(call, 1.0 * n ** 3)
+            got = C.double().cpu().numpy().T[:, cols]
+            r["fp64_err"] = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+            res[label] = r
+        out[f"{tname}trmm_LLNN_4096"] = res
+        del A, B, C, T, B0
+
+    nn, kk = 8192, 2048
+    A = torch.rand((kk, nn), generator=g, device="cuda", dtype=torch.float32) * 2 - 1  # column-major n x k
+    B = torch.rand((kk, nn), generator=g, device="cuda", dtype=torch.float32) * 2 - 1
+    C = torch.zeros((nn, nn), device="cuda", dtype=torch.float32)
+    rows = np.sort(np.random.default_rng(9).choice(nn, 128, replace=False))
+    Ah, Bh = A.double().cpu().numpy().T, B.double().cpu().numpy().T
+    ref = Ah[rows] @ Bh.T + Bh[rows] @ Ah.T
+    mask = np.arange(nn)[None, :] <= rows[:, None]
+    res = {}
+    for label, md in (("plain_fp32", L.MODE_PLAIN), ("bf16x3", L.MODE_BF16X3), ("bf16x6", L.MODE_BF16X6)):
+        def call():
+            check(lib.mbg_ssyr2k_ex(md, b"L", b"N", nn, kk, 1.0, A.data_ptr(), nn, B.data_ptr(), nn, 0.0,
+                                    C.data_ptr(), nn), "syr2k")
+        r = timed(call, 2.0 * nn * (nn + 1) * kk)
+        got = C.double().cpu().numpy().T[rows]
+        r["fp64_err"] = float(np.max(np.abs((got - ref)[mask])) / np.max(np.abs(ref[mask])))
+        res[label] = r
+    out["ssyr2k_LN_8192x2048"] = res
+    out["note"] = ("flops: symm 2 m^2 n, trmm m^2 n (each timed trmm call includes a device copy restoring B), "
+                   "syr2k 2 n(n+1) k")
+    del A, B, C
+    return out
+
+
 def run_cfg4(torch, lib, L, stream):
     """Batched: 4096 sgemm problems (m, n, k log-uniform 16..512, NN, uniform[-1,1))
     and 2048 lower-triangular strsm problems (n log-uniform 8..256, nrhs uniform
@@ -688,6 +778,7 @@ def run_ours(args, rank, world, dist):
     cfg3 = {} if args.skip_cfg3 else run_cfg3(torch, lib, L, stream)
     cfg4 = {} if args.skip_cfg4 else run_cfg4(torch, lib, L, stream)
     cfg5 = {} if args.skip_cfg5 else run_cfg5(torch, lib, L, stream)
+    neighbours = {} if args.skip_neighbours else run_neighbours(torch, lib, L, stream)
 
     # ---- e2e through the C ABI with pinned host buffers ----
     hA = A.cpu().pin_memory()
@@ -749,6 +840,7 @@ def run_ours(args, rank, world, dist):
         "cfg3": cfg3,
         "cfg4_batched": cfg4,
         "cfg5_adjoints": cfg5,
+        "symm_syr2k_trmm": neighbours,
         "roofline_fractions": leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk),
         "e2e": {"value": round(e2e_value, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_out, "ms_per_step": round(e2e_ms, 2)},
@@ -818,6 +910,7 @@ def main():
     ap.add_argument("--skip-cfg3", action="store_true")
     ap.add_argument("--skip-cfg4", action="store_true")
     ap.add_argument("--skip-cfg5", action="store_true")
+    ap.add_argument("--skip-neighbours", action="store_true")
     ap.add_argument("--skip-context", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -1,7 +1,8 @@
 /*
  * mojoblas_gpu.h — C ABI of the B200 (sm_100a) level-3 BLAS library.
  *
- * Drop-in boundary for mojoBLAS's level-3 hot path.  Every routine keeps the
+ * Drop-in boundary for mojoBLAS's level-3 routines (the gemm / syrk / trsm hot
+ * path, and symm / syr2k / trmm on the same kernels).  Every routine keeps the
  * argument order and meaning of the mojoBLAS routine it replaces (column-major
  * storage, element (i,j) of a matrix at p[i + j*ld], Netlib transpose / uplo /
  * side / diag characters), and returns:
@@ -79,6 +80,32 @@ int mbg_strsm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t 
 int mbg_dtrsm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t n,
               double alpha, const double* a, int64_t lda, double* b, int64_t ldb);
 
+/* C := alpha*A*B + beta*C (side 'L', A is m x m) or alpha*B*A + beta*C (side 'R',
+ * A is n x n), A symmetric with only its `uplo` triangle read.
+ * Replaces mojoBLAS symm (src/level3/symm.mojo:20-241).  Where B(l,j) == 0 the
+ * reference also drops alpha * sum_i A(i,l) B(i,j) from C(l,j) (:113, :131);
+ * this library computes the full product. */
+int mbg_ssymm(char side, char uplo, int64_t m, int64_t n, float alpha, const float* a,
+              int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc);
+int mbg_dsymm(char side, char uplo, int64_t m, int64_t n, double alpha, const double* a,
+              int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc);
+
+/* C := alpha*(A*B^T + B*A^T) + beta*C (trans 'N', A and B n x k) or
+ * alpha*(A^T*B + B^T*A) + beta*C (trans 'T' / 'C', A and B k x n), on the
+ * `uplo` triangle of C only.  Replaces mojoBLAS syr2k (src/level3/syr2k.mojo:20-190). */
+int mbg_ssyr2k(char uplo, char trans, int64_t n, int64_t k, float alpha, const float* a,
+               int64_t lda, const float* b, int64_t ldb, float beta, float* c, int64_t ldc);
+int mbg_dsyr2k(char uplo, char trans, int64_t n, int64_t k, double alpha, const double* a,
+               int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc);
+
+/* B := alpha*op(A)*B (side 'L') or alpha*B*op(A) (side 'R'), A triangular
+ * (`uplo`, unit diagonal not read when diag 'U'), B overwritten.
+ * Replaces mojoBLAS trmm (src/level3/trmm.mojo:20-305); alpha == 0 writes zeros. */
+int mbg_strmm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t n,
+              float alpha, const float* a, int64_t lda, float* b, int64_t ldb);
+int mbg_dtrmm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t n,
+              double alpha, const double* a, int64_t lda, double* b, int64_t ldb);
+
 /* ---- the same routines with a precision mode ----------------------------
  * mode: MBG_MODE_PLAIN, MBG_MODE_BF16X3 or MBG_MODE_BF16X6 for float;
  *       MBG_MODE_PLAIN or MBG_MODE_OZAKI for double.
@@ -106,6 +133,24 @@ int mbg_strsm_ex(int mode, int refine, char side, char uplo, char trans_a, char 
 int mbg_dtrsm_ex(int mode, int slices, int refine, char side, char uplo, char trans_a,
                  char diag, int64_t m, int64_t n, double alpha, const double* a,
                  int64_t lda, double* b, int64_t ldb);
+/* symm, syr2k and trmm with a precision mode (same modes and slices as gemm). */
+int mbg_ssymm_ex(int mode, char side, char uplo, int64_t m, int64_t n, float alpha,
+                 const float* a, int64_t lda, const float* b, int64_t ldb, float beta,
+                 float* c, int64_t ldc);
+int mbg_dsymm_ex(int mode, int slices, char side, char uplo, int64_t m, int64_t n,
+                 double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                 double beta, double* c, int64_t ldc);
+int mbg_ssyr2k_ex(int mode, char uplo, char trans, int64_t n, int64_t k, float alpha,
+                  const float* a, int64_t lda, const float* b, int64_t ldb, float beta,
+                  float* c, int64_t ldc);
+int mbg_dsyr2k_ex(int mode, int slices, char uplo, char trans, int64_t n, int64_t k,
+                  double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                  double beta, double* c, int64_t ldc);
+int mbg_strmm_ex(int mode, char side, char uplo, char trans_a, char diag, int64_t m,
+                 int64_t n, float alpha, const float* a, int64_t lda, float* b, int64_t ldb);
+int mbg_dtrmm_ex(int mode, int slices, char side, char uplo, char trans_a, char diag,
+                 int64_t m, int64_t n, double alpha, const double* a, int64_t lda,
+                 double* b, int64_t ldb);
 
 /* ---- split-precision sgemm that allocates nothing -------------------------
  * No counterpart in the reference (mojoBLAS allocates host memory freely).

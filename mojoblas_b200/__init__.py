@@ -6,7 +6,7 @@ binding (_lib.py) and a Python mirror of the reference routines (level3.py).
 """
 from ._lib import LIB_PATH, load  # noqa: F401
 from .level3 import (BF16X3, BF16X6, OZAKI, PLAIN, MbgError, gemm, set_stream,  # noqa: F401
-                     set_sync, synchronize, syrk, trsm)
+                     set_sync, symm, synchronize, syr2k, syrk, trmm, trsm)
 
-__all__ = ["gemm", "syrk", "trsm", "set_stream", "set_sync", "synchronize", "MbgError",
+__all__ = ["gemm", "syrk", "trsm", "symm", "syr2k", "trmm", "set_stream", "set_sync", "synchronize", "MbgError",
            "PLAIN", "BF16X3", "BF16X6", "OZAKI", "load", "LIB_PATH"]

@@ -44,6 +44,18 @@ SIGNATURES = {
     "mbg_dtrsm": [_ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
     "mbg_strsm_ex": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],
     "mbg_dtrsm_ex": [_i, _i, _i, _ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
+    "mbg_ssymm": [_ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
+    "mbg_dsymm": [_ch, _ch, i64, i64, _d, _vp, i64, _vp, i64, _d, _vp, i64],
+    "mbg_ssymm_ex": [_i, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
+    "mbg_dsymm_ex": [_i, _i, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64, _d, _vp, i64],
+    "mbg_ssyr2k": [_ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
+    "mbg_dsyr2k": [_ch, _ch, i64, i64, _d, _vp, i64, _vp, i64, _d, _vp, i64],
+    "mbg_ssyr2k_ex": [_i, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
+    "mbg_dsyr2k_ex": [_i, _i, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64, _d, _vp, i64],
+    "mbg_strmm": [_ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],
+    "mbg_dtrmm": [_ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
+    "mbg_strmm_ex": [_i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],
+    "mbg_dtrmm_ex": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
     "mbg_sgemm_adjoint": [_i, _ch, _ch, i64, i64, i64, _f, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp, i64],
     "mbg_dgemm_adjoint": [_i, _i, _ch, _ch, i64, i64, i64, _d, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp, i64],
     "mbg_strsm_adjoint": [_i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp, i64],

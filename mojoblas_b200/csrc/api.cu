@@ -42,6 +42,33 @@ static int trsm_info(char side, char uplo, char ta, char diag, i64 m, i64 n, i64
     return 0;
 }
 
+// src/level3/symm.mojo:69-82
+static int symm_info(char side, char uplo, i64 m, i64 n, i64 lda, i64 ldb, i64 ldc) {
+    if (!is_l(side) && !is_r(side)) return 1;
+    if (!is_u(uplo) && !is_l(uplo)) return 2;
+    if (m < 0) return 3;
+    if (n < 0) return 4;
+    if (lda < imax(1, is_l(side) ? m : n)) return 7;
+    if (ldb < imax(1, m)) return 9;
+    if (ldc < imax(1, m)) return 12;
+    return 0;
+}
+// src/level3/syr2k.mojo:69-89
+static int syr2k_info(char uplo, char trans, i64 n, i64 k, i64 lda, i64 ldb, i64 ldc) {
+    if (!is_u(uplo) && !is_l(uplo)) return 1;
+    if (!is_n(trans) && !is_t(trans)) return 2;
+    if (n < 0) return 3;
+    if (k < 0) return 4;
+    if (lda < imax(1, is_n(trans) ? n : k)) return 7;
+    if (ldb < imax(1, is_n(trans) ? n : k)) return 9;
+    if (ldc < imax(1, n)) return 12;
+    return 0;
+}
+// src/level3/trmm.mojo:63-85 (the same numbering as trsm)
+static int trmm_info(char side, char uplo, char ta, char diag, i64 m, i64 n, i64 lda, i64 ldb) {
+    return trsm_info(side, uplo, ta, diag, m, n, lda, ldb);
+}
+
 static bool valid_smode(int mode) {
     return mode == MBG_MODE_PLAIN || mode == MBG_MODE_BF16X3 || mode == MBG_MODE_BF16X6;
 }
@@ -245,6 +272,65 @@ static int trsm_entry(int mode, int slices, int refine, char side, char uplo, ch
     return finish_call(A.staged || B.staged);
 }
 
+template <typename T>
+static int symm_entry(int mode, int slices, char side, char uplo, i64 m, i64 n, T alpha, const T* a, i64 lda,
+                      const T* b, i64 ldb, T beta, T* c, i64 ldc) {
+    int info = symm_info(side, uplo, m, n, lda, ldb, ldc);
+    if (info) return info;
+    if (m == 0 || n == 0 || (alpha == T(0) && beta == T(1))) return MBG_OK;  // symm.mojo:88-89
+    const bool need_ab = alpha != T(0);
+    const i64 na = is_l(side) ? m : n;
+    Operand A, B, Cc;
+    if (need_ab) {
+        MBG_TRY(A.prepare(a, na, na, lda, sizeof(T), true, false));
+        MBG_TRY(B.prepare(b, m, n, ldb, sizeof(T), true, false));
+    }
+    MBG_TRY(Cc.prepare(c, m, n, ldc, sizeof(T), beta != T(0), true));
+    int st = symm_device<T>(mode, slices, side, uplo, m, n, alpha, (const T*)A.dev, A.dev_ld, (const T*)B.dev,
+                            B.dev_ld, beta, (T*)Cc.dev, Cc.dev_ld);
+    if (st) return st;
+    MBG_TRY(Cc.finish());
+    return finish_call(A.staged || B.staged || Cc.staged);
+}
+
+template <typename T>
+static int syr2k_entry(int mode, int slices, char uplo, char trans, i64 n, i64 k, T alpha, const T* a, i64 lda,
+                       const T* b, i64 ldb, T beta, T* c, i64 ldc) {
+    int info = syr2k_info(uplo, trans, n, k, lda, ldb, ldc);
+    if (info) return info;
+    if (n == 0 || (alpha == T(0) && beta == T(1))) return MBG_OK;  // syr2k.mojo:95-96
+    const bool need_ab = !(alpha == T(0) || k == 0);
+    const i64 rows = is_n(trans) ? n : k, cols = is_n(trans) ? k : n;
+    Operand A, B, Cc;
+    if (need_ab) {
+        MBG_TRY(A.prepare(a, rows, cols, lda, sizeof(T), true, false));
+        MBG_TRY(B.prepare(b, rows, cols, ldb, sizeof(T), true, false));
+    }
+    MBG_TRY(Cc.prepare(c, n, n, ldc, sizeof(T), true, true));  // the other triangle must survive
+    int st = syr2k_device<T>(mode, slices, uplo, trans, n, k, alpha, (const T*)A.dev, A.dev_ld, (const T*)B.dev,
+                             B.dev_ld, beta, (T*)Cc.dev, Cc.dev_ld);
+    if (st) return st;
+    MBG_TRY(Cc.finish());
+    return finish_call(A.staged || B.staged || Cc.staged);
+}
+
+template <typename T>
+static int trmm_entry(int mode, int slices, char side, char uplo, char ta, char diag, i64 m, i64 n, T alpha,
+                      const T* a, i64 lda, T* b, i64 ldb) {
+    int info = trmm_info(side, uplo, ta, diag, m, n, lda, ldb);
+    if (info) return info;
+    if (m == 0 || n == 0) return MBG_OK;  // trmm.mojo:91-92
+    const i64 na = is_l(side) ? m : n;
+    Operand A, B;
+    if (alpha != T(0)) MBG_TRY(A.prepare(a, na, na, lda, sizeof(T), true, false));
+    MBG_TRY(B.prepare(b, m, n, ldb, sizeof(T), alpha != T(0), true));
+    int st = trmm_device<T>(mode, slices, side, uplo, ta, diag, m, n, alpha, (const T*)A.dev, A.dev_ld,
+                            (T*)B.dev, B.dev_ld);
+    if (st) return st;
+    MBG_TRY(B.finish());
+    return finish_call(A.staged || B.staged);
+}
+
 }  // namespace mbg
 
 using namespace mbg;
@@ -309,6 +395,65 @@ int mbg_dtrsm_ex(int mode, int slices, int refine, char side, char uplo, char ta
                  int64_t ldb) {
     if (!valid_dmode(mode, slices) || refine < 0) return MBG_ERR_INVALID_MODE;
     return trsm_entry<double>(mode, slices, refine, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+
+// ---- symm / syr2k / trmm ----
+int mbg_ssymm(char side, char uplo, int64_t m, int64_t n, float alpha, const float* a, int64_t lda,
+              const float* b, int64_t ldb, float beta, float* c, int64_t ldc) {
+    return symm_entry<float>(MBG_MODE_PLAIN, 0, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_dsymm(char side, char uplo, int64_t m, int64_t n, double alpha, const double* a, int64_t lda,
+              const double* b, int64_t ldb, double beta, double* c, int64_t ldc) {
+    return symm_entry<double>(MBG_MODE_PLAIN, 0, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_ssymm_ex(int mode, char side, char uplo, int64_t m, int64_t n, float alpha, const float* a, int64_t lda,
+                 const float* b, int64_t ldb, float beta, float* c, int64_t ldc) {
+    if (!valid_smode(mode)) return MBG_ERR_INVALID_MODE;
+    return symm_entry<float>(mode, 0, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_dsymm_ex(int mode, int slices, char side, char uplo, int64_t m, int64_t n, double alpha, const double* a,
+                 int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc) {
+    if (!valid_dmode(mode, slices)) return MBG_ERR_INVALID_MODE;
+    return symm_entry<double>(mode, slices, side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+int mbg_ssyr2k(char uplo, char trans, int64_t n, int64_t k, float alpha, const float* a, int64_t lda,
+               const float* b, int64_t ldb, float beta, float* c, int64_t ldc) {
+    return syr2k_entry<float>(MBG_MODE_PLAIN, 0, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_dsyr2k(char uplo, char trans, int64_t n, int64_t k, double alpha, const double* a, int64_t lda,
+               const double* b, int64_t ldb, double beta, double* c, int64_t ldc) {
+    return syr2k_entry<double>(MBG_MODE_PLAIN, 0, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_ssyr2k_ex(int mode, char uplo, char trans, int64_t n, int64_t k, float alpha, const float* a, int64_t lda,
+                  const float* b, int64_t ldb, float beta, float* c, int64_t ldc) {
+    if (!valid_smode(mode)) return MBG_ERR_INVALID_MODE;
+    return syr2k_entry<float>(mode, 0, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+int mbg_dsyr2k_ex(int mode, int slices, char uplo, char trans, int64_t n, int64_t k, double alpha,
+                  const double* a, int64_t lda, const double* b, int64_t ldb, double beta, double* c,
+                  int64_t ldc) {
+    if (!valid_dmode(mode, slices)) return MBG_ERR_INVALID_MODE;
+    return syr2k_entry<double>(mode, slices, uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+int mbg_strmm(char side, char uplo, char ta, char diag, int64_t m, int64_t n, float alpha, const float* a,
+              int64_t lda, float* b, int64_t ldb) {
+    return trmm_entry<float>(MBG_MODE_PLAIN, 0, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int mbg_dtrmm(char side, char uplo, char ta, char diag, int64_t m, int64_t n, double alpha, const double* a,
+              int64_t lda, double* b, int64_t ldb) {
+    return trmm_entry<double>(MBG_MODE_PLAIN, 0, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int mbg_strmm_ex(int mode, char side, char uplo, char ta, char diag, int64_t m, int64_t n, float alpha,
+                 const float* a, int64_t lda, float* b, int64_t ldb) {
+    if (!valid_smode(mode)) return MBG_ERR_INVALID_MODE;
+    return trmm_entry<float>(mode, 0, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+int mbg_dtrmm_ex(int mode, int slices, char side, char uplo, char ta, char diag, int64_t m, int64_t n,
+                 double alpha, const double* a, int64_t lda, double* b, int64_t ldb) {
+    if (!valid_dmode(mode, slices)) return MBG_ERR_INVALID_MODE;
+    return trmm_entry<double>(mode, slices, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
 }
 
 }  // extern "C"

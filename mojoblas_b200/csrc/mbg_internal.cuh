@@ -149,9 +149,20 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
                    const double* a, i64 lda, const double* b, i64 ldb, double beta,
                    double* c, i64 ldc, char tri_uplo = 0);
 
-// trsm on device operands (trsm.cu)
+// trsm and trmm on device operands (trsm.cu)
 template <typename T>
 int trsm_device(int mode, int slices, int refine, char side, char uplo, char ta, char diag,
                 i64 m, i64 n, T alpha, const T* a, i64 lda, T* b, i64 ldb);
+template <typename T>
+int trmm_device(int mode, int slices, char side, char uplo, char ta, char diag, i64 m, i64 n, T alpha,
+                const T* a, i64 lda, T* b, i64 ldb);
+
+// symm and syr2k on device operands (symm.cu)
+template <typename T>
+int symm_device(int mode, int slices, char side, char uplo, i64 m, i64 n, T alpha, const T* a, i64 lda,
+                const T* b, i64 ldb, T beta, T* c, i64 ldc);
+template <typename T>
+int syr2k_device(int mode, int slices, char uplo, char trans, i64 n, i64 k, T alpha, const T* a, i64 lda,
+                 const T* b, i64 ldb, T beta, T* c, i64 ldc);
 
 }  // namespace mbg

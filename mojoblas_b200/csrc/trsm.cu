@@ -22,6 +22,15 @@
 // R = alpha*B - op(A) X with the accurate residual product (FP64 / BF16x6 /
 // 8-slice Ozaki by recursion, diagonal blocks in the input precision), solve
 // op(A) D = R in the caller's mode and add D to X.
+//
+// Triangular multiply (trmm, src/level3/trmm.mojo:20-305), at the end of this
+// file, uses the same recursion with products in place of solves:
+//     left, op(A) lower:   B2 = alpha op(A)22 B2 + alpha op(A)21 B1, then B1 = alpha op(A)11 B1
+//     left, op(A) upper:   B1 = alpha op(A)11 B1 + alpha op(A)12 B2, then B2 = alpha op(A)22 B2
+// (the right side likewise over column blocks of B), ordered so that every
+// update reads the block of B that is still unmodified.  Diagonal blocks of at
+// most TRMM_LEAF rows are one GEMM of a dense copy of the triangle with a copy
+// of the block of B.
 #include "mbg_internal.cuh"
 #include "block_solve.cuh"
 
@@ -405,7 +414,92 @@ int solve_left_refined(int mode, int slices, int refine, bool lower, bool trans,
     return MBG_OK;
 }
 
+// ---- triangular multiply ---------------------------------------------------
+constexpr i64 TRMM_LEAF = 256;
+
+template <typename T>
+int launch_tri_dense(i64 m, const T* a, i64 lda, bool lower, bool trans, bool unit, T* w) {
+    ProfScope prof("trsm_tri_dense");
+    dim3 g((unsigned)imin(cdiv(m, 256), 64), (unsigned)imin(m, 65535));
+    tri_dense_kernel<T><<<g, 256, 0, stream()>>>(m, a, lda, lower, trans, unit, w);
+    return check_launch("trsm_tri_dense");
+}
+
+// Leaf: B[0:nb, 0:n] := alpha tri(op(A)) B (left) or B[0:m, 0:nb] := alpha B tri(op(A))
+// (right), nb <= TRMM_LEAF: one plain GEMM of the dense triangle with a copy of B.
+template <typename T>
+int trmm_leaf(bool left, bool lower, bool trans, bool unit, i64 m, i64 n, T alpha, const T* a, i64 lda, T* b,
+              i64 ldb) {
+    const i64 nb = left ? m : n;
+    Workspace ww, wt;
+    MBG_TRY(ww.reserve(sizeof(T) * size_t(nb) * size_t(nb)));
+    MBG_TRY(wt.reserve(sizeof(T) * size_t(m) * size_t(n)));
+    T* w = ww.as<T>();
+    T* t = wt.as<T>();
+    MBG_TRY(launch_tri_dense<T>(nb, a, lda, lower, trans, unit, w));
+    MBG_TRY(launch_copy<T>(m, n, T(1), b, ldb, t, m));
+    if (left) return gemm_plain<T>('N', 'N', m, n, m, alpha, w, nb, t, m, T(0), b, ldb);
+    return gemm_plain<T>('N', 'N', m, n, n, alpha, t, m, w, nb, T(0), b, ldb);
+}
+
+// B := alpha op(A) B, op(A) effectively lower / upper; A is m x m.
+template <typename T>
+int trmm_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, T alpha, const T* a,
+              i64 lda, T* b, i64 ldb) {
+    if (m <= TRMM_LEAF) return trmm_leaf<T>(true, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
+    const i64 m1 = split_point(m), m2 = m - m1;
+    const char tc = trans ? 'T' : 'N';
+    const T* a22 = a + m1 + m1 * lda;
+    if (lower) {  // B2 first: its update reads the unmodified B1
+        MBG_TRY(trmm_left<T>(mode, slices, lower, trans, unit, m2, n, alpha, a22, lda, b + m1, ldb));
+        MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m2, n, m1, alpha, op_at(a, lda, trans, m1, 0), lda, b, ldb,
+                             T(1), b + m1, ldb));
+        return trmm_left<T>(mode, slices, lower, trans, unit, m1, n, alpha, a, lda, b, ldb);
+    }
+    MBG_TRY(trmm_left<T>(mode, slices, lower, trans, unit, m1, n, alpha, a, lda, b, ldb));
+    MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m1, n, m2, alpha, op_at(a, lda, trans, 0, m1), lda, b + m1, ldb,
+                         T(1), b, ldb));
+    return trmm_left<T>(mode, slices, lower, trans, unit, m2, n, alpha, a22, lda, b + m1, ldb);
+}
+
+// B := alpha B op(A), op(A) effectively lower / upper; A is n x n.
+template <typename T>
+int trmm_right(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, T alpha, const T* a,
+               i64 lda, T* b, i64 ldb) {
+    if (n <= TRMM_LEAF) return trmm_leaf<T>(false, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
+    const i64 n1 = split_point(n), n2 = n - n1;
+    const char tc = trans ? 'T' : 'N';
+    const T* a22 = a + n1 + n1 * lda;
+    T* b2 = b + n1 * ldb;
+    if (lower) {  // B1 = B1 P11 + B2 P21 first: it reads the unmodified B2
+        MBG_TRY(trmm_right<T>(mode, slices, lower, trans, unit, m, n1, alpha, a, lda, b, ldb));
+        MBG_TRY(gemm_in_mode(mode, slices, 'N', tc, m, n1, n2, alpha, b2, ldb, op_at(a, lda, trans, n1, 0), lda,
+                             T(1), b, ldb));
+        return trmm_right<T>(mode, slices, lower, trans, unit, m, n2, alpha, a22, lda, b2, ldb);
+    }
+    // B2 = B1 P12 + B2 P22 first: it reads the unmodified B1
+    MBG_TRY(trmm_right<T>(mode, slices, lower, trans, unit, m, n2, alpha, a22, lda, b2, ldb));
+    MBG_TRY(gemm_in_mode(mode, slices, 'N', tc, m, n2, n1, alpha, b, ldb, op_at(a, lda, trans, 0, n1), lda, T(1),
+                         b2, ldb));
+    return trmm_right<T>(mode, slices, lower, trans, unit, m, n1, alpha, a, lda, b, ldb);
+}
+
 }  // namespace
+
+template <typename T>
+int trmm_device(int mode, int slices, char side, char uplo, char ta, char diag, i64 m, i64 n, T alpha,
+                const T* a, i64 lda, T* b, i64 ldb) {
+    if (m == 0 || n == 0) return MBG_OK;
+    if (alpha == T(0)) return scale_matrix<T>(m, n, T(0), b, ldb);  // trmm.mojo:94-98: zeros
+    const bool trans = is_t(ta), unit = is_u(diag);
+    const bool lower = (!is_u(uplo)) != trans;  // effective op(A) lower triangular
+    if (is_l(side)) return trmm_left<T>(mode, slices, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
+    return trmm_right<T>(mode, slices, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
+}
+
+template int trmm_device<float>(int, int, char, char, char, char, i64, i64, float, const float*, i64, float*, i64);
+template int trmm_device<double>(int, int, char, char, char, char, i64, i64, double, const double*, i64, double*,
+                                 i64);
 
 template <typename T>
 int trsm_device(int mode, int slices, int refine, char side, char uplo, char ta, char diag, i64 m,

@@ -1,9 +1,10 @@
 """Python mirror of mojoBLAS's level-3 routines on the CUDA library.
 
 Same routine names, argument order and meaning as the reference
-(src/level3/gemm.mojo:56, syrk.mojo:20, trsm.mojo:20; docs/reference.md:264-325):
-column-major storage with leading dimensions, Netlib transpose / uplo / side /
-diag characters, results written in place into `c` (gemm, syrk) or `b` (trsm).
+(src/level3/gemm.mojo:56, syrk.mojo:20, trsm.mojo:20, symm.mojo:20, syr2k.mojo:20,
+trmm.mojo:20; docs/reference.md:264-325): column-major storage with leading
+dimensions, Netlib transpose / uplo / side / diag characters, results written in
+place into `c` (gemm, syrk, symm, syr2k) or `b` (trsm, trmm).
 The dtype is taken from the buffers (float32 or float64), as the reference
 takes it from its `dtype` parameter.
 
@@ -118,6 +119,52 @@ def trsm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, 
     else:
         raise TypeError(f"unsupported dtype {dt}")
     return _report("trsm", st)
+
+
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN, slices=8,
+         dtype=None) -> int:
+    """C := alpha*A*B + beta*C or alpha*B*A + beta*C, A symmetric (symm.mojo:20-241)."""
+    dt = _dtype_of(c, dtype)
+    lib = L.load()
+    args = (_ch(side), _ch(uplo), m, n, float(alpha), _ptr(a), lda, _ptr(b), ldb, float(beta), _ptr(c), ldc)
+    if dt == np.float32:
+        st = lib.mbg_ssymm(*args) if mode == PLAIN else lib.mbg_ssymm_ex(mode, *args)
+    elif dt == np.float64:
+        st = lib.mbg_dsymm(*args) if mode == PLAIN else lib.mbg_dsymm_ex(mode, slices, *args)
+    else:
+        raise TypeError(f"unsupported dtype {dt}")
+    return _report("symm", st)
+
+
+def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN, slices=8,
+          dtype=None) -> int:
+    """C := alpha*(A*B^T + B*A^T) + beta*C or alpha*(A^T*B + B^T*A) + beta*C on one
+    triangle (syr2k.mojo:20-190)."""
+    dt = _dtype_of(c, dtype)
+    lib = L.load()
+    args = (_ch(uplo), _ch(trans), n, k, float(alpha), _ptr(a), lda, _ptr(b), ldb, float(beta), _ptr(c), ldc)
+    if dt == np.float32:
+        st = lib.mbg_ssyr2k(*args) if mode == PLAIN else lib.mbg_ssyr2k_ex(mode, *args)
+    elif dt == np.float64:
+        st = lib.mbg_dsyr2k(*args) if mode == PLAIN else lib.mbg_dsyr2k_ex(mode, slices, *args)
+    else:
+        raise TypeError(f"unsupported dtype {dt}")
+    return _report("syr2k", st)
+
+
+def trmm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, slices=8,
+         dtype=None) -> int:
+    """B := alpha*op(A)*B or alpha*B*op(A), A triangular, B overwritten (trmm.mojo:20-305)."""
+    dt = _dtype_of(b, dtype)
+    lib = L.load()
+    args = (_ch(side), _ch(uplo), _ch(trans_a), _ch(diag), m, n, float(alpha), _ptr(a), lda, _ptr(b), ldb)
+    if dt == np.float32:
+        st = lib.mbg_strmm(*args) if mode == PLAIN else lib.mbg_strmm_ex(mode, *args)
+    elif dt == np.float64:
+        st = lib.mbg_dtrmm(*args) if mode == PLAIN else lib.mbg_dtrmm_ex(mode, slices, *args)
+    else:
+        raise TypeError(f"unsupported dtype {dt}")
+    return _report("trmm", st)
 
 
 def set_stream(stream) -> None:

@@ -124,3 +124,67 @@ def test_cuda_failure_is_reported_not_silent():
     a = np.ones((2, 2), np.float32, order="F")
     with pytest.raises(mb.MbgError):
         mb.gemm("N", "N", 2, 2, 2, 1.0, a, 2, a, 2, 0.0, a.copy(order="F"), 2)
+
+
+@pytest.mark.parametrize("args,info", [
+    (("X", "U", 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 1),
+    (("L", "X", 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 2),
+    (("L", "U", -1, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 3),
+    (("L", "U", 2, -1, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 4),
+    (("L", "U", 3, 2, 1.0, Z, 2, Z, 3, 0.0, Z, 3), 7),
+    (("R", "U", 2, 3, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 7),
+    (("L", "U", 3, 2, 1.0, Z, 3, Z, 2, 0.0, Z, 3), 9),
+    (("L", "U", 3, 2, 1.0, Z, 3, Z, 3, 0.0, Z, 2), 12),
+])
+def test_symm_info_codes(args, info, capsys):
+    """Numbering of mojoBLAS symm (src/level3/symm.mojo:69-86)."""
+    assert mb.symm(*args) == info
+    assert f"symm: Info {info}" in capsys.readouterr().out
+
+
+@pytest.mark.parametrize("args,info", [
+    (("X", "N", 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 1),
+    (("U", "X", 2, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 2),
+    (("U", "N", -1, 2, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 3),
+    (("U", "N", 2, -1, 1.0, Z, 2, Z, 2, 0.0, Z, 2), 4),
+    (("U", "N", 3, 2, 1.0, Z, 2, Z, 3, 0.0, Z, 3), 7),
+    (("U", "T", 2, 3, 1.0, Z, 2, Z, 3, 0.0, Z, 2), 7),
+    (("U", "C", 2, 3, 1.0, Z, 3, Z, 2, 0.0, Z, 2), 9),
+    (("U", "N", 3, 2, 1.0, Z, 3, Z, 3, 0.0, Z, 2), 12),
+])
+def test_syr2k_info_codes(args, info):
+    """Numbering of mojoBLAS syr2k (src/level3/syr2k.mojo:69-93)."""
+    assert mb.syr2k(*args) == info
+
+
+@pytest.mark.parametrize("args,info", [
+    (("X", "L", "N", "N", 2, 2, 1.0, Z, 2, Z, 2), 1),
+    (("L", "X", "N", "N", 2, 2, 1.0, Z, 2, Z, 2), 2),
+    (("L", "L", "X", "N", 2, 2, 1.0, Z, 2, Z, 2), 3),
+    (("L", "L", "N", "X", 2, 2, 1.0, Z, 2, Z, 2), 4),
+    (("L", "L", "N", "N", -1, 2, 1.0, Z, 2, Z, 2), 5),
+    (("L", "L", "N", "N", 2, -1, 1.0, Z, 2, Z, 2), 6),
+    (("L", "L", "N", "N", 3, 2, 1.0, Z, 2, Z, 3), 9),
+    (("R", "L", "N", "N", 2, 3, 1.0, Z, 2, Z, 2), 9),
+    (("L", "L", "N", "N", 3, 2, 1.0, Z, 3, Z, 2), 11),
+])
+def test_trmm_info_codes(args, info):
+    """Numbering of mojoBLAS trmm (src/level3/trmm.mojo:63-89)."""
+    assert mb.trmm(*args) == info
+
+
+def test_neighbour_quick_returns_and_modes():
+    # m == 0 / n == 0 / alpha == 0 and beta == 1 return before any CUDA call
+    assert mb.symm("L", "U", 0, 3, 1.0, Z, 1, Z, 1, 0.0, Z, 1) == 0
+    assert mb.symm("R", "L", 3, 3, 0.0, Z, 3, Z, 3, 1.0, Z, 3) == 0
+    assert mb.syr2k("L", "N", 0, 3, 1.0, Z, 1, Z, 1, 0.0, Z, 1) == 0
+    assert mb.syr2k("U", "T", 3, 3, 0.0, Z, 3, Z, 3, 1.0, Z, 3) == 0
+    assert mb.trmm("L", "L", "N", "N", 0, 3, 1.0, Z, 1, Z, 1) == 0
+    assert mb.trmm("R", "U", "T", "U", 3, 0, 1.0, Z, 1, Z, 3) == 0
+    lib = L.load()
+    p = Z.ctypes.data
+    assert lib.mbg_ssymm_ex(L.MODE_OZAKI, b"L", b"U", 1, 1, 1.0, p, 1, p, 1, 0.0, p, 1) == L.MBG_ERR_INVALID_MODE
+    assert lib.mbg_dsyr2k_ex(L.MODE_BF16X6, 8, b"L", b"N", 1, 1, 1.0, p, 1, p, 1, 0.0, p, 1) == \
+        L.MBG_ERR_INVALID_MODE
+    assert lib.mbg_dtrmm_ex(L.MODE_OZAKI, 1, b"L", b"L", b"N", b"N", 1, 1, 1.0, p, 1, p, 1) == \
+        L.MBG_ERR_INVALID_MODE
