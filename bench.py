@@ -252,6 +252,25 @@ def run_neighbours(torch, lib, L, stream):
         if st:
             raise RuntimeError(f"{what} failed {st}: {L.last_error()}")
 
+    def kernel_ms(call, names):
+        # device time of each library kernel in one call (CUDA events around every launch)
+        import ctypes as C
+        lib.mbg_prof_enable(1)
+        lib.mbg_prof_reset()
+        call()
+        torch.cuda.synchronize()
+        out_ms = {}
+        for nm in names:
+            tot, cnt = C.c_double(0), C.c_int64(0)
+            lib.mbg_prof_query(nm.encode(), C.byref(tot), C.byref(cnt))
+            if cnt.value:
+                out_ms[nm] = round(tot.value, 4)
+        lib.mbg_prof_enable(0)
+        return out_ms
+
+    trmm_kernels = ("copy", "trsm_tri_dense", "trmm_diag", "split_bf16", "tc_gemm_bf16x6", "ozaki_exponent",
+                    "ozaki_slice", "tc_gemm_ozaki", "gemm_f32", "gemm_dmma_f64")
+
     n = 4096
     for dt, tname, modes in ((torch.float32, "s", (("plain_fp32", L.MODE_PLAIN, 0), ("bf16x6", L.MODE_BF16X6, 0))),
                              (torch.float64, "d", (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s8", L.MODE_OZAKI, 8)))):
@@ -286,6 +305,7 @@ def run_neighbours(torch, lib, L, stream):
             r = timed(call, 1.0 * n ** 3)
             got = C.double().cpu().numpy().T[:, cols]
             r["fp64_err"] = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+            r["kernels_ms"] = kernel_ms(call, trmm_kernels)
             res[label] = r
         out[f"{tname}trmm_LLNN_4096"] = res
         del A, B, C, T, B0

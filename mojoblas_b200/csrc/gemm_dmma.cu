@@ -74,7 +74,7 @@ struct DmmaCfg {
 template <class C, bool TA, bool TB, int TRI, int BM, int BN, int VEC>
 __global__ void __launch_bounds__(C::THREADS, 1)
 gemm_dmma_kernel(i64 m, i64 n, i64 k, double alpha, const double* __restrict__ A, i64 lda,
-                 const double* __restrict__ B, i64 ldb, double beta, double* __restrict__ Cm, i64 ldc) {
+                 const double* __restrict__ B, i64 ldb, double beta, double* __restrict__ Cm, i64 ldc, int band) {
     extern __shared__ __align__(16) double dsm[];
     // A: TA (k contiguous in memory) -> [m][DKP], else [k][BM + 8]; B: !TB -> [n][DKP], else [k][BN + 8]
     constexpr int LA = TA ? DKP : BM + 8, LB = TB ? BN + 8 : DKP;
@@ -85,6 +85,7 @@ gemm_dmma_kernel(i64 m, i64 n, i64 k, double alpha, const double* __restrict__ A
     if (TRI == 0) {
         tm = blockIdx.x;
         tn = blockIdx.y;
+        band_order(band, tm, tn);
     } else {
         i64 ti, tj;
         dmma_tri_tile(blockIdx.x, ti, tj);
@@ -142,16 +143,19 @@ gemm_dmma_kernel(i64 m, i64 n, i64 k, double alpha, const double* __restrict__ A
 #pragma unroll
         for (int j = 0; j < C::NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-    const i64 nk = (k + DK - 1) / DK;
+    // slabs [kt0, kt0 + nk) of the reduction: all of them, or the tile's band
+    i64 kt0 = 0, kt1 = (k + DK - 1) / DK;
+    if (band != KB_NONE) band_slabs(band, m0, BM, n0, BN, 0, DK, kt1, kt0, kt1);
+    const i64 nk = kt1 - kt0;
 #pragma unroll
     for (int s = 0; s < DSTAGES - 1; ++s) {
-        if (s < nk) issue(s, s);
+        if (s < nk) issue(kt0 + s, s);
         cp_commit();
     }
     for (i64 kt = 0; kt < nk; ++kt) {
         cp_wait<DSTAGES - 2>();
         __syncthreads();  // slab kt has landed; the buffer of slab kt - 1 is free
-        if (kt + DSTAGES - 1 < nk) issue(kt + DSTAGES - 1, int((kt + DSTAGES - 1) % DSTAGES));
+        if (kt + DSTAGES - 1 < nk) issue(kt0 + kt + DSTAGES - 1, int((kt + DSTAGES - 1) % DSTAGES));
         cp_commit();
         const int st = int(kt % DSTAGES);
         // fragment element (row wm0 + 8i + lr, k kk + lk) and (k kk + lk, column wn0 + 8j + lr)
@@ -206,7 +210,7 @@ using Small = DmmaCfg<64, 64, 32, 32>;   // 4 warps
 
 template <class C, int TRI, int BM, int BN, int VEC>
 int launch_dmma_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
-                  const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+                  const double* b, i64 ldb, double beta, double* c, i64 ldc, int band) {
     static unsigned configured = 0;  // one bit per device
     int dev = 0;
     MBG_CUDA(cudaGetDevice(&dev));
@@ -223,7 +227,7 @@ int launch_dmma_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha
     }
     cudaStream_t s = stream();
 #define DM(TA_, TB_) \
-    gemm_dmma_kernel<C, TA_, TB_, TRI, BM, BN, VEC><<<grid, C::THREADS, C::SMEM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    gemm_dmma_kernel<C, TA_, TB_, TRI, BM, BN, VEC><<<grid, C::THREADS, C::SMEM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band)
     if (!ta && !tb) DM(false, false);
     else if (!ta && tb) DM(false, true);
     else if (ta && !tb) DM(true, false);
@@ -234,29 +238,30 @@ int launch_dmma_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha
 
 template <class C, int TRI, int BM, int BN>
 int launch_dmma(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
-                const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+                const double* b, i64 ldb, double beta, double* c, i64 ldc, int band = KB_NONE) {
     const bool vec = (reinterpret_cast<uintptr_t>(a) % 16 == 0) && (reinterpret_cast<uintptr_t>(b) % 16 == 0) &&
                      lda % 2 == 0 && ldb % 2 == 0;
-    if (vec) return launch_dmma_v<C, TRI, BM, BN, 2>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    return launch_dmma_v<C, TRI, BM, BN, 1>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (vec) return launch_dmma_v<C, TRI, BM, BN, 2>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
+    return launch_dmma_v<C, TRI, BM, BN, 1>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
 }
 
 }  // namespace
 
 // C := alpha op(A) op(B) + beta C in FP64 on the tensor pipe (alpha != 0, k > 0).
+// band (KB_*): one operand is a dense triangle; each tile runs its part of k.
 int dgemm_dmma(char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
-               const double* b, i64 ldb, double beta, double* c, i64 ldc) {
+               const double* b, i64 ldb, double beta, double* c, i64 ldc, int band) {
     ProfScope prof("gemm_dmma_f64");
     const i64 gm = cdiv(m, 128), gn = cdiv(n, 128);
     if (gm * gn < 2 * 148) {  // under two waves of 128 x 128 tiles: 64 x 64 tiles
         const i64 sm = cdiv(m, 64), sn = cdiv(n, 64);
         if (sn > 65535 || sm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
         return launch_dmma<Small, 0, 64, 64>(is_t(ta), is_t(tb), dim3((unsigned)sm, (unsigned)sn), m, n, k, alpha,
-                                             a, lda, b, ldb, beta, c, ldc);
+                                             a, lda, b, ldb, beta, c, ldc, band);
     }
     if (gn > 65535 || gm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
     return launch_dmma<Big, 0, 128, 128>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha, a,
-                                         lda, b, ldb, beta, c, ldc);
+                                         lda, b, ldb, beta, c, ldc, band);
 }
 
 // Lower ('L') or upper triangle of C := alpha op(A) op(B) + beta C (dsyrk).

@@ -19,24 +19,25 @@ using namespace f32t;
 template <int FT, bool TA, bool TB, int TRI, bool VA, bool VB>
 __global__ void __launch_bounds__(FNT, FT == 128 ? 2 : 4)
 gemm_f32_kernel(i64 m, i64 n, i64 k, float alpha, const float* __restrict__ A, i64 lda,
-                const float* __restrict__ B, i64 ldb, float beta, float* __restrict__ C, i64 ldc) {
+                const float* __restrict__ B, i64 ldb, float beta, float* __restrict__ C, i64 ldc, int band) {
     extern __shared__ __align__(16) float fsm[];
     i64 tm, tn;
     if (TRI == 0) {
         tm = blockIdx.x;
         tn = blockIdx.y;
+        band_order(band, tm, tn);
     } else {
         i64 ti, tj;
         f32_tri_tile(blockIdx.x, ti, tj);
         if (TRI == 1) { tm = ti; tn = tj; } else { tm = tj; tn = ti; }
     }
-    f32_tile<FT, TA, TB, TRI, VA, VB>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tm, tn, fsm);
+    f32_tile<FT, TA, TB, TRI, VA, VB>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tm, tn, fsm, band);
 }
 
 
 template <int FT, int TRI, bool VA, bool VB>
 int launch_f32_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
-                 const float* b, i64 ldb, float beta, float* c, i64 ldc) {
+                 const float* b, i64 ldb, float beta, float* c, i64 ldc, int band) {
     constexpr size_t SM = f32_smem<FT>();
     static unsigned configured = 0;  // one bit per device: more than 48 KB of shared memory needs an opt-in
     int dev = 0;
@@ -54,7 +55,7 @@ int launch_f32_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, 
     }
     cudaStream_t s = stream();
 #define F32(TA_, TB_) \
-    gemm_f32_kernel<FT, TA_, TB_, TRI, VA, VB><<<grid, FNT, SM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    gemm_f32_kernel<FT, TA_, TB_, TRI, VA, VB><<<grid, FNT, SM, s>>>(m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band)
     if (!ta && !tb) F32(false, false);
     else if (!ta && tb) F32(false, true);
     else if (ta && !tb) F32(true, false);
@@ -66,31 +67,35 @@ int launch_f32_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, 
 
 template <int FT, int TRI>
 int launch_f32(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
-               const float* b, i64 ldb, float beta, float* c, i64 ldc) {
+               const float* b, i64 ldb, float beta, float* c, i64 ldc, int band = KB_NONE) {
     const bool va = f32_vec(!ta, a, lda), vb = f32_vec(tb, b, ldb);
-    if (va && vb) return launch_f32_v<FT, TRI, true, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    if (va) return launch_f32_v<FT, TRI, true, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    if (vb) return launch_f32_v<FT, TRI, false, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
-    return launch_f32_v<FT, TRI, false, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+    if (va && vb)
+        return launch_f32_v<FT, TRI, true, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
+    if (va)
+        return launch_f32_v<FT, TRI, true, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
+    if (vb)
+        return launch_f32_v<FT, TRI, false, true>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
+    return launch_f32_v<FT, TRI, false, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
 }
 
 }  // namespace
 
 // C := alpha op(A) op(B) + beta C (alpha != 0, k > 0): 128 x 128 tiles, or 64 x 64
 // tiles (4 x 4 per thread) when 128-tiles would fill fewer than two waves.
+// band (KB_*): one operand is a dense triangle; each tile runs its part of k.
 int sgemm_f32(char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda, const float* b,
-              i64 ldb, float beta, float* c, i64 ldc) {
+              i64 ldb, float beta, float* c, i64 ldc, int band) {
     ProfScope prof("gemm_f32");
     const i64 gm = cdiv(m, 128), gn = cdiv(n, 128);
     if (gm * gn < 2 * 148) {
         const i64 sm = cdiv(m, 64), sn = cdiv(n, 64);
         if (sn > 65535 || sm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
         return launch_f32<64, 0>(is_t(ta), is_t(tb), dim3((unsigned)sm, (unsigned)sn), m, n, k, alpha, a, lda, b,
-                                 ldb, beta, c, ldc);
+                                 ldb, beta, c, ldc, band);
     }
     if (gn > 65535 || gm > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
     return launch_f32<128, 0>(is_t(ta), is_t(tb), dim3((unsigned)gm, (unsigned)gn), m, n, k, alpha, a, lda, b,
-                              ldb, beta, c, ldc);
+                              ldb, beta, c, ldc, band);
 }
 
 // Lower ('L') or upper triangle of C := alpha op(A) op(B) + beta C (ssyrk).

@@ -75,11 +75,11 @@ __device__ __forceinline__ void f32_stage(float* tile, const float* __restrict__
 
 // One FT x FT tile (tm, tn) of C := alpha op(A) op(B) + beta C by the whole CTA,
 // staging through `fsm` (f32_smem<FT>() bytes); every copy it issued has landed
-// when it returns.
+// when it returns.  band (KB_*): one operand triangular, only the tile's slabs run.
 template <int FT, bool TA, bool TB, int TRI, bool VA, bool VB>
 __device__ __forceinline__ void f32_tile(i64 m, i64 n, i64 k, float alpha, const float* __restrict__ A, i64 lda,
                                          const float* __restrict__ B, i64 ldb, float beta, float* __restrict__ C,
-                                         i64 ldc, i64 tm, i64 tn, float* fsm) {
+                                         i64 ldc, i64 tm, i64 tn, float* fsm, int band = KB_NONE) {
     constexpr int FLD = FTile<FT>::LD, TM = FTile<FT>::TM;
     float* As = fsm;                               // [stage][k][FLD]
     float* Bs = fsm + size_t(FSTAGES) * FK * FLD;  // [stage][k][FLD]
@@ -98,16 +98,19 @@ __device__ __forceinline__ void f32_tile(i64 m, i64 n, i64 k, float alpha, const
 #pragma unroll
         for (int j = 0; j < TM; ++j) acc[i][j] = 0.0f;
 
-    const i64 nk = (k + FK - 1) / FK;
+    // slabs [kt0, kt0 + nk) of the reduction: all of them, or the tile's band
+    i64 kt0 = 0, kt1 = (k + FK - 1) / FK;
+    if (band != KB_NONE) band_slabs(band, m0, FT, n0, FT, 0, FK, kt1, kt0, kt1);
+    const i64 nk = kt1 - kt0;
 #pragma unroll
     for (int s = 0; s < FSTAGES - 1; ++s) {
-        if (s < nk) issue(s, s);
+        if (s < nk) issue(kt0 + s, s);
         cpa_commit();
     }
     for (i64 kt = 0; kt < nk; ++kt) {
         cpa_wait<FSTAGES - 2>();
         __syncthreads();  // slab kt has landed; the buffer of slab kt - 1 is free
-        if (kt + FSTAGES - 1 < nk) issue(kt + FSTAGES - 1, int((kt + FSTAGES - 1) % FSTAGES));
+        if (kt + FSTAGES - 1 < nk) issue(kt0 + kt + FSTAGES - 1, int((kt + FSTAGES - 1) % FSTAGES));
         cpa_commit();
         const float* as = As + size_t(kt % FSTAGES) * FK * FLD;
         const float* bs = Bs + size_t(kt % FSTAGES) * FK * FLD;

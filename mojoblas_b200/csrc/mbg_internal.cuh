@@ -111,18 +111,61 @@ struct Tuning {
 };
 Tuning& tuning();
 
+// ---- banded reduction: one operand triangular --------------------------------
+// When op(A) (or op(B)) is a dense copy of a triangular matrix, zero outside its
+// triangle, an output tile needs only part of the reduction:
+//   KB_A_LOWER  op(A)(i, l) = 0 for l > i:  l < m0 + bm
+//   KB_A_UPPER  op(A)(i, l) = 0 for l < i:  l >= m0
+//   KB_B_LOWER  op(B)(l, j) = 0 for l < j:  l >= n0
+//   KB_B_UPPER  op(B)(l, j) = 0 for l > j:  l < n0 + bn
+// band_slabs gives the slabs [s0, s1) of `slab` elements (of `nslabs`; this
+// launch's reduction starts at element k0 of the full one) that a tile at
+// (m0, n0) of bm x bn must run; the skipped slabs multiply exact zeros.  At
+// least one slab is kept, so every tile's pipeline runs (an extra slab outside
+// the band adds only zero products).
+enum { KB_NONE = 0, KB_A_LOWER = 1, KB_A_UPPER = 2, KB_B_LOWER = 3, KB_B_UPPER = 4 };
+
+__host__ __device__ inline void band_slabs(int band, i64 m0, i64 bm, i64 n0, i64 bn, i64 k0, i64 slab,
+                                           i64 nslabs, i64& s0, i64& s1) {
+    const i64 end = nslabs * slab;
+    i64 lo = 0, hi = end;
+    if (band == KB_A_LOWER) hi = m0 + bm - k0;
+    else if (band == KB_A_UPPER) lo = m0 - k0;
+    else if (band == KB_B_LOWER) lo = n0 - k0;
+    else if (band == KB_B_UPPER) hi = n0 + bn - k0;
+    s0 = lo <= 0 ? 0 : lo / slab;
+    s1 = hi >= end ? nslabs : (hi <= 0 ? 0 : (hi + slab - 1) / slab);
+    if (s0 > nslabs - 1) s0 = nslabs - 1;
+    if (s1 < s0 + 1) s1 = s0 + 1;
+}
+
+// Tile order of a banded launch on a (tiles_m, tiles_n) grid, heaviest tiles
+// first so that the last wave holds the short ones: for an op(A) band the block
+// index walks the n-tiles of one m-tile row before the next row (rows by
+// decreasing work), for KB_B_UPPER the n-tiles are taken from the last.
+__device__ inline void band_order(int band, i64& tm, i64& tn) {
+    if (band == KB_A_LOWER || band == KB_A_UPPER) {
+        const i64 lin = blockIdx.x + i64(blockIdx.y) * gridDim.x;
+        tn = lin % gridDim.y;
+        tm = lin / gridDim.y;
+        if (band == KB_A_LOWER) tm = gridDim.x - 1 - tm;
+    } else if (band == KB_B_UPPER) {
+        tn = gridDim.y - 1 - tn;
+    }
+}
+
 // ---- kernels (implemented in the other translation units) --------------------
 template <typename T>
 int gemm_plain(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a, i64 lda,
                const T* b, i64 ldb, T beta, T* c, i64 ldc);
 // FP32 CUDA-core GEMM, 128 x 128 tiles, cp.async pipeline (gemm_f32.cu): alpha != 0, k > 0
 int sgemm_f32(char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda, const float* b,
-              i64 ldb, float beta, float* c, i64 ldc);
+              i64 ldb, float beta, float* c, i64 ldc, int band = KB_NONE);
 int sgemmt_f32(char uplo, char ta, char tb, i64 n, i64 k, float alpha, const float* a, i64 lda,
                const float* b, i64 ldb, float beta, float* c, i64 ldc);
 // FP64 tensor-pipe GEMM (gemm_dmma.cu): alpha != 0, k > 0
 int dgemm_dmma(char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
-               const double* b, i64 ldb, double beta, double* c, i64 ldc);
+               const double* b, i64 ldb, double beta, double* c, i64 ldc, int band = KB_NONE);
 int dgemmt_dmma(char uplo, char ta, char tb, i64 n, i64 k, double alpha, const double* a, i64 lda,
                 const double* b, i64 ldb, double beta, double* c, i64 ldc);
 // lower (uplo 'L') or upper triangle of C := alpha*op(A)*op(B) + beta*C
@@ -141,13 +184,29 @@ int dgemm_mode(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, doub
                const double* a, i64 lda, const double* b, i64 ldb, double beta, double* c,
                i64 ldc);
 // tensor-core paths (tc_gemm.cu)
+// A triangular operand read straight from the user's matrix (trmm): its split /
+// slicing pre-pass keeps only the strict triangle of the logical operand (row r,
+// reduction index l; keep 1: l < r, keep 2: l > r; the other triangle and the
+// diagonal read as zero and are never loaded), and the epilogue forms
+//     C = alpha op(A) op(B) + d .* C,   d per row (dvec_mode 1) or column (2),
+// reading each element of C before the same thread overwrites it, so C may be
+// the other operand: the GEMM reads the operands only through the pre-pass planes.
+struct TriOperand {
+    int keep_a = 0, keep_b = 0;   // pre-pass masks of op(A) and of op(B)^T
+    const void* dvec = nullptr;   // float* or double* by the routine's precision
+    int dvec_mode = 0;
+};
+// tri_uplo 'L' / 'U': only that triangle of C is written (syrk, triangular adjoints);
+// band: one operand triangular (KB_*), each tile runs only its part of the reduction
 int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha,
                    const float* a, i64 lda, const float* b, i64 ldb, float beta, float* c,
-                   i64 ldc, char tri_uplo);
-// tri_uplo 'L' / 'U': only that triangle of C is written (syrk, triangular adjoints)
+                   i64 ldc, char tri_uplo, int band = KB_NONE, const TriOperand* tri_op = nullptr);
 int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
                    const double* a, i64 lda, const double* b, i64 ldb, double beta,
-                   double* c, i64 ldc, char tri_uplo = 0);
+                   double* c, i64 ldc, char tri_uplo = 0, int band = KB_NONE,
+                   const TriOperand* tri_op = nullptr);
+// longest reduction of one Ozaki launch (int32-exact accumulators)
+i64 ozaki_max_k(int slices);
 
 // trsm and trmm on device operands (trsm.cu)
 template <typename T>

@@ -249,6 +249,10 @@ struct Params {
     int num_kb;            // k slabs
     int tiles_m, tiles_n;  // output tiles
     int tri;               // 0 full, 1 lower, 2 upper (element mask + tile skip)
+    int band;              // KB_*: one operand triangular, each tile runs its band of slabs
+    i64 band_k0;           // first k element of this launch within the full reduction
+    const float* dvec;     // non-null: C = alpha acc + d .* C, d per row (dvec_mode 1) or column (2)
+    int dvec_mode;
     void* c;
     i64 ldc;
     double alpha, beta;
@@ -314,14 +318,25 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int first_m = g * group;
     const int gsize = min(group, P.tiles_m - first_m);
     const int in_g = tile - g * per_group;
-    const int tm = first_m + in_g % gsize;
-    const int tn = in_g / gsize;
+    int tm = first_m + in_g % gsize;
+    int tn = in_g / gsize;
+    // banded launches: heaviest tiles first (the last wave holds the short ones)
+    if (P.band == KB_A_LOWER) tm = P.tiles_m - 1 - tm;
+    if (P.band == KB_B_UPPER) tn = P.tiles_n - 1 - tn;
     const i64 m0 = i64(tm) * BM, n0 = i64(tn) * C::BN;
     if (P.tri == 1 && m0 + BM <= n0) return;        // tile strictly above the diagonal
     if (P.tri == 2 && m0 > n0 + C::BN - 1) return;  // tile strictly below the diagonal
 
-    const int chunk_slabs = C::OZAKI ? P.num_kb : C::CHUNK;
-    const int nchunks = (P.num_kb + chunk_slabs - 1) / chunk_slabs;
+    // slabs [kb0, kb0 + nkb) of the reduction: all of them, or the tile's band
+    int kb0 = 0, nkb = P.num_kb;
+    if (P.band != KB_NONE) {
+        i64 s0, s1;
+        band_slabs(P.band, m0, BM, n0, C::BN, P.band_k0, C::BK, P.num_kb, s0, s1);
+        kb0 = int(s0);
+        nkb = int(s1 - s0);
+    }
+    const int chunk_slabs = C::OZAKI ? nkb : C::CHUNK;
+    const int nchunks = (nkb + chunk_slabs - 1) / chunk_slabs;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -349,26 +364,26 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             // ---------------- TMA producer ----------------
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
-            for (int kb = 0; kb < P.num_kb; ++kb) {
+            for (int kb = 0; kb < nkb; ++kb) {
                 const int s = kb % C::STAGES;
                 const uint32_t ph = (kb / C::STAGES) & 1;
                 if (!mbar_wait(&empty[s], ph ^ 1, P.err, 1)) break;
                 uint8_t* sa = smem + s * C::STAGE_BYTES;
                 uint8_t* sb = sa + C::TERMS * C::A_PLANE;
                 mbar_expect_tx(&full[s], C::STAGE_BYTES);
-                tma_load_3d(sa, &tmA, &full[s], kb * C::BK, int(m0), 0);
-                tma_load_3d(sb, &tmB, &full[s], kb * C::BK, int(n0), 0);
+                tma_load_3d(sa, &tmA, &full[s], (kb0 + kb) * C::BK, int(m0), 0);
+                tma_load_3d(sb, &tmB, &full[s], (kb0 + kb) * C::BK, int(n0), 0);
             }
             // all issued loads must land before the CTA can exit: the last
             // STAGES slabs are the only ones possibly still in flight
-            for (int kb = max(0, P.num_kb - C::STAGES); kb < P.num_kb; ++kb)
+            for (int kb = max(0, nkb - C::STAGES); kb < nkb; ++kb)
                 mbar_wait(&full[kb % C::STAGES], (kb / C::STAGES) & 1, P.err, 2);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             // ---------------- MMA issuer ----------------
             int chunk = 0;
-            for (int kb = 0; kb < P.num_kb; ++kb) {
+            for (int kb = 0; kb < nkb; ++kb) {
                 const int kin = kb % chunk_slabs;  // slab index within the chunk
                 const int buf = chunk & 1;
                 if (!C::OZAKI && kin == 0 && chunk >= 2) {
@@ -398,7 +413,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                     }
                 }
                 umma_commit(&empty[s]);  // slot s is free once these MMAs have read it
-                if (kin == chunk_slabs - 1 || kb == P.num_kb - 1) {
+                if (kin == chunk_slabs - 1 || kb == nkb - 1) {
                     umma_commit(&tfull[buf]);  // chunk complete
                     ++chunk;
                 }
@@ -441,7 +456,25 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 // waits for memory once per 8 columns, not once per column
                 // beta == 1 (the trsm updates): C += v as a reduction in L2 — one
                 // add per element, rounded as c + v, with no read in the thread
-                if (beta == 1.0f) {
+                if (P.dvec) {  // trmm: C = alpha acc + d C, d per row or per column
+                    const float drow = P.dvec_mode == 1 ? P.dvec[row] : 0.0f;
+#pragma unroll
+                    for (int c0 = 0; c0 < C::EPI_COLS; c0 += 8) {
+                        float cv[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const i64 col = cbase + c0 + j;
+                            cv[j] = col < P.n ? Cm[row + col * P.ldc] : 0.0f;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const i64 col = cbase + c0 + j;
+                            if (col >= P.n) continue;
+                            const float d = P.dvec_mode == 1 ? drow : P.dvec[col];
+                            Cm[row + col * P.ldc] = fmaf(d, cv[j], alpha * acc[c0 + j]);
+                        }
+                    }
+                } else if (beta == 1.0f) {
 #pragma unroll
                     for (int j = 0; j < C::EPI_COLS; ++j) {
                         const i64 col = cbase + j;
@@ -539,6 +572,10 @@ struct OzParams {
     i64 m, n;
     int num_kb, tiles_m, tiles_n;
     int tri;  // 0 full, 1 lower, 2 upper (element mask + tile skip)
+    int band;     // KB_*: one operand triangular, each tile runs its band of slabs
+    i64 band_k0;  // first k element of this launch within the full reduction
+    const double* dvec;  // non-null: C = alpha acc + d .* C, d per row (dvec_mode 1) or column (2)
+    int dvec_mode;
     double* c;
     i64 ldc;
     double alpha, beta;
@@ -556,15 +593,15 @@ template <int S, int PASS> struct OzPass {
 // Issues one pass: every k slab, the products of diagonals [LO, HI), then
 // commits the accumulators to the epilogue.  Returns false if a wait expired.
 template <class C, int PASS>
-__device__ __forceinline__ bool oz_mma_pass(const OzParams& P, uint8_t* smem, uint64_t* full, uint64_t* empty,
-                                            uint64_t* tfull, uint64_t* tempty, uint32_t tmem) {
+__device__ __forceinline__ bool oz_mma_pass(const OzParams& P, int nkb, uint8_t* smem, uint64_t* full,
+                                            uint64_t* empty, uint64_t* tfull, uint64_t* tempty, uint32_t tmem) {
     constexpr int LO = OzPass<C::S, PASS>::LO, HI = OzPass<C::S, PASS>::HI;
     if (PASS > 0) {  // the epilogue must have read the previous pass's accumulators
         if (!mbar_wait(tempty, (PASS - 1) & 1, P.err, 13)) return false;
         tc_fence_after();
     }
-    for (int kb = 0; kb < P.num_kb; ++kb) {
-        const int it = PASS * P.num_kb + kb;
+    for (int kb = 0; kb < nkb; ++kb) {
+        const int it = PASS * nkb + kb;
         const int s = it % C::STAGES;
         if (!mbar_wait(&full[s], (it / C::STAGES) & 1, P.err, 14)) return false;
         tc_fence_after();
@@ -605,9 +642,22 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
     const int first_m = g * group;
     const int gsize = min(group, P.tiles_m - first_m);
     const int in_g = tile - g * per_group;
-    const i64 m0 = i64(first_m + in_g % gsize) * BM, n0 = i64(in_g / gsize) * C::BN;
+    int tm = first_m + in_g % gsize, tn = in_g / gsize;
+    // banded launches: heaviest tiles first (the last wave holds the short ones)
+    if (P.band == KB_A_LOWER) tm = P.tiles_m - 1 - tm;
+    if (P.band == KB_B_UPPER) tn = P.tiles_n - 1 - tn;
+    const i64 m0 = i64(tm) * BM, n0 = i64(tn) * C::BN;
     if (P.tri == 1 && m0 + BM <= n0) return;        // tile strictly above the diagonal
     if (P.tri == 2 && m0 > n0 + C::BN - 1) return;  // tile strictly below the diagonal
+
+    // slabs [kb0, kb0 + nkb) of the reduction: all of them, or the tile's band
+    int kb0 = 0, nkb = P.num_kb;
+    if (P.band != KB_NONE) {
+        i64 s0, s1;
+        band_slabs(P.band, m0, BM, n0, C::BN, P.band_k0, C::BKB, P.num_kb, s0, s1);
+        kb0 = int(s0);
+        nkb = int(s1 - s0);
+    }
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -627,7 +677,7 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int total = C::NPASS * P.num_kb;
+    const int total = C::NPASS * nkb;
 
     if (warp == 0) {
         if (lane == 0) {
@@ -635,7 +685,7 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
             for (int it = 0; it < total; ++it) {
-                const int pass = it / P.num_kb, kb = it - pass * P.num_kb;
+                const int pass = it / nkb, kb = it - pass * nkb;
                 int lo, hi, planes;
                 pass_range<C>(pass, lo, hi, planes);
                 const int s = it % C::STAGES;
@@ -645,8 +695,8 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
                 uint8_t* sb = sa + C::S * C::PLANE;
                 mbar_expect_tx(&full[s], uint32_t(2 * planes * C::PLANE));
                 const bool all = planes == C::S;
-                tma_load_3d(sa, all ? &tmA : &tmAlo, &full[s], kb * C::BKB, int(m0), 0);
-                tma_load_3d(sb, all ? &tmB : &tmBlo, &full[s], kb * C::BKB, int(n0), 0);
+                tma_load_3d(sa, all ? &tmA : &tmAlo, &full[s], (kb0 + kb) * C::BKB, int(m0), 0);
+                tma_load_3d(sb, all ? &tmB : &tmBlo, &full[s], (kb0 + kb) * C::BKB, int(n0), 0);
             }
             for (int it = max(0, total - C::STAGES); it < total; ++it)
                 mbar_wait(&full[it % C::STAGES], (it / C::STAGES) & 1, P.err, 12);
@@ -654,8 +704,8 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
     } else if (warp == 1) {
         if (lane == 0) {
             // ---------------- MMA issuer ----------------
-            if (oz_mma_pass<C, 0>(P, smem, full, empty, tfull, tempty, tmem) && C::NPASS > 1)
-                oz_mma_pass<C, 1>(P, smem, full, empty, tfull, tempty, tmem);
+            if (oz_mma_pass<C, 0>(P, nkb, smem, full, empty, tfull, tempty, tmem) && C::NPASS > 1)
+                oz_mma_pass<C, 1>(P, nkb, smem, full, empty, tfull, tempty, tmem);
         }
     } else {
         // ---------------- epilogue warps ----------------
@@ -695,7 +745,27 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
             // beta == 1: reductions in L2, as in the split kernel's epilogue; else
             // 4 columns at a time, loads first (the 64 fp64 accumulators leave
             // room for no more)
-            if (P.beta == 1.0) {
+            if (P.dvec) {  // trmm: C = alpha acc + d C, d per row or per column
+                const double drow = P.dvec_mode == 1 ? P.dvec[row] : 0.0;
+#pragma unroll
+                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+                    double cv[4];
+                    int ec[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const i64 col = cbase + c0 + j;
+                        ec[j] = col < P.n ? P.eb[col] : 0;
+                        cv[j] = col < P.n ? P.c[row + col * P.ldc] : 0.0;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const i64 col = cbase + c0 + j;
+                        if (col >= P.n) continue;
+                        const double d = P.dvec_mode == 1 ? drow : P.dvec[col];
+                        P.c[row + col * P.ldc] = fma(d, cv[j], P.alpha * (acc[c0 + j] * pow2_exact(er + ec[j])));
+                    }
+                }
+            } else if (P.beta == 1.0) {
 #pragma unroll
                 for (int j = 0; j < C::EPI_COLS; ++j) {
                     const i64 col = cbase + j;
@@ -739,16 +809,23 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
 constexpr int PT_R = 64, PT_K = 32;  // pre-pass tile: 64 rows x 32 k
 
 // value(r, l) of the logical rows x K operand: K-major source src[l + r*ld],
-// otherwise src[r + l*ld]; outside rows x K it is zero (padding).
+// otherwise src[r + l*ld]; outside rows x K it is zero (padding).  keep (a
+// triangular operand read from the user's matrix): 0 every element, 1 only
+// l < r, 2 only l > r; the rest (the other triangle and the diagonal) is zero
+// and never read.
+__device__ __forceinline__ bool kept(int keep, i64 r, i64 l) {
+    return keep == 0 || (keep == 1 ? l < r : l > r);
+}
+
 template <typename T, bool KMAJOR>
 __device__ __forceinline__ void load_tile(const T* __restrict__ src, i64 ld, i64 rows, i64 K, i64 r0,
-                                          i64 l0, T (&tile)[PT_R][PT_K + 1]) {
+                                          i64 l0, int keep, T (&tile)[PT_R][PT_K + 1]) {
     for (int e = threadIdx.x; e < PT_R * PT_K; e += blockDim.x) {
         int rr, ll;
         if (KMAJOR) { rr = e / PT_K; ll = e % PT_K; } else { rr = e % PT_R; ll = e / PT_R; }
         const i64 r = r0 + rr, l = l0 + ll;
         T v = T(0);
-        if (r < rows && l < K) v = KMAJOR ? src[l + r * ld] : src[r + l * ld];
+        if (r < rows && l < K && kept(keep, r, l)) v = KMAJOR ? src[l + r * ld] : src[r + l * ld];
         tile[rr][ll] = v;
     }
 }
@@ -756,10 +833,10 @@ __device__ __forceinline__ void load_tile(const T* __restrict__ src, i64 ld, i64
 template <int TERMS, bool KMAJOR>
 __global__ void __launch_bounds__(256)
 split_bf16_kernel(const float* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp,
-                  __nv_bfloat16* __restrict__ planes) {
+                  __nv_bfloat16* __restrict__ planes, int keep = 0) {
     __shared__ float tile[PT_R][PT_K + 1];
     const i64 r0 = i64(blockIdx.y) * PT_R, l0 = i64(blockIdx.x) * PT_K;
-    load_tile<float, KMAJOR>(src, ld, rows, K, r0, l0, tile);
+    load_tile<float, KMAJOR>(src, ld, rows, K, r0, l0, keep, tile);
     __syncthreads();
     const size_t plane = size_t(Rp) * size_t(Kp);
     for (int e = threadIdx.x; e < PT_R * (PT_K / 2); e += blockDim.x) {
@@ -793,11 +870,13 @@ __device__ __forceinline__ void oz_exponent_max(int* e, i64 r, double mx) {
 
 template <bool KMAJOR>
 __global__ void __launch_bounds__(256)
-row_exponent_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, int* __restrict__ e) {
+row_exponent_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, int* __restrict__ e, int keep) {
     if (KMAJOR) {  // warp per row and k chunk, lanes along k (coalesced)
         const i64 r = i64(blockIdx.x) * 8 + (threadIdx.x >> 5);
         if (r >= rows) return;
-        const i64 l0 = i64(blockIdx.y) * OZ_EXP_KWARP, l1 = min(K, l0 + OZ_EXP_KWARP);
+        i64 l0 = i64(blockIdx.y) * OZ_EXP_KWARP, l1 = min(K, l0 + OZ_EXP_KWARP);
+        if (keep == 1) l1 = min(l1, r);       // only l < r
+        if (keep == 2) l0 = max(l0, r + 1);   // only l > r
         const double* row = src + r * ld;
         double mx = 0.0;
 #pragma unroll 8
@@ -815,7 +894,7 @@ row_exponent_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, int
 #pragma unroll
             for (int j = 0; j < OZ_EXP_KCHUNK / 8; ++j) {
                 const i64 l = l0 + ty + 8 * j;
-                if (l < K) mx = fmax(mx, fabs(src[r + l * ld]));
+                if (l < K && kept(keep, r, l)) mx = fmax(mx, fabs(src[r + l * ld]));
             }
         }
         part[ty][tx] = mx;
@@ -845,10 +924,10 @@ __device__ __forceinline__ unsigned long long oz_fixed56(double v, int er, bool&
 template <bool KMAJOR>
 __global__ void __launch_bounds__(256)
 slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
-                int* __restrict__ e, int8_t* __restrict__ planes) {
+                int* __restrict__ e, int8_t* __restrict__ planes, int keep) {
     __shared__ double tile[PT_R][PT_K + 1];
     const i64 r0 = i64(blockIdx.y) * PT_R, l0 = i64(blockIdx.x) * PT_K;
-    load_tile<double, KMAJOR>(src, ld, rows, K, r0, l0, tile);
+    load_tile<double, KMAJOR>(src, ld, rows, K, r0, l0, keep, tile);
     __syncthreads();
     const size_t plane = size_t(Rp) * size_t(Kp);
     for (int q = threadIdx.x; q < PT_R * (PT_K / 4); q += blockDim.x) {
@@ -937,36 +1016,37 @@ int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, Params& P, const cha
 }
 
 template <int TERMS>
-int launch_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, __nv_bfloat16* planes) {
+int launch_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, __nv_bfloat16* planes,
+                 int keep = 0) {
     ProfScope prof("split_bf16");
     dim3 g(unsigned(Kp / PT_K), unsigned(Rp / PT_R));
     if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
-    if (kmajor) split_bf16_kernel<TERMS, true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
-    else split_bf16_kernel<TERMS, false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
+    if (kmajor) split_bf16_kernel<TERMS, true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes, keep);
+    else split_bf16_kernel<TERMS, false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes, keep);
     return check_launch("split_bf16");
 }
 
 int launch_slices(const double* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
-                  int* e, int8_t* planes) {
+                  int* e, int8_t* planes, int keep = 0) {
     {
         ProfScope prof("ozaki_exponent");
         MBG_CUDA(cudaMemsetAsync(e, 0x80, sizeof(int) * size_t(rows), stream()));  // 0x80808080 < any exponent
         if (kmajor) {
             dim3 g(unsigned(cdiv(rows, 8)), unsigned(cdiv(K, OZ_EXP_KWARP)));
             if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
-            row_exponent_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, e);
+            row_exponent_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, e, keep);
         } else {
             dim3 g(unsigned(cdiv(rows, 32)), unsigned(cdiv(K, OZ_EXP_KCHUNK)));
             if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
-            row_exponent_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, e);
+            row_exponent_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, e, keep);
         }
         MBG_TRY(check_launch("ozaki_exponent"));
     }
     ProfScope prof("ozaki_slice");
     dim3 g(unsigned(Kp / PT_K), unsigned(Rp / PT_R));
     if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
-    if (kmajor) slice_i8_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes);
-    else slice_i8_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes);
+    if (kmajor) slice_i8_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes, keep);
+    else slice_i8_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes, keep);
     return check_launch("ozaki_slice");
 }
 
@@ -976,7 +1056,9 @@ inline i64 roundup(i64 x, i64 m) { return cdiv(x, m) * m; }
 
 // ---- split-precision sgemm ------------------------------------------------------
 int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a,
-                   i64 lda, const float* b, i64 ldb, float beta, float* c, i64 ldc, char tri_uplo) {
+                   i64 lda, const float* b, i64 ldb, float beta, float* c, i64 ldc, char tri_uplo, int band,
+                   const TriOperand* tri_op) {
+    const int keep_a = tri_op ? tri_op->keep_a : 0, keep_b = tri_op ? tri_op->keep_b : 0;
     using namespace tc;
     if (m == 0 || n == 0) return MBG_OK;
     if (terms != 2 && terms != 3) return MBG_ERR_INVALID_MODE;
@@ -995,11 +1077,11 @@ int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha
     __nv_bfloat16* pb = shared_planes ? pa : reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + a_bytes);
     // op(A) rows are K-contiguous when A is transposed; op(B)^T rows when B is not
     if (terms == 2) {
-        MBG_TRY(launch_split<2>(a, lda, is_t(ta), m, k, Mp, Kp, pa));
-        if (!shared_planes) MBG_TRY(launch_split<2>(b, ldb, is_n(tb), n, k, Np, Kp, pb));
+        MBG_TRY(launch_split<2>(a, lda, is_t(ta), m, k, Mp, Kp, pa, keep_a));
+        if (!shared_planes) MBG_TRY(launch_split<2>(b, ldb, is_n(tb), n, k, Np, Kp, pb, keep_b));
     } else {
-        MBG_TRY(launch_split<3>(a, lda, is_t(ta), m, k, Mp, Kp, pa));
-        if (!shared_planes) MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, k, Np, Kp, pb));
+        MBG_TRY(launch_split<3>(a, lda, is_t(ta), m, k, Mp, Kp, pa, keep_a));
+        if (!shared_planes) MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, k, Np, Kp, pb, keep_b));
     }
     CUtensorMap ma, mb;
     MBG_TRY(make_map(&ma, pa, false, Kp, Mp, terms, 64, BM));
@@ -1008,6 +1090,11 @@ int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha
     P.m = m; P.n = n; P.num_kb = int(Kp / 32);
     P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
     P.tri = tri ? (is_l(tri_uplo) ? 1 : 2) : 0;
+    P.band = band; P.band_k0 = 0;
+    if (tri_op && tri_op->dvec_mode) {
+        P.dvec = static_cast<const float*>(tri_op->dvec);
+        P.dvec_mode = tri_op->dvec_mode;
+    }
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
     if (terms == 2) return launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
     return launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
@@ -1032,14 +1119,21 @@ int launch_ozaki(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap
 }
 }  // namespace tc
 
+// Longest reduction one Ozaki launch takes: its int32 accumulators hold at most
+// `slices` products of K terms of 127^2 each; longer k runs in several launches.
+i64 ozaki_max_k(int slices) { return (i64(0x7fffffff) / (i64(slices) * 127 * 127)) / 32 * 32; }
+
 int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a,
-                   i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc, char tri_uplo) {
+                   i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc, char tri_uplo, int band,
+                   const TriOperand* tri_op) {
     using namespace tc;
     if (m == 0 || n == 0) return MBG_OK;
     if (slices < 2 || slices > 8) return MBG_ERR_INVALID_MODE;
     const int BN = 128;
-    // int32 accumulators hold at most `slices` products of K terms of 127^2 each
-    const i64 kchunk_max = (i64(0x7fffffff) / (i64(slices) * 127 * 127)) / 32 * 32;
+    const i64 kchunk_max = ozaki_max_k(slices);
+    // a masked triangular operand and the in-place epilogue need the whole k in one launch
+    if (tri_op && k > kchunk_max) return MBG_ERR_UNSUPPORTED;
+    const int keep_a = tri_op ? tri_op->keep_a : 0, keep_b = tri_op ? tri_op->keep_b : 0;
     const bool tri = tri_uplo != 0;
     // syrk shares one set of slices and exponents for both operands (op(B)^T = op(A))
     const bool shared_planes = tri && a == b && lda == ldb && (is_n(ta) != is_n(tb)) && m == n;
@@ -1060,8 +1154,8 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
         // op(A)[:, k0:k0+klen] and op(B)[k0:k0+klen, :]
         const double* ak = is_n(ta) ? a + k0 * lda : a + k0;
         const double* bk = is_n(tb) ? b + k0 : b + k0 * ldb;
-        MBG_TRY(launch_slices(ak, lda, is_t(ta), m, klen, Mp, Kpc, slices, ea, pa));
-        if (!shared_planes) MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb));
+        MBG_TRY(launch_slices(ak, lda, is_t(ta), m, klen, Mp, Kpc, slices, ea, pa, keep_a));
+        if (!shared_planes) MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb, keep_b));
         CUtensorMap ma, mb, mal, mbl;
         MBG_TRY(make_map(&ma, pa, true, Kpc, Mp, slices, 32, BM));
         MBG_TRY(make_map(&mb, pb, true, Kpc, Np, slices, 32, BN));
@@ -1071,6 +1165,11 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
         P.m = m; P.n = n; P.num_kb = int(Kpc / 32);
         P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
         P.tri = tri ? (is_l(tri_uplo) ? 1 : 2) : 0;
+        P.band = band; P.band_k0 = k0;
+        if (tri_op && tri_op->dvec_mode) {
+            P.dvec = static_cast<const double*>(tri_op->dvec);
+            P.dvec_mode = tri_op->dvec_mode;
+        }
         P.c = c; P.ldc = ldc; P.alpha = alpha;
         P.beta = (k0 == 0) ? beta : 1.0;
         P.ea = ea; P.eb = eb;

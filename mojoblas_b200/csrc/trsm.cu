@@ -24,13 +24,9 @@
 // op(A) D = R in the caller's mode and add D to X.
 //
 // Triangular multiply (trmm, src/level3/trmm.mojo:20-305), at the end of this
-// file, uses the same recursion with products in place of solves:
-//     left, op(A) lower:   B2 = alpha op(A)22 B2 + alpha op(A)21 B1, then B1 = alpha op(A)11 B1
-//     left, op(A) upper:   B1 = alpha op(A)11 B1 + alpha op(A)12 B2, then B2 = alpha op(A)22 B2
-// (the right side likewise over column blocks of B), ordered so that every
-// update reads the block of B that is still unmodified.  Diagonal blocks of at
-// most TRMM_LEAF rows are one GEMM of a dense copy of the triangle with a copy
-// of the block of B.
+// file, needs no recursion: it is one GEMM of a dense copy of the triangle with a
+// copy of B, each output tile running only the slabs of the reduction where the
+// triangle is nonzero.
 #include "mbg_internal.cuh"
 #include "block_solve.cuh"
 
@@ -318,15 +314,16 @@ int solve_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i
 }
 
 // W[0:m, 0:m] = tri(op(A)) as a dense column-major block: the effective triangle
-// (unit diagonal when UNIT), zeros elsewhere; the other triangle of A is not read.
+// (unit diagonal when UNIT, a zero diagonal when ZERO_DIAG), zeros elsewhere; the
+// other triangle of A is not read.
 template <typename T>
 __global__ void tri_dense_kernel(i64 m, const T* __restrict__ A, i64 lda, bool lower, bool trans, bool unit,
-                                 T* __restrict__ W) {
+                                 bool zero_diag, T* __restrict__ W) {
     for (i64 l = blockIdx.y; l < m; l += gridDim.y)
         for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x) {
             const bool in = lower ? i > l : i < l;
             T v = T(0);
-            if (i == l) v = unit ? T(1) : (trans ? A[l + i * lda] : A[i + l * lda]);
+            if (i == l) v = zero_diag ? T(0) : (unit ? T(1) : A[i + i * lda]);
             else if (in) v = trans ? A[l + i * lda] : A[i + l * lda];
             W[i + l * m] = v;
         }
@@ -344,7 +341,7 @@ int residual_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m
         {
             ProfScope prof("trsm_tri_dense");
             dim3 g((unsigned)imin(cdiv(m, 256), 64), (unsigned)imin(m, 65535));
-            tri_dense_kernel<T><<<g, 256, 0, stream()>>>(m, a, lda, lower, trans, unit, ww.as<T>());
+            tri_dense_kernel<T><<<g, 256, 0, stream()>>>(m, a, lda, lower, trans, unit, false, ww.as<T>());
             MBG_TRY(check_launch("trsm_tri_dense"));
         }
         return gemm_plain<T>('N', 'N', m, n, m, T(-1), ww.as<T>(), m, x, ldx, T(1), r, ldr);
@@ -415,88 +412,149 @@ int solve_left_refined(int mode, int slices, int refine, bool lower, bool trans,
 }
 
 // ---- triangular multiply ---------------------------------------------------
-constexpr i64 TRMM_LEAF = 256;
-
 template <typename T>
-int launch_tri_dense(i64 m, const T* a, i64 lda, bool lower, bool trans, bool unit, T* w) {
+int launch_tri_dense(i64 m, const T* a, i64 lda, bool lower, bool trans, bool unit, bool zero_diag, T* w) {
     ProfScope prof("trsm_tri_dense");
     dim3 g((unsigned)imin(cdiv(m, 256), 64), (unsigned)imin(m, 65535));
-    tri_dense_kernel<T><<<g, 256, 0, stream()>>>(m, a, lda, lower, trans, unit, w);
+    tri_dense_kernel<T><<<g, 256, 0, stream()>>>(m, a, lda, lower, trans, unit, zero_diag, w);
     return check_launch("trsm_tri_dense");
 }
 
-// Leaf: B[0:nb, 0:n] := alpha tri(op(A)) B (left) or B[0:m, 0:nb] := alpha B tri(op(A))
-// (right), nb <= TRMM_LEAF: one plain GEMM of the dense triangle with a copy of B.
+// B += alpha diag(A) X (left) or alpha X diag(A) (right): the diagonal term of a
+// triangular product in working precision, one fused multiply-add per element.
+// Each thread owns rows i and walks columns j: a left-side diagonal entry is
+// loaded once per row, a right-side one is the same for the whole block.
 template <typename T>
-int trmm_leaf(bool left, bool lower, bool trans, bool unit, i64 m, i64 n, T alpha, const T* a, i64 lda, T* b,
-              i64 ldb) {
-    const i64 nb = left ? m : n;
-    Workspace ww, wt;
-    MBG_TRY(ww.reserve(sizeof(T) * size_t(nb) * size_t(nb)));
-    MBG_TRY(wt.reserve(sizeof(T) * size_t(m) * size_t(n)));
-    T* w = ww.as<T>();
-    T* t = wt.as<T>();
-    MBG_TRY(launch_tri_dense<T>(nb, a, lda, lower, trans, unit, w));
-    MBG_TRY(launch_copy<T>(m, n, T(1), b, ldb, t, m));
-    if (left) return gemm_plain<T>('N', 'N', m, n, m, alpha, w, nb, t, m, T(0), b, ldb);
-    return gemm_plain<T>('N', 'N', m, n, n, alpha, t, m, w, nb, T(0), b, ldb);
+__global__ void trmm_diag_kernel(i64 m, i64 n, T alpha, const T* __restrict__ A, i64 lda, bool unit, bool left,
+                                 const T* __restrict__ X, i64 ldx, T* __restrict__ B, i64 ldb) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x) {
+        const T arow = (left && !unit) ? alpha * A[i + i * lda] : alpha;
+#pragma unroll 4
+        for (i64 j = blockIdx.y; j < n; j += gridDim.y) {
+            const T ad = (left || unit) ? arow : alpha * A[j + j * lda];
+            B[i + j * ldb] = fma(ad, X[i + j * ldx], B[i + j * ldb]);
+        }
+    }
 }
 
-// B := alpha op(A) B, op(A) effectively lower / upper; A is m x m.
 template <typename T>
-int trmm_left(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, T alpha, const T* a,
-              i64 lda, T* b, i64 ldb) {
-    if (m <= TRMM_LEAF) return trmm_leaf<T>(true, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
-    const i64 m1 = split_point(m), m2 = m - m1;
-    const char tc = trans ? 'T' : 'N';
-    const T* a22 = a + m1 + m1 * lda;
-    if (lower) {  // B2 first: its update reads the unmodified B1
-        MBG_TRY(trmm_left<T>(mode, slices, lower, trans, unit, m2, n, alpha, a22, lda, b + m1, ldb));
-        MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m2, n, m1, alpha, op_at(a, lda, trans, m1, 0), lda, b, ldb,
-                             T(1), b + m1, ldb));
-        return trmm_left<T>(mode, slices, lower, trans, unit, m1, n, alpha, a, lda, b, ldb);
-    }
-    MBG_TRY(trmm_left<T>(mode, slices, lower, trans, unit, m1, n, alpha, a, lda, b, ldb));
-    MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m1, n, m2, alpha, op_at(a, lda, trans, 0, m1), lda, b + m1, ldb,
-                         T(1), b, ldb));
-    return trmm_left<T>(mode, slices, lower, trans, unit, m2, n, alpha, a22, lda, b + m1, ldb);
+int launch_trmm_diag(i64 m, i64 n, T alpha, const T* a, i64 lda, bool unit, bool left, const T* x, i64 ldx, T* b,
+                     i64 ldb) {
+    ProfScope prof("trmm_diag");
+    dim3 g((unsigned)imin(cdiv(m, 256), 1024), (unsigned)imin(n, 64));
+    trmm_diag_kernel<T><<<g, 256, 0, stream()>>>(m, n, alpha, a, lda, unit, left, x, ldx, b, ldb);
+    return check_launch("trmm_diag");
 }
 
-// B := alpha B op(A), op(A) effectively lower / upper; A is n x n.
+// C := alpha op(A) op(B) (NN, beta = 0) with one operand a dense triangle (band
+// KB_*), in a precision mode: every tile runs only the slabs its band needs.
+inline int gemm_banded(int mode, int slices, int band, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
+                       const float* b, i64 ldb, float* c, i64 ldc) {
+    (void)slices;
+    if (mode == MBG_MODE_PLAIN) return sgemm_f32('N', 'N', m, n, k, alpha, a, lda, b, ldb, 0.0f, c, ldc, band);
+    if (mode != MBG_MODE_BF16X3 && mode != MBG_MODE_BF16X6) return MBG_ERR_INVALID_MODE;
+    return sgemm_split_tc(mode == MBG_MODE_BF16X6 ? 3 : 2, 'N', 'N', m, n, k, alpha, a, lda, b, ldb, 0.0f, c, ldc,
+                          0, band);
+}
+inline int gemm_banded(int mode, int slices, int band, i64 m, i64 n, i64 k, double alpha, const double* a,
+                       i64 lda, const double* b, i64 ldb, double* c, i64 ldc) {
+    if (mode == MBG_MODE_PLAIN) return dgemm_dmma('N', 'N', m, n, k, alpha, a, lda, b, ldb, 0.0, c, ldc, band);
+    if (mode != MBG_MODE_OZAKI) return MBG_ERR_INVALID_MODE;
+    return dgemm_ozaki_tc(slices, 'N', 'N', m, n, k, alpha, a, lda, b, ldb, 0.0, c, ldc, 0, band);
+}
+
+// d[i] = alpha * A(i, i) (alpha for a unit diagonal): the epilogue's multiplier of B.
 template <typename T>
-int trmm_right(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, T alpha, const T* a,
-               i64 lda, T* b, i64 ldb) {
-    if (n <= TRMM_LEAF) return trmm_leaf<T>(false, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
-    const i64 n1 = split_point(n), n2 = n - n1;
-    const char tc = trans ? 'T' : 'N';
-    const T* a22 = a + n1 + n1 * lda;
-    T* b2 = b + n1 * ldb;
-    if (lower) {  // B1 = B1 P11 + B2 P21 first: it reads the unmodified B2
-        MBG_TRY(trmm_right<T>(mode, slices, lower, trans, unit, m, n1, alpha, a, lda, b, ldb));
-        MBG_TRY(gemm_in_mode(mode, slices, 'N', tc, m, n1, n2, alpha, b2, ldb, op_at(a, lda, trans, n1, 0), lda,
-                             T(1), b, ldb));
-        return trmm_right<T>(mode, slices, lower, trans, unit, m, n2, alpha, a22, lda, b2, ldb);
+__global__ void trmm_dvec_kernel(i64 n, T alpha, const T* __restrict__ A, i64 lda, bool unit, T* __restrict__ d) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        d[i] = unit ? alpha : alpha * A[i + i * lda];
+}
+
+inline int gemm_tri_operand(int mode, int slices, int band, char ta, char tb, i64 m, i64 n, i64 k, float alpha,
+                            const float* a, i64 lda, const float* b, i64 ldb, float* c, i64 ldc,
+                            const TriOperand* t) {
+    (void)slices;
+    if (mode != MBG_MODE_BF16X3 && mode != MBG_MODE_BF16X6) return MBG_ERR_INVALID_MODE;
+    return sgemm_split_tc(mode == MBG_MODE_BF16X6 ? 3 : 2, ta, tb, m, n, k, alpha, a, lda, b, ldb, 0.0f, c, ldc, 0,
+                          band, t);
+}
+inline int gemm_tri_operand(int mode, int slices, int band, char ta, char tb, i64 m, i64 n, i64 k, double alpha,
+                            const double* a, i64 lda, const double* b, i64 ldb, double* c, i64 ldc,
+                            const TriOperand* t) {
+    if (mode != MBG_MODE_OZAKI) return MBG_ERR_INVALID_MODE;
+    return dgemm_ozaki_tc(slices, ta, tb, m, n, k, alpha, a, lda, b, ldb, 0.0, c, ldc, 0, band, t);
+}
+
+// Split / Ozaki trmm in place, with no copy of A or B: the pre-pass reads the
+// strict triangle of op(A) straight from A and B into its planes, the GEMM's
+// tiles run their band of the reduction, and each epilogue thread forms
+// alpha * (off-diagonal sum) + alpha d_i B(i, j) from the old B(i, j) it then
+// overwrites (the diagonal term in working precision, one FMA).
+template <typename T>
+int trmm_in_place(int mode, int slices, bool left, bool lower, bool trans, bool unit, i64 m, i64 n, T alpha,
+                  const T* a, i64 lda, T* b, i64 ldb) {
+    const i64 na = left ? m : n;
+    Workspace wd;
+    MBG_TRY(wd.reserve(sizeof(T) * size_t(na)));
+    T* dv = wd.as<T>();
+    {
+        ProfScope prof("trmm_diag");
+        trmm_dvec_kernel<T><<<(unsigned)imin(cdiv(na, 256), 1024), 256, 0, stream()>>>(na, alpha, a, lda, unit, dv);
+        MBG_TRY(check_launch("trmm_diag"));
     }
-    // B2 = B1 P12 + B2 P22 first: it reads the unmodified B1
-    MBG_TRY(trmm_right<T>(mode, slices, lower, trans, unit, m, n2, alpha, a22, lda, b2, ldb));
-    MBG_TRY(gemm_in_mode(mode, slices, 'N', tc, m, n2, n1, alpha, b, ldb, op_at(a, lda, trans, 0, n1), lda, T(1),
-                         b2, ldb));
-    return trmm_right<T>(mode, slices, lower, trans, unit, m, n1, alpha, a, lda, b, ldb);
+    TriOperand t;
+    t.dvec = dv;
+    const char tc = trans ? 'T' : 'N';
+    if (left) {
+        t.keep_a = lower ? 1 : 2;  // op(A)(r, l) kept for l < r (lower) or l > r
+        t.dvec_mode = 1;
+        return gemm_tri_operand(mode, slices, lower ? KB_A_LOWER : KB_A_UPPER, tc, 'N', m, n, m, alpha, a, lda, b,
+                                ldb, b, ldb, &t);
+    }
+    t.keep_b = lower ? 2 : 1;  // op(B)^T(r, l) = op(A)(l, r): kept for l > r (lower) or l < r
+    t.dvec_mode = 2;
+    return gemm_tri_operand(mode, slices, lower ? KB_B_LOWER : KB_B_UPPER, 'N', tc, m, n, n, alpha, b, ldb, a, lda,
+                            b, ldb, &t);
 }
 
 }  // namespace
 
+// B := alpha op(A) B (side 'L') or alpha B op(A) (side 'R'), A triangular.
+// One GEMM out of place: W = tri(op(A)) as a dense block (zeros outside the
+// triangle, unit diagonal when diag 'U'; the other triangle of A is not read),
+// X = a copy of B, then B = alpha W X (or alpha X W) with the triangular band, so
+// each output tile runs only the part of the reduction where W is nonzero:
+// m^2 n multiply-adds plus the diagonal tiles' halves, in one launch.
+// The split / Ozaki modes keep the diagonal out of the split product: its term
+// alpha d_i x_ij is added with one FMA in working precision, so the product's
+// accuracy does not depend on the ratio between the diagonal and the rest of a
+// row (Ozaki slices are scaled per row, so a dominant diagonal would leave the
+// off-diagonal entries few bits).  They run in place (trmm_in_place above); an
+// Ozaki product longer than one exact launch (ozaki_max_k) takes this path with W
+// holding the strictly triangular part and a separate diagonal pass.
 template <typename T>
 int trmm_device(int mode, int slices, char side, char uplo, char ta, char diag, i64 m, i64 n, T alpha,
                 const T* a, i64 lda, T* b, i64 ldb) {
     if (m == 0 || n == 0) return MBG_OK;
     if (alpha == T(0)) return scale_matrix<T>(m, n, T(0), b, ldb);  // trmm.mojo:94-98: zeros
-    const bool trans = is_t(ta), unit = is_u(diag);
+    const bool trans = is_t(ta), unit = is_u(diag), left = is_l(side);
     const bool lower = (!is_u(uplo)) != trans;  // effective op(A) lower triangular
-    if (is_l(side)) return trmm_left<T>(mode, slices, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
-    return trmm_right<T>(mode, slices, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
+    const i64 na = left ? m : n;
+    if (mode != MBG_MODE_PLAIN && !(sizeof(T) == 8 && na > ozaki_max_k(slices)))
+        return trmm_in_place<T>(mode, slices, left, lower, trans, unit, m, n, alpha, a, lda, b, ldb);
+    Workspace ww, wx;
+    MBG_TRY(ww.reserve(sizeof(T) * size_t(na) * size_t(na)));
+    MBG_TRY(wx.reserve(sizeof(T) * size_t(m) * size_t(n)));
+    T* w = ww.as<T>();
+    T* x = wx.as<T>();
+    const bool split_diag = mode != MBG_MODE_PLAIN;
+    MBG_TRY(launch_tri_dense<T>(na, a, lda, lower, trans, unit, split_diag, w));
+    MBG_TRY(launch_copy<T>(m, n, T(1), b, ldb, x, m));
+    if (left) MBG_TRY(gemm_banded(mode, slices, lower ? KB_A_LOWER : KB_A_UPPER, m, n, m, alpha, w, na, x, m, b, ldb));
+    else MBG_TRY(gemm_banded(mode, slices, lower ? KB_B_LOWER : KB_B_UPPER, m, n, n, alpha, x, m, w, na, b, ldb));
+    if (!split_diag) return MBG_OK;
+    return launch_trmm_diag<T>(m, n, alpha, a, lda, unit, left, x, m, b, ldb);
 }
-
 template int trmm_device<float>(int, int, char, char, char, char, i64, i64, float, const float*, i64, float*, i64);
 template int trmm_device<double>(int, int, char, char, char, char, i64, i64, double, const double*, i64, double*,
                                  i64);

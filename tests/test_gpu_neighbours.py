@@ -150,10 +150,12 @@ def test_syr2k(oracle, dt, mode, uplo, trans, n, k, alpha, beta):
 @pytest.mark.parametrize("uplo", ["U", "L"])
 @pytest.mark.parametrize("ta", ["N", "T"])
 @pytest.mark.parametrize("diag", ["N", "U"])
-@pytest.mark.parametrize("na,nb,alpha", [(200, 37, 0.75), (1000, 70, -1.5)])
+@pytest.mark.parametrize("na,nb,alpha", [(200, 37, 0.75), (1000, 70, -1.5), (700, 5, 2.0), (129, 600, 1.0)])
 def test_trmm(oracle, dt, mode, side, uplo, ta, diag, na, nb, alpha):
-    """na = order of A: 200 is one dense leaf, 1000 recurses over four leaves (two split
-    levels, ragged) with GEMM updates between them; nb = the other dimension of B."""
+    """na = order of A, nb = the other dimension of B.  The product runs as one GEMM
+    whose tiles skip the zero half of the triangle: ragged orders (200, 700, 129 =
+    one row of tiles plus one), 1000 with several tile rows, and thin (5) or wide
+    (600) B, so both tile sizes and every band (left / right, lower / upper) run."""
     rng = np.random.default_rng(na + nb)
     m, n = (na, nb) if side == "L" else (nb, na)
     lda, ldb = na + 2, m + 1
@@ -181,8 +183,8 @@ def test_trmm_alpha_zero_writes_zeros():
     assert np.all(b == 0.0)
 
 
-def test_device_pointers_and_recursion_depth(oracle):
-    """Device-resident operands (the fast path) at a size with three split levels."""
+def test_device_pointers(oracle):
+    """Device-resident operands (the fast path), trmm with a 2100-order triangle."""
     torch = need_gpu()
     rng = np.random.default_rng(9)
     m, n = 2100, 300
