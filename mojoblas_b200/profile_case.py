@@ -3,8 +3,9 @@
     python mojoblas_b200/profile_case.py --op sgemm --mode bf16x6 --m 4096 --n 4096 --k 8192
     python mojoblas_b200/profile_case.py --op dgemm --mode ozaki --slices 8 --m 2048 --n 2048 --k 4096
     python mojoblas_b200/profile_case.py --op dtrsm --mode ozaki --m 4096 --n 4096
+    python mojoblas_b200/profile_case.py --op strmm --mode bf16x6 --m 4096 --n 4096
 
-Inputs are uniform[-1, 1) (trsm: diagonally dominant lower triangle), device
+Inputs are uniform[-1, 1) (trsm, trmm: diagonally dominant lower triangle), device
 resident; each rep is one call through the C ABI.  Prints the mean CUDA-event
 time per call.
 """
@@ -20,7 +21,8 @@ sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--op", choices=["sgemm", "dgemm", "ssyrk", "dtrsm", "strsm", "grouped_sgemm", "grouped_strsm"],
+    ap.add_argument("--op", choices=["sgemm", "dgemm", "ssyrk", "dtrsm", "strsm", "grouped_sgemm", "grouped_strsm",
+                                     "strmm", "dtrmm", "ssymm", "dsymm", "ssyr2k", "dsyr2k"],
                     default="sgemm")
     ap.add_argument("--mode", choices=["plain", "bf16x3", "bf16x6", "ozaki"], default="bf16x6")
     ap.add_argument("--slices", type=int, default=8)
@@ -95,6 +97,18 @@ def main():
 
         def call():
             return lib.mbg_ssyrk_ex(mode, b"L", b"N", a.n, a.k, 1.0, A.data_ptr(), a.n, 0.0, Cm.data_ptr(), a.n)
+    elif a.op in ("ssymm", "dsymm"):  # Left, Upper: C (m x n) = A (m x m, symmetric) B
+        A, B, Cm = cm(a.m, a.m), cm(a.m, a.n), cm(a.m, a.n)
+
+        def call():
+            args = (b"L", b"U", a.m, a.n, 1.0, A.data_ptr(), a.m, B.data_ptr(), a.m, 0.0, Cm.data_ptr(), a.m)
+            return lib.mbg_ssymm_ex(mode, *args) if a.op == "ssymm" else lib.mbg_dsymm_ex(mode, a.slices, *args)
+    elif a.op in ("ssyr2k", "dsyr2k"):  # Lower, NoTrans: A, B n x k
+        A, B, Cm = cm(a.n, a.k), cm(a.n, a.k), cm(a.n, a.n)
+
+        def call():
+            args = (b"L", b"N", a.n, a.k, 1.0, A.data_ptr(), a.n, B.data_ptr(), a.n, 0.0, Cm.data_ptr(), a.n)
+            return lib.mbg_ssyr2k_ex(mode, *args) if a.op == "ssyr2k" else lib.mbg_dsyr2k_ex(mode, a.slices, *args)
     else:
         m = a.m
         A = torch.randn((m, m), generator=g, device="cuda", dtype=dt) / m ** 0.5
@@ -104,6 +118,9 @@ def main():
 
         def call():
             X.copy_(B0)
+            if a.op in ("strmm", "dtrmm"):  # Left, Lower, NoTrans, NonUnit
+                args = (b"L", b"L", b"N", b"N", m, a.n, 1.0, A.data_ptr(), m, X.data_ptr(), m)
+                return lib.mbg_strmm_ex(mode, *args) if a.op == "strmm" else lib.mbg_dtrmm_ex(mode, a.slices, *args)
             if a.op == "dtrsm":
                 return lib.mbg_dtrsm_ex(mode, a.slices, a.refine, b"L", b"L", b"N", b"N", m, a.n, 1.0, A.data_ptr(),
                                         m, X.data_ptr(), m)
