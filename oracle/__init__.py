@@ -1,7 +1,8 @@
 """ORACLE — test infrastructure only.
 
-Python access to the CPU restatement of mojoBLAS's level-3 routines
-(ref_level3.cpp, built into liboracle_level3.so by the Makefile beside it) plus
+Python access to the CPU restatement of mojoBLAS's level-3 routines and of
+gemv / trsv (ref_level3.cpp, ref_level2.cpp, built into liboracle_level3.so by
+the Makefile beside it) plus
 float64 / extended-precision reference products.  Only tests, the smoke check
 and bench.py's CPU-baseline legs import this package; the CUDA library never
 does.
@@ -56,6 +57,10 @@ def lib():
             "orc_ssyr2k": [ch, ch, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_float, f32p, i64],
             "orc_dsyr2k": [ch, ch, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64],
             "orc_strmm": [ch, ch, ch, ch, i64, i64, C.c_float, f32p, i64, f32p, i64],
+            "orc_sgemv": [ch, i64, i64, C.c_float, f32p, i64, f32p, i64, C.c_float, f32p, i64],
+            "orc_dgemv": [ch, i64, i64, C.c_double, f64p, i64, f64p, i64, C.c_double, f64p, i64],
+            "orc_strsv": [ch, ch, ch, i64, f32p, i64, f32p, i64],
+            "orc_dtrsv": [ch, ch, ch, i64, f64p, i64, f64p, i64],
             "orc_dtrmm": [ch, ch, ch, ch, i64, i64, C.c_double, f64p, i64, f64p, i64],
         }
         for name, argtypes in sig.items():
@@ -142,6 +147,45 @@ def trmm(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb) -> int:
     dt = _dt(b)
     fn = lib().orc_strmm if dt == np.float32 else lib().orc_dtrmm
     return fn(_c(side), _c(uplo), _c(ta), _c(diag), m, n, alpha, _p(a, dt), lda, _p(b, dt), ldb)
+
+
+def gemv(trans, m, n, alpha, a, lda, x, incx, beta, y, incy) -> int:
+    """The reference's gemv (src/level2/gemv.mojo:23-212), in place on y."""
+    dt = _dt(y)
+    fn = lib().orc_sgemv if dt == np.float32 else lib().orc_dgemv
+    return fn(_c(trans), m, n, alpha, _p(a, dt), lda, _p(x, dt), incx, beta, _p(y, dt), incy)
+
+
+def trsv(uplo, trans, diag, n, a, lda, x, incx) -> int:
+    """The reference's trsv (src/level2/trsv.mojo:20-214), in place on x."""
+    dt = _dt(x)
+    fn = lib().orc_strsv if dt == np.float32 else lib().orc_dtrsv
+    return fn(_c(uplo), _c(trans), _c(diag), n, _p(a, dt), lda, _p(x, dt), incx)
+
+
+def vec(buf: np.ndarray, n: int, inc: int) -> np.ndarray:
+    """The n-vector stored in buf with increment inc (inc < 0: element 0 at (1 - n) * inc)."""
+    start = 0 if inc > 0 else (1 - n) * inc
+    return buf[start + np.arange(n) * inc]
+
+
+def gemv_f64(trans, m, n, alpha, a, lda, x, incx, beta, y, incy) -> np.ndarray:
+    """float64 y := alpha op(A) x + beta y as a dense vector (y untouched)."""
+    A = view(a, m, n, lda).astype(np.float64)
+    notrans = _c(trans) in (b"N", b"n")
+    lenx, leny = (n, m) if notrans else (m, n)
+    out = float(alpha) * ((A if notrans else A.T) @ vec(x, lenx, incx).astype(np.float64))
+    if beta != 0:
+        out = out + float(beta) * vec(y, leny, incy).astype(np.float64)
+    return out
+
+
+def trsv_f64(uplo, trans, diag, n, a, lda, x, incx) -> np.ndarray:
+    """float64 solution of op(A) z = x as a dense vector (x untouched)."""
+    import scipy.linalg as sl
+    A = op(tri(view(a, n, n, lda).astype(np.float64), uplo, diag), trans)
+    lower = (_c(uplo) in (b"L", b"l")) == (_c(trans) in (b"N", b"n"))
+    return sl.solve_triangular(A, vec(x, n, incx).astype(np.float64), lower=lower)
 
 
 # ---------------------------------------------------------------------------

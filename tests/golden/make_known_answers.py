@@ -1,11 +1,13 @@
-"""Generate tests/golden/level3_known_answers.json from the reference's own tests.
+"""Generate tests/golden/level3_known_answers.json and level2_known_answers.json
+from the reference's own tests.
 
 The reference's level-3 tests (mojoBLAS tests/test_level3.mojo) hard-code tiny
 column-major inputs and the expected outputs of gemm / syrk / trsm / trmm / symm /
-syr2k.  Mojo cannot run in this container, so this script reads that file as
-text, replays each test's assignments and records the call and its expected
-values.  The JSON it writes is committed; nothing reads the reference at test
-time.
+syr2k; its level-2 tests (tests/test_level2.mojo, tests/test_level2_extended.mojo)
+do the same for gemv and trsv, among others.  Mojo cannot run in this container,
+so this script reads those files as text, replays each test's assignments and
+records the call and its expected values.  The JSON it writes is committed;
+nothing reads the reference at test time.
 
 Run:  python tests/golden/make_known_answers.py [path/to/mojoBLAS]
 (default path: /root/reference)
@@ -18,6 +20,7 @@ import sys
 from pathlib import Path
 
 ROUTINES = ("gemm", "syrk", "trsm", "trmm", "symm", "syr2k")
+LEVEL2_ROUTINES = ("gemv", "trsv")
 
 
 def _split_args(s: str) -> list[str]:
@@ -47,7 +50,7 @@ def _eval(expr: str, env: dict):
     return eval(expr, {"__builtins__": {}, "max": max, "min": min}, env)  # ints / floats / names
 
 
-def parse(path: Path) -> list[dict]:
+def parse(path: Path, routines=ROUTINES) -> list[dict]:
     text = path.read_text()
     cases = []
     for fm in re.finditer(r"^def (test_\w+)\(\) raises:\n(.*?)(?=^def |\Z)", text, re.S | re.M):
@@ -87,8 +90,8 @@ def parse(path: Path) -> list[dict]:
             if m and m.group(1) in arrays:
                 arrays[m.group(1)][int(m.group(2))] = float(_eval(m.group(3), env))
                 continue
-            m = re.match(r"(%s)(\[DType\.(float32|float64)\])?\($" % "|".join(ROUTINES), ln) or \
-                re.match(r"(%s)(\[DType\.(float32|float64)\])?\((.*)\)$" % "|".join(ROUTINES), ln)
+            m = re.match(r"(%s)(\[DType\.(float32|float64)\])?\($" % "|".join(routines), ln) or \
+                re.match(r"(%s)(\[DType\.(float32|float64)\])?\((.*)\)$" % "|".join(routines), ln)
             if m:
                 routine = m.group(1)
                 if ln.endswith("("):  # call spans lines
@@ -136,6 +139,20 @@ def main() -> None:
     dst = Path(__file__).with_name("level3_known_answers.json")
     dst.write_text(json.dumps(out, indent=1) + "\n")
     print(f"wrote {len(cases)} cases to {dst}")
+    cases2 = []
+    for name in ("test_level2.mojo", "test_level2_extended.mojo"):
+        for c in parse(root / "tests" / name, LEVEL2_ROUTINES):
+            c["file"] = f"tests/{name}"
+            cases2.append(c)
+    out2 = {
+        "source": "mojoBLAS tests/test_level2.mojo and tests/test_level2_extended.mojo (gemv / trsv known "
+                  "answers, column-major)",
+        "default_float32_tolerance": "assert_almost_equal defaults: atol=1e-8, rtol=1e-5",
+        "cases": cases2,
+    }
+    dst2 = Path(__file__).with_name("level2_known_answers.json")
+    dst2.write_text(json.dumps(out2, indent=1) + "\n")
+    print(f"wrote {len(cases2)} cases to {dst2}")
 
 
 if __name__ == "__main__":
