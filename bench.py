@@ -334,6 +334,91 @@ def run_neighbours(torch, lib, L, stream):
     return out
 
 
+def run_level2(torch, lib, L, stream):
+    """gemv (NoTrans and Trans, 8192 x 8192, float32 and float64, alpha 1.5, beta 0.5, uniform[-1,1)) and
+    trsv (Lower / Upper, NoTrans, order 4096, the trsm configuration's triangle scaled to a vector), device
+    resident.  Bytes per call: gemv m n + m + 2n (x read, y read and written) elements; trsv n(n+1)/2 + 2n.
+    A is 256 / 512 MiB for gemv (larger than L2); the 4096-order triangle (32 / 64 MiB) fits in L2, so each
+    trsv call is preceded by a 256 MiB L2 flush."""
+    out = {}
+    pk = peaks()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(55)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+
+    def timed(call, nbytes, reps=5, flush_l2=False):
+        call()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            if flush_l2:
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        ms = tot / reps
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        return {"gbs": round(gbs, 1), "ms": round(ms, 4), "hbm_frac": round(gbs / pk["hbm_gbs"], 3)}
+
+    m = n = 8192
+    for dt, tn in ((torch.float32, "s"), (torch.float64, "d")):
+        esz = 4 if dt == torch.float32 else 8
+        A = torch.rand((n, m), generator=g, device="cuda", dtype=dt) * 2 - 1  # column-major m x n
+        x = torch.rand(max(m, n), generator=g, device="cuda", dtype=dt) * 2 - 1
+        y0 = torch.rand(max(m, n), generator=g, device="cuda", dtype=dt) * 2 - 1
+        y = y0.clone()
+        Ah = A.double().cpu().numpy().T
+        fn = lib.mbg_sgemv if tn == "s" else lib.mbg_dgemv
+        for trans in ("N", "T"):
+            def call():
+                st = fn(trans.encode(), m, n, 1.5, A.data_ptr(), m, x.data_ptr(), 1, 0.5, y.data_ptr(), 1)
+                if st:
+                    raise RuntimeError(f"gemv failed {st}: {L.last_error()}")
+            y.copy_(y0)
+            call()
+            torch.cuda.synchronize()
+            op = Ah if trans == "N" else Ah.T
+            ref = 1.5 * op @ x.double().cpu().numpy()[:op.shape[1]] + 0.5 * y0.double().cpu().numpy()[:op.shape[0]]
+            err = float(np.max(np.abs(y.double().cpu().numpy()[:op.shape[0]] - ref)) / np.max(np.abs(ref)))
+            r = timed(call, esz * (m * n + m + 2 * n))
+            r["fp64_err"] = err
+            out[f"{tn}gemv_{trans}_8192"] = r
+        del A, Ah
+
+    nt = 4096
+    for dt, tn in ((torch.float32, "s"), (torch.float64, "d")):
+        esz = 4 if dt == torch.float32 else 8
+        T = torch.randn((nt, nt), generator=g, device="cuda", dtype=dt) / np.sqrt(nt)
+        T.diagonal().copy_(2.0 + torch.randn(nt, generator=g, device="cuda", dtype=dt).abs())
+        b0 = torch.randn(nt, generator=g, device="cuda", dtype=dt)
+        xb = b0.clone()
+        Th = T.double().cpu().numpy().T
+        fn = lib.mbg_strsv if tn == "s" else lib.mbg_dtrsv
+        import scipy.linalg as sla
+        for uplo in ("L", "U"):
+            def call():
+                xb.copy_(b0)
+                st = fn(uplo.encode(), b"N", b"N", nt, T.data_ptr(), nt, xb.data_ptr(), 1)
+                if st:
+                    raise RuntimeError(f"trsv failed {st}: {L.last_error()}")
+            call()
+            torch.cuda.synchronize()
+            tri = np.tril(Th) if uplo == "L" else np.triu(Th)
+            ref = sla.solve_triangular(tri, b0.double().cpu().numpy(), lower=uplo == "L")
+            err = float(np.max(np.abs(xb.double().cpu().numpy() - ref)) / np.max(np.abs(ref)))
+            r = timed(call, esz * (nt * (nt + 1) // 2 + 2 * nt), flush_l2=True)
+            r["fp64_err"] = err
+            out[f"{tn}trsv_{uplo}N_4096"] = r
+        del T
+    out["note"] = ("GB/s = algorithmic bytes / CUDA-event time; each timed trsv call includes a 16 / 32 KiB "
+                   "device copy restoring b; hbm_frac against the " + pk["source"] + " HBM copy bandwidth")
+    del flush
+    return out
+
+
 def run_cfg4(torch, lib, L, stream):
     """Batched: 4096 sgemm problems (m, n, k log-uniform 16..512, NN, uniform[-1,1))
     and 2048 lower-triangular strsm problems (n log-uniform 8..256, nrhs uniform
@@ -799,6 +884,7 @@ def run_ours(args, rank, world, dist):
     cfg4 = {} if args.skip_cfg4 else run_cfg4(torch, lib, L, stream)
     cfg5 = {} if args.skip_cfg5 else run_cfg5(torch, lib, L, stream)
     neighbours = {} if args.skip_neighbours else run_neighbours(torch, lib, L, stream)
+    level2 = {} if args.skip_level2 else run_level2(torch, lib, L, stream)
 
     # ---- e2e through the C ABI with pinned host buffers ----
     hA = A.cpu().pin_memory()
@@ -861,6 +947,7 @@ def run_ours(args, rank, world, dist):
         "cfg4_batched": cfg4,
         "cfg5_adjoints": cfg5,
         "symm_syr2k_trmm": neighbours,
+        "gemv_trsv": level2,
         "roofline_fractions": leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk),
         "e2e": {"value": round(e2e_value, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_out, "ms_per_step": round(e2e_ms, 2)},
@@ -931,6 +1018,7 @@ def main():
     ap.add_argument("--skip-cfg4", action="store_true")
     ap.add_argument("--skip-cfg5", action="store_true")
     ap.add_argument("--skip-neighbours", action="store_true")
+    ap.add_argument("--skip-level2", action="store_true")
     ap.add_argument("--skip-context", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

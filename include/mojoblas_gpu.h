@@ -2,7 +2,8 @@
  * mojoblas_gpu.h — C ABI of the B200 (sm_100a) level-3 BLAS library.
  *
  * Drop-in boundary for mojoBLAS's level-3 routines (the gemm / syrk / trsm hot
- * path, and symm / syr2k / trmm on the same kernels).  Every routine keeps the
+ * path, and symm / syr2k / trmm on the same kernels) and for the level-2
+ * gemv / trsv next to them.  Every routine keeps the
  * argument order and meaning of the mojoBLAS routine it replaces (column-major
  * storage, element (i,j) of a matrix at p[i + j*ld], Netlib transpose / uplo /
  * side / diag characters), and returns:
@@ -105,6 +106,28 @@ int mbg_strmm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t 
               float alpha, const float* a, int64_t lda, float* b, int64_t ldb);
 int mbg_dtrmm(char side, char uplo, char trans_a, char diag, int64_t m, int64_t n,
               double alpha, const double* a, int64_t lda, double* b, int64_t ldb);
+
+/* ---- level 2: the matrix-vector neighbours --------------------------------
+ * Vectors are strided: element i of x sits at x[i * incx] for incx > 0 and at
+ * x[(n - 1 - i) * |incx|] for incx < 0 (Netlib's convention); incx == 0 is an
+ * argument error. */
+
+/* y := alpha*op(A)*x + beta*y, A m x n.  Replaces mojoBLAS gemv
+ * (src/level2/gemv.mojo:23-212); like the reference, trans must be 'N', 'T' or
+ * 'C' in upper case (anything else is info 1). */
+int mbg_sgemv(char trans, int64_t m, int64_t n, float alpha, const float* a, int64_t lda,
+              const float* x, int64_t incx, float beta, float* y, int64_t incy);
+int mbg_dgemv(char trans, int64_t m, int64_t n, double alpha, const double* a, int64_t lda,
+              const double* x, int64_t incx, double beta, double* y, int64_t incy);
+
+/* op(A)*x = b, A n x n triangular, the solution overwrites b in x.  Replaces
+ * mojoBLAS trsv (src/level2/trsv.mojo:20-214).  With uplo 'U', trans 'N' and
+ * incx != 1 the reference pairs x[j - 1] with column j and reads before the
+ * start of x (:113-125); this library solves the system. */
+int mbg_strsv(char uplo, char trans, char diag, int64_t n, const float* a, int64_t lda,
+              float* x, int64_t incx);
+int mbg_dtrsv(char uplo, char trans, char diag, int64_t n, const double* a, int64_t lda,
+              double* x, int64_t incx);
 
 /* ---- the same routines with a precision mode ----------------------------
  * mode: MBG_MODE_PLAIN, MBG_MODE_BF16X3 or MBG_MODE_BF16X6 for float;

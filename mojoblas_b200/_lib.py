@@ -44,6 +44,10 @@ SIGNATURES = {
     "mbg_dtrsm": [_ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
     "mbg_strsm_ex": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64],
     "mbg_dtrsm_ex": [_i, _i, _i, _ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64],
+    "mbg_sgemv": [_ch, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
+    "mbg_dgemv": [_ch, i64, i64, _d, _vp, i64, _vp, i64, _d, _vp, i64],
+    "mbg_strsv": [_ch, _ch, _ch, i64, _vp, i64, _vp, i64],
+    "mbg_dtrsv": [_ch, _ch, _ch, i64, _vp, i64, _vp, i64],
     "mbg_ssymm": [_ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
     "mbg_dsymm": [_ch, _ch, i64, i64, _d, _vp, i64, _vp, i64, _d, _vp, i64],
     "mbg_ssymm_ex": [_i, _ch, _ch, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],

@@ -69,6 +69,27 @@ static int trmm_info(char side, char uplo, char ta, char diag, i64 m, i64 n, i64
     return trsm_info(side, uplo, ta, diag, m, n, lda, ldb);
 }
 
+// src/level2/gemv.mojo:69-84 (trans in upper case only, as the reference checks it)
+static int gemv_info(char trans, i64 m, i64 n, i64 lda, i64 incx, i64 incy) {
+    if (trans != 'N' && trans != 'T' && trans != 'C') return 1;
+    if (m < 0) return 2;
+    if (n < 0) return 3;
+    if (lda < imax(1, m)) return 6;
+    if (incx == 0) return 8;
+    if (incy == 0) return 11;
+    return 0;
+}
+// src/level2/trsv.mojo:56-79
+static int trsv_info(char uplo, char trans, char diag, i64 n, i64 lda, i64 incx) {
+    if (!is_u(uplo) && !is_l(uplo)) return 1;
+    if (!is_n(trans) && !is_t(trans)) return 2;
+    if (!is_u(diag) && !is_n(diag)) return 3;
+    if (n < 0) return 4;
+    if (lda < imax(1, n)) return 6;
+    if (incx == 0) return 8;
+    return 0;
+}
+
 static bool valid_smode(int mode) {
     return mode == MBG_MODE_PLAIN || mode == MBG_MODE_BF16X3 || mode == MBG_MODE_BF16X6;
 }
@@ -331,6 +352,53 @@ static int trmm_entry(int mode, int slices, char side, char uplo, char ta, char 
     return finish_call(A.staged || B.staged);
 }
 
+// A strided vector of `len` elements as a 1 x len operand with leading dimension
+// |inc| (storage order kept, so a negative increment stays negative); a staged
+// copy is compact, increment +-1.
+static int prepare_vector(Operand& v, const void* p, i64 len, i64 inc, size_t elem, bool copy_in, bool copy_out,
+                          i64* dev_inc) {
+    const i64 ainc = inc > 0 ? inc : -inc;
+    MBG_TRY(v.prepare(p, 1, len, ainc, elem, copy_in, copy_out));
+    *dev_inc = v.staged ? (inc > 0 ? 1 : -1) : inc;
+    return MBG_OK;
+}
+
+template <typename T>
+static int gemv_entry(char trans, i64 m, i64 n, T alpha, const T* a, i64 lda, const T* x, i64 incx, T beta, T* y,
+                      i64 incy) {
+    int info = gemv_info(trans, m, n, lda, incx, incy);
+    if (info) return info;
+    if (m == 0 || n == 0 || (alpha == T(0) && beta == T(1))) return MBG_OK;  // gemv.mojo:86-87
+    const i64 lenx = trans == 'N' ? n : m, leny = trans == 'N' ? m : n;
+    Operand A, X, Y;
+    i64 dix = incx, diy = incy;
+    if (alpha != T(0)) {
+        MBG_TRY(A.prepare(a, m, n, lda, sizeof(T), true, false));
+        MBG_TRY(prepare_vector(X, x, lenx, incx, sizeof(T), true, false, &dix));
+    }
+    MBG_TRY(prepare_vector(Y, y, leny, incy, sizeof(T), beta != T(0), true, &diy));
+    int st = gemv_device<T>(trans, m, n, alpha, (const T*)A.dev, A.dev_ld, (const T*)X.dev, dix, beta, (T*)Y.dev,
+                            diy);
+    if (st) return st;
+    MBG_TRY(Y.finish());
+    return finish_call(A.staged || X.staged || Y.staged);
+}
+
+template <typename T>
+static int trsv_entry(char uplo, char trans, char diag, i64 n, const T* a, i64 lda, T* x, i64 incx) {
+    int info = trsv_info(uplo, trans, diag, n, lda, incx);
+    if (info) return info;
+    if (n == 0) return MBG_OK;  // trsv.mojo:81-82
+    Operand A, X;
+    i64 dix = incx;
+    MBG_TRY(A.prepare(a, n, n, lda, sizeof(T), true, false));
+    MBG_TRY(prepare_vector(X, x, n, incx, sizeof(T), true, true, &dix));
+    int st = trsv_device<T>(uplo, trans, diag, n, (const T*)A.dev, A.dev_ld, (T*)X.dev, dix);
+    if (st) return st;
+    MBG_TRY(X.finish());
+    return finish_call(A.staged || X.staged);
+}
+
 }  // namespace mbg
 
 using namespace mbg;
@@ -395,6 +463,23 @@ int mbg_dtrsm_ex(int mode, int slices, int refine, char side, char uplo, char ta
                  int64_t ldb) {
     if (!valid_dmode(mode, slices) || refine < 0) return MBG_ERR_INVALID_MODE;
     return trsm_entry<double>(mode, slices, refine, side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb);
+}
+
+// ---- gemv / trsv ----
+int mbg_sgemv(char trans, int64_t m, int64_t n, float alpha, const float* a, int64_t lda, const float* x,
+              int64_t incx, float beta, float* y, int64_t incy) {
+    return gemv_entry<float>(trans, m, n, alpha, a, lda, x, incx, beta, y, incy);
+}
+int mbg_dgemv(char trans, int64_t m, int64_t n, double alpha, const double* a, int64_t lda, const double* x,
+              int64_t incx, double beta, double* y, int64_t incy) {
+    return gemv_entry<double>(trans, m, n, alpha, a, lda, x, incx, beta, y, incy);
+}
+int mbg_strsv(char uplo, char trans, char diag, int64_t n, const float* a, int64_t lda, float* x, int64_t incx) {
+    return trsv_entry<float>(uplo, trans, diag, n, a, lda, x, incx);
+}
+int mbg_dtrsv(char uplo, char trans, char diag, int64_t n, const double* a, int64_t lda, double* x,
+              int64_t incx) {
+    return trsv_entry<double>(uplo, trans, diag, n, a, lda, x, incx);
 }
 
 // ---- symm / syr2k / trmm ----

@@ -1,0 +1,410 @@
+// Level-2 gemv and trsv — the matrix-vector neighbours of the level-3 path
+// (mojoBLAS src/level2/gemv.mojo:23-212, src/level2/trsv.mojo:20-214).
+//
+// gemv streams A once from HBM, which bounds it: m n elements read, no reuse.
+//   NoTrans (y = alpha A x + beta y): each thread owns one row and walks a
+//     range of columns, eight independent loads in flight; a warp reads 32
+//     consecutive rows of a column (one coalesced segment); sixteen for float32.  The columns are cut
+//     into S ranges so that the grid fills the GPU, and a second pass adds the S
+//     partial sums in a fixed order (no atomics: the result does not depend on
+//     scheduling) and applies alpha and beta.
+//   Trans (y = alpha A^T x + beta y): one warp per column, lanes along the
+//     column (contiguous), eight (float32: sixteen) loads per lane in flight, a shuffle reduction
+//     in a fixed order; long columns are cut into R row ranges the same way.
+//   As in the reference, beta scales y first (beta == 0 stores zeros), and a
+//   zero product sum leaves beta y unchanged; zero entries of x skip their
+//   column (NoTrans).  Any increments, negative ones included, are indexed in
+//   place.
+//
+// trsv (op(A) x = b, x overwrites b) is a dependency chain: the row block b of
+// the solution needs every earlier block in solve order.  One persistent launch
+// does all of it.  Each 256-thread CTA takes a ticket from an atomic counter and
+// solves row block `ticket` in solve order (forward for an effectively lower
+// op(A), backward otherwise), so a CTA only ever waits for CTAs that started
+// before it.  For each earlier block it loads its tile of op(A) into registers,
+// waits for that block's flag (acquire; bounded by %globaltimer, with an abort
+// flag so that one expired wait ends the others at once), reads the published
+// x values from L2 and accumulates.  Then it reduces the partial sums, and one
+// warp solves the 64 x 64 diagonal block by substitution (pivot broadcast by a
+// shuffle, multiply by the reciprocal of the diagonal), writes its part of x
+// and releases its flag.  The reference skips zero entries of x in the NoTrans
+// substitution; so does this one.
+#include "mbg_internal.cuh"
+
+namespace mbg {
+
+namespace {
+
+constexpr int GV_THREADS = 256;
+// loads in flight per thread: 64 bytes of A (eight doubles, sixteen floats)
+template <typename T> constexpr int gv_unroll() { return sizeof(T) == 4 ? 16 : 8; }
+
+// NoTrans: P[s * m + i] = sum over columns [s * cps, (s + 1) * cps) of A(i, j) x(j),
+// or, with a single range (direct), y(i) itself.
+template <typename T>
+__global__ void __launch_bounds__(GV_THREADS)
+gemv_n_kernel(i64 m, i64 n, const T* __restrict__ A, i64 lda, const T* __restrict__ x, i64 incx, i64 kx,
+              i64 cps, T* __restrict__ P, bool direct, T alpha, T beta, T* __restrict__ y, i64 incy, i64 ky) {
+    const i64 i = blockIdx.x * (i64)GV_THREADS + threadIdx.x;
+    if (i >= m) return;
+    const i64 j0 = blockIdx.y * cps, j1 = min(n, j0 + cps);
+    constexpr int U = gv_unroll<T>();
+    const T* a = A + i;
+    T acc = T(0);
+    i64 j = j0;
+    for (; j + U <= j1; j += U) {
+        T av[U], xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            xv[u] = x[kx + (j + u) * incx];
+            av[u] = a[(j + u) * lda];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (xv[u] != T(0)) acc = fma(av[u], xv[u], acc);
+    }
+    for (; j < j1; ++j) {
+        const T xj = x[kx + j * incx];
+        if (xj != T(0)) acc = fma(a[j * lda], xj, acc);
+    }
+    if (direct) {
+        T& yi = y[ky + i * incy];
+        T v = beta == T(0) ? T(0) : (beta == T(1) ? yi : beta * yi);
+        if (acc != T(0)) v = v + alpha * acc;
+        yi = v;
+    } else {
+        P[blockIdx.y * m + i] = acc;
+    }
+}
+
+// Trans: one warp per column j and row range r: P[r * n + j] = sum_i A(i, j) x(i)
+// (or y(j) itself with a single range).
+template <typename T>
+__global__ void __launch_bounds__(GV_THREADS)
+gemv_t_kernel(i64 m, i64 n, const T* __restrict__ A, i64 lda, const T* __restrict__ x, i64 incx, i64 kx,
+              i64 rpr, T* __restrict__ P, bool direct, T alpha, T beta, T* __restrict__ y, i64 incy, i64 ky) {
+    const int lane = threadIdx.x & 31;
+    const i64 j = blockIdx.x * (i64)(GV_THREADS / 32) + (threadIdx.x >> 5);
+    if (j >= n) return;
+    const i64 i0 = blockIdx.y * rpr, i1 = min(m, i0 + rpr);
+    constexpr int U = gv_unroll<T>();
+    const T* a = A + j * lda;
+    T acc = T(0);
+    i64 i = i0 + lane;
+    for (; i + 32 * (U - 1) < i1; i += 32 * U) {
+        T av[U], xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            av[u] = a[i + 32 * u];
+            xv[u] = x[kx + (i + 32 * u) * incx];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc = fma(av[u], xv[u], acc);
+    }
+    for (; i < i1; i += 32) acc = fma(a[i], x[kx + i * incx], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane != 0) return;
+    if (direct) {
+        T& yj = y[ky + j * incy];
+        T v = beta == T(0) ? T(0) : (beta == T(1) ? yj : beta * yj);
+        if (acc != T(0)) v = v + alpha * acc;
+        yj = v;
+    } else {
+        P[blockIdx.y * n + j] = acc;
+    }
+}
+
+// y(i) = beta y(i) + alpha sum_s P[s * len + i] (partial sums in a fixed order)
+template <typename T>
+__global__ void gemv_finish_kernel(i64 len, i64 parts, const T* __restrict__ P, T alpha, T beta,
+                                   T* __restrict__ y, i64 incy, i64 ky) {
+    const i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (i >= len) return;
+    T s = T(0);
+    for (i64 p = 0; p < parts; ++p) s += P[p * len + i];
+    T& yi = y[ky + i * incy];
+    T v = beta == T(0) ? T(0) : (beta == T(1) ? yi : beta * yi);
+    if (s != T(0)) v = v + alpha * s;
+    yi = v;
+}
+
+template <typename T>
+__global__ void scale_vector_kernel(i64 len, T beta, T* __restrict__ y, i64 incy, i64 ky) {
+    const i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (i >= len) return;
+    T& yi = y[ky + i * incy];
+    yi = beta == T(0) ? T(0) : beta * yi;
+}
+
+// ---- trsv ----------------------------------------------------------------------
+constexpr int TV_NB = 64, TV_THREADS = 256, TV_GROUPS = TV_THREADS / TV_NB, TV_PER = TV_NB / TV_GROUPS;
+constexpr unsigned long long TV_WAIT_NS = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long tv_clock() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ int tv_load_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void tv_store_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+struct TrsvSync {
+    int* flags;   // per row block: 1 once its part of x is published
+    int* ticket;  // solve-order counter
+    int* abort;   // set by an expired wait: every other wait gives up at once
+    int* err;     // library error flag (code, site)
+};
+
+// Thread 0 only: wait (bounded) for `flag`; false if the launch is aborting.
+__device__ bool tv_wait(const int* flag, const TrsvSync& s) {
+    if (tv_load_acquire(flag)) return true;
+    const unsigned long long t0 = tv_clock();
+    while (true) {
+#pragma unroll 1
+        for (int k = 0; k < 64; ++k)
+            if (tv_load_acquire(flag)) return true;
+        if (*(volatile int*)s.abort) return false;
+        if (tv_clock() - t0 > TV_WAIT_NS) {
+            atomicExch(s.abort, 1);
+            if (s.err) {
+                atomicExch(s.err, 1);
+                atomicExch(s.err + 1, 40);
+            }
+            return false;
+        }
+    }
+}
+
+// op(A)[i, l] for a column-major A
+template <typename T, bool TRANS>
+__device__ __forceinline__ T opa(const T* __restrict__ A, i64 lda, i64 i, i64 l) {
+    return TRANS ? A[l + i * lda] : A[i + l * lda];
+}
+
+template <typename T, bool TRANS>
+__global__ void __launch_bounds__(TV_THREADS)
+trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx, i64 kx, bool lower, bool unit,
+            TrsvSync s) {
+    __shared__ T diag[TV_NB][TV_NB + 1];  // op(A) diagonal block, the triangle only
+    __shared__ T red[2 * TV_GROUPS][TV_NB];
+    __shared__ int sticket, sok[2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const i64 nb = (n + TV_NB - 1) / TV_NB;
+    if (tid == 0) sticket = atomicAdd(s.ticket, 1);
+    __syncthreads();
+    const i64 t = sticket;
+    const i64 b = lower ? t : nb - 1 - t;
+    const i64 r0 = b * TV_NB;
+    const int rows = int(min(i64(TV_NB), n - r0));
+
+    // the diagonal block (no dependence on x): op(A)(r0 + i, r0 + l) on and inside the triangle
+    for (int e = tid; e < TV_NB * TV_NB; e += TV_THREADS) {
+        const int f = e % TV_NB, g = e / TV_NB;  // f runs along A's contiguous index
+        const int i = TRANS ? g : f, l = TRANS ? f : g;
+        const bool in = lower ? (l < i) : (l > i);
+        T v = T(0);
+        if (i < rows && l < rows && (in || (l == i && !unit))) v = opa<T, TRANS>(A, lda, r0 + i, r0 + l);
+        diag[i][l] = v;
+    }
+
+    __syncthreads();  // the diagonal block is staged
+    // warp 0 reads its right-hand side and the reciprocals of the diagonal now, while it
+    // waits for the blocks before it; lane owns rows lane and lane + 32
+    T rhs0 = T(0), rhs1 = T(0), inv0 = T(1), inv1 = T(1);
+    if (warp == 0) {
+        if (lane < rows) rhs0 = x[kx + (r0 + lane) * incx];
+        if (lane + 32 < rows) rhs1 = x[kx + (r0 + lane + 32) * incx];
+        if (!unit) {
+            if (lane < rows) inv0 = T(1) / diag[lane][lane];
+            if (lane + 32 < rows) inv1 = T(1) / diag[lane + 32][lane + 32];
+        }
+    }
+
+    // contributions of the blocks solved before this one
+    // NoTrans: thread (row r = tid % 64, columns g * 16 .. g * 16 + 15 of each tile), one sum
+    // Trans:   thread (column l = tid % 64, rows g * 16 .. g * 16 + 15), sixteen sums
+    const int f = tid % TV_NB, g = tid / TV_NB;
+    T acc[TV_PER];
+#pragma unroll
+    for (int u = 0; u < TV_PER; ++u) acc[u] = T(0);
+    for (i64 q = 0; q < t; ++q) {
+        const i64 jb = lower ? q : nb - 1 - q;
+        const i64 c0 = jb * TV_NB;
+        const int cols = int(min(i64(TV_NB), n - c0));  // the last block of a backward solve may be short
+        // the tile of op(A) is loaded before the wait: it does not depend on x
+        T av[TV_PER];
+#pragma unroll
+        for (int u = 0; u < TV_PER; ++u) {
+            const int i = TRANS ? g * TV_PER + u : f, l = TRANS ? f : g * TV_PER + u;
+            av[u] = (i < rows && l < cols) ? opa<T, TRANS>(A, lda, r0 + i, c0 + l) : T(0);
+        }
+        if (tid == 0) sok[q & 1] = tv_wait(s.flags + jb, s) ? 1 : 0;
+        __syncthreads();
+        if (!sok[q & 1]) return;
+        if (TRANS) {
+            const T xl = f < cols ? __ldcg(x + kx + (c0 + f) * incx) : T(0);
+#pragma unroll
+            for (int u = 0; u < TV_PER; ++u) acc[u] = fma(av[u], xl, acc[u]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < TV_PER; ++u) {
+                const int l = g * TV_PER + u;
+                const T xl = l < cols ? __ldcg(x + kx + (c0 + l) * incx) : T(0);
+                if (xl != T(0)) acc[0] = fma(av[u], xl, acc[0]);  // the reference's zero skip
+            }
+        }
+    }
+
+    // reduce: red[.][i] partial sums of row i
+    if (TRANS) {
+#pragma unroll
+        for (int u = 0; u < TV_PER; ++u) {
+            T v = acc[u];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[(warp & 1)][g * TV_PER + u] = v;  // two warps per group of columns
+        }
+    } else {
+        red[g][f] = acc[0];
+    }
+    __syncthreads();
+    if (warp != 0) return;
+
+    // one warp: right-hand side minus the contributions, then substitution.  Per pivot p the
+    // owner lane scales its own value by its own reciprocal, one shuffle broadcasts x_p, every
+    // lane updates its rows after p; the column of the next pivot is loaded one step ahead.
+    // Rows at or beyond `rows` hold zeros and see zero coefficients.  (Four pivots per step,
+    // every lane solving the 4 x 4 group triangle itself, measured slower: 7.1 us against
+    // 4.9 us per 64-row block in float64.)
+    T v0, v1;
+    if (TRANS) {
+        v0 = rhs0 - (red[0][lane] + red[1][lane]);
+        v1 = rhs1 - (red[0][lane + 32] + red[1][lane + 32]);
+    } else {
+        v0 = rhs0 - ((red[0][lane] + red[1][lane]) + (red[2][lane] + red[3][lane]));
+        v1 = rhs1 - ((red[0][lane + 32] + red[1][lane + 32]) + (red[2][lane + 32] + red[3][lane + 32]));
+    }
+    if (lane >= rows) v0 = T(0);
+    if (lane + 32 >= rows) v1 = T(0);
+    const int dp = lower ? 1 : -1;
+    int p = lower ? 0 : rows - 1;
+    T d0 = diag[lane][p], d1 = diag[lane + 32][p];
+    for (int st = 0; st < rows; ++st, p += dp) {
+        const int owner = p & 31;
+        const bool hi = p >= 32;
+        T mine = hi ? v1 : v0;
+        const T mi = hi ? inv1 : inv0;
+        if (!unit && (TRANS || mine != T(0))) mine = mine * mi;  // the reference skips zeros (NoTrans)
+        const T xp = __shfl_sync(0xffffffffu, mine, owner);
+        const int pn = (st + 1 < rows) ? p + dp : p;
+        const T d0n = diag[lane][pn], d1n = diag[lane + 32][pn];
+        if (lane == owner) {
+            if (hi) v1 = xp;
+            else v0 = xp;
+        }
+        if (TRANS || xp != T(0)) {
+            if (lower ? lane > p : lane < p) v0 = fma(-d0, xp, v0);
+            if (lower ? lane + 32 > p : lane + 32 < p) v1 = fma(-d1, xp, v1);
+        }
+        d0 = d0n;
+        d1 = d1n;
+    }
+    if (lane < rows) x[kx + (r0 + lane) * incx] = v0;
+    if (lane + 32 < rows) x[kx + (r0 + lane + 32) * incx] = v1;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) tv_store_release(s.flags + b, 1);
+}
+
+inline i64 vec_start(i64 len, i64 inc) { return inc > 0 ? 0 : -(len - 1) * inc; }
+
+}  // namespace
+
+template <typename T>
+int gemv_device(char trans, i64 m, i64 n, T alpha, const T* a, i64 lda, const T* x, i64 incx, T beta, T* y,
+                i64 incy) {
+    const bool notrans = trans == 'N';
+    const i64 lenx = notrans ? n : m, leny = notrans ? m : n;
+    const i64 kx = vec_start(lenx, incx), ky = vec_start(leny, incy);
+    cudaStream_t s = stream();
+    if (alpha == T(0)) {  // gemv.mojo:107-129: y = beta y, then return
+        ProfScope prof("gemv");
+        scale_vector_kernel<T><<<(unsigned)cdiv(leny, 256), 256, 0, s>>>(leny, beta, y, incy, ky);
+        return check_launch("gemv");
+    }
+    const i64 target = 8 * 148;  // CTAs for a full GPU
+    Workspace wp;
+    if (notrans) {
+        const i64 rb = cdiv(m, GV_THREADS);
+        const i64 splits = imax(1, imin(cdiv(target, rb), cdiv(n, 64)));
+        const i64 cps = cdiv(n, splits), parts = cdiv(n, cps);
+        if (rb > 0x7fffffff || parts > 65535) return MBG_ERR_UNSUPPORTED;
+        T* P = nullptr;
+        if (parts > 1) {
+            MBG_TRY(wp.reserve(sizeof(T) * size_t(parts) * size_t(m)));
+            P = wp.as<T>();
+        }
+        {
+            ProfScope prof("gemv");
+            gemv_n_kernel<T><<<dim3((unsigned)rb, (unsigned)parts), GV_THREADS, 0, s>>>(
+                m, n, a, lda, x, incx, kx, cps, P, parts == 1, alpha, beta, y, incy, ky);
+            MBG_TRY(check_launch("gemv"));
+        }
+        if (parts == 1) return MBG_OK;
+        ProfScope prof("gemv_finish");
+        gemv_finish_kernel<T><<<(unsigned)cdiv(m, 256), 256, 0, s>>>(m, parts, P, alpha, beta, y, incy, ky);
+        return check_launch("gemv_finish");
+    }
+    const i64 cb = cdiv(n, GV_THREADS / 32);
+    const i64 splits = imax(1, imin(cdiv(target, cb), cdiv(m, 32 * gv_unroll<T>() * 4)));
+    const i64 rpr = cdiv(m, splits), parts = cdiv(m, rpr);
+    if (cb > 0x7fffffff || parts > 65535) return MBG_ERR_UNSUPPORTED;
+    T* P = nullptr;
+    if (parts > 1) {
+        MBG_TRY(wp.reserve(sizeof(T) * size_t(parts) * size_t(n)));
+        P = wp.as<T>();
+    }
+    {
+        ProfScope prof("gemv");
+        gemv_t_kernel<T><<<dim3((unsigned)cb, (unsigned)parts), GV_THREADS, 0, s>>>(
+            m, n, a, lda, x, incx, kx, rpr, P, parts == 1, alpha, beta, y, incy, ky);
+        MBG_TRY(check_launch("gemv"));
+    }
+    if (parts == 1) return MBG_OK;
+    ProfScope prof("gemv_finish");
+    gemv_finish_kernel<T><<<(unsigned)cdiv(n, 256), 256, 0, s>>>(n, parts, P, alpha, beta, y, incy, ky);
+    return check_launch("gemv_finish");
+}
+
+template <typename T>
+int trsv_device(char uplo, char trans, char diag, i64 n, const T* a, i64 lda, T* x, i64 incx) {
+    const bool tr = is_t(trans), unit = is_u(diag);
+    const bool lower = (!is_u(uplo)) != tr;  // effective op(A) lower: forward substitution
+    const i64 nb = cdiv(n, TV_NB);
+    if (nb > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    Workspace ws;
+    MBG_TRY(ws.reserve(sizeof(int) * size_t(nb + 2)));
+    int* flags = ws.as<int>();
+    cudaStream_t s = stream();
+    MBG_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * size_t(nb + 2), s));
+    TrsvSync sync{flags, flags + nb, flags + nb + 1, device_error_flag()};
+    ProfScope prof("trsv");
+    if (tr) trsv_kernel<T, true><<<(unsigned)nb, TV_THREADS, 0, s>>>(n, a, lda, x, incx, vec_start(n, incx), lower, unit, sync);
+    else trsv_kernel<T, false><<<(unsigned)nb, TV_THREADS, 0, s>>>(n, a, lda, x, incx, vec_start(n, incx), lower, unit, sync);
+    return check_launch("trsv");
+}
+
+template int gemv_device<float>(char, i64, i64, float, const float*, i64, const float*, i64, float, float*, i64);
+template int gemv_device<double>(char, i64, i64, double, const double*, i64, const double*, i64, double, double*,
+                                 i64);
+template int trsv_device<float>(char, char, char, i64, const float*, i64, float*, i64);
+template int trsv_device<double>(char, char, char, i64, const double*, i64, double*, i64);
+
+}  // namespace mbg

@@ -216,6 +216,13 @@ template <typename T>
 int trmm_device(int mode, int slices, char side, char uplo, char ta, char diag, i64 m, i64 n, T alpha,
                 const T* a, i64 lda, T* b, i64 ldb);
 
+// gemv and trsv on device operands (level2.cu)
+template <typename T>
+int gemv_device(char trans, i64 m, i64 n, T alpha, const T* a, i64 lda, const T* x, i64 incx, T beta, T* y,
+                i64 incy);
+template <typename T>
+int trsv_device(char uplo, char trans, char diag, i64 n, const T* a, i64 lda, T* x, i64 incx);
+
 // symm and syr2k on device operands (symm.cu)
 template <typename T>
 int symm_device(int mode, int slices, char side, char uplo, i64 m, i64 n, T alpha, const T* a, i64 lda,

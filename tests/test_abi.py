@@ -188,3 +188,38 @@ def test_neighbour_quick_returns_and_modes():
         L.MBG_ERR_INVALID_MODE
     assert lib.mbg_dtrmm_ex(L.MODE_OZAKI, 1, b"L", b"L", b"N", b"N", 1, 1, 1.0, p, 1, p, 1) == \
         L.MBG_ERR_INVALID_MODE
+
+
+@pytest.mark.parametrize("args,info", [
+    (("n", 2, 2, 1.0, Z, 2, Z, 1, 0.0, Z, 1), 1),   # upper case only, as the reference checks it
+    (("X", 2, 2, 1.0, Z, 2, Z, 1, 0.0, Z, 1), 1),
+    (("N", -1, 2, 1.0, Z, 2, Z, 1, 0.0, Z, 1), 2),
+    (("N", 2, -1, 1.0, Z, 2, Z, 1, 0.0, Z, 1), 3),
+    (("T", 3, 2, 1.0, Z, 2, Z, 1, 0.0, Z, 1), 6),
+    (("N", 2, 2, 1.0, Z, 2, Z, 0, 0.0, Z, 1), 8),
+    (("C", 2, 2, 1.0, Z, 2, Z, 1, 0.0, Z, 0), 11),
+])
+def test_gemv_info_codes(args, info, capsys):
+    """Numbering of mojoBLAS gemv (src/level2/gemv.mojo:69-84)."""
+    assert mb.gemv(*args) == info
+    assert f"gemv: Info {info}" in capsys.readouterr().out
+
+
+@pytest.mark.parametrize("args,info", [
+    (("X", "N", "N", 2, Z, 2, Z, 1), 1),
+    (("U", "X", "N", 2, Z, 2, Z, 1), 2),
+    (("U", "n", "X", 2, Z, 2, Z, 1), 3),
+    (("U", "N", "N", -1, Z, 2, Z, 1), 4),
+    (("l", "t", "u", 3, Z, 2, Z, 1), 6),
+    (("U", "N", "N", 2, Z, 2, Z, 0), 8),
+])
+def test_trsv_info_codes(args, info):
+    """Numbering of mojoBLAS trsv (src/level2/trsv.mojo:56-79)."""
+    assert mb.trsv(*args) == info
+
+
+def test_level2_quick_returns_touch_no_device():
+    assert mb.gemv("N", 0, 3, 1.0, Z, 1, Z, 1, 0.0, Z, 1) == 0
+    assert mb.gemv("T", 3, 0, 1.0, Z, 3, Z, 1, 0.0, Z, 1) == 0
+    assert mb.gemv("N", 3, 3, 0.0, Z, 3, Z, 1, 1.0, Z, 1) == 0
+    assert mb.trsv("L", "N", "N", 0, Z, 1, Z, 1) == 0
