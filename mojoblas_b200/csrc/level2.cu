@@ -115,6 +115,118 @@ gemv_t_kernel(i64 m, i64 n, const T* __restrict__ A, i64 lda, const T* __restric
     }
 }
 
+// float32 with A 16-byte aligned and lda % 4 == 0: each thread owns four consecutive rows
+// and reads them with one 16-byte load per column (a warp moves 512 bytes per load
+// instruction instead of 128); the last partial group of rows is read element-wise.
+__global__ void __launch_bounds__(GV_THREADS)
+sgemv_n4_kernel(i64 m, i64 n, const float* __restrict__ A, i64 lda, const float* __restrict__ x, i64 incx, i64 kx,
+                i64 cps, float* __restrict__ P, bool direct, float alpha, float beta, float* __restrict__ y,
+                i64 incy, i64 ky) {
+    constexpr int U = 8;
+    const i64 i0 = 4 * (blockIdx.x * (i64)GV_THREADS + threadIdx.x);
+    if (i0 >= m) return;
+    const i64 j0 = blockIdx.y * cps, j1 = min(n, j0 + cps);
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (i0 + 4 <= m) {
+        i64 j = j0;
+        for (; j + U <= j1; j += U) {
+            float4 av[U];
+            float xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                xv[u] = x[kx + (j + u) * incx];
+                av[u] = *reinterpret_cast<const float4*>(A + i0 + (j + u) * lda);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (xv[u] == 0.0f) continue;
+                acc[0] = fmaf(av[u].x, xv[u], acc[0]);
+                acc[1] = fmaf(av[u].y, xv[u], acc[1]);
+                acc[2] = fmaf(av[u].z, xv[u], acc[2]);
+                acc[3] = fmaf(av[u].w, xv[u], acc[3]);
+            }
+        }
+        for (; j < j1; ++j) {
+            const float xj = x[kx + j * incx];
+            if (xj == 0.0f) continue;
+            const float4 a4 = *reinterpret_cast<const float4*>(A + i0 + j * lda);
+            acc[0] = fmaf(a4.x, xj, acc[0]);
+            acc[1] = fmaf(a4.y, xj, acc[1]);
+            acc[2] = fmaf(a4.z, xj, acc[2]);
+            acc[3] = fmaf(a4.w, xj, acc[3]);
+        }
+    } else {
+        for (i64 j = j0; j < j1; ++j) {
+            const float xj = x[kx + j * incx];
+            if (xj == 0.0f) continue;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (i0 + r < m) acc[r] = fmaf(A[i0 + r + j * lda], xj, acc[r]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const i64 i = i0 + r;
+        if (i >= m) break;
+        if (direct) {
+            float& yi = y[ky + i * incy];
+            float v = beta == 0.0f ? 0.0f : (beta == 1.0f ? yi : beta * yi);
+            if (acc[r] != 0.0f) v = v + alpha * acc[r];
+            yi = v;
+        } else {
+            P[blockIdx.y * m + i] = acc[r];
+        }
+    }
+}
+
+// float32 Trans with A 16-byte aligned and lda % 4 == 0: lanes read four consecutive
+// elements of the column with one 16-byte load (x likewise when incx == 1 and x is
+// aligned); a warp-uniform loop over 512-element steps, then the ragged rest element-wise.
+// Row ranges (rpr) are multiples of 512.
+__global__ void __launch_bounds__(GV_THREADS)
+sgemv_t4_kernel(i64 m, i64 n, const float* __restrict__ A, i64 lda, const float* __restrict__ x, i64 incx, i64 kx,
+                bool x4, i64 rpr, float* __restrict__ P, bool direct, float alpha, float beta,
+                float* __restrict__ y, i64 incy, i64 ky) {
+    constexpr int U = 4;  // 16-byte loads per lane per step: a step covers 32 x 4 x U = 512 rows
+    const int lane = threadIdx.x & 31;
+    const i64 j = blockIdx.x * (i64)(GV_THREADS / 32) + (threadIdx.x >> 5);
+    if (j >= n) return;
+    const i64 i0 = blockIdx.y * rpr, i1 = min(m, i0 + rpr);
+    const float* a = A + j * lda;
+    float acc = 0.0f;
+    i64 base = i0;
+    for (; base + 128 * U <= i1; base += 128 * U) {
+        float4 av[U], xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const i64 i = base + 128 * u + 4 * lane;
+            av[u] = *reinterpret_cast<const float4*>(a + i);
+            if (x4) xv[u] = *reinterpret_cast<const float4*>(x + i);
+            else xv[u] = make_float4(x[kx + i * incx], x[kx + (i + 1) * incx], x[kx + (i + 2) * incx],
+                                     x[kx + (i + 3) * incx]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            acc = fmaf(av[u].x, xv[u].x, acc);
+            acc = fmaf(av[u].y, xv[u].y, acc);
+            acc = fmaf(av[u].z, xv[u].z, acc);
+            acc = fmaf(av[u].w, xv[u].w, acc);
+        }
+    }
+    for (i64 i = base + lane; i < i1; i += 32) acc = fmaf(a[i], x[kx + i * incx], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane != 0) return;
+    if (direct) {
+        float& yj = y[ky + j * incy];
+        float v = beta == 0.0f ? 0.0f : (beta == 1.0f ? yj : beta * yj);
+        if (acc != 0.0f) v = v + alpha * acc;
+        yj = v;
+    } else {
+        P[blockIdx.y * n + j] = acc;
+    }
+}
+
 // y(i) = beta y(i) + alpha sum_s P[s * len + i] (partial sums in a fixed order)
 template <typename T>
 __global__ void gemv_finish_kernel(i64 len, i64 parts, const T* __restrict__ P, T alpha, T beta,
@@ -341,6 +453,55 @@ int gemv_device(char trans, i64 m, i64 n, T alpha, const T* a, i64 lda, const T*
     }
     const i64 target = 8 * 148;  // CTAs for a full GPU
     Workspace wp;
+    // float32 with a 16-byte aligned A and lda % 4 == 0: the 16-byte load kernels
+    const bool v4 = sizeof(T) == 4 && reinterpret_cast<uintptr_t>(a) % 16 == 0 && lda % 4 == 0;
+    if (notrans && v4) {
+        const i64 rb = cdiv(m, 4 * GV_THREADS);
+        const i64 splits = imax(1, imin(cdiv(target, rb), cdiv(n, 64)));
+        const i64 cps = cdiv(n, splits), parts = cdiv(n, cps);
+        if (rb > 0x7fffffff || parts > 65535) return MBG_ERR_UNSUPPORTED;
+        float* P = nullptr;
+        if (parts > 1) {
+            MBG_TRY(wp.reserve(sizeof(float) * size_t(parts) * size_t(m)));
+            P = wp.as<float>();
+        }
+        {
+            ProfScope prof("gemv");
+            sgemv_n4_kernel<<<dim3((unsigned)rb, (unsigned)parts), GV_THREADS, 0, s>>>(
+                m, n, (const float*)a, lda, (const float*)x, incx, kx, cps, P, parts == 1, (float)alpha,
+                (float)beta, (float*)y, incy, ky);
+            MBG_TRY(check_launch("gemv"));
+        }
+        if (parts == 1) return MBG_OK;
+        ProfScope prof("gemv_finish");
+        gemv_finish_kernel<float><<<(unsigned)cdiv(m, 256), 256, 0, s>>>(m, parts, P, (float)alpha, (float)beta,
+                                                                         (float*)y, incy, ky);
+        return check_launch("gemv_finish");
+    }
+    if (!notrans && v4) {
+        const i64 cb = cdiv(n, GV_THREADS / 32);
+        const i64 splits = imax(1, imin(cdiv(target, cb), cdiv(m, 2048)));
+        const i64 rpr = cdiv(cdiv(m, splits), 512) * 512, parts = cdiv(m, rpr);
+        if (cb > 0x7fffffff || parts > 65535) return MBG_ERR_UNSUPPORTED;
+        const bool x4 = incx == 1 && reinterpret_cast<uintptr_t>(x) % 16 == 0;
+        float* P = nullptr;
+        if (parts > 1) {
+            MBG_TRY(wp.reserve(sizeof(float) * size_t(parts) * size_t(n)));
+            P = wp.as<float>();
+        }
+        {
+            ProfScope prof("gemv");
+            sgemv_t4_kernel<<<dim3((unsigned)cb, (unsigned)parts), GV_THREADS, 0, s>>>(
+                m, n, (const float*)a, lda, (const float*)x, incx, kx, x4, rpr, P, parts == 1, (float)alpha,
+                (float)beta, (float*)y, incy, ky);
+            MBG_TRY(check_launch("gemv"));
+        }
+        if (parts == 1) return MBG_OK;
+        ProfScope prof("gemv_finish");
+        gemv_finish_kernel<float><<<(unsigned)cdiv(n, 256), 256, 0, s>>>(n, parts, P, (float)alpha, (float)beta,
+                                                                         (float*)y, incy, ky);
+        return check_launch("gemv_finish");
+    }
     if (notrans) {
         const i64 rb = cdiv(m, GV_THREADS);
         const i64 splits = imax(1, imin(cdiv(target, rb), cdiv(n, 64)));
