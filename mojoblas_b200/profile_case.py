@@ -4,6 +4,7 @@
     python mojoblas_b200/profile_case.py --op dgemm --mode ozaki --slices 8 --m 2048 --n 2048 --k 4096
     python mojoblas_b200/profile_case.py --op dtrsm --mode ozaki --m 4096 --n 4096
     python mojoblas_b200/profile_case.py --op strmm --mode bf16x6 --m 4096 --n 4096
+    python mojoblas_b200/profile_case.py --op dgemv --ta N --m 8192 --n 8192
 
 Inputs are uniform[-1, 1) (trsm, trmm: diagonally dominant lower triangle), device
 resident; each rep is one call through the C ABI.  Prints the mean CUDA-event
@@ -22,7 +23,8 @@ sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--op", choices=["sgemm", "dgemm", "ssyrk", "dtrsm", "strsm", "grouped_sgemm", "grouped_strsm",
-                                     "strmm", "dtrmm", "ssymm", "dsymm", "ssyr2k", "dsyr2k"],
+                                     "strmm", "dtrmm", "ssymm", "dsymm", "ssyr2k", "dsyr2k",
+                                     "sgemv", "dgemv", "strsv", "dtrsv"],
                     default="sgemm")
     ap.add_argument("--mode", choices=["plain", "bf16x3", "bf16x6", "ozaki"], default="bf16x6")
     ap.add_argument("--slices", type=int, default=8)
@@ -97,6 +99,22 @@ def main():
 
         def call():
             return lib.mbg_ssyrk_ex(mode, b"L", b"N", a.n, a.k, 1.0, A.data_ptr(), a.n, 0.0, Cm.data_ptr(), a.n)
+    elif a.op in ("sgemv", "dgemv"):  # y = 1.5 op(A) x + 0.5 y, A m x n, op by --ta
+        A, x, y = cm(a.m, a.n), cm(max(a.m, a.n), 1), cm(max(a.m, a.n), 1)
+
+        def call():
+            args = (a.ta.encode(), a.m, a.n, 1.5, A.data_ptr(), a.m, x.data_ptr(), 1, 0.5, y.data_ptr(), 1)
+            return lib.mbg_sgemv(*args) if a.op == "sgemv" else lib.mbg_dgemv(*args)
+    elif a.op in ("strsv", "dtrsv"):  # Lower, NoTrans, NonUnit, order --m, diagonally dominant
+        A = torch.randn((a.m, a.m), generator=g, device="cuda", dtype=dt) / a.m ** 0.5
+        A.diagonal().copy_(2.0 + torch.rand(a.m, generator=g, device="cuda", dtype=dt))
+        b0 = torch.randn(a.m, generator=g, device="cuda", dtype=dt)
+        xb = b0.clone()
+
+        def call():
+            xb.copy_(b0)
+            args = (b"L", b"N", b"N", a.m, A.data_ptr(), a.m, xb.data_ptr(), 1)
+            return lib.mbg_strsv(*args) if a.op == "strsv" else lib.mbg_dtrsv(*args)
     elif a.op in ("ssymm", "dsymm"):  # Left, Upper: C (m x n) = A (m x m, symmetric) B
         A, B, Cm = cm(a.m, a.m), cm(a.m, a.n), cm(a.m, a.n)
 
