@@ -102,7 +102,8 @@ class Clocks:
                 continue
             try:
                 ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                rows.append((ts, float(f[1]), float(f[2]), f[5:9]))
+                pw = float(f[3]) if f[3] not in ("", "[N/A]", "N/A") else float("nan")
+                rows.append((ts, float(f[1]), float(f[2]), f[5:9], pw))
             except ValueError:
                 continue
         inside = [r for r in rows if self.window and self.window[0] <= r[0] <= self.window[1]]
@@ -110,7 +111,9 @@ class Clocks:
         if not use:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
         reasons = sorted({nm for r in use for nm, v in zip(names, r[3]) if v.lower() == "active"})
+        pw = [r[4] for r in use if r[4] == r[4]]
         return {"sm_mhz": float(np.median([r[1] for r in use])), "sm_max_mhz": use[-1][2], "reasons": reasons,
+                "power_w": round(float(np.median(pw)), 1) if pw else None,
                 "samples": len(use), "samples_in_timed_region": len(inside)}
 
 
@@ -1008,7 +1011,7 @@ def run_cpu_baseline(args, threads=None, rows=N_S, calls=("NT", "TN")):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="bf16x6", choices=["bf16x3", "bf16x6"])
