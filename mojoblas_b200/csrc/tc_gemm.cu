@@ -830,25 +830,86 @@ __device__ __forceinline__ void load_tile(const T* __restrict__ src, i64 ld, i64
     }
 }
 
+// Split pre-pass: planes[t][r][l] = term t of value(r, l), TERMS bf16 terms per fp32 value
+// (a1 = bf16(v), a2 = bf16(v - a1), a3 = bf16(v - a1 - a2); each subtraction is exact),
+// zeros outside rows x K up to Rp x Kp.  One 256-thread CTA per 64 x 64 tile; each thread
+// turns four consecutive k of one row into one 8-byte store per plane.  A k-contiguous
+// source is read four values at a time (16-byte loads when aligned); a row-contiguous one
+// is read four rows at a time along m and transposed through shared memory.
+constexpr int SP_R = 64, SP_K = 64;
+
+inline dim3 split_grid(i64 Rp, i64 Kp) { return dim3(unsigned((Kp + SP_K - 1) / SP_K), unsigned(Rp / SP_R)); }
+
+template <int TERMS>
+__device__ __forceinline__ void split_store4(float4 v, __nv_bfloat16* out, size_t plane) {
+    float x[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int t = 0; t < TERMS; ++t) {
+        __nv_bfloat16 h[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            h[u] = __float2bfloat16_rn(x[u]);
+            x[u] -= __bfloat162float(h[u]);  // exact: x and h agree in their leading bits
+        }
+        const __nv_bfloat162 lo = __halves2bfloat162(h[0], h[1]), hi = __halves2bfloat162(h[2], h[3]);
+        uint2 w;
+        w.x = *reinterpret_cast<const unsigned*>(&lo);
+        w.y = *reinterpret_cast<const unsigned*>(&hi);
+        *reinterpret_cast<uint2*>(out + plane * t) = w;
+    }
+}
+
 template <int TERMS, bool KMAJOR>
 __global__ void __launch_bounds__(256)
 split_bf16_kernel(const float* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp,
                   __nv_bfloat16* __restrict__ planes, int keep = 0) {
-    __shared__ float tile[PT_R][PT_K + 1];
-    const i64 r0 = i64(blockIdx.y) * PT_R, l0 = i64(blockIdx.x) * PT_K;
-    load_tile<float, KMAJOR>(src, ld, rows, K, r0, l0, keep, tile);
-    __syncthreads();
+    const i64 r0 = i64(blockIdx.y) * SP_R, l0 = i64(blockIdx.x) * SP_K;
     const size_t plane = size_t(Rp) * size_t(Kp);
-    for (int e = threadIdx.x; e < PT_R * (PT_K / 2); e += blockDim.x) {
-        const int rr = e / (PT_K / 2), lp = (e % (PT_K / 2)) * 2;
-        float x0 = tile[rr][lp], x1 = tile[rr][lp + 1];
-        __nv_bfloat162* out = reinterpret_cast<__nv_bfloat162*>(planes + size_t(r0 + rr) * Kp + l0 + lp);
+    const bool vec = reinterpret_cast<uintptr_t>(src) % 16 == 0 && ld % 4 == 0 && keep == 0;
+    if (KMAJOR) {  // value(r, l) = src[l + r * ld]
+        for (int q = threadIdx.x; q < SP_R * (SP_K / 4); q += 256) {
+            const int rr = q / (SP_K / 4), lq = (q % (SP_K / 4)) * 4;
+            const i64 r = r0 + rr, l = l0 + lq;
+            if (l >= Kp) continue;
+            float t[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (r < rows) {
+                if (vec && l + 3 < K) {
+                    const float4 v = *reinterpret_cast<const float4*>(src + l + r * ld);
+                    t[0] = v.x; t[1] = v.y; t[2] = v.z; t[3] = v.w;
+                } else {
 #pragma unroll
-        for (int t = 0; t < TERMS; ++t) {
-            const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
-            out[(plane / 2) * t] = __halves2bfloat162(h0, h1);
-            x0 -= __bfloat162float(h0);  // exact: x0 and h0 agree in their leading bits
-            x1 -= __bfloat162float(h1);
+                    for (int u = 0; u < 4; ++u)
+                        if (l + u < K && kept(keep, r, l + u)) t[u] = src[l + u + r * ld];
+                }
+            }
+            split_store4<TERMS>(make_float4(t[0], t[1], t[2], t[3]), planes + size_t(r) * Kp + l, plane);
+        }
+    } else {  // value(r, l) = src[r + l * ld]
+        __shared__ float tile[SP_K][SP_R + 1];
+        for (int q = threadIdx.x; q < SP_K * (SP_R / 4); q += 256) {
+            const int lk = q / (SP_R / 4), rq = (q % (SP_R / 4)) * 4;
+            const i64 r = r0 + rq, l = l0 + lk;
+            float t[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (l < K) {
+                if (vec && r + 3 < rows) {
+                    const float4 v = *reinterpret_cast<const float4*>(src + r + l * ld);
+                    t[0] = v.x; t[1] = v.y; t[2] = v.z; t[3] = v.w;
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (r + u < rows && kept(keep, r + u, l)) t[u] = src[r + u + l * ld];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) tile[lk][rq + u] = t[u];
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < SP_R * (SP_K / 4); q += 256) {
+            const int rr = q / (SP_K / 4), lq = (q % (SP_K / 4)) * 4;
+            const i64 l = l0 + lq;
+            if (l >= Kp) continue;
+            const float4 v = make_float4(tile[lq][rr], tile[lq + 1][rr], tile[lq + 2][rr], tile[lq + 3][rr]);
+            split_store4<TERMS>(v, planes + size_t(r0 + rr) * Kp + l, plane);
         }
     }
 }
@@ -1019,8 +1080,8 @@ template <int TERMS>
 int launch_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, __nv_bfloat16* planes,
                  int keep = 0) {
     ProfScope prof("split_bf16");
-    dim3 g(unsigned(Kp / PT_K), unsigned(Rp / PT_R));
-    if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
+    const dim3 g = split_grid(Rp, Kp);
+    if (Rp / SP_R > 65535) return MBG_ERR_UNSUPPORTED;
     if (kmajor) split_bf16_kernel<TERMS, true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes, keep);
     else split_bf16_kernel<TERMS, false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes, keep);
     return check_launch("split_bf16");
@@ -1246,7 +1307,7 @@ int noalloc_setup(NoallocDevice** out) {
 template <int TERMS>
 void noalloc_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp,
                    __nv_bfloat16* planes) {
-    dim3 g(unsigned(Kp / tc::PT_K), unsigned(Rp / tc::PT_R));
+    const dim3 g = tc::split_grid(Rp, Kp);
     if (kmajor) tc::split_bf16_kernel<TERMS, true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
     else tc::split_bf16_kernel<TERMS, false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, planes);
 }
