@@ -177,7 +177,7 @@ def run_cfg3(torch, lib, L, stream):
             raise RuntimeError(f"dtrsm failed {st}: {L.last_error()}")
 
     tr = {}
-    for label, md, s_, r_ in (("plain_fp64", L.MODE_PLAIN, 0, 0), ("ozaki_s8", L.MODE_OZAKI, 8, 0),
+    for label, md, s_, r_ in (("plain_fp64", L.MODE_PLAIN, 0, 0), ("ozaki_s7", L.MODE_OZAKI, 7, 0),
                               ("ozaki_s4_ir1", L.MODE_OZAKI, 4, 1)):
         tcall(md, s_, r_)
         torch.cuda.synchronize()
@@ -276,7 +276,7 @@ def run_neighbours(torch, lib, L, stream):
 
     n = 4096
     for dt, tname, modes in ((torch.float32, "s", (("plain_fp32", L.MODE_PLAIN, 0), ("bf16x6", L.MODE_BF16X6, 0))),
-                             (torch.float64, "d", (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s8", L.MODE_OZAKI, 8)))):
+                             (torch.float64, "d", (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s7", L.MODE_OZAKI, 7)))):
         A = torch.rand((n, n), generator=g, device="cuda", dtype=dt) * 2 - 1
         B = torch.rand((n, n), generator=g, device="cuda", dtype=dt) * 2 - 1
         C = torch.empty_like(B)
@@ -646,8 +646,8 @@ def run_cfg5(torch, lib, L, stream):
 def leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk):
     """Each leg's achieved rate over the peak of the pipe that bounds it: the measured
     bf16 burst for split-precision tensor work (P bf16 products per FP32 product), the
-    run's own probes for the FP32 / FP64 pipes and the int8 tensor pipe (36 int8 products
-    per FP64 product at 8 slices), the measured HBM copy for the batched trsm."""
+    run's own probes for the FP32 / FP64 pipes and the int8 tensor pipe (28 int8 products
+    per FP64 product at 7 slices), the measured HBM copy for the batched trsm."""
     out = {}
     f32, f64, i8 = probes.get("fp32_fma_tflops"), probes.get("fp64_fma_tflops"), probes.get("int8_mma_tops")
 
@@ -656,7 +656,7 @@ def leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk):
             out[key] = {"frac": round(value / peak, 3), "peak": round(peak, 1), "bound": note}
     if dg:
         put("dgemm_plain_fp64", dg["plain_fp64"]["tflops"], f64, "fp64 pipe (probe)")
-        put("dgemm_ozaki_s8_int8", 36 * dg["ozaki_s8"]["tflops"], i8, "int8 tensor pipe (probe), whole call")
+        put("dgemm_ozaki_s7_int8", 28 * dg["ozaki_s7"]["tflops"], i8, "int8 tensor pipe (probe), whole call")
     sy = cfg3.get("ssyrk_LN_8192x2048", {}) if cfg3 else {}
     if sy:
         put("ssyrk_plain_fp32", sy["plain_fp32"]["tflops"], f32, "fp32 pipe (probe)")
@@ -856,8 +856,8 @@ def run_ours(args, rank, world, dist):
         probes["plain_fp32_frac"] = round(plain_tflops / pv[0].value, 3)
         if dg:
             probes["plain_fp64_frac"] = round(dg["plain_fp64"]["tflops"] / pv[1].value, 3)
-            probes["ozaki_s8_int8_frac"] = round(36 * FLOPS_D / (dg["ozaki_s8"]["kernel_ms"] * 1e-3) / 1e12
-                                                 / pv[3].value, 3) if dg["ozaki_s8"].get("kernel_ms") else None
+            probes["ozaki_s7_int8_frac"] = round(28 * FLOPS_D / (dg["ozaki_s7"]["kernel_ms"] * 1e-3) / 1e12
+                                                 / pv[3].value, 3) if dg["ozaki_s7"].get("kernel_ms") else None
 
     # ---- context: the vendor library's plain FP32 / FP64 GEMM on the same sizes ----
     ctx = {}

@@ -132,7 +132,8 @@ int mbg_dtrsv(char uplo, char trans, char diag, int64_t n, const double* a, int6
 /* ---- the same routines with a precision mode ----------------------------
  * mode: MBG_MODE_PLAIN, MBG_MODE_BF16X3 or MBG_MODE_BF16X6 for float;
  *       MBG_MODE_PLAIN or MBG_MODE_OZAKI for double.
- * slices: Ozaki int8 slices per operand (2..8, each carries 7 bits); ignored
+ * slices: Ozaki int8 slices per operand (2..8; s slices keep 8s - 2 bits of each
+ *         value relative to its row's (column's) largest); ignored
  *         by the other modes.
  * refine: trsm only — iterative-refinement steps after the solve (0 or more):
  *         R = alpha*B - op(A)*X in the accurate mode, solve, X += correction.

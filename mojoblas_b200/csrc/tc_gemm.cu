@@ -11,13 +11,15 @@
 //    3 products for T=2 (BF16x3), 6 for T=3 (BF16x6).
 //
 //  * Ozaki-scheme dgemm (int8 slices).  A pre-pass scales each row of op(A) and
-//    each column of op(B) by a power of two so that |x'| < 1 and cuts x' into
-//    s slices of 7 bits, x' = sum_p d_p 2^(-7(p+1)), d_p in [-127, 127] (exact in
-//    fp64: multiply by 128, truncate, subtract).  The kernel forms, for each
-//    diagonal t = p+q < s, D_t = sum_{p+q=t} A_p B_q exactly with
+//    each column of op(B) by a power of two (x = x' 2^e, |x'| < 1), truncates x'
+//    to the integer F = trunc(x' 2^(8s-2)) and writes F's signed base-256 digits,
+//    x' ~ sum_p d_p 2^(-8p-6), d_p in [-128, 127] (two's-complement digits, least
+//    significant first; |F| < 2^(8s-2) keeps the leading one within [-65, 65]),
+//    so s slices keep 8s - 2 bits.  The kernel forms, for each diagonal
+//    t = p+q < s, D_t = sum_{p+q=t} A_p B_q exactly with
 //    tcgen05.mma.kind::i8 (int32 accumulation, one TMEM accumulator per t, at
 //    most four at a time: more than four slices run two passes over k), and
-//    the epilogue sums 2^(-7(t+2)) D_t from the smallest term up in fp64 and
+//    the epilogue sums 2^(-8t-12) D_t from the smallest term up in fp64 and
 //    applies the row and column scales (Ootomo, Ozaki, Yokota, "DGEMM on integer
 //    matrix multiplication unit", IJHPCA 2024; Ozaki, Ogita, Oishi, Rump, 2012).
 //
@@ -725,7 +727,7 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
             tc_fence_after();
 #pragma unroll 1
             for (int d = hi - 1; d >= lo; --d) {  // smallest weight first
-                const double w = pow2_exact(-7 * (d + 2));
+                const double w = pow2_exact(-8 * d - 12);
 #pragma unroll
                 for (int c0 = 0; c0 < C::EPI_COLS; c0 += 16) {
                     uint32_t r[16];
@@ -968,18 +970,18 @@ row_exponent_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, int
     }
 }
 
-// floor(|v| / 2^er * 2^56) from the bits of v: |v| = M 2^(max(E,1) - 1075) with the
-// 53-bit significand M.  Every step of the truncation loop (y = 128 x, digit =
-// trunc(y), x = y - digit) is exact, so its digits are the 7-bit fields of this
-// integer, most significant first; integer shifts keep the FP64 pipe free.
-__device__ __forceinline__ unsigned long long oz_fixed56(double v, int er, bool& neg) {
+// trunc(v / 2^er * 2^B) from the bits of v, with v's sign: |v| = M 2^(max(E,1) - 1075)
+// with the 53-bit significand M; |v| < 2^er and B <= 62 keep the magnitude below 2^B.
+// Integer shifts keep the FP64 pipe free.
+__device__ __forceinline__ long long oz_fixed(double v, int er, int B) {
     const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(v));
-    neg = (b >> 63) != 0;
     const int E = int((b >> 52) & 0x7ff);
     const unsigned long long M = (b & 0xfffffffffffffULL) | (E ? (1ULL << 52) : 0ULL);
-    const int sh = (E ? E : 1) - 1075 - er + 56;
-    if (sh >= 0) return sh < 64 ? M << sh : 0ULL;  // |v| < 2^er keeps a live result below 2^56
-    return sh > -64 ? M >> -sh : 0ULL;
+    const int sh = (E ? E : 1) - 1075 - er + B;
+    unsigned long long F;
+    if (sh >= 0) F = sh < 64 ? M << sh : 0ULL;
+    else F = sh > -64 ? M >> -sh : 0ULL;
+    return (b >> 63) ? -static_cast<long long>(F) : static_cast<long long>(F);
 }
 
 template <bool KMAJOR>
@@ -999,20 +1001,25 @@ slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp,
             er = 0;
             if (blockIdx.x == 0 && lq == 0) e[r] = 0;
         }
-        unsigned long long F[4];
-        bool neg[4];
+        // signed base-256 digits of G = trunc(v 2^(8s-2-er)) (d in [-128, 127], G = sum_j d_j 256^j):
+        // with H = G + 0x80...80 (s bytes of 0x80, modulo 2^64), byte j of H is d_j + 128, since
+        // adding 128 to each byte turns the digits' borrows into plain carries.  Slice p holds the
+        // digit of weight 256^(s-1-p) (weight 2^(er - 8p - 6) of v), so one add per value and a
+        // byte gather per slice write it; XOR 0x80 makes each byte the signed digit.
+        const int B = 8 * slices - 2;
+        const unsigned long long bias = 0x8080808080808080ULL >> (64 - 8 * slices);
+        unsigned long long H[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) F[u] = oz_fixed56(tile[rr][lq + u], er, neg[u]);
-        char4* out = reinterpret_cast<char4*>(planes + size_t(r) * Kp + l0 + lq);
+        for (int u = 0; u < 4; ++u)
+            H[u] = static_cast<unsigned long long>(oz_fixed(tile[rr][lq + u], er, B)) + bias;
+        unsigned* out = reinterpret_cast<unsigned*>(planes + size_t(r) * Kp + l0 + lq);
         for (int p = 0; p < slices; ++p) {
-            int d[4];
+            const int byte = slices - 1 - p;
+            const int sh = 8 * (byte & 3), hiword = byte & 4 ? 32 : 0;
+            unsigned packed = 0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int dig = int((F[u] >> (49 - 7 * p)) & 127);
-                d[u] = neg[u] ? -dig : dig;
-            }
-            out[(plane / 4) * p] = make_char4((signed char)d[0], (signed char)d[1], (signed char)d[2],
-                                              (signed char)d[3]);
+            for (int u = 0; u < 4; ++u) packed |= ((unsigned(H[u] >> hiword) >> sh) & 255u) << (8 * u);
+            out[(plane / 4) * p] = packed ^ 0x80808080u;
         }
     }
 }
@@ -1181,8 +1188,8 @@ int launch_ozaki(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap
 }  // namespace tc
 
 // Longest reduction one Ozaki launch takes: its int32 accumulators hold at most
-// `slices` products of K terms of 127^2 each; longer k runs in several launches.
-i64 ozaki_max_k(int slices) { return (i64(0x7fffffff) / (i64(slices) * 127 * 127)) / 32 * 32; }
+// `slices` products of K terms of at most 128^2 each; longer k runs in several launches.
+i64 ozaki_max_k(int slices) { return (i64(0x7fffffff) / (i64(slices) * 128 * 128)) / 32 * 32; }
 
 int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a,
                    i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc, char tri_uplo, int band,

@@ -14,7 +14,8 @@ An invalid argument behaves like the reference: "<routine>: Info <n>" is
 printed and n is returned.  A CUDA-side failure raises MbgError.
 
 Keyword extensions (not in the reference): `mode` (PLAIN, BF16X3, BF16X6 for
-float32; PLAIN, OZAKI for float64), `slices` (Ozaki int8 slices, 2..8) and
+float32; PLAIN, OZAKI for float64), `slices` (Ozaki int8 slices, 2..8; s slices
+keep 8s - 2 bits, and the default 7 meets plain FP64's error) and
 `refine` (trsm iterative-refinement steps).
 """
 from __future__ import annotations
@@ -72,7 +73,7 @@ def _report(routine: str, st: int) -> int:
 
 
 def gemm(trans_a, trans_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN,
-         slices=8, dtype=None) -> int:
+         slices=7, dtype=None) -> int:
     """C := alpha*op(A)*op(B) + beta*C (mojoBLAS gemm, gemm.mojo:56-124)."""
     dt = _dtype_of(c, dtype)
     lib = L.load()
@@ -89,7 +90,7 @@ def gemm(trans_a, trans_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode
     return _report("gemm", st)
 
 
-def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, *, mode=PLAIN, slices=8, dtype=None) -> int:
+def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, *, mode=PLAIN, slices=7, dtype=None) -> int:
     """C := alpha*A*A^T + beta*C or alpha*A^T*A + beta*C on one triangle (syrk.mojo:20-200)."""
     dt = _dtype_of(c, dtype)
     lib = L.load()
@@ -103,7 +104,7 @@ def syrk(uplo, trans, n, k, alpha, a, lda, beta, c, ldc, *, mode=PLAIN, slices=8
     return _report("syrk", st)
 
 
-def trsm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, slices=8,
+def trsm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, slices=7,
          refine=0, dtype=None) -> int:
     """op(A) X = alpha B or X op(A) = alpha B, X overwrites B (trsm.mojo:20-275)."""
     dt = _dtype_of(b, dtype)
@@ -121,7 +122,7 @@ def trsm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, 
     return _report("trsm", st)
 
 
-def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN, slices=8,
+def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN, slices=7,
          dtype=None) -> int:
     """C := alpha*A*B + beta*C or alpha*B*A + beta*C, A symmetric (symm.mojo:20-241)."""
     dt = _dtype_of(c, dtype)
@@ -136,7 +137,7 @@ def symm(side, uplo, m, n, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN, s
     return _report("symm", st)
 
 
-def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN, slices=8,
+def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN, slices=7,
           dtype=None) -> int:
     """C := alpha*(A*B^T + B*A^T) + beta*C or alpha*(A^T*B + B^T*A) + beta*C on one
     triangle (syr2k.mojo:20-190)."""
@@ -152,7 +153,7 @@ def syr2k(uplo, trans, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode=PLAIN,
     return _report("syr2k", st)
 
 
-def trmm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, slices=8,
+def trmm(side, uplo, trans_a, diag, m, n, alpha, a, lda, b, ldb, *, mode=PLAIN, slices=7,
          dtype=None) -> int:
     """B := alpha*op(A)*B or alpha*B*op(A), A triangular, B overwritten (trmm.mojo:20-305)."""
     dt = _dtype_of(b, dtype)

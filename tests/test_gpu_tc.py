@@ -5,7 +5,7 @@ Tolerances (max relative error, normwise max|X - X64| / max|X64|):
     BF16X3 (2-term bf16 split, 3 products):  TOL_X3 = 1.5e-5 (split residual ~2^-17)
     BF16X6 (3-term bf16 split, 6 products):  TOL32(k) = 1e-6 * sqrt(max(k, 16)),
                                              the plain float32 tolerance
-    OZAKI s slices of 7 bits:                TOL_OZ(s, k) = 16 * 2^(-7 s) + TOL64(k),
+    OZAKI s slices (8s - 2 bits kept):       TOL_OZ(s, k) = 16 * 2^(-(8 s - 2)) + TOL64(k),
                                              TOL64(k) = 4e-16 * sqrt(max(k, 16));
                                              rows scaled by 2^[-20, 20]: 64 * 2^(-7 s) + TOL64(k)
 Each result is also compared with the oracle's restatement of the reference
@@ -31,7 +31,7 @@ def tol64(k):
 
 
 def tol_oz(s, k):
-    return 16 * 2.0 ** (-7 * s) + tol64(k)
+    return 16 * 2.0 ** (-(8 * s - 2)) + tol64(k)
 
 
 def tol_mode(mode, k, slices=8):
@@ -190,7 +190,7 @@ def test_ozaki_scaled_rows(oracle, slices):
     the int8 slices exact relative to each row's maximum."""
     g, _, ref, _, _ = _gemm(oracle, np.float64, mb.OZAKI, "N", "N", 256, 192, 512, 1.0, 0.0, slices=slices,
                             scaled=True)
-    assert oracle.max_rel_err(g, ref) < 64 * 2.0 ** (-7 * slices) + tol64(512)
+    assert oracle.max_rel_err(g, ref) < 64 * 2.0 ** (-(8 * slices - 2)) + tol64(512)
 
 
 def test_ozaki_s8_at_least_as_accurate_as_plain_fp64(oracle):
@@ -200,7 +200,7 @@ def test_ozaki_s8_at_least_as_accurate_as_plain_fp64(oracle):
 
 
 def test_ozaki_int32_chunking_long_k(oracle):
-    """k beyond the int32-exact range of one pass (16640 for 8 slices) is split
+    """k beyond the int32-exact range of one pass (16384 for 8 slices) is split
     into chunks accumulated in fp64."""
     g, _, ref, _, _ = _gemm(oracle, np.float64, mb.OZAKI, "T", "N", 64, 40, 17000, 1.0, 0.25, slices=8)
     assert oracle.max_rel_err(g, ref) < tol_oz(8, 17000)
