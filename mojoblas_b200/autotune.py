@@ -11,7 +11,7 @@ Keys swept:
   trsm_block_rows    0 (64-row leaves), 256, 512 — diagonal blocks solved in
   trsm_tc_min_k      one fused launch, and the reduction length below which
                      the blocked trsm's off-diagonal updates stay on the plain
-                     kernel; swept jointly on dtrsm 4096^2 with 8-slice Ozaki
+                     kernel; swept jointly on dtrsm 4096^2 with Ozaki
                      updates (the blocked-trsm configuration);
   trsm_block_min_cols  the fewest right-hand sides for which the fused launch
                      beats the 64-row leaves, timed on dtrsm 4096 x nrhs.
