@@ -106,7 +106,7 @@ def tune(out: Path) -> dict:
     def time_trsm(mode, nrhs, reps=3):
         def call():
             X[:, :nrhs].copy_(B0[:, :nrhs])
-            st = lib.mbg_dtrsm_ex(mode, 8, 0, b"L", b"L", b"N", b"N", n, nrhs, 1.0, A.data_ptr(), n,
+            st = lib.mbg_dtrsm_ex(mode, 7, 0, b"L", b"L", b"N", b"N", n, nrhs, 1.0, A.data_ptr(), n,
                                   X.data_ptr(), n)
             if st:
                 raise RuntimeError(L.last_error())
