@@ -134,13 +134,34 @@ static int gemm_compute(int mode, int slices, char ta, char tb, i64 m, i64 n, i6
 }
 
 // Large gemm with host operands: the host <-> device copies overlap the
-// arithmetic.  C is cut into GEMM_PIPE_BLOCKS column blocks.  A copy stream
-// brings op(A) over first and then, block by block, the columns of op(B) (and
-// of C when beta != 0); the library's stream computes each block as soon as its
-// operands have landed; a second copy stream returns each finished block of C,
-// so the two directions of the PCIe link run at the same time.  The device
-// buffers are the same full-size copies the sequential path uses.
+// arithmetic.  C is cut into column blocks: GEMM_PIPE_BLOCKS blocks of equal
+// width (multiples of 256 columns, so every tile of C is the same as in one call
+// over all of C), the last of them halved down to 256 columns so that little
+// arithmetic and little copying is left after op(B)'s last columns land.  A copy
+// stream brings op(A) over first and then, block by block, the columns of op(B)
+// (and of C when beta != 0); the library's stream computes each block as soon as
+// its operands have landed (in the split modes op(A) is split once, when it has
+// landed, and its planes serve every block); a second copy stream returns each
+// finished block of C, so the two directions of the PCIe link run at the same
+// time.  The device buffers are the same full-size copies the sequential path uses.
 constexpr int GEMM_PIPE_BLOCKS = 8;
+
+static std::vector<i64> pipeline_widths(i64 n) {
+    const i64 nb = cdiv(cdiv(n, GEMM_PIPE_BLOCKS), 256) * 256;
+    std::vector<i64> w;
+    i64 rest = n;
+    while (rest > nb) {
+        w.push_back(nb);
+        rest -= nb;
+    }
+    while (rest > 256) {  // the last block: 1/2, 1/4, ... down to 256 columns
+        const i64 h = cdiv(cdiv(rest, 2), 256) * 256;
+        w.push_back(h);
+        rest -= h;
+    }
+    w.push_back(rest);
+    return w;
+}
 
 template <typename T>
 static bool gemm_pipeline_pays(const T* a, const T* b, const T* c, i64 m, i64 n, i64 k) {
@@ -173,7 +194,8 @@ static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i6
                 if (x) cudaEventDestroy(x);
         }
     } events;
-    events.v.assign(2 * GEMM_PIPE_BLOCKS + 2, nullptr);
+    const std::vector<i64> widths = pipeline_widths(n);
+    events.v.assign(2 * widths.size() + 2, nullptr);
     auto& ev = events.v;
     for (auto& x : ev) MBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
     cudaEvent_t ev_start = ev[0], ev_end = ev[1];
@@ -183,11 +205,14 @@ static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i6
     if (ha)
         MBG_CUDA(cudaMemcpy2DAsync(const_cast<T*>(da), size_t(ar) * e, a, size_t(lda) * e, size_t(ar) * e,
                                    size_t(ac), cudaMemcpyHostToDevice, sin));
-    const i64 nb = cdiv(cdiv(n, GEMM_PIPE_BLOCKS), 256) * 256;
+    // split modes: op(A)'s planes once, on the library stream after op(A) has landed
+    const bool split_once = sizeof(T) == 4 && (mode == MBG_MODE_BF16X3 || mode == MBG_MODE_BF16X6);
+    SplitA sa;
     int st = MBG_OK;
     int used = 0;
-    for (i64 j0 = 0; j0 < n && !st; j0 += nb, ++used) {
-        const i64 w = imin(nb, n - j0);
+    i64 j0 = 0;
+    for (size_t blk = 0; blk < widths.size() && !st; ++blk, ++used) {
+        const i64 w = widths[blk];
         cudaEvent_t ev_in = ev[2 + 2 * used], ev_done = ev[3 + 2 * used];
         // op(B)[:, j0 : j0 + w] is columns j0.. of B ('N') or rows j0.. of B ('T')
         if (hb) {
@@ -204,13 +229,23 @@ static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i6
         MBG_CUDA(cudaEventRecord(ev_in, sin));
         MBG_CUDA(cudaStreamWaitEvent(s, ev_in, 0));
         const T* bj = is_n(tb) ? db + j0 * dldb : db + j0;
-        st = gemm_compute<T>(mode, slices, ta, tb, m, w, k, alpha, da, dlda, bj, dldb, beta, dc + j0 * dldc, dldc);
+        if (split_once) {
+            if (blk == 0)
+                st = split_a_planes(mode == MBG_MODE_BF16X6 ? 3 : 2, ta, m, k, (const float*)da, dlda, sa);
+            if (!st)
+                st = sgemm_split_tc_with_a(sa, tb, w, (float)alpha, (const float*)bj, dldb, (float)beta,
+                                           (float*)(dc + j0 * dldc), dldc);
+        } else {
+            st = gemm_compute<T>(mode, slices, ta, tb, m, w, k, alpha, da, dlda, bj, dldb, beta, dc + j0 * dldc,
+                                 dldc);
+        }
         MBG_CUDA(cudaEventRecord(ev_done, s));
         if (hc) {
             MBG_CUDA(cudaStreamWaitEvent(sout, ev_done, 0));
             MBG_CUDA(cudaMemcpy2DAsync(c + j0 * ldc, size_t(ldc) * e, dc + j0 * dldc, size_t(dldc) * e,
                                        size_t(m) * e, size_t(w), cudaMemcpyDeviceToHost, sout));
         }
+        j0 += w;
     }
     MBG_CUDA(cudaEventRecord(ev_end, sout));
     MBG_CUDA(cudaStreamWaitEvent(s, ev_end, 0));  // the library stream completes after the last copy back

@@ -207,6 +207,16 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
                    const TriOperand* tri_op = nullptr);
 // longest reduction of one Ozaki launch (int32-exact accumulators)
 i64 ozaki_max_k(int slices);
+// op(A)'s bf16 split planes made once for several column blocks of op(B) (the
+// pipelined host path); the workspace lives as long as the SplitA
+struct SplitA {
+    Workspace ws;
+    int terms = 0;
+    i64 m = 0, k = 0, Mp = 0, Kp = 0;
+};
+int split_a_planes(int terms, char ta, i64 m, i64 k, const float* a, i64 lda, SplitA& out);
+int sgemm_split_tc_with_a(const SplitA& A, char tb, i64 n, float alpha, const float* b, i64 ldb, float beta,
+                          float* c, i64 ldc);
 
 // trsm and trmm on device operands (trsm.cu)
 template <typename T>

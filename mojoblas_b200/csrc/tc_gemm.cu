@@ -1168,6 +1168,47 @@ int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha
     return launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
 }
 
+// op(A)'s split planes made once and used for several products with column blocks of
+// op(B): the pipelined host path computes C block by block as op(B) arrives.
+int split_a_planes(int terms, char ta, i64 m, i64 k, const float* a, i64 lda, SplitA& out) {
+    using namespace tc;
+    if (terms != 2 && terms != 3) return MBG_ERR_INVALID_MODE;
+    out.terms = terms;
+    out.m = m;
+    out.k = k;
+    out.Mp = roundup(m, BM);
+    out.Kp = roundup(k, 32);
+    if (out.Kp > 0x7fffffff || out.Mp > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    MBG_TRY(out.ws.reserve(size_t(terms) * out.Mp * out.Kp * 2));
+    __nv_bfloat16* pa = out.ws.as<__nv_bfloat16>();
+    if (terms == 2) return launch_split<2>(a, lda, is_t(ta), m, k, out.Mp, out.Kp, pa);
+    return launch_split<3>(a, lda, is_t(ta), m, k, out.Mp, out.Kp, pa);
+}
+
+// C[:, 0:n] := alpha op(A) op(B) + beta C with op(A)'s planes from split_a_planes (alpha != 0, k > 0).
+int sgemm_split_tc_with_a(const SplitA& A, char tb, i64 n, float alpha, const float* b, i64 ldb, float beta,
+                          float* c, i64 ldc) {
+    using namespace tc;
+    if (A.m == 0 || n == 0) return MBG_OK;
+    const int BN = 256;
+    const i64 Np = roundup(n, BN);
+    if (Np > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    Workspace ws;
+    MBG_TRY(ws.reserve(size_t(A.terms) * Np * A.Kp * 2));
+    __nv_bfloat16* pb = ws.as<__nv_bfloat16>();
+    if (A.terms == 2) MBG_TRY(launch_split<2>(b, ldb, is_n(tb), n, A.k, Np, A.Kp, pb));
+    else MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, A.k, Np, A.Kp, pb));
+    CUtensorMap ma, mb;
+    MBG_TRY(make_map(&ma, A.ws.as<__nv_bfloat16>(), false, A.Kp, A.Mp, A.terms, 64, BM));
+    MBG_TRY(make_map(&mb, pb, false, A.Kp, Np, A.terms, 64, BN));
+    Params P{};
+    P.m = A.m; P.n = n; P.num_kb = int(A.Kp / 32);
+    P.tiles_m = int(cdiv(A.m, BM)); P.tiles_n = int(cdiv(n, BN));
+    P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
+    if (A.terms == 2) return launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
+    return launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
+}
+
 // ---- Ozaki dgemm ----------------------------------------------------------------
 namespace tc {
 template <class C>
