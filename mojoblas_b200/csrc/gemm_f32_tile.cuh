@@ -3,8 +3,9 @@
 //
 // One 256-thread CTA computes an FT x FT tile of C (FT = 128: 8 x 8 register
 // block per thread, rows tx*4+{0..3} and 64+tx*4+{0..3}, columns likewise from
-// ty; FT = 64: 4 x 4), one FMA per product, each element's sum running over k in
-// ascending order as in the reference's column loops.  K advances in slabs of 16
+// ty; FT = 64: 4 x 4), one FMA per product (two products per fma.rn.f32x2
+// instruction), each element's sum running over k in ascending order as in the
+// reference's column loops.  K advances in slabs of 16
 // through a 3-stage cp.async pipeline straight into shared memory: an operand
 // contiguous along m (n), 16-byte aligned with ld % 4 == 0, is copied 16 bytes
 // at a time, any other operand element by element into the same k-major tiles
@@ -34,6 +35,20 @@ __device__ __forceinline__ void cpa16(void* dst, const void* src, int bytes) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// Two fp32 values in one 64-bit register, and the packed FMA of sm_100 (fma.rn.f32x2:
+// two independent IEEE fused multiply-adds, so every element's arithmetic is that of fmaf).
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ void f2_fma(unsigned long long& acc, unsigned long long a, unsigned long long b) {
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
 template <int N>
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -92,11 +107,12 @@ __device__ __forceinline__ void f32_tile(i64 m, i64 n, i64 k, float alpha, const
         f32_stage<FT, TB, VB>(Bs + size_t(st) * FK * FLD, B, ldb, n0, n, kt * FK, k, tid);
     };
 
-    float acc[TM][TM];
+    // accumulators in pairs of adjacent columns: accp[i][jp] = (acc[i][2 jp], acc[i][2 jp + 1])
+    unsigned long long accp[TM][TM / 2];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < TM; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < TM / 2; ++j) accp[i][j] = 0ull;
 
     // slabs [kt0, kt0 + nk) of the reduction: all of them, or the tile's band
     i64 kt0 = 0, kt1 = (k + FK - 1) / FK;
@@ -116,24 +132,35 @@ __device__ __forceinline__ void f32_tile(i64 m, i64 n, i64 k, float alpha, const
         const float* bs = Bs + size_t(kt % FSTAGES) * FK * FLD;
 #pragma unroll
         for (int l = 0; l < FK; ++l) {
-            float a[TM], b[TM];
+            // b in pairs of adjacent columns straight from the 16-byte loads; each a duplicated
+            // into both halves, so one packed FMA updates two columns of a row
+            float a[TM];
+            unsigned long long bp[TM / 2];
             const float4 a0 = *reinterpret_cast<const float4*>(as + l * FLD + tx * 4);
-            const float4 b0 = *reinterpret_cast<const float4*>(bs + l * FLD + ty * 4);
+            const ulonglong2 b0 = *reinterpret_cast<const ulonglong2*>(bs + l * FLD + ty * 4);
             a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
-            b[0] = b0.x; b[1] = b0.y; b[2] = b0.z; b[3] = b0.w;
+            bp[0] = b0.x; bp[1] = b0.y;
             if constexpr (TM == 8) {
                 const float4 a1 = *reinterpret_cast<const float4*>(as + l * FLD + 64 + tx * 4);
-                const float4 b1 = *reinterpret_cast<const float4*>(bs + l * FLD + 64 + ty * 4);
+                const ulonglong2 b1 = *reinterpret_cast<const ulonglong2*>(bs + l * FLD + 64 + ty * 4);
                 a[TM - 4] = a1.x; a[TM - 3] = a1.y; a[TM - 2] = a1.z; a[TM - 1] = a1.w;
-                b[TM - 4] = b1.x; b[TM - 3] = b1.y; b[TM - 2] = b1.z; b[TM - 1] = b1.w;
+                bp[2] = b1.x; bp[3] = b1.y;
             }
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+            for (int i = 0; i < TM; ++i) {
+                const unsigned long long ai = f2_pack(a[i], a[i]);
 #pragma unroll
-                for (int j = 0; j < TM; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < TM / 2; ++j) f2_fma(accp[i][j], ai, bp[j]);
+            }
         }
     }
     cpa_wait<0>();
+
+    float acc[TM][TM];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TM / 2; ++j) f2_unpack(accp[i][j], acc[i][2 * j], acc[i][2 * j + 1]);
 
 #pragma unroll
     for (int j = 0; j < TM; ++j) {
