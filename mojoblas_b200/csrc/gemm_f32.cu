@@ -78,13 +78,62 @@ int launch_f32(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, co
     return launch_f32_v<FT, TRI, false, false>(ta, tb, grid, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
 }
 
+// dst[j + i * ldd] = src[i + j * lds] for i < rows, j < cols (32 x 32 tiles through shared memory)
+__global__ void f32_transpose_kernel(i64 rows, i64 cols, const float* __restrict__ src, i64 lds,
+                                     float* __restrict__ dst, i64 ldd) {
+    __shared__ float tile[32][33];
+    const i64 i0 = (i64)blockIdx.x * 32, j0 = (i64)blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const i64 i = i0 + threadIdx.x, j = j0 + r;
+        if (i < rows && j < cols) tile[r][threadIdx.x] = src[i + j * lds];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const i64 j = j0 + threadIdx.x, i = i0 + r;
+        if (i < rows && j < cols) dst[j + i * ldd] = tile[threadIdx.x][r];
+    }
+}
+
+int launch_f32_transpose(i64 rows, i64 cols, const float* src, i64 lds, float* dst, i64 ldd) {
+    ProfScope prof("gemm_f32_transpose");
+    dim3 g((unsigned)cdiv(rows, 32), (unsigned)cdiv(cols, 32)), blk(32, 8);
+    if (g.y > 65535) return MBG_ERR_UNSUPPORTED;
+    f32_transpose_kernel<<<g, blk, 0, stream()>>>(rows, cols, src, lds, dst, ldd);
+    return check_launch("gemm_f32_transpose");
+}
+
 }  // namespace
 
 // C := alpha op(A) op(B) + beta C (alpha != 0, k > 0): 128 x 128 tiles, or 64 x 64
 // tiles (4 x 4 per thread) when 128-tiles would fill fewer than two waves.
 // band (KB_*): one operand is a dense triangle; each tile runs its part of k.
+// The tiles copy an operand 16 bytes at a time only when it is contiguous along m
+// (op(A)) or n (op(B)), as in NT.  In a large call (m n k >= 2^30) an operand that is
+// contiguous along k instead (A with 'T', B with 'N') is first transposed into a
+// workspace (2 x 4 bytes per element against the GEMM's 2k flops per element of C);
+// every element's sum is unchanged, the NT tiles run.
 int sgemm_f32(char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda, const float* b,
               i64 ldb, float beta, float* c, i64 ldc, int band) {
+    if (double(m) * double(n) * double(k) >= double(1ll << 30) && (is_t(ta) || is_n(tb))) {
+        Workspace wa, wb;
+        if (is_t(ta)) {  // A is k x m (k contiguous): At = m x k
+            const i64 ld = cdiv(m, 4) * 4;
+            MBG_TRY(wa.reserve(sizeof(float) * size_t(ld) * size_t(k)));
+            MBG_TRY(launch_f32_transpose(k, m, a, lda, wa.as<float>(), ld));
+            a = wa.as<float>();
+            lda = ld;
+            ta = 'N';
+        }
+        if (is_n(tb)) {  // B is k x n (k contiguous): Bt = n x k, used as op(B) = Bt^T
+            const i64 ld = cdiv(n, 4) * 4;
+            MBG_TRY(wb.reserve(sizeof(float) * size_t(ld) * size_t(k)));
+            MBG_TRY(launch_f32_transpose(k, n, b, ldb, wb.as<float>(), ld));
+            b = wb.as<float>();
+            ldb = ld;
+            tb = 'T';
+        }
+        return sgemm_f32(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, band);
+    }
     ProfScope prof("gemm_f32");
     const i64 gm = cdiv(m, 128), gn = cdiv(n, 128);
     if (gm * gn < 2 * 148) {
