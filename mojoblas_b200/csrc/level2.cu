@@ -300,53 +300,116 @@ __device__ __forceinline__ T opa(const T* __restrict__ A, i64 lda, i64 i, i64 l)
     return TRANS ? A[l + i * lda] : A[i + l * lda];
 }
 
+inline i64 vec_start(i64 len, i64 inc) { return inc > 0 ? 0 : -(len - 1) * inc; }
+
+constexpr int TV_LD = TV_NB + 1;  // shared-memory row of a 64 x 64 block
+
+template <typename T>
+constexpr size_t trsv_smem_bytes() {
+    return sizeof(T) * (size_t(2) * TV_NB * TV_LD + 2 * TV_GROUPS * TV_NB + 2 * TV_NB) + 4 * sizeof(int);
+}
+
+// Block b of the solution, with p the block solved just before it (b - 1 forward,
+// b + 1 backward) and L the diagonal block of op(A):
+//     x_b = L^-1 (b_b - sum_{j before p} op(A)_bj x_j) - (L^-1 op(A)_bp) x_p = y - M x_p.
+// M does not depend on x, and y needs every block but p: both are computed while
+// block p is still being solved, so once x_p is published only the 64 x 64
+// product M x_p remains on the chain of blocks.  M's 64 columns are solved by the
+// 8 warps, 8 each (lanes own rows lane and lane + 32; pivot by shuffle, scaled by
+// the reciprocal of the diagonal); y by warp 0 the same way.  The reference's
+// zero skip (NoTrans) is kept: a zero pivot updates nothing, and a zero entry of
+// x_p skips its column of M.
 template <typename T, bool TRANS>
 __global__ void __launch_bounds__(TV_THREADS)
 trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx, i64 kx, bool lower, bool unit,
             TrsvSync s) {
-    __shared__ T diag[TV_NB][TV_NB + 1];  // op(A) diagonal block, the triangle only
-    __shared__ T red[2 * TV_GROUPS][TV_NB];
-    __shared__ int sticket, sok[2];
+    extern __shared__ __align__(16) unsigned char tv_smem[];
+    T* diag = reinterpret_cast<T*>(tv_smem);      // [64][TV_LD] op(A) diagonal block, the triangle only
+    T* Mt = diag + TV_NB * TV_LD;                  // [64][TV_LD] op(A)_bp, then M = L^-1 op(A)_bp
+    T* red = Mt + TV_NB * TV_LD;                   // [2 * TV_GROUPS][64] partial sums
+    T* invs = red + 2 * TV_GROUPS * TV_NB;         // [64] reciprocals of the diagonal (1 for unit)
+    T* ys = invs + TV_NB;                          // [64] y
+    int* sint = reinterpret_cast<int*>(ys + TV_NB);  // [0] ticket, [1], [2] wait results
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const i64 nb = (n + TV_NB - 1) / TV_NB;
-    if (tid == 0) sticket = atomicAdd(s.ticket, 1);
+    if (tid == 0) sint[0] = atomicAdd(s.ticket, 1);
     __syncthreads();
-    const i64 t = sticket;
+    const i64 t = sint[0];
     const i64 b = lower ? t : nb - 1 - t;
     const i64 r0 = b * TV_NB;
     const int rows = int(min(i64(TV_NB), n - r0));
+    const bool has_prev = t >= 1;
+    const i64 bp = lower ? b - 1 : b + 1;  // the block solved just before this one
+    const i64 cp0 = bp * TV_NB;
+    const int pcols = has_prev ? int(min(i64(TV_NB), n - cp0)) : 0;
+    const int dp = lower ? 1 : -1;
 
-    // the diagonal block (no dependence on x): op(A)(r0 + i, r0 + l) on and inside the triangle
+    // the diagonal block and the tile op(A)(rows of b, columns of p); f runs along A's contiguous index
     for (int e = tid; e < TV_NB * TV_NB; e += TV_THREADS) {
-        const int f = e % TV_NB, g = e / TV_NB;  // f runs along A's contiguous index
+        const int f = e % TV_NB, g = e / TV_NB;
         const int i = TRANS ? g : f, l = TRANS ? f : g;
         const bool in = lower ? (l < i) : (l > i);
         T v = T(0);
         if (i < rows && l < rows && (in || (l == i && !unit))) v = opa<T, TRANS>(A, lda, r0 + i, r0 + l);
-        diag[i][l] = v;
+        diag[i * TV_LD + l] = v;
+        T w = T(0);
+        if (i < rows && l < pcols) w = opa<T, TRANS>(A, lda, r0 + i, cp0 + l);
+        Mt[i * TV_LD + l] = w;
     }
-
-    __syncthreads();  // the diagonal block is staged
-    // warp 0 reads its right-hand side and the reciprocals of the diagonal now, while it
-    // waits for the blocks before it; lane owns rows lane and lane + 32
-    T rhs0 = T(0), rhs1 = T(0), inv0 = T(1), inv1 = T(1);
+    __syncthreads();
+    if (tid < TV_NB) invs[tid] = (tid < rows && !unit) ? T(1) / diag[tid * TV_LD + tid] : T(1);
+    T rhs0 = T(0), rhs1 = T(0);
     if (warp == 0) {
         if (lane < rows) rhs0 = x[kx + (r0 + lane) * incx];
         if (lane + 32 < rows) rhs1 = x[kx + (r0 + lane + 32) * incx];
-        if (!unit) {
-            if (lane < rows) inv0 = T(1) / diag[lane][lane];
-            if (lane + 32 < rows) inv1 = T(1) / diag[lane + 32][lane + 32];
+    }
+    __syncthreads();  // invs complete
+
+    // M := L^-1 op(A)_bp, columns warp * 8 .. warp * 8 + 7
+    if (has_prev) {
+        T m0[8], m1[8];
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+            m0[cc] = Mt[lane * TV_LD + warp * 8 + cc];
+            m1[cc] = Mt[(lane + 32) * TV_LD + warp * 8 + cc];
+        }
+        int p = lower ? 0 : rows - 1;
+        for (int st = 0; st < rows; ++st, p += dp) {
+            const int owner = p & 31;
+            const bool hi = p >= 32;
+            const T ip = invs[p];
+            const T d0 = diag[lane * TV_LD + p], d1 = diag[(lane + 32) * TV_LD + p];
+            const bool up0 = lower ? lane > p : lane < p, up1 = lower ? lane + 32 > p : lane + 32 < p;
+#pragma unroll
+            for (int cc = 0; cc < 8; ++cc) {
+                T mine = hi ? m1[cc] : m0[cc];
+                if (!unit && (TRANS || mine != T(0))) mine = mine * ip;
+                const T xp = __shfl_sync(0xffffffffu, mine, owner);
+                if (lane == owner) {
+                    if (hi) m1[cc] = xp;
+                    else m0[cc] = xp;
+                }
+                if (TRANS || xp != T(0)) {
+                    if (up0) m0[cc] = fma(-d0, xp, m0[cc]);
+                    if (up1) m1[cc] = fma(-d1, xp, m1[cc]);
+                }
+            }
+        }
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+            Mt[lane * TV_LD + warp * 8 + cc] = m0[cc];
+            Mt[(lane + 32) * TV_LD + warp * 8 + cc] = m1[cc];
         }
     }
 
-    // contributions of the blocks solved before this one
+    // contributions of the blocks solved before p
     // NoTrans: thread (row r = tid % 64, columns g * 16 .. g * 16 + 15 of each tile), one sum
     // Trans:   thread (column l = tid % 64, rows g * 16 .. g * 16 + 15), sixteen sums
     const int f = tid % TV_NB, g = tid / TV_NB;
     T acc[TV_PER];
 #pragma unroll
     for (int u = 0; u < TV_PER; ++u) acc[u] = T(0);
-    for (i64 q = 0; q < t; ++q) {
+    for (i64 q = 0; q + 1 < t; ++q) {
         const i64 jb = lower ? q : nb - 1 - q;
         const i64 c0 = jb * TV_NB;
         const int cols = int(min(i64(TV_NB), n - c0));  // the last block of a backward solve may be short
@@ -357,9 +420,9 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
             const int i = TRANS ? g * TV_PER + u : f, l = TRANS ? f : g * TV_PER + u;
             av[u] = (i < rows && l < cols) ? opa<T, TRANS>(A, lda, r0 + i, c0 + l) : T(0);
         }
-        if (tid == 0) sok[q & 1] = tv_wait(s.flags + jb, s) ? 1 : 0;
+        if (tid == 0) sint[1 + (q & 1)] = tv_wait(s.flags + jb, s) ? 1 : 0;
         __syncthreads();
-        if (!sok[q & 1]) return;
+        if (!sint[1 + (q & 1)]) return;
         if (TRANS) {
             const T xl = f < cols ? __ldcg(x + kx + (c0 + f) * incx) : T(0);
 #pragma unroll
@@ -381,61 +444,100 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
             T v = acc[u];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) red[(warp & 1)][g * TV_PER + u] = v;  // two warps per group of columns
+            if (lane == 0) red[(warp & 1) * TV_NB + g * TV_PER + u] = v;  // two warps per group of columns
         }
     } else {
-        red[g][f] = acc[0];
+        red[g * TV_NB + f] = acc[0];
     }
     __syncthreads();
-    if (warp != 0) return;
 
-    // one warp: right-hand side minus the contributions, then substitution.  Per pivot p the
-    // owner lane scales its own value by its own reciprocal, one shuffle broadcasts x_p, every
-    // lane updates its rows after p; the column of the next pivot is loaded one step ahead.
-    // Rows at or beyond `rows` hold zeros and see zero coefficients.  (Four pivots per step,
-    // every lane solving the 4 x 4 group triangle itself, measured slower: 7.1 us against
-    // 4.9 us per 64-row block in float64.)
-    T v0, v1;
-    if (TRANS) {
-        v0 = rhs0 - (red[0][lane] + red[1][lane]);
-        v1 = rhs1 - (red[0][lane + 32] + red[1][lane + 32]);
+    // warp 0: y = L^-1 (right-hand side minus the contributions), one pivot per step (the
+    // owner scales its own value, one shuffle broadcasts it, every lane updates its rows
+    // after the pivot; the next pivot's column is loaded one step ahead)
+    if (warp == 0) {
+        T v0, v1;
+        if (TRANS) {
+            v0 = rhs0 - (red[lane] + red[TV_NB + lane]);
+            v1 = rhs1 - (red[lane + 32] + red[TV_NB + lane + 32]);
+        } else {
+            v0 = rhs0 - ((red[lane] + red[TV_NB + lane]) + (red[2 * TV_NB + lane] + red[3 * TV_NB + lane]));
+            v1 = rhs1 - ((red[lane + 32] + red[TV_NB + lane + 32]) +
+                         (red[2 * TV_NB + lane + 32] + red[3 * TV_NB + lane + 32]));
+        }
+        if (lane >= rows) v0 = T(0);
+        if (lane + 32 >= rows) v1 = T(0);
+        const T inv0 = invs[lane], inv1 = invs[lane + 32];
+        int p = lower ? 0 : rows - 1;
+        T d0 = diag[lane * TV_LD + p], d1 = diag[(lane + 32) * TV_LD + p];
+        for (int st = 0; st < rows; ++st, p += dp) {
+            const int owner = p & 31;
+            const bool hi = p >= 32;
+            T mine = hi ? v1 : v0;
+            const T mi = hi ? inv1 : inv0;
+            if (!unit && (TRANS || mine != T(0))) mine = mine * mi;  // the reference skips zeros (NoTrans)
+            const T xp = __shfl_sync(0xffffffffu, mine, owner);
+            const int pn = (st + 1 < rows) ? p + dp : p;
+            const T d0n = diag[lane * TV_LD + pn], d1n = diag[(lane + 32) * TV_LD + pn];
+            if (lane == owner) {
+                if (hi) v1 = xp;
+                else v0 = xp;
+            }
+            if (TRANS || xp != T(0)) {
+                if (lower ? lane > p : lane < p) v0 = fma(-d0, xp, v0);
+                if (lower ? lane + 32 > p : lane + 32 < p) v1 = fma(-d1, xp, v1);
+            }
+            d0 = d0n;
+            d1 = d1n;
+        }
+        ys[lane] = v0;
+        ys[lane + 32] = v1;
+    }
+
+    // x_b = y - M x_p once block p is published
+    if (has_prev) {
+        if (tid == 0) sint[1] = tv_wait(s.flags + bp, s) ? 1 : 0;
+        __syncthreads();  // also orders warp 0's reads of red before the writes below
+        if (!sint[1]) return;
+        T part = T(0);
+#pragma unroll
+        for (int u = 0; u < TV_PER; ++u) {
+            const int c = g * TV_PER + u;
+            const T xc = c < pcols ? __ldcg(x + kx + (cp0 + c) * incx) : T(0);
+            if (TRANS || xc != T(0)) part = fma(Mt[f * TV_LD + c], xc, part);
+        }
+        red[g * TV_NB + f] = part;
+        __syncthreads();
     } else {
-        v0 = rhs0 - ((red[0][lane] + red[1][lane]) + (red[2][lane] + red[3][lane]));
-        v1 = rhs1 - ((red[0][lane + 32] + red[1][lane + 32]) + (red[2][lane + 32] + red[3][lane + 32]));
+        __syncthreads();  // ys complete
     }
-    if (lane >= rows) v0 = T(0);
-    if (lane + 32 >= rows) v1 = T(0);
-    const int dp = lower ? 1 : -1;
-    int p = lower ? 0 : rows - 1;
-    T d0 = diag[lane][p], d1 = diag[lane + 32][p];
-    for (int st = 0; st < rows; ++st, p += dp) {
-        const int owner = p & 31;
-        const bool hi = p >= 32;
-        T mine = hi ? v1 : v0;
-        const T mi = hi ? inv1 : inv0;
-        if (!unit && (TRANS || mine != T(0))) mine = mine * mi;  // the reference skips zeros (NoTrans)
-        const T xp = __shfl_sync(0xffffffffu, mine, owner);
-        const int pn = (st + 1 < rows) ? p + dp : p;
-        const T d0n = diag[lane][pn], d1n = diag[lane + 32][pn];
-        if (lane == owner) {
-            if (hi) v1 = xp;
-            else v0 = xp;
-        }
-        if (TRANS || xp != T(0)) {
-            if (lower ? lane > p : lane < p) v0 = fma(-d0, xp, v0);
-            if (lower ? lane + 32 > p : lane + 32 < p) v1 = fma(-d1, xp, v1);
-        }
-        d0 = d0n;
-        d1 = d1n;
+    if (warp != 0) return;
+    T r0v = ys[lane], r1v = ys[lane + 32];
+    if (has_prev) {
+        r0v -= (red[lane] + red[TV_NB + lane]) + (red[2 * TV_NB + lane] + red[3 * TV_NB + lane]);
+        r1v -= (red[lane + 32] + red[TV_NB + lane + 32]) + (red[2 * TV_NB + lane + 32] + red[3 * TV_NB + lane + 32]);
     }
-    if (lane < rows) x[kx + (r0 + lane) * incx] = v0;
-    if (lane + 32 < rows) x[kx + (r0 + lane + 32) * incx] = v1;
+    if (lane < rows) x[kx + (r0 + lane) * incx] = r0v;
+    if (lane + 32 < rows) x[kx + (r0 + lane + 32) * incx] = r1v;
     __threadfence();
     __syncwarp();
     if (lane == 0) tv_store_release(s.flags + b, 1);
 }
 
-inline i64 vec_start(i64 len, i64 inc) { return inc > 0 ? 0 : -(len - 1) * inc; }
+template <typename T, bool TRANS>
+int launch_trsv_t(i64 n, const T* a, i64 lda, T* x, i64 incx, bool lower, bool unit, const TrsvSync& sync,
+                  i64 nb) {
+    constexpr size_t SM = trsv_smem_bytes<T>();
+    static unsigned configured = 0;  // one bit per device: more than 48 KB of shared memory needs an opt-in
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    if (dev >= 32 || !(configured & (1u << dev))) {
+        MBG_CUDA(cudaFuncSetAttribute(trsv_kernel<T, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
+        if (dev < 32) configured |= 1u << dev;
+    }
+    trsv_kernel<T, TRANS><<<(unsigned)nb, TV_THREADS, SM, stream()>>>(n, a, lda, x, incx, vec_start(n, incx), lower,
+                                                                       unit, sync);
+    return check_launch("trsv");
+}
 
 }  // namespace
 
@@ -557,9 +659,8 @@ int trsv_device(char uplo, char trans, char diag, i64 n, const T* a, i64 lda, T*
     MBG_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * size_t(nb + 2), s));
     TrsvSync sync{flags, flags + nb, flags + nb + 1, device_error_flag()};
     ProfScope prof("trsv");
-    if (tr) trsv_kernel<T, true><<<(unsigned)nb, TV_THREADS, 0, s>>>(n, a, lda, x, incx, vec_start(n, incx), lower, unit, sync);
-    else trsv_kernel<T, false><<<(unsigned)nb, TV_THREADS, 0, s>>>(n, a, lda, x, incx, vec_start(n, incx), lower, unit, sync);
-    return check_launch("trsv");
+    if (tr) return launch_trsv_t<T, true>(n, a, lda, x, incx, lower, unit, sync, nb);
+    return launch_trsv_t<T, false>(n, a, lda, x, incx, lower, unit, sync, nb);
 }
 
 template int gemv_device<float>(char, i64, i64, float, const float*, i64, const float*, i64, float, float*, i64);
