@@ -21,13 +21,15 @@
 // does all of it.  Each 256-thread CTA takes a ticket from an atomic counter and
 // solves row block `ticket` in solve order (forward for an effectively lower
 // op(A), backward otherwise), so a CTA only ever waits for CTAs that started
-// before it.  For each earlier block it loads its tile of op(A) into registers,
-// waits for that block's flag (acquire; bounded by %globaltimer, with an abort
-// flag so that one expired wait ends the others at once), reads the published
-// x values from L2 and accumulates.  Then it reduces the partial sums, and one
-// warp solves the 64 x 64 diagonal block by substitution (pivot broadcast by a
-// shuffle, multiply by the reciprocal of the diagonal), writes its part of x
-// and releases its flag.  The reference skips zero entries of x in the NoTrans
+// before it.  Waits are on per-block flags (acquire; bounded by %globaltimer,
+// with an abort flag so that one expired wait ends the others at once), and the
+// published x values are read from L2.  The two blocks solved just before b
+// enter through precomputed 64 x 64 matrices (L^-1 op(A)_b,p, see trsv_kernel),
+// so the chain of blocks carries only a matrix-vector product per block; every
+// earlier block is accumulated tile by tile as it arrives, its tile of op(A)
+// loaded before the wait, and one warp solves the 64 x 64 diagonal block by
+// substitution (pivot broadcast by a shuffle, multiply by the reciprocal of the
+// diagonal).  The reference skips zero entries of x in the NoTrans
 // substitution; so does this one.
 #include "mbg_internal.cuh"
 
@@ -306,27 +308,31 @@ constexpr int TV_LD = TV_NB + 1;  // shared-memory row of a 64 x 64 block
 
 template <typename T>
 constexpr size_t trsv_smem_bytes() {
-    return sizeof(T) * (size_t(2) * TV_NB * TV_LD + 2 * TV_GROUPS * TV_NB + 2 * TV_NB) + 4 * sizeof(int);
+    return sizeof(T) * (size_t(3) * TV_NB * TV_LD + 2 * TV_GROUPS * TV_NB + 2 * TV_NB) + 4 * sizeof(int);
 }
 
-// Block b of the solution, with p the block solved just before it (b - 1 forward,
-// b + 1 backward) and L the diagonal block of op(A):
-//     x_b = L^-1 (b_b - sum_{j before p} op(A)_bj x_j) - (L^-1 op(A)_bp) x_p = y - M x_p.
-// M does not depend on x, and y needs every block but p: both are computed while
-// block p is still being solved, so once x_p is published only the 64 x 64
-// product M x_p remains on the chain of blocks.  M's 64 columns are solved by the
-// 8 warps, 8 each (lanes own rows lane and lane + 32; pivot by shuffle, scaled by
-// the reciprocal of the diagonal); y by warp 0 the same way.  The reference's
-// zero skip (NoTrans) is kept: a zero pivot updates nothing, and a zero entry of
-// x_p skips its column of M.
+// Block b of the solution, with p1 and p2 the blocks solved one and two steps
+// before it (b - 1, b - 2 forward; b + 1, b + 2 backward) and L the diagonal
+// block of op(A):
+//     x_b = L^-1 (b_b - sum_{j before p2} op(A)_bj x_j) - M2 x_p2 - M1 x_p1,
+//     M1 = L^-1 op(A)_b,p1,  M2 = L^-1 op(A)_b,p2.
+// M1 and M2 do not depend on x, y = L^-1 (...) needs every block before p2, and
+// M2 x_p2 is applied as soon as p2 is published: once x_p1 arrives, only the
+// 64 x 64 product M1 x_p1 remains on the chain of blocks, and y's 64-step
+// substitution has two block steps to finish.  M1's and M2's 128 columns are
+// solved by the 8 warps, 16 each (lanes own rows lane and lane + 32; pivot by
+// shuffle, scaled by the reciprocal of the diagonal); y by warp 0 the same way.
+// The reference's zero skip (NoTrans) is kept: a zero pivot updates nothing, and
+// a zero entry of x_p1 / x_p2 skips its column of M1 / M2.
 template <typename T, bool TRANS>
 __global__ void __launch_bounds__(TV_THREADS)
 trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx, i64 kx, bool lower, bool unit,
             TrsvSync s) {
     extern __shared__ __align__(16) unsigned char tv_smem[];
     T* diag = reinterpret_cast<T*>(tv_smem);      // [64][TV_LD] op(A) diagonal block, the triangle only
-    T* Mt = diag + TV_NB * TV_LD;                  // [64][TV_LD] op(A)_bp, then M = L^-1 op(A)_bp
-    T* red = Mt + TV_NB * TV_LD;                   // [2 * TV_GROUPS][64] partial sums
+    T* M1 = diag + TV_NB * TV_LD;                  // [64][TV_LD] op(A)_b,p1, then L^-1 op(A)_b,p1
+    T* M2 = M1 + TV_NB * TV_LD;                    // [64][TV_LD] op(A)_b,p2, then L^-1 op(A)_b,p2
+    T* red = M2 + TV_NB * TV_LD;                   // [2 * TV_GROUPS][64] partial sums
     T* invs = red + 2 * TV_GROUPS * TV_NB;         // [64] reciprocals of the diagonal (1 for unit)
     T* ys = invs + TV_NB;                          // [64] y
     int* sint = reinterpret_cast<int*>(ys + TV_NB);  // [0] ticket, [1], [2] wait results
@@ -338,10 +344,11 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
     const i64 b = lower ? t : nb - 1 - t;
     const i64 r0 = b * TV_NB;
     const int rows = int(min(i64(TV_NB), n - r0));
-    const bool has_prev = t >= 1;
-    const i64 bp = lower ? b - 1 : b + 1;  // the block solved just before this one
-    const i64 cp0 = bp * TV_NB;
-    const int pcols = has_prev ? int(min(i64(TV_NB), n - cp0)) : 0;
+    const bool has_p1 = t >= 1, has_p2 = t >= 2;
+    const i64 bp1 = lower ? b - 1 : b + 1, bp2 = lower ? b - 2 : b + 2;  // solved one / two steps before
+    const i64 c10 = bp1 * TV_NB, c20 = bp2 * TV_NB;
+    const int cols1 = has_p1 ? int(min(i64(TV_NB), n - c10)) : 0;
+    const int cols2 = has_p2 ? int(min(i64(TV_NB), n - c20)) : 0;
     const int dp = lower ? 1 : -1;
 
     // the diagonal block and the tile op(A)(rows of b, columns of p); f runs along A's contiguous index
@@ -352,9 +359,11 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
         T v = T(0);
         if (i < rows && l < rows && (in || (l == i && !unit))) v = opa<T, TRANS>(A, lda, r0 + i, r0 + l);
         diag[i * TV_LD + l] = v;
-        T w = T(0);
-        if (i < rows && l < pcols) w = opa<T, TRANS>(A, lda, r0 + i, cp0 + l);
-        Mt[i * TV_LD + l] = w;
+        T w1 = T(0), w2 = T(0);
+        if (i < rows && l < cols1) w1 = opa<T, TRANS>(A, lda, r0 + i, c10 + l);
+        if (i < rows && l < cols2) w2 = opa<T, TRANS>(A, lda, r0 + i, c20 + l);
+        M1[i * TV_LD + l] = w1;
+        M2[i * TV_LD + l] = w2;
     }
     __syncthreads();
     if (tid < TV_NB) invs[tid] = (tid < rows && !unit) ? T(1) / diag[tid * TV_LD + tid] : T(1);
@@ -365,13 +374,15 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
     }
     __syncthreads();  // invs complete
 
-    // M := L^-1 op(A)_bp, columns warp * 8 .. warp * 8 + 7
-    if (has_prev) {
-        T m0[8], m1[8];
+    // M1 := L^-1 op(A)_b,p1 and M2 := L^-1 op(A)_b,p2: warp w solves columns w * 8 .. w * 8 + 7 of both
+    if (has_p1) {
+        constexpr int NC = 16;  // columns per warp: 8 of M1, then 8 of M2
+        T m0[NC], m1[NC];
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) {
-            m0[cc] = Mt[lane * TV_LD + warp * 8 + cc];
-            m1[cc] = Mt[(lane + 32) * TV_LD + warp * 8 + cc];
+        for (int cc = 0; cc < NC; ++cc) {
+            const T* Mc = cc < 8 ? M1 : M2;
+            m0[cc] = Mc[lane * TV_LD + warp * 8 + (cc & 7)];
+            m1[cc] = Mc[(lane + 32) * TV_LD + warp * 8 + (cc & 7)];
         }
         int p = lower ? 0 : rows - 1;
         for (int st = 0; st < rows; ++st, p += dp) {
@@ -381,7 +392,7 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
             const T d0 = diag[lane * TV_LD + p], d1 = diag[(lane + 32) * TV_LD + p];
             const bool up0 = lower ? lane > p : lane < p, up1 = lower ? lane + 32 > p : lane + 32 < p;
 #pragma unroll
-            for (int cc = 0; cc < 8; ++cc) {
+            for (int cc = 0; cc < NC; ++cc) {
                 T mine = hi ? m1[cc] : m0[cc];
                 if (!unit && (TRANS || mine != T(0))) mine = mine * ip;
                 const T xp = __shfl_sync(0xffffffffu, mine, owner);
@@ -396,20 +407,21 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
             }
         }
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) {
-            Mt[lane * TV_LD + warp * 8 + cc] = m0[cc];
-            Mt[(lane + 32) * TV_LD + warp * 8 + cc] = m1[cc];
+        for (int cc = 0; cc < NC; ++cc) {
+            T* Mc = cc < 8 ? M1 : M2;
+            Mc[lane * TV_LD + warp * 8 + (cc & 7)] = m0[cc];
+            Mc[(lane + 32) * TV_LD + warp * 8 + (cc & 7)] = m1[cc];
         }
     }
 
-    // contributions of the blocks solved before p
+    // contributions of the blocks solved before p2
     // NoTrans: thread (row r = tid % 64, columns g * 16 .. g * 16 + 15 of each tile), one sum
     // Trans:   thread (column l = tid % 64, rows g * 16 .. g * 16 + 15), sixteen sums
     const int f = tid % TV_NB, g = tid / TV_NB;
     T acc[TV_PER];
 #pragma unroll
     for (int u = 0; u < TV_PER; ++u) acc[u] = T(0);
-    for (i64 q = 0; q + 1 < t; ++q) {
+    for (i64 q = 0; q + 2 < t; ++q) {
         const i64 jb = lower ? q : nb - 1 - q;
         const i64 c0 = jb * TV_NB;
         const int cols = int(min(i64(TV_NB), n - c0));  // the last block of a backward solve may be short
@@ -493,31 +505,36 @@ trsv_kernel(i64 n, const T* __restrict__ A, i64 lda, T* __restrict__ x, i64 incx
         ys[lane + 32] = v1;
     }
 
-    // x_b = y - M x_p once block p is published
-    if (has_prev) {
-        if (tid == 0) sint[1] = tv_wait(s.flags + bp, s) ? 1 : 0;
-        __syncthreads();  // also orders warp 0's reads of red before the writes below
+    // y -= M2 x_p2 once block p2 is published, then x_b = y - M1 x_p1 once p1 is: each a 64 x 64
+    // product by all threads, partial sums over four column groups added by warp 0
+    for (int step = 0; step < 2; ++step) {
+        const bool live = step == 0 ? has_p2 : has_p1;
+        if (!live) continue;  // uniform across the CTA
+        const T* Mm = step == 0 ? M2 : M1;
+        const i64 cb = step == 0 ? c20 : c10;
+        const int cn = step == 0 ? cols2 : cols1;
+        if (tid == 0) sint[1] = tv_wait(s.flags + (step == 0 ? bp2 : bp1), s) ? 1 : 0;
+        __syncthreads();  // also orders warp 0's earlier reads of red before the writes below
         if (!sint[1]) return;
         T part = T(0);
 #pragma unroll
         for (int u = 0; u < TV_PER; ++u) {
             const int c = g * TV_PER + u;
-            const T xc = c < pcols ? __ldcg(x + kx + (cp0 + c) * incx) : T(0);
-            if (TRANS || xc != T(0)) part = fma(Mt[f * TV_LD + c], xc, part);
+            const T xc = c < cn ? __ldcg(x + kx + (cb + c) * incx) : T(0);
+            if (TRANS || xc != T(0)) part = fma(Mm[f * TV_LD + c], xc, part);
         }
         red[g * TV_NB + f] = part;
         __syncthreads();
-    } else {
-        __syncthreads();  // ys complete
+        if (warp == 0) {
+            ys[lane] -= (red[lane] + red[TV_NB + lane]) + (red[2 * TV_NB + lane] + red[3 * TV_NB + lane]);
+            ys[lane + 32] -= (red[lane + 32] + red[TV_NB + lane + 32]) +
+                             (red[2 * TV_NB + lane + 32] + red[3 * TV_NB + lane + 32]);
+        }
     }
     if (warp != 0) return;
-    T r0v = ys[lane], r1v = ys[lane + 32];
-    if (has_prev) {
-        r0v -= (red[lane] + red[TV_NB + lane]) + (red[2 * TV_NB + lane] + red[3 * TV_NB + lane]);
-        r1v -= (red[lane + 32] + red[TV_NB + lane + 32]) + (red[2 * TV_NB + lane + 32] + red[3 * TV_NB + lane + 32]);
-    }
-    if (lane < rows) x[kx + (r0 + lane) * incx] = r0v;
-    if (lane + 32 < rows) x[kx + (r0 + lane + 32) * incx] = r1v;
+    __syncwarp();
+    if (lane < rows) x[kx + (r0 + lane) * incx] = ys[lane];
+    if (lane + 32 < rows) x[kx + (r0 + lane + 32) * incx] = ys[lane + 32];
     __threadfence();
     __syncwarp();
     if (lane == 0) tv_store_release(s.flags + b, 1);
