@@ -8,7 +8,7 @@ float64 numpy computation.  Tolerance (normwise max relative error against
 float64, k = the reduction length):
     plain float32, BF16x6:  1e-6 * sqrt(max(k, 16))
     BF16x3:                 1e-5 (two bf16 terms keep ~2^-17 per product at any k)
-    plain float64, Ozaki s = 8:  4e-16 * sqrt(max(k, 16))
+    plain float64, Ozaki (the default 7 slices):  4e-16 * sqrt(max(k, 16))
 each times 4; GPU and oracle agree within twice that.  Entries that the routine
 must not read (the other triangle of A, the diagonal of a unit triangle) are
 NaN, and entries it must not write (padding rows, the other triangle of C) are
