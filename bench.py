@@ -1008,6 +1008,41 @@ def run_cpu_baseline(args, threads=None, rows=N_S, calls=("NT", "TN")):
             "seconds": round(secs, 3), "flops": flops}
 
 
+def run_cpu_context_numpy(cols=512, min_seconds=1.0):
+    """Context beside the CPU baseline: numpy's float32 matmul (the BLAS numpy ships) on the
+    same 8192 x 8192 operands, columns 0..cols-1 of C for the NT and TN calls, repeated until
+    min_seconds have passed (mean rate); threads as the BLAS library reports them."""
+    n = N_S
+    if "ab" not in _CPU_DATA:
+        rng = np.random.default_rng(1234)
+        _CPU_DATA["ab"] = (np.asfortranarray(rng.uniform(-1, 1, (n, n)).astype(np.float32)),
+                           np.asfortranarray(rng.uniform(-1, 1, (n, n)).astype(np.float32)))
+    a, b = _CPU_DATA["ab"]
+    calls = {"NT": lambda: a @ b[:cols, :].T, "TN": lambda: a.T @ b[:, :cols]}
+    for f in calls.values():
+        f()  # warm-up: thread pool start, first touch of the result
+    secs, reps = 0.0, 0
+    while secs < min_seconds or reps < 2:
+        for f in calls.values():
+            t0 = time.perf_counter()
+            f()
+            secs += time.perf_counter() - t0
+        reps += 1
+    flops = 2.0 * n * n * cols * len(calls) * reps
+    lib = {}
+    try:
+        from threadpoolctl import threadpool_info
+        blas = [i for i in threadpool_info() if i.get("user_api") == "blas"]
+        if blas:
+            lib = {"library": f"{blas[0].get('internal_api')} {blas[0].get('version')}",
+                   "threads": blas[0].get("num_threads")}
+    except Exception as e:  # context only: a missing introspection module is reported, not fatal
+        lib = {"library": f"unknown ({type(e).__name__})"}
+    return {"value": round(flops / secs / 1e12, 3), "unit": "TFLOP/s", "kind": "numpy matmul (context)",
+            "sample": f"columns 0..{cols - 1} of C for NT and TN 8192^3, float32, mean over {reps} repetitions",
+            "seconds": round(secs, 3), **lib}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1070,6 +1105,7 @@ def main():
     if rank == 0 and not args.skip_cpu:
         cb = run_cpu_baseline(args)
         out["cpu_baseline"] = cb
+        out["cpu_context_numpy"] = run_cpu_context_numpy()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
