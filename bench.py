@@ -150,25 +150,20 @@ def rows_error(c, ref, rows):
     return float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
 
 
-def run_cfg3(torch, lib, L, stream):
-    """Blocked trsm (Left/Lower/NoTrans/NonUnit, 4096^2 float64, A off-diagonal
-    N(0,1)/sqrt(4096), diagonal 4096 + |N(0,1)|, B N(0,1)) and syrk (Lower/NoTrans,
-    N = 8192, K = 2048, float32, A uniform[-1,1)), plain vs split / Ozaki, with the
-    float64-oracle error on sampled columns (trsm) / rows (syrk)."""
+def dtrsm_leg(torch, lib, L, stream, n, g, variants):
+    """Left/Lower/NoTrans/NonUnit dtrsm of order n with n right-hand sides (A off-diagonal
+    N(0,1)/sqrt(n), diagonal n + |N(0,1)|, B N(0,1)): CUDA-event time of each variant
+    (label, mode, slices, refinement steps) and its float64-oracle error on 128 sampled
+    columns of X (scipy's triangular solve)."""
     import scipy.linalg as sl
-    out = {}
-    g = torch.Generator(device="cuda")
-    g.manual_seed(99)
-    n = 4096
     A = torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64) / np.sqrt(n)
     A.diagonal().copy_(n + torch.randn(n, generator=g, device="cuda", dtype=torch.float64).abs())
     B0 = torch.randn((n, n), generator=g, device="cuda", dtype=torch.float64)
     X = torch.empty_like(B0)
     cols = np.random.default_rng(5).choice(n, 128, replace=False)
-    An = A.cpu().numpy().T  # column-major view: An[i, l]
-    L_ = np.tril(An)
-    Bn = B0.cpu().numpy().T
-    Xref = sl.solve_triangular(L_, Bn[:, cols], lower=True)
+    L_ = np.tril(A.cpu().numpy().T)  # column-major view: A[i, l]
+    Xref = sl.solve_triangular(L_, B0.cpu().numpy().T[:, cols], lower=True)
+    del L_
 
     def tcall(md, s_, r_):
         X.copy_(B0)
@@ -177,8 +172,7 @@ def run_cfg3(torch, lib, L, stream):
             raise RuntimeError(f"dtrsm failed {st}: {L.last_error()}")
 
     tr = {}
-    for label, md, s_, r_ in (("plain_fp64", L.MODE_PLAIN, 0, 0), ("ozaki_s7", L.MODE_OZAKI, 7, 0),
-                              ("ozaki_s4_ir1", L.MODE_OZAKI, 4, 1)):
+    for label, md, s_, r_ in variants:
         tcall(md, s_, r_)
         torch.cuda.synchronize()
         got = X.cpu().numpy().T[:, cols]
@@ -192,9 +186,25 @@ def run_cfg3(torch, lib, L, stream):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
         tr[label] = {"tflops": round(n ** 3 / (ms * 1e-3) / 1e12, 2), "ms": round(ms, 3), "fp64_err": err}
-    out["dtrsm_LLNN_4096"] = tr
-    out["dtrsm_note"] = "flops m^2 n; each timed call includes a 128 MiB device copy restoring B"
     del A, B0, X
+    return tr
+
+
+def run_cfg3(torch, lib, L, stream):
+    """Blocked trsm (Left/Lower/NoTrans/NonUnit, 4096^2 float64, A off-diagonal
+    N(0,1)/sqrt(4096), diagonal 4096 + |N(0,1)|, B N(0,1); and the same at order 8192,
+    the size the split forms' 3x target is stated at) and syrk (Lower/NoTrans, N = 8192,
+    K = 2048, float32, A uniform[-1,1)), plain vs split / Ozaki, with the float64-oracle
+    error on sampled columns (trsm) / rows (syrk)."""
+    out = {}
+    g = torch.Generator(device="cuda")
+    g.manual_seed(99)
+    out["dtrsm_LLNN_4096"] = dtrsm_leg(torch, lib, L, stream, 4096, g, (
+        ("plain_fp64", L.MODE_PLAIN, 0, 0), ("ozaki_s7", L.MODE_OZAKI, 7, 0), ("ozaki_s4_ir1", L.MODE_OZAKI, 4, 1)))
+    out["dtrsm_LLNN_8192"] = dtrsm_leg(torch, lib, L, stream, 8192, g, (
+        ("plain_fp64", L.MODE_PLAIN, 0, 0), ("ozaki_s7", L.MODE_OZAKI, 7, 0)))
+    out["dtrsm_note"] = ("flops m^2 n; each timed call includes a device copy restoring B "
+                         "(128 MiB at 4096, 512 MiB at 8192)")
 
     nn, kk = 8192, 2048
     As = torch.rand((kk, nn), generator=g, device="cuda", dtype=torch.float32) * 2 - 1  # column-major n x k
@@ -797,7 +807,7 @@ def run_ours(args, rank, world, dist):
         errs[ta + tb][other] = rows_error(Cm, refs[ta + tb], rs)
 
     # ---- dgemm 4096^3 NN: plain FP64 vs Ozaki ----
-    dg = {}
+    dg, dg8 = {}, {}
     if not args.skip_dgemm:
         Ad = col_major(torch, N_D, N_D, g, "f64", "cuda")
         Bd = col_major(torch, N_D, N_D, g, "f64", "cuda")
@@ -845,6 +855,33 @@ def run_ours(args, rank, world, dist):
             dcall(md, s_)
             torch.cuda.synchronize()
             dg[label]["fp64_err_scaled_rows"] = rows_error(Cd, refd, rsd)
+        del Ad, Bd, Cd
+
+        # the size the split forms' 3x target is stated at: M = N = K = 8192, plain FP64 vs Ozaki s = 7
+        n8 = 2 * N_D
+        Ad = col_major(torch, n8, n8, g, "f64", "cuda")
+        Bd = col_major(torch, n8, n8, g, "f64", "cuda")
+        Cd = torch.empty((n8, n8), dtype=torch.float64, device="cuda")
+        rs8 = np.random.default_rng(10).choice(n8, 128, replace=False)
+        ref8 = ref_rows("N", "N", Ad, Bd, rs8)
+        for label, md, s in (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s7", L.MODE_OZAKI, 7)):
+            def call8():
+                st = lib.mbg_dgemm_ex(md, s, b"N", b"N", n8, n8, n8, 1.0, Ad.data_ptr(), n8, Bd.data_ptr(), n8,
+                                      0.0, Cd.data_ptr(), n8)
+                if st:
+                    raise RuntimeError(f"mbg_dgemm_ex failed: {st} {L.last_error()}")
+            call8()
+            torch.cuda.synchronize()
+            err = rows_error(Cd, ref8, rs8)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(3):
+                call8()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms8 = e0.elapsed_time(e1) / 3
+            dg8[label] = {"tflops": round(2.0 * n8 ** 3 / (ms8 * 1e-3) / 1e12, 2), "ms": round(ms8, 3),
+                          "fp64_err": err}
         del Ad, Bd, Cd
 
     # ---- own peak probes (FMA loops, back-to-back tcgen05.mma) ----
@@ -944,6 +981,7 @@ def run_ours(args, rank, world, dist):
                                          for m_ in ("bf16x3", "bf16x6")},
         "error_metric": f"max|C-C64|/max|C64| over {SAMPLE_ROWS} sampled rows, C64 = float64 numpy",
         "dgemm_4096": dg,
+        "dgemm_8192": dg8,
         "context_vendor_plain_gemm": ctx,
         "probe_peaks": probes,
         "cfg3": cfg3,
