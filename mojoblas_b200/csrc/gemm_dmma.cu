@@ -211,10 +211,10 @@ using Small = DmmaCfg<64, 64, 32, 32>;   // 4 warps
 template <class C, int TRI, int BM, int BN, int VEC>
 int launch_dmma_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha, const double* a, i64 lda,
                   const double* b, i64 ldb, double beta, double* c, i64 ldc, int band) {
-    static unsigned configured = 0;  // one bit per device
+    static std::atomic<unsigned> configured{0};  // one bit per device
     int dev = 0;
     MBG_CUDA(cudaGetDevice(&dev));
-    if (dev >= 32 || !(configured & (1u << dev))) {  // all four transposes, on a device's first call
+    if (!configured_on(configured, dev)) {  // all four transposes, on a device's first call
         MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, false, false, TRI, BM, BN, VEC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
         MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, false, true, TRI, BM, BN, VEC>,
@@ -223,7 +223,7 @@ int launch_dmma_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, double alpha
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
         MBG_CUDA(cudaFuncSetAttribute(gemm_dmma_kernel<C, true, true, TRI, BM, BN, VEC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM));
-        if (dev < 32) configured |= 1u << dev;
+        mark_configured(configured, dev);
     }
     cudaStream_t s = stream();
 #define DM(TA_, TB_) \

@@ -39,10 +39,10 @@ template <int FT, int TRI, bool VA, bool VB>
 int launch_f32_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,
                  const float* b, i64 ldb, float beta, float* c, i64 ldc, int band) {
     constexpr size_t SM = f32_smem<FT>();
-    static unsigned configured = 0;  // one bit per device: more than 48 KB of shared memory needs an opt-in
+    static std::atomic<unsigned> configured{0};  // one bit per device: more than 48 KB of shared memory needs an opt-in
     int dev = 0;
     MBG_CUDA(cudaGetDevice(&dev));
-    if (dev >= 32 || !(configured & (1u << dev))) {
+    if (!configured_on(configured, dev)) {
         MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<FT, false, false, TRI, VA, VB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
         MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<FT, false, true, TRI, VA, VB>,
@@ -51,7 +51,7 @@ int launch_f32_v(bool ta, bool tb, dim3 grid, i64 m, i64 n, i64 k, float alpha, 
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
         MBG_CUDA(cudaFuncSetAttribute(gemm_f32_kernel<FT, true, true, TRI, VA, VB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
-        if (dev < 32) configured |= 1u << dev;
+        mark_configured(configured, dev);
     }
     cudaStream_t s = stream();
 #define F32(TA_, TB_) \

@@ -150,15 +150,13 @@ grouped_block_strsm_kernel(const TrsmDesc* __restrict__ probs, const TrsmItem* _
     }
 }
 
+// SMs of the current device (queried per plan: plans are built once, off the hot path)
 int num_sms() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
-            cudaGetLastError();
-            sms = 148;
-        }
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+        cudaGetLastError();
+        sms = 148;
     }
     return sms;
 }

@@ -544,12 +544,12 @@ template <typename T, bool TRANS>
 int launch_trsv_t(i64 n, const T* a, i64 lda, T* x, i64 incx, bool lower, bool unit, const TrsvSync& sync,
                   i64 nb) {
     constexpr size_t SM = trsv_smem_bytes<T>();
-    static unsigned configured = 0;  // one bit per device: more than 48 KB of shared memory needs an opt-in
+    static std::atomic<unsigned> configured{0};  // one bit per device: more than 48 KB of shared memory needs an opt-in
     int dev = 0;
     MBG_CUDA(cudaGetDevice(&dev));
-    if (dev >= 32 || !(configured & (1u << dev))) {
+    if (!configured_on(configured, dev)) {
         MBG_CUDA(cudaFuncSetAttribute(trsv_kernel<T, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM));
-        if (dev < 32) configured |= 1u << dev;
+        mark_configured(configured, dev);
     }
     trsv_kernel<T, TRANS><<<(unsigned)nb, TV_THREADS, SM, stream()>>>(n, a, lda, x, incx, vec_start(n, incx), lower,
                                                                        unit, sync);

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstddef>
 #include <cstdio>
@@ -22,6 +23,19 @@ inline bool is_r(char t) { return t == 'R' || t == 'r'; }
 inline i64 imax(i64 a, i64 b) { return a > b ? a : b; }
 inline i64 imin(i64 a, i64 b) { return a < b ? a : b; }
 inline i64 cdiv(i64 a, i64 b) { return (a + b - 1) / b; }
+
+// ---- one-time per-device setup ----------------------------------------------
+// Kernel attributes (the dynamic shared-memory opt-in) belong to a device's
+// context, so each kernel is configured once per device, from any host thread:
+// a caller that finds its device's bit clear sets the attribute (setting it
+// twice is harmless) and only then publishes the bit, so no thread launches
+// before the attribute is in place.  Devices 32 and up are configured on every call.
+inline bool configured_on(const std::atomic<unsigned>& mask, int dev) {
+    return dev < 32 && (mask.load(std::memory_order_acquire) & (1u << dev));
+}
+inline void mark_configured(std::atomic<unsigned>& mask, int dev) {
+    if (dev < 32) mask.fetch_or(1u << dev, std::memory_order_release);
+}
 
 // ---- runtime state ----------------------------------------------------------
 cudaStream_t stream();

@@ -1069,11 +1069,13 @@ int make_map(CUtensorMap* map, const void* base, bool int8, i64 Kp, i64 Rp, int 
 
 template <class C>
 int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, Params& P, const char* name) {
-    static bool configured = false;  // per instantiation
-    if (!configured) {
+    static std::atomic<unsigned> configured{0};  // one bit per device
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    if (!configured_on(configured, dev)) {
         MBG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       C::SMEM_BYTES));
-        configured = true;
+        mark_configured(configured, dev);
     }
     P.err = device_error_flag();
     const i64 tiles = i64(P.tiles_m) * P.tiles_n;
@@ -1214,10 +1216,12 @@ namespace tc {
 template <class C>
 int launch_ozaki(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mal, const CUtensorMap& mbl,
                  OzParams& P) {
-    static bool configured = false;  // per instantiation
-    if (!configured) {
+    static std::atomic<unsigned> configured{0};  // one bit per device
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    if (!configured_on(configured, dev)) {
         MBG_CUDA(cudaFuncSetAttribute(ozaki_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
-        configured = true;
+        mark_configured(configured, dev);
     }
     P.err = device_error_flag();
     const i64 tiles = i64(P.tiles_m) * P.tiles_n;

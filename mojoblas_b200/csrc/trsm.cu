@@ -210,13 +210,13 @@ constexpr int bs_max_rows() { return sizeof(T) == 8 ? 512 : 1024; }
 template <typename T, bool L, bool TR, bool U>
 int launch_block_solve_t(int nb, i64 n, const T* a, i64 lda, T* b, i64 ldb) {
     auto kern = block_solve_kernel<T, L, TR, U, BS_COLS>;
-    static unsigned configured = 0;  // one bit per device
+    static std::atomic<unsigned> configured{0};  // one bit per device
     int dev = 0;
     MBG_CUDA(cudaGetDevice(&dev));
-    if (dev < 32 && !(configured & (1u << dev))) {
+    if (!configured_on(configured, dev)) {
         MBG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)bs_smem_bytes<T>(bs_max_rows<T>())));
-        configured |= 1u << dev;
+        mark_configured(configured, dev);
     }
     const i64 strips = cdiv(n, BS_COLS);
     kern<<<(unsigned)imin(strips, 1 << 20), BS_THREADS, bs_smem_bytes<T>(nb), stream()>>>(nb, n, a, lda, b, ldb);
