@@ -144,6 +144,17 @@ def ref_rows(ta, tb, a, b, rows):
     return opA[rows, :] @ opB
 
 
+def compensated_rows(a, b, count, seed):
+    """`count` sampled rows of A B (NN, column-major float64 device tensors) from the
+    oracle's compensated dot products: accurate to about 2^-106, so a float64 GEMM's own
+    rounding error shows against it (a float64 numpy product has errors of that size)."""
+    import oracle as orc
+    n = a.shape[0]
+    rows = np.sort(np.random.default_rng(seed).choice(n, count, replace=False))
+    A, B = a.cpu().numpy().T, b.cpu().numpy().T  # column-major (n x n) views
+    return orc.gemm_rows_dot2("N", "N", n, n, A, n, B, n, rows), rows
+
+
 def rows_error(c, ref, rows):
     """max|C - C64| / max|C64| on the sampled rows."""
     got = c.double().cpu().numpy().T[rows, :]
@@ -814,6 +825,7 @@ def run_ours(args, rank, world, dist):
         Cd = torch.empty((N_D, N_D), dtype=torch.float64, device="cuda")
         rsd = np.random.default_rng(8).choice(N_D, SAMPLE_ROWS, replace=False)
         refd = ref_rows("N", "N", Ad, Bd, rsd)
+        refc, rsc = compensated_rows(Ad, Bd, 32, 11)
 
         def dcall(md, s):
             st = lib.mbg_dgemm_ex(md, s, b"N", b"N", N_D, N_D, N_D, 1.0, Ad.data_ptr(), N_D, Bd.data_ptr(), N_D,
@@ -835,7 +847,8 @@ def run_ours(args, rank, world, dist):
             torch.cuda.synchronize()
             dms = e0.elapsed_time(e1) / reps
             dg[label] = {"tflops": round(FLOPS_D / (dms * 1e-3) / 1e12, 2), "ms": round(dms, 3),
-                         "fp64_err": rows_error(Cd, refd, rsd)}
+                         "fp64_err": rows_error(Cd, refd, rsd),
+                         "err_vs_compensated": rows_error(Cd, refc, rsc)}
             if md == L.MODE_OZAKI:  # kernel-only time (CUDA events around the tcgen05 launch)
                 lib.mbg_prof_enable(1)
                 lib.mbg_prof_reset()
@@ -864,6 +877,7 @@ def run_ours(args, rank, world, dist):
         Cd = torch.empty((n8, n8), dtype=torch.float64, device="cuda")
         rs8 = np.random.default_rng(10).choice(n8, 128, replace=False)
         ref8 = ref_rows("N", "N", Ad, Bd, rs8)
+        refc8, rsc8 = compensated_rows(Ad, Bd, 32, 12)
         for label, md, s in (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s7", L.MODE_OZAKI, 7)):
             def call8():
                 st = lib.mbg_dgemm_ex(md, s, b"N", b"N", n8, n8, n8, 1.0, Ad.data_ptr(), n8, Bd.data_ptr(), n8,
@@ -881,7 +895,7 @@ def run_ours(args, rank, world, dist):
             torch.cuda.synchronize()
             ms8 = e0.elapsed_time(e1) / 3
             dg8[label] = {"tflops": round(2.0 * n8 ** 3 / (ms8 * 1e-3) / 1e12, 2), "ms": round(ms8, 3),
-                          "fp64_err": err}
+                          "fp64_err": err, "err_vs_compensated": rows_error(Cd, refc8, rsc8)}
         del Ad, Bd, Cd
 
     # ---- own peak probes (FMA loops, back-to-back tcgen05.mma) ----

@@ -67,6 +67,9 @@ def lib():
             fn = getattr(_lib, name)
             fn.argtypes = argtypes
             fn.restype = C.c_int
+        _lib.orc_dgemm_dot2_rows.argtypes = [ch, ch, i64, i64, f64p, i64, f64p, i64, C.POINTER(C.c_int64), i64,
+                                             f64p]
+        _lib.orc_dgemm_dot2_rows.restype = C.c_int
         _lib.orc_set_threads.argtypes = [C.c_int]
         _lib.orc_max_threads.restype = C.c_int
     return _lib
@@ -273,6 +276,19 @@ def trmm_f64(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb) -> np.ndarray:
     opA = op(tri(view(a, na, na, lda).astype(np.float64), uplo, diag), ta)
     B = view(b, m, n, ldb).astype(np.float64)
     return float(alpha) * (opA @ B if _c(side) in (b"L", b"l") else B @ opA)
+
+
+def gemm_rows_dot2(ta, tb, n, k, a, lda, b, ldb, rows) -> np.ndarray:
+    """Rows `rows` of op(A) op(B) (float64 inputs, shape (len(rows), n)), every element a
+    compensated dot product (dot2.cpp): as accurate as a twice-working-precision sum,
+    so a float64 GEMM's own rounding error shows against it."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    out = np.empty((len(rows), n), dtype=np.float64, order="F")
+    lib().orc_dgemm_dot2_rows(_c(ta), _c(tb), n, k, _p(a, np.float64), lda, _p(b, np.float64), ldb,
+                              rows.ctypes.data_as(C.POINTER(C.c_int64)), len(rows), _p(out, np.float64))
+    return out
 
 
 def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:
