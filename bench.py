@@ -1027,7 +1027,7 @@ def run_ours(args, rank, world, dist):
 _CPU_DATA = {}
 
 
-def run_cpu_baseline(args, threads=None, rows=N_S, calls=("NT", "TN")):
+def run_cpu_baseline(args, threads=None, rows=None, calls=("NT", "TN")):
     """Reference algorithm (oracle restatement of _gemm_naive NT/TN) on host cores,
     over a bounded sample of each 8192^3 call in `calls`: rows 0..rows-1 of one
     column of C per thread (the reference parallelises over columns).  Only
@@ -1037,6 +1037,7 @@ def run_cpu_baseline(args, threads=None, rows=N_S, calls=("NT", "TN")):
     nth = threads or os.cpu_count() or 1
     orc.set_threads(nth)
     n = N_S
+    rows = n if rows is None else min(rows, n)
     if "ab" not in _CPU_DATA:
         rng = np.random.default_rng(1234)
         _CPU_DATA["ab"] = (np.asfortranarray(rng.uniform(-1, 1, (n, n)).astype(np.float32)),
@@ -1054,8 +1055,8 @@ def run_cpu_baseline(args, threads=None, rows=N_S, calls=("NT", "TN")):
     secs = sum(sample(cl[0], cl[1]) for cl in calls)
     flops = 2.0 * rows * n * cols * len(calls)
     return {"value": flops / secs / 1e12, "unit": "TFLOP/s", "cores": nth, "kind": "port",
-            "sample": f"rows 0..{rows - 1} x columns 0..{cols - 1} of C for {' and '.join(calls)} 8192^3 "
-                      f"(2*{rows}*8192*{cols} flop each), float32, mojoBLAS _gemm_naive restated "
+            "sample": f"rows 0..{rows - 1} x columns 0..{cols - 1} of C for {' and '.join(calls)} {n}^3 "
+                      f"(2*{rows}*{n}*{cols} flop each), float32, mojoBLAS _gemm_naive restated "
                       f"(oracle/ref_level3.cpp), OpenMP {nth} threads",
             "seconds": round(secs, 3), "flops": flops}
 
@@ -1123,7 +1124,7 @@ def main():
         # the NT call (even steps) or the TN call (odd steps), about 8 s with 16 threads, so K steps
         # plus W short warm-up samples stay within a few minutes
         for _ in range(args.warmup):
-            run_cpu_baseline(args, rows=512)
+            run_cpu_baseline(args, rows=min(512, N_S))
         flops = secs = 0.0
         info = None
         for i in range(args.steps):
@@ -1132,8 +1133,8 @@ def main():
             secs += info["seconds"]
         v = flops / secs / 1e12
         cols = max(info["cores"], 8)
-        info.update(sample=f"per step: rows 0..8191 x columns 0..{cols - 1} of C of the NT (even steps) or TN "
-                           f"(odd steps) 8192^3 call (2*8192*8192*{cols} flop), float32, mojoBLAS _gemm_naive "
+        info.update(sample=f"per step: rows 0..{N_S - 1} x columns 0..{cols - 1} of C of the NT (even steps) or TN "
+                           f"(odd steps) {N_S}^3 call (2*{N_S}*{N_S}*{cols} flop), float32, mojoBLAS _gemm_naive "
                            f"restated (oracle/ref_level3.cpp), OpenMP {info['cores']} threads",
                     seconds=round(secs, 2), flops=flops)
         line = {"impl": "reference", "metric": "TFLOP/s at fixed FP64-oracle error (split-precision tensor-core "
