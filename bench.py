@@ -1130,7 +1130,7 @@ def main():
         for i in range(args.steps):
             info = run_cpu_baseline(args, calls=("NT",) if i % 2 == 0 else ("TN",))
             flops += info["flops"]
-            secs += info["seconds"]
+            secs += info["flops"] / (info["value"] * 1e12)  # the step's time, unrounded
         v = flops / secs / 1e12
         cols = max(info["cores"], 8)
         info.update(sample=f"per step: rows 0..{N_S - 1} x columns 0..{cols - 1} of C of the NT (even steps) or TN "
