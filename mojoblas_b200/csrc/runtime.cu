@@ -3,8 +3,10 @@
 #include "mbg_internal.cuh"
 
 #include <atomic>
+#include <cctype>
 #include <map>
 #include <mutex>
+#include <sstream>
 #include <vector>
 #include <cstring>
 #include <cstdlib>
@@ -348,7 +350,12 @@ int64_t mbg_get_tuning(const char* key) {
     return -1;
 }
 
-// Reads "key value" pairs: plain lines, or a flat JSON object {"key": value, ...}.
+// Reads the tuning file: either plain "key value" lines ('#' starts a comment), or
+// a JSON object whose top-level members with integer values are applied; string,
+// boolean, non-integral and nested (object / array) values are skipped, so a
+// file may carry its measurements and a device name beside the keys.  Unknown
+// keys and out-of-range values are ignored.  MBG_OK when at least one key was
+// applied.
 int mbg_load_tuning(const char* path) {
     FILE* f = path ? std::fopen(path, "r") : nullptr;
     if (!f) {
@@ -360,23 +367,75 @@ int mbg_load_tuning(const char* path) {
     size_t got;
     while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
     std::fclose(f);
-    for (char& ch : text)
-        if (ch == '{' || ch == '}' || ch == ',' || ch == ':' || ch == '"' || ch == '\n' || ch == '\r' || ch == '\t')
-            ch = ' ';
-    size_t pos = 0;
     int applied = 0;
-    auto next = [&](std::string& tok) {
-        while (pos < text.size() && text[pos] == ' ') ++pos;
-        size_t st = pos;
-        while (pos < text.size() && text[pos] != ' ') ++pos;
-        tok = text.substr(st, pos - st);
-        return !tok.empty();
-    };
-    std::string key, val;
-    while (next(key) && next(val)) {
+    auto apply = [&](const std::string& key, const char* num) {
         char* end = nullptr;
-        const long long v = std::strtoll(val.c_str(), &end, 10);
-        if (end && *end == '\0' && mbg_set_tuning(key.c_str(), v) == MBG_OK) ++applied;
+        const long long v = std::strtoll(num, &end, 10);
+        const bool integral = end != num && !(*end == '.' || *end == 'e' || *end == 'E');
+        if (integral && mbg_set_tuning(key.c_str(), v) == MBG_OK) ++applied;
+        return end;
+    };
+    const size_t first = text.find_first_not_of(" \t\r\n");
+    if (first != std::string::npos && text[first] == '{') {
+        int depth = 0;
+        std::string key;
+        bool want_value = false;  // after "key": at depth 1
+        for (size_t i = first; i < text.size(); ++i) {
+            const char c = text[i];
+            if (c == '"') {  // a string: a key, or a value to skip
+                std::string str;
+                size_t j = i + 1;
+                for (; j < text.size() && text[j] != '"'; ++j) {
+                    if (text[j] == '\\' && j + 1 < text.size()) ++j;
+                    str += text[j];
+                }
+                i = j;
+                if (depth == 1) {
+                    if (want_value) key.clear();
+                    else key = str;
+                    want_value = false;
+                }
+            } else if (c == '{' || c == '[') {
+                if (depth == 1 && want_value) {  // a nested value: skipped with its contents
+                    key.clear();
+                    want_value = false;
+                }
+                ++depth;
+            } else if (c == '}' || c == ']') {
+                --depth;
+            } else if (depth != 1) {
+                continue;
+            } else if (c == ':') {
+                want_value = !key.empty();
+            } else if (c == ',') {
+                key.clear();
+                want_value = false;
+            } else if (want_value && (c == '-' || std::isdigit((unsigned char)c))) {
+                const char* end = apply(key, text.c_str() + i);
+                while (*end && (std::isalnum((unsigned char)*end) || *end == '.' || *end == '+' || *end == '-'))
+                    ++end;  // the rest of a non-integral number
+                i = size_t(end - text.c_str()) - 1;
+                key.clear();
+                want_value = false;
+            } else if (want_value && std::isalpha((unsigned char)c)) {  // true / false / null
+                while (i + 1 < text.size() && std::isalpha((unsigned char)text[i + 1])) ++i;
+                key.clear();
+                want_value = false;
+            }
+        }
+    } else {
+        std::istringstream in(text);
+        std::string line;
+        while (std::getline(in, line)) {
+            const size_t hash = line.find('#');
+            if (hash != std::string::npos) line.resize(hash);
+            std::istringstream ls(line);
+            std::string k, v;
+            if (!(ls >> k >> v)) continue;
+            char* end = nullptr;
+            const long long val = std::strtoll(v.c_str(), &end, 10);
+            if (end != v.c_str() && *end == '\0' && mbg_set_tuning(k.c_str(), val) == MBG_OK) ++applied;
+        }
     }
     return applied > 0 ? MBG_OK : MBG_ERR_INVALID_MODE;
 }
