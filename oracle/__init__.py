@@ -291,6 +291,54 @@ def gemm_rows_dot2(ta, tb, n, k, a, lda, b, ldb, rows) -> np.ndarray:
     return out
 
 
+def ozaki_gemm_emulated(ta, tb, m, n, k, alpha, a, lda, b, ldb, slices) -> np.ndarray:
+    """The library's Ozaki dgemm (beta = 0) restated step by step on the CPU, as the
+    checker for bit-for-bit comparisons with the GPU result:
+
+    1. e = frexp exponent of the largest magnitude of each row of op(A) and each
+       column of op(B) (0 for an all-zero row or column): every value is below 2^e;
+    2. G = trunc(x 2^(8s - 2 - e)) (exact: x keeps its 53-bit significand);
+    3. G's signed base-256 digits, most significant first, from the bytes of
+       G + 0x80...80 (s bytes, modulo 2^64), each XOR 0x80 read as int8;
+    4. for each diagonal d = p + q < s the exact integer product
+       D_d = sum_{p+q=d} A_p B_q (int32 on the GPU, exact within its k chunk);
+    5. acc = sum of D_d 2^(-8d-12) in fp64 from d = s-1 down to 0 (each product is
+       exact, so this is the kernel's fused multiply-add order), and
+       C = alpha (acc 2^(e_row + e_col)).
+    For k within one exact chunk (k <= 18720 at 7 slices) and no overflow or
+    underflow in the scalings.  Returns C (m x n, float64)."""
+    A = op(view(np.asarray(a, np.float64), *((m, k) if _c(ta) in (b"N", b"n") else (k, m)), lda), ta)
+    Bm = op(view(np.asarray(b, np.float64), *((k, n) if _c(tb) in (b"N", b"n") else (n, k)), ldb), tb)
+    s = int(slices)
+    nbits = 8 * s - 2
+
+    def exponents(x, axis):
+        mx = np.max(np.abs(x), axis=axis) if x.size else np.zeros(x.shape[1 - axis])
+        e = np.frexp(mx)[1].astype(np.int64)
+        return np.where(mx > 0, e, 0)
+
+    def digits(x, e):
+        G = np.trunc(np.ldexp(x, (nbits - e).astype(np.int32))).astype(np.int64)
+        bias = np.uint64(0x8080808080808080 >> (64 - 8 * s))
+        H = G.astype(np.uint64) + bias  # modulo 2^64
+        out = []
+        for p in range(s):
+            byte = ((H >> np.uint64(8 * (s - 1 - p))) & np.uint64(255)) ^ np.uint64(0x80)
+            out.append(byte.astype(np.uint8).view(np.int8).astype(np.int64))
+        return out
+
+    er, ec = exponents(A, 1), exponents(Bm, 0)
+    # digit products in float64: every partial sum is an integer below k 128^2 s < 2^53, so the
+    # BLAS product is exact in any summation order (and equals the GPU's int32 sums)
+    dA = [x.astype(np.float64) for x in digits(A, er[:, None])]
+    dB = [x.astype(np.float64) for x in digits(Bm, ec[None, :])]
+    acc = np.zeros((m, n))
+    for d in range(s - 1, -1, -1):
+        D = sum(dA[p] @ dB[d - p] for p in range(d + 1))
+        acc = acc + D * 2.0 ** (-8 * d - 12)
+    return alpha * np.ldexp(acc, (er[:, None] + ec[None, :]).astype(np.int32))
+
+
 def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:
     """max|x - ref| / max|ref| (normwise, the error metric quoted with every result)."""
     den = float(np.max(np.abs(ref)))
