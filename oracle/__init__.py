@@ -291,22 +291,30 @@ def gemm_rows_dot2(ta, tb, n, k, a, lda, b, ldb, rows) -> np.ndarray:
     return out
 
 
-def ozaki_gemm_emulated(ta, tb, m, n, k, alpha, a, lda, b, ldb, slices) -> np.ndarray:
-    """The library's Ozaki dgemm (beta = 0) restated step by step on the CPU, as the
-    checker for bit-for-bit comparisons with the GPU result:
+def ozaki_max_k(slices: int) -> int:
+    """The longest k one Ozaki launch keeps exact in int32: s pairs of digits of magnitude
+    at most 128 per k step, rounded down to the 32-byte k slab."""
+    return ((2 ** 31 - 1) // (int(slices) * 128 * 128)) // 32 * 32
+
+
+def ozaki_gemm_emulated(ta, tb, m, n, k, alpha, a, lda, b, ldb, slices, beta=0.0, c=None, ldc=None) -> np.ndarray:
+    """The library's Ozaki dgemm restated step by step on the CPU, as the checker for
+    bit-for-bit comparisons with the GPU result.  For each k chunk of at most
+    ozaki_max_k(s) columns (one GPU launch each):
 
     1. e = frexp exponent of the largest magnitude of each row of op(A) and each
-       column of op(B) (0 for an all-zero row or column): every value is below 2^e;
+       column of op(B) within the chunk (0 for an all-zero one): every value is below 2^e;
     2. G = trunc(x 2^(8s - 2 - e)) (exact: x keeps its 53-bit significand);
     3. G's signed base-256 digits, most significant first, from the bytes of
        G + 0x80...80 (s bytes, modulo 2^64), each XOR 0x80 read as int8;
     4. for each diagonal d = p + q < s the exact integer product
-       D_d = sum_{p+q=d} A_p B_q (int32 on the GPU, exact within its k chunk);
+       D_d = sum_{p+q=d} A_p B_q (int32 on the GPU, exact within the chunk);
     5. acc = sum of D_d 2^(-8d-12) in fp64 from d = s-1 down to 0 (each product is
-       exact, so this is the kernel's fused multiply-add order), and
-       C = alpha (acc 2^(e_row + e_col)).
-    For k within one exact chunk (k <= 18720 at 7 slices) and no overflow or
-    underflow in the scalings.  Returns C (m x n, float64)."""
+       exact, so this is the kernel's fused multiply-add order), v = alpha (acc 2^(e_row + e_col)).
+    The first chunk writes v (beta = 0) or C + v (beta = 1, the GPU's L2 reduction); each
+    later chunk adds its v with one rounding.  beta must be 0 or 1 (c and ldc given for 1),
+    and the scalings must neither overflow nor underflow.  Returns C (m x n, float64)."""
+    assert beta in (0.0, 1.0)
     A = op(view(np.asarray(a, np.float64), *((m, k) if _c(ta) in (b"N", b"n") else (k, m)), lda), ta)
     Bm = op(view(np.asarray(b, np.float64), *((k, n) if _c(tb) in (b"N", b"n") else (n, k)), ldb), tb)
     s = int(slices)
@@ -324,19 +332,24 @@ def ozaki_gemm_emulated(ta, tb, m, n, k, alpha, a, lda, b, ldb, slices) -> np.nd
         out = []
         for p in range(s):
             byte = ((H >> np.uint64(8 * (s - 1 - p))) & np.uint64(255)) ^ np.uint64(0x80)
-            out.append(byte.astype(np.uint8).view(np.int8).astype(np.int64))
+            out.append(byte.astype(np.uint8).view(np.int8).astype(np.float64))
         return out
 
-    er, ec = exponents(A, 1), exponents(Bm, 0)
-    # digit products in float64: every partial sum is an integer below k 128^2 s < 2^53, so the
-    # BLAS product is exact in any summation order (and equals the GPU's int32 sums)
-    dA = [x.astype(np.float64) for x in digits(A, er[:, None])]
-    dB = [x.astype(np.float64) for x in digits(Bm, ec[None, :])]
-    acc = np.zeros((m, n))
-    for d in range(s - 1, -1, -1):
-        D = sum(dA[p] @ dB[d - p] for p in range(d + 1))
-        acc = acc + D * 2.0 ** (-8 * d - 12)
-    return alpha * np.ldexp(acc, (er[:, None] + ec[None, :]).astype(np.int32))
+    out = np.array(view(np.asarray(c, np.float64), m, n, ldc), dtype=np.float64) if beta == 1.0 else None
+    kc = min(k, ozaki_max_k(s))
+    for k0 in range(0, k, kc):
+        Ak, Bk = A[:, k0:k0 + kc], Bm[k0:k0 + kc, :]
+        er, ec = exponents(Ak, 1), exponents(Bk, 0)
+        # digit products in float64: every partial sum is an integer below k 128^2 s < 2^53, so the
+        # BLAS product is exact in any summation order (and equals the GPU's int32 sums)
+        dA, dB = digits(Ak, er[:, None]), digits(Bk, ec[None, :])
+        acc = np.zeros((m, n))
+        for d in range(s - 1, -1, -1):
+            D = sum(dA[p] @ dB[d - p] for p in range(d + 1))
+            acc = acc + D * 2.0 ** (-8 * d - 12)
+        v = alpha * np.ldexp(acc, (er[:, None] + ec[None, :]).astype(np.int32))
+        out = v if out is None else out + v
+    return out
 
 
 def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:

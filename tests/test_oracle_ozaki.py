@@ -7,7 +7,9 @@ references on the CPU:
 * against compensated (Dot2) products, the error falls by about 2^-8 per added
   slice and stays within the truncation bound: each operand keeps 8s - 2 bits
   of its row's (column's) scale, so |error| <= 2 k 2^-(8s-2) max|A| max|B|
-  per element, relative to max|C|.
+  per element, relative to max|C|;
+* k beyond one exact int32 chunk (each chunk with its own exponents, added to C
+  one at a time) and beta = 1 stay at float64 rounding.
 """
 import numpy as np
 import pytest
@@ -51,3 +53,20 @@ def test_error_per_slice(oracle):
     for s in range(2, 7):  # about 2^-8 per slice until the fp64 epilogue's own rounding is reached
         assert errs[s - 1] < errs[s - 2] / 64, errs
     assert errs[-2] < 2 * 2.0 ** -53 and errs[-1] < 2 * 2.0 ** -53  # 7 and 8 slices: at fp64 rounding
+
+
+def test_chunked_k_and_beta_one(oracle):
+    """k over two chunk boundaries (8 slices: chunks of ozaki_max_k(8) = 16352), each chunk with its
+    own exponents, added to C one chunk at a time; beta = 1 adds to C's values."""
+    assert oracle.ozaki_max_k(8) == 16352 and oracle.ozaki_max_k(7) == 18720
+    rng = np.random.default_rng(63)
+    m, n, k = 16, 12, 2 * 16352 + 100
+    a = np.asfortranarray(rng.uniform(-1, 1, (k, m)))  # op(A) = A^T, k-contiguous
+    b = np.asfortranarray(rng.uniform(-1, 1, (k, n)))
+    a[20000:, :] *= 2.0 ** 12  # k from 20000 on (part of the second chunk, all of the third) at another scale
+    c = np.asfortranarray(rng.uniform(-1, 1, (m + 1, n)))
+    ref = oracle.gemm_rows_dot2("T", "N", n, k, a, k, b, k, np.arange(m))
+    got0 = oracle.ozaki_gemm_emulated("T", "N", m, n, k, 1.0, a, k, b, k, 8)
+    assert oracle.max_rel_err(got0, ref) < 4 * 2.0 ** -53
+    got1 = oracle.ozaki_gemm_emulated("T", "N", m, n, k, 1.0, a, k, b, k, 8, beta=1.0, c=c, ldc=m + 1)
+    assert oracle.max_rel_err(got1, ref + c[:m]) < 4 * 2.0 ** -53
