@@ -352,6 +352,17 @@ def ozaki_gemm_emulated(ta, tb, m, n, k, alpha, a, lda, b, ldb, slices, beta=0.0
     return out
 
 
+def ozaki_syrk_emulated(uplo, trans, n, k, alpha, a, lda, slices) -> np.ndarray:
+    """The library's Ozaki dsyrk (beta = 0) restated: one set of planes and exponents
+    serves op(A) and op(A)^T, so the stored triangle is the Ozaki product of
+    op(A) op(A)^T as ozaki_gemm_emulated forms it; the other triangle is NaN (not
+    written).  Returns n x n float64."""
+    t = "N" if _c(trans) in (b"N", b"n") else "T"
+    full = ozaki_gemm_emulated(t, "T" if t == "N" else "N", n, n, k, alpha, a, lda, a, lda, slices)
+    keep = np.tril(np.ones((n, n), bool)) if _c(uplo) in (b"L", b"l") else np.triu(np.ones((n, n), bool))
+    return np.where(keep, full, np.nan)
+
+
 def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:
     """max|x - ref| / max|ref| (normwise, the error metric quoted with every result)."""
     den = float(np.max(np.abs(ref)))

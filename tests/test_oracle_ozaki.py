@@ -70,3 +70,22 @@ def test_chunked_k_and_beta_one(oracle):
     assert oracle.max_rel_err(got0, ref) < 4 * 2.0 ** -53
     got1 = oracle.ozaki_gemm_emulated("T", "N", m, n, k, 1.0, a, k, b, k, 8, beta=1.0, c=c, ldc=m + 1)
     assert oracle.max_rel_err(got1, ref + c[:m]) < 4 * 2.0 ** -53
+
+
+@pytest.mark.parametrize("uplo,trans", [("L", "N"), ("U", "T")])
+def test_syrk_restatement(oracle, uplo, trans):
+    """The dsyrk restatement: the stored triangle of alpha op(A) op(A)^T at float64 accuracy, the
+    other triangle left unwritten (NaN), symmetric entries bit-identical (one set of planes)."""
+    rng = np.random.default_rng(64)
+    n, k = 45, 70
+    a = np.asfortranarray(rng.uniform(-1, 1, ((n if trans == "N" else k) + 1, k if trans == "N" else n)))
+    lda = a.shape[0]
+    got = oracle.ozaki_syrk_emulated(uplo, trans, n, k, 0.5, a, lda, 7)
+    A = oracle.op(oracle.view(a, *((n, k) if trans == "N" else (k, n)), lda), trans)
+    ref = 0.5 * A @ A.T
+    keep = np.tril(np.ones((n, n), bool)) if uplo == "L" else np.triu(np.ones((n, n), bool))
+    assert np.all(np.isnan(got[~keep]))
+    assert np.max(np.abs(got[keep] - ref[keep])) / np.max(np.abs(ref)) < 4e-15
+    full = oracle.ozaki_gemm_emulated("N" if trans == "N" else "T", "T" if trans == "N" else "N", n, n, k, 0.5,
+                                      a, lda, a, lda, 7)
+    assert np.array_equal(full, full.T)  # the same planes on both sides: an exactly symmetric product
