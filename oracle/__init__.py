@@ -70,6 +70,8 @@ def lib():
         _lib.orc_dgemm_dot2_rows.argtypes = [ch, ch, i64, i64, f64p, i64, f64p, i64, C.POINTER(C.c_int64), i64,
                                              f64p]
         _lib.orc_dgemm_dot2_rows.restype = C.c_int
+        _lib.orc_fma.argtypes = [i64, f64p, f64p, f64p, f64p]
+        _lib.orc_fma.restype = C.c_int
         _lib.orc_set_threads.argtypes = [C.c_int]
         _lib.orc_max_threads.restype = C.c_int
     return _lib
@@ -361,6 +363,40 @@ def ozaki_syrk_emulated(uplo, trans, n, k, alpha, a, lda, slices) -> np.ndarray:
     full = ozaki_gemm_emulated(t, "T" if t == "N" else "N", n, n, k, alpha, a, lda, a, lda, slices)
     keep = np.tril(np.ones((n, n), bool)) if _c(uplo) in (b"L", b"l") else np.triu(np.ones((n, n), bool))
     return np.where(keep, full, np.nan)
+
+
+def fma(x, y, z) -> np.ndarray:
+    """x y + z element-wise with one rounding (broadcast, float64)."""
+    x, y, z = np.broadcast_arrays(*(np.asarray(v, np.float64) for v in (x, y, z)))
+    shape = x.shape
+    x, y, z = (np.ascontiguousarray(v).reshape(-1) for v in (x, y, z))
+    out = np.empty(x.size)
+    lib().orc_fma(x.size, _p(x, np.float64), _p(y, np.float64), _p(z, np.float64), _p(out, np.float64))
+    return out.reshape(shape)
+
+
+def ozaki_trmm_emulated(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb, slices) -> np.ndarray:
+    """The library's Ozaki dtrmm (in place, triangle order within one exact chunk) restated:
+    the strict triangle of op(A) goes through the Ozaki product (its exponents from the
+    kept entries only), and the diagonal term is added with one fused multiply-add,
+        B := fma(d, B_old, alpha (strict(op(A)) B))   (side 'L', d per row),
+        B := fma(d, B_old, alpha (B strict(op(A))))   (side 'R', d per column),
+    with d = alpha A(i, i) (alpha for a unit diagonal).  Returns m x n float64."""
+    left = _c(side) in (b"L", b"l")
+    trans = _c(ta) not in (b"N", b"n")
+    lower = (_c(uplo) in (b"L", b"l")) != trans  # op(A) lower triangular
+    na = m if left else n
+    assert na <= ozaki_max_k(slices)
+    Av = view(np.asarray(a, np.float64), na, na, lda)
+    opA = Av.T if trans else Av
+    strict = np.asfortranarray(np.tril(opA, -1) if lower else np.triu(opA, 1))
+    d = np.full(na, float(alpha)) if _c(diag) in (b"U", b"u") else alpha * np.diagonal(Av)
+    B = np.asfortranarray(view(np.asarray(b, np.float64), m, n, ldb))
+    if left:
+        v = ozaki_gemm_emulated("N", "N", m, n, m, alpha, strict, na, B, m, slices)
+        return fma(d[:, None], B, v)
+    v = ozaki_gemm_emulated("N", "N", m, n, n, alpha, B, m, strict, na, slices)
+    return fma(d[None, :], B, v)
 
 
 def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:

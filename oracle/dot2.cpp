@@ -12,6 +12,9 @@
 // error (about sqrt(k) u relative at k = 4096) is therefore visible against it,
 // which a float64 numpy reference cannot show.
 //
+// Also an element-wise fused multiply-add (x y + z with one rounding, C++'s
+// std::fma), which numpy lacks, for restating epilogues that use one.
+//
 // Nothing in the shipped library links, loads or calls this file; it is built
 // into the oracle's shared object beside the reference restatements.
 
@@ -62,6 +65,12 @@ int orc_dgemm_dot2_rows(char ta, char tb, i64 n, i64 k, const double* a, i64 lda
             out[r + j * nrows] = s + c;
         }
     }
+    return 0;
+}
+
+// out[i] = fma(x[i], y[i], z[i]): x y + z rounded once.
+int orc_fma(i64 n, const double* x, const double* y, const double* z, double* out) {
+    for (i64 i = 0; i < n; ++i) out[i] = std::fma(x[i], y[i], z[i]);
     return 0;
 }
 

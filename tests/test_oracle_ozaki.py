@@ -9,7 +9,11 @@ references on the CPU:
   of its row's (column's) scale, so |error| <= 2 k 2^-(8s-2) max|A| max|B|
   per element, relative to max|C|;
 * k beyond one exact int32 chunk (each chunk with its own exponents, added to C
-  one at a time) and beta = 1 stay at float64 rounding.
+  one at a time) and beta = 1 stay at float64 rounding;
+* the dsyrk restatement (one set of planes: an exactly symmetric product) and the
+  in-place dtrmm restatement (strict triangle through the slices, the diagonal
+  term by one fused multiply-add, oracle.fma) agree with float64, and never read
+  the triangle's other half.
 """
 import numpy as np
 import pytest
@@ -89,3 +93,36 @@ def test_syrk_restatement(oracle, uplo, trans):
     full = oracle.ozaki_gemm_emulated("N" if trans == "N" else "T", "T" if trans == "N" else "N", n, n, k, 0.5,
                                       a, lda, a, lda, 7)
     assert np.array_equal(full, full.T)  # the same planes on both sides: an exactly symmetric product
+
+
+def test_fma_rounds_once(oracle):
+    x = 1.0 + 2.0 ** -30
+    p = x * x  # 1 + 2^-29 + 2^-60 rounds to 1 + 2^-29
+    assert oracle.fma(x, x, -p) == 2.0 ** -60
+    assert np.array_equal(oracle.fma(np.array([2.0, 3.0]), 0.5, 1.0), np.array([2.0, 2.5]))
+
+
+@pytest.mark.parametrize("side", ["L", "R"])
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("ta", ["N", "T"])
+@pytest.mark.parametrize("diag", ["N", "U"])
+def test_trmm_restatement(oracle, side, uplo, ta, diag):
+    """The dtrmm restatement against float64, for every side / uplo / trans / diag; the
+    triangle's other half and (for a unit diagonal) the diagonal are never read (NaN)."""
+    rng = np.random.default_rng(65)
+    m, n = 40, 33
+    na = m if side == "L" else n
+    a = rng.standard_normal((na + 1, na)) / np.sqrt(na)
+    a[np.arange(na), np.arange(na)] = na + np.abs(rng.standard_normal(na))  # a dominant diagonal
+    other = np.triu(np.ones((na, na), bool), 1) if uplo == "L" else np.tril(np.ones((na, na), bool), -1)
+    if diag == "U":
+        other |= np.eye(na, dtype=bool)
+    a_nan = a.copy()
+    a_nan[:na][other] = np.nan
+    a, a_nan = np.asfortranarray(a), np.asfortranarray(a_nan)
+    b = np.asfortranarray(rng.uniform(-1, 1, (m + 2, n)))
+    ref = oracle.trmm_f64(side, uplo, ta, diag, m, n, 1.5, a, na + 1, b, m + 2)
+    got = oracle.ozaki_trmm_emulated(side, uplo, ta, diag, m, n, 1.5, a_nan, na + 1, b, m + 2, 7)
+    assert np.all(np.isfinite(got))
+    # the float64 reference rounds too (about sqrt(na) units of 2^-53): the float64 tolerance of the parity tests
+    assert oracle.max_rel_err(got, ref) < 4e-16 * np.sqrt(max(na, 16))
