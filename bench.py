@@ -1021,18 +1021,55 @@ def run_ours(args, rank, world, dist):
                      "split_prepass_ms": round(split_ms, 3)},
         "clocks": clocks.summary(),
     }
+    out["targets"] = targets_summary(value, plain_tflops, errs, args.mode, dg, dg8, cfg3)
     return out
+
+
+def targets_summary(split_tflops, plain_tflops, errs, mode, dg, dg8, cfg3):
+    """The 3x-at-equal-error targets, one compact entry per operation: plain and split /
+    Ozaki TFLOP/s, their ratio, and the float64-oracle error of each (the maximum over
+    the input sets measured).  Printed as the line's last key."""
+    def entry(p_tf, s_tf, e_p, e_s, form):
+        return {"form": form, "plain_tflops": p_tf, "split_tflops": s_tf,
+                "ratio": round(s_tf / p_tf, 2) if p_tf else None,
+                "err_plain": float(f"{e_p:.2g}") if e_p is not None else None,
+                "err_split": float(f"{e_s:.2g}") if e_s is not None else None}
+    t = {"sgemm_NT_TN_8192": entry(round(plain_tflops, 1), round(split_tflops, 1),
+                                   max(v["plain_fp32"] for v in errs.values()),
+                                   max(v[mode] for v in errs.values() if mode in v), mode)}
+
+    def from_legs(legs, plain_key, split_key, err_key):
+        if not legs or plain_key not in legs or split_key not in legs:
+            return None
+        p, q = legs[plain_key], legs[split_key]
+        return entry(p["tflops"], q["tflops"], p.get(err_key), q.get(err_key), split_key)
+    for name, legs, ek in (("dgemm_NN_4096", dg, "err_vs_compensated"), ("dgemm_NN_8192", dg8, "err_vs_compensated"),
+                           ("dtrsm_LLNN_4096", cfg3.get("dtrsm_LLNN_4096"), "fp64_err"),
+                           ("dtrsm_LLNN_8192", cfg3.get("dtrsm_LLNN_8192"), "fp64_err")):
+        e = from_legs(legs, "plain_fp64", "ozaki_s7", ek)
+        if e is not None:
+            t[name] = e
+    return t
 
 
 _CPU_DATA = {}
 
 
+def cpu_sample_cols(threads: int) -> int:
+    """Columns of C in one CPU sample: at least the reference's parallel threshold (64,
+    gemm.mojo:255 / :276, restated at oracle/ref_level3.cpp PAR_THRESHOLD), so the sampled
+    _gemm_naive call takes the same multi-threaded branch as the full 8192-column call,
+    and four columns per thread so the dynamic schedule keeps every thread busy."""
+    return max(64, 4 * threads)
+
+
 def run_cpu_baseline(args, threads=None, rows=None, calls=("NT", "TN")):
     """Reference algorithm (oracle restatement of _gemm_naive NT/TN) on host cores,
-    over a bounded sample of each 8192^3 call in `calls`: rows 0..rows-1 of one
-    column of C per thread (the reference parallelises over columns).  Only
-    full-height columns give the full call's rate: shorter ones keep more of A
-    in cache (4096 rows already run 1.6x faster per flop)."""
+    over a bounded sample of each 8192^3 call in `calls`: rows 0..rows-1 of the first
+    cpu_sample_cols(threads) columns of C (the reference parallelises over columns).
+    Only full-height columns give the full call's rate: shorter ones keep more of A
+    in cache (4096 rows already run 1.6x faster per flop).  `cores` is the thread
+    count the oracle reports for the sampled call's column loop."""
     import oracle as orc
     nth = threads or os.cpu_count() or 1
     orc.set_threads(nth)
@@ -1043,22 +1080,24 @@ def run_cpu_baseline(args, threads=None, rows=None, calls=("NT", "TN")):
         _CPU_DATA["ab"] = (np.asfortranarray(rng.uniform(-1, 1, (n, n)).astype(np.float32)),
                            np.asfortranarray(rng.uniform(-1, 1, (n, n)).astype(np.float32)))
     a, b = _CPU_DATA["ab"]
-    cols = max(nth, 8)
+    cols = cpu_sample_cols(nth)
     c = np.zeros((n, cols), np.float32, order="F")
-    # NT: op(B)[l, j] = B[j + l*ldb]  -> columns j0.. of C use b + j0
-    # TN: op(B)[l, j] = B[l + j*ldb]  -> columns j0.. use b + j0*ldb
+    used = []
 
     def sample(ta, tb):
         t0 = time.perf_counter()
         orc.gemm_naive(ta, tb, rows, cols, n, 1.0, a, n, b, n, 0.0, c, n)
-        return time.perf_counter() - t0
+        dt = time.perf_counter() - t0
+        used.append(orc.naive_threads())
+        return dt
     secs = sum(sample(cl[0], cl[1]) for cl in calls)
     flops = 2.0 * rows * n * cols * len(calls)
-    return {"value": flops / secs / 1e12, "unit": "TFLOP/s", "cores": nth, "kind": "port",
+    cores = min(used)
+    return {"value": flops / secs / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",
             "sample": f"rows 0..{rows - 1} x columns 0..{cols - 1} of C for {' and '.join(calls)} {n}^3 "
                       f"(2*{rows}*{n}*{cols} flop each), float32, mojoBLAS _gemm_naive restated "
-                      f"(oracle/ref_level3.cpp), OpenMP {nth} threads",
-            "seconds": round(secs, 3), "flops": flops}
+                      f"(oracle/ref_level3.cpp), OpenMP, {cores} threads in the column loop",
+            "seconds": round(secs, 3), "flops": flops, "columns": cols, "threads_used": cores}
 
 
 def run_cpu_context_numpy(cols=512, min_seconds=1.0):
@@ -1120,9 +1159,10 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        # each step is a bounded sample of the workload: one full-height column of C per thread of
-        # the NT call (even steps) or the TN call (odd steps), about 8 s with 16 threads, so K steps
-        # plus W short warm-up samples stay within a few minutes
+        # each step is a bounded sample of the workload: 64 full-height columns of C (four per
+        # thread above 16 threads) of the NT call (even steps, well under a second) or the TN call
+        # (odd steps, about 4-10 s: the reference's TN loop reads A with a stride of lda), so K
+        # steps plus W short warm-up samples stay within a few minutes
         for _ in range(args.warmup):
             run_cpu_baseline(args, rows=min(512, N_S))
         flops = secs = 0.0
@@ -1132,10 +1172,10 @@ def main():
             flops += info["flops"]
             secs += info["flops"] / (info["value"] * 1e12)  # the step's time, unrounded
         v = flops / secs / 1e12
-        cols = max(info["cores"], 8)
+        cols = info["columns"]
         info.update(sample=f"per step: rows 0..{N_S - 1} x columns 0..{cols - 1} of C of the NT (even steps) or TN "
                            f"(odd steps) {N_S}^3 call (2*{N_S}*{N_S}*{cols} flop), float32, mojoBLAS _gemm_naive "
-                           f"restated (oracle/ref_level3.cpp), OpenMP {info['cores']} threads",
+                           f"restated (oracle/ref_level3.cpp), OpenMP, {info['cores']} threads in the column loop",
                     seconds=round(secs, 2), flops=flops)
         line = {"impl": "reference", "metric": "TFLOP/s at fixed FP64-oracle error (split-precision tensor-core "
                 "sgemm vs plain FP32)", "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -1163,6 +1203,7 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
+        out["targets"] = out.pop("targets")  # last key: it stays in a truncated tail of the output
         print(json.dumps(out), flush=True)
 
 

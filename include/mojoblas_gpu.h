@@ -47,7 +47,8 @@ extern "C" {
 #define MBG_ERR_SCRATCH_LIMIT -7  /* problem exceeds mbg_sgemm_ex_noalloc's fixed scratch */
 
 /* ---- precision modes ---------------------------------------------------- */
-#define MBG_MODE_PLAIN   0  /* FP32 / FP64 FMA on the CUDA cores (the drop-in)           */
+#define MBG_MODE_PLAIN   0  /* the drop-in: FP32 FMA on the CUDA cores; FP64 on the FP64
+                               tensor pipe (DMMA, mma.sync m8n8k4 f64: IEEE FP64 FMAs)   */
 #define MBG_MODE_BF16X3  1  /* fp32: a = a1 + a2 in bf16, a1b1 + a1b2 + a2b1 on tcgen05  */
 #define MBG_MODE_BF16X6  2  /* fp32: a = a1 + a2 + a3 in bf16, 6 products on tcgen05     */
 #define MBG_MODE_OZAKI   3  /* fp64: int8 slices, exact int32 tcgen05 products, fp64 sum */
@@ -193,7 +194,9 @@ int mbg_dtrmm_ex(int mode, int slices, char side, char uplo, char trans_a, char 
  *   - the first call on a device resolves that array's device address and sets
  *     the kernels' shared-memory limit, so make it before any stream capture;
  *   - every call reuses the same array: calls that overlap on the GPU (other
- *     streams, other host threads) race and must be serialised by the caller.
+ *     streams, other host threads) race and must be serialised by the caller;
+ *   - an expired kernel wait is returned as MBG_ERR_TIMEOUT by the call itself
+ *     in synchronous mode, else by the next mbg_synchronize() (once).
  * No cudaMalloc, cudaFree or other allocating routine is called. */
 int mbg_sgemm_ex_noalloc(int mode, char trans_a, char trans_b, int64_t m, int64_t n, int64_t k,
                          float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
@@ -268,6 +271,14 @@ int mbg_strsm_grouped(int mode, int count, const mbg_strsm_problem* problems);
 /* Stream for subsequent calls from any thread (a cudaStream_t; NULL = legacy
  * default stream, the initial value). */
 int   mbg_set_stream(void* stream);
+/* on != 0: subsequent calls from the calling host thread use `stream` instead
+ * of the process-wide one; on == 0: back to the process-wide stream.  Threads
+ * that each set their own stream run their calls concurrently: device
+ * workspace blocks are pooled per stream, so no block is shared by work in
+ * flight on two streams.  (The reference's routines take no stream; a Mojo
+ * caller that runs them from several threads sets one stream per thread.) */
+int   mbg_set_thread_stream(int on, void* stream);
+/* the stream the calling thread's calls use */
 void* mbg_get_stream(void);
 /* 1 (default): every call returns after its device work finished.
  * 0: calls whose operands are all device pointers return after enqueueing. */
@@ -323,6 +334,10 @@ int mbg_debug_fail_alloc(int nth);
  * gives up after limit_ns (at most 5 s): returns MBG_ERR_TIMEOUT with the
  * context still usable — the failure path of every tcgen05 kernel's waits. */
 int mbg_debug_wait_probe(int64_t limit_ns);
+/* Store `code` in mbg_sgemm_ex_noalloc's kernel wait flag on the current device,
+ * as an expired wait would; the next synchronous call or mbg_synchronize()
+ * reports it once as MBG_ERR_TIMEOUT. */
+int mbg_debug_set_noalloc_error(int code);
 
 #ifdef __cplusplus
 }

@@ -67,6 +67,7 @@ SIGNATURES = {
                           i64],
     "mbg_sgemm_ex_noalloc": [_i, _ch, _ch, i64, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
     "mbg_set_stream": [_vp],
+    "mbg_set_thread_stream": [_i, _vp],
     "mbg_get_stream": [],
     "mbg_set_sync": [_i],
     "mbg_synchronize": [],
@@ -80,6 +81,7 @@ SIGNATURES = {
     "mbg_launch_count": [],
     "mbg_debug_fail_alloc": [_i],
     "mbg_debug_wait_probe": [i64],
+    "mbg_debug_set_noalloc_error": [_i],
     "mbg_probe_peaks": [C.POINTER(_d)] * 4,
     "mbg_set_tuning": [C.c_char_p, i64],
     "mbg_get_tuning": [C.c_char_p],

@@ -185,8 +185,9 @@ struct mbg_plan {
 namespace mbg {
 namespace {
 
-int enqueue_plan(mbg_plan* p) {
-    cudaStream_t s = stream();
+// Enqueues the plan's work on stream s (the capture stream: the library stream that
+// other host threads may be using is never touched).
+int enqueue_plan(mbg_plan* p, cudaStream_t s) {
     if (p->kind == 1) {
         MBG_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
         if (p->tile == 128)
@@ -203,19 +204,18 @@ int enqueue_plan(mbg_plan* p) {
     return check_launch("grouped_strsm");
 }
 
-// Records the plan's work into a CUDA graph on a private capture stream.
+// Records the plan's work into a CUDA graph on a private capture stream.  The
+// library's stream setting is left alone, so calls that other host threads make
+// meanwhile stay on their stream and out of this graph.
 int capture_plan(mbg_plan* p) {
     cudaStream_t cap = nullptr;
     MBG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-    cudaStream_t saved = stream();
-    mbg_set_stream(cap);
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     int st = MBG_OK;
     if (e == cudaSuccess) {
-        st = enqueue_plan(p);
+        st = enqueue_plan(p, cap);
         e = cudaStreamEndCapture(cap, &p->graph);
     }
-    mbg_set_stream(saved);
     cudaStreamDestroy(cap);
     if (e != cudaSuccess) {
         set_error("graph capture of a grouped plan", e);

@@ -67,17 +67,23 @@ int check_launch(const char* name);
 // copies of the pipelined host path), created on first use and kept.
 int copy_streams(cudaStream_t* in, cudaStream_t* out);
 
-// ---- device workspace: a per-device cache of blocks, stream-ordered reuse ---
+// ---- device workspace: a per-device, per-stream cache of blocks ---------------
 // Blocks are handed out for the duration of one library call and returned to
-// the cache when the call finishes enqueueing; all library work runs on one
-// stream, so a block reused by the next call is ordered after its last use.
+// the pool of the stream that call ran on when it finishes enqueueing; a pool
+// serves only calls on its own stream, so a block reused by a later call is
+// ordered after its last use by stream order (calls from several host threads
+// on their own streams never share a block in flight).
 struct Workspace {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t owner = nullptr;  // the stream whose pool the block returns to
     Workspace() = default;
     Workspace(const Workspace&) = delete;
     Workspace& operator=(const Workspace&) = delete;
-    Workspace(Workspace&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    Workspace(Workspace&& o) noexcept : ptr(o.ptr), bytes(o.bytes), owner(o.owner) {
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
     ~Workspace();
     int reserve(size_t nbytes);   // MBG_OK or MBG_ERR_ALLOC
     template <typename T> T* as() const { return static_cast<T*>(ptr); }
@@ -110,7 +116,8 @@ void count_launch(int n = 1);
 // Device-side error flag (bounded waits that expired set it): a mapped pinned
 // int[4] — [0] error code, [1] site — or nullptr if it could not be created.
 int* device_error_flag();
-int read_and_clear_device_error();
+int read_and_clear_device_error();  // the mapped flag and the no-allocation flag
+int noalloc_take_error(int* site);   // the no-allocation kernels' flag: code, cleared (tc_gemm.cu)
 int finish_call(bool any_staged);  // synchronises when required, checks flag
 
 // ---- tuning table (defaults; mbg_set_tuning / mbg_load_tuning override) ------

@@ -15,15 +15,19 @@ namespace mbg {
 
 namespace {
 std::mutex g_mu;
-cudaStream_t g_stream = nullptr;
+cudaStream_t g_stream = nullptr;               // mbg_set_stream: the process-wide stream
+thread_local cudaStream_t t_stream = nullptr;  // mbg_set_thread_stream: this thread's override
+thread_local bool t_stream_on = false;
 std::atomic<bool> g_sync{true};
 thread_local std::string g_last_error;
 std::atomic<int> g_fail_alloc_countdown{0};
 std::atomic<int64_t> g_launches{0};
 
 struct DeviceCache {
-    std::multimap<size_t, void*> free_blocks;  // size -> block
-    std::map<void*, size_t> sizes;
+    // free workspace blocks per stream (size -> block): a block goes back to the
+    // pool of the stream its call ran on and is handed out again only to calls on
+    // that stream, so its reuse is ordered after its last use by stream order
+    std::map<cudaStream_t, std::multimap<size_t, void*>> free_blocks;
     int* err_host = nullptr;                    // mapped pinned flag
     int* err_dev = nullptr;
     cudaStream_t copy_in = nullptr, copy_out = nullptr;  // pipelined host path
@@ -61,7 +65,7 @@ Tuning& tuning() {
     return t;
 }
 
-cudaStream_t stream() { return g_stream; }
+cudaStream_t stream() { return t_stream_on ? t_stream : g_stream; }
 bool sync_mode() { return g_sync.load(); }
 
 void set_error(const char* what, cudaError_t e) {
@@ -86,8 +90,7 @@ void count_launch(int n) { g_launches += n; }
 Workspace::~Workspace() {
     if (!ptr) return;
     std::lock_guard<std::mutex> lk(g_mu);
-    int d = current_device();
-    g_cache[d].free_blocks.emplace(bytes, ptr);
+    g_cache[current_device()].free_blocks[owner].emplace(bytes, ptr);
     ptr = nullptr;
 }
 
@@ -96,18 +99,20 @@ int Workspace::reserve(size_t nbytes) {
     if (ptr && bytes >= nbytes) return MBG_OK;
     if (ptr) {  // give back the smaller block
         std::lock_guard<std::mutex> lk(g_mu);
-        g_cache[current_device()].free_blocks.emplace(bytes, ptr);
+        g_cache[current_device()].free_blocks[owner].emplace(bytes, ptr);
         ptr = nullptr;
     }
     const size_t gran = size_t(2) << 20;
     size_t want = (nbytes + gran - 1) / gran * gran;
+    owner = stream();
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceCache& dc = g_cache[current_device()];
-    auto it = dc.free_blocks.lower_bound(want);
-    if (it != dc.free_blocks.end() && it->first <= 2 * want) {
+    auto& pool = dc.free_blocks[owner];
+    auto it = pool.lower_bound(want);
+    if (it != pool.end() && it->first <= 2 * want) {
         ptr = it->second;
         bytes = it->first;
-        dc.free_blocks.erase(it);
+        pool.erase(it);
         return MBG_OK;
     }
     int cd = g_fail_alloc_countdown.load();
@@ -121,8 +126,9 @@ int Workspace::reserve(size_t nbytes) {
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
-        // drop the cache and retry once
-        for (auto& kv : dc.free_blocks) cudaFree(kv.second);
+        // drop every stream's cached blocks (cudaFree waits for the device) and retry once
+        for (auto& sp : dc.free_blocks)
+            for (auto& kv : sp.second) cudaFree(kv.second);
         dc.free_blocks.clear();
         cudaGetLastError();
         e = cudaMalloc(&p, want);
@@ -201,17 +207,32 @@ int* device_error_flag() {
 }
 
 int read_and_clear_device_error() {
-    std::lock_guard<std::mutex> lk(g_mu);
-    DeviceCache& dc = g_cache[current_device()];
-    if (!dc.err_host) return 0;
-    volatile int* f = dc.err_host;
-    int v = f[0];
+    int v = 0, site = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        DeviceCache& dc = g_cache[current_device()];
+        if (dc.err_host) {
+            volatile int* f = dc.err_host;
+            v = f[0];
+            site = f[1];
+            if (v) {
+                f[0] = 0;
+                f[1] = 0;
+            }
+        }
+    }
+    // the no-allocation entry point's kernels record into a flag of their own
+    int site2 = 0;
+    const int v2 = noalloc_take_error(&site2);
+    if (!v && v2) {
+        v = v2;
+        site = site2;
+    }
     if (v) {
         char buf[160];
-        std::snprintf(buf, sizeof buf, "a kernel's bounded wait expired (code %d, site %d); results are invalid", v, f[1]);
+        std::snprintf(buf, sizeof buf, "a kernel's bounded wait expired (code %d, site %d); results are invalid", v,
+                      site);
         g_last_error = buf;
-        f[0] = 0;
-        f[1] = 0;
     }
     return v;
 }
@@ -247,17 +268,22 @@ extern "C" {
 
 int mbg_set_stream(void* s) {
     if (g_stream != static_cast<cudaStream_t>(s)) {
-        // work still queued on the old stream may use cached workspace blocks
+        // earlier calls' work finishes first, as when the library had one stream
         if (cudaStreamSynchronize(g_stream) != cudaSuccess) cudaGetLastError();
         g_stream = static_cast<cudaStream_t>(s);
     }
     return MBG_OK;
 }
-void* mbg_get_stream(void) { return g_stream; }
+int mbg_set_thread_stream(int on, void* s) {
+    t_stream_on = (on != 0);
+    t_stream = on ? static_cast<cudaStream_t>(s) : nullptr;
+    return MBG_OK;
+}
+void* mbg_get_stream(void) { return stream(); }
 int mbg_set_sync(int on) { g_sync = (on != 0); return MBG_OK; }
 
 int mbg_synchronize(void) {
-    MBG_CUDA(cudaStreamSynchronize(g_stream));
+    MBG_CUDA(cudaStreamSynchronize(stream()));
     if (read_and_clear_device_error()) return MBG_ERR_TIMEOUT;
     return MBG_OK;
 }
@@ -280,10 +306,11 @@ const char* mbg_last_error(void) { return g_last_error.c_str(); }
 int mbg_version(void) { return 100; }
 
 int mbg_release_workspace(void) {
-    MBG_CUDA(cudaStreamSynchronize(g_stream));
+    MBG_CUDA(cudaStreamSynchronize(stream()));
     std::lock_guard<std::mutex> lk(g_mu);
     for (auto& kv : g_cache) {
-        for (auto& b : kv.second.free_blocks) cudaFree(b.second);
+        for (auto& sp : kv.second.free_blocks)
+            for (auto& b : sp.second) cudaFree(b.second);  // cudaFree waits for the device
         kv.second.free_blocks.clear();
     }
     return MBG_OK;

@@ -1385,6 +1385,12 @@ extern "C" int mbg_sgemm_ex_noalloc(int mode, char ta, char tb, int64_t m, int64
     if (ldc < imax(1, m)) return 13;
     if (m == 0 || n == 0) return MBG_OK;
     const int terms = mode == MBG_MODE_BF16X6 ? 3 : 2;
+    // any dimension this large cannot fit; checked first so the padded sizes below cannot wrap
+    if (m > i64(NOALLOC_SCRATCH_BYTES) || n > i64(NOALLOC_SCRATCH_BYTES) || k > i64(NOALLOC_SCRATCH_BYTES)) {
+        set_error_msg("mbg_sgemm_ex_noalloc: a dimension exceeds the scratch limit of " +
+                      std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes");
+        return MBG_ERR_SCRATCH_LIMIT;
+    }
     const i64 Mp = roundup(m, BM), Np = roundup(n, 256), Kp = roundup(imax(k, 1), 32);
     const size_t need = size_t(terms) * size_t(Mp + Np) * size_t(Kp) * 2;
     if (need > NOALLOC_SCRATCH_BYTES) {
@@ -1430,17 +1436,46 @@ extern "C" int mbg_sgemm_ex_noalloc(int mode, char ta, char tb, int64_t m, int64
             tc_gemm_kernel<CfgBF16x6><<<tiles, CfgBF16x6::THREADS, CfgBF16x6::SMEM_BYTES, stream()>>>(ma, mb, P);
         MBG_TRY(check_launch(terms == 2 ? "tc_gemm_bf16x3" : "tc_gemm_bf16x6"));
     }
-    if (sync_mode()) {
-        MBG_CUDA(cudaStreamSynchronize(stream()));
-        int flag[4] = {0, 0, 0, 0};
-        MBG_CUDA(cudaMemcpyFromSymbol(flag, g_noalloc_err, sizeof(flag)));
-        if (flag[0]) {
-            const int zero[4] = {0, 0, 0, 0};
-            MBG_CUDA(cudaMemcpyToSymbol(g_noalloc_err, zero, sizeof(zero)));
-            set_error_msg("mbg_sgemm_ex_noalloc: a kernel's bounded wait expired; results are invalid");
-            return MBG_ERR_TIMEOUT;
-        }
+    // synchronous mode: wait, then report an expired wait (this entry point's flag is read
+    // and cleared by read_and_clear_device_error, as mbg_synchronize does in asynchronous mode)
+    return finish_call(false);
+}
+
+// The no-allocation kernels' bounded-wait flag on the current device: returns its code
+// (0 when no wait expired) and clears it.  Called by read_and_clear_device_error, so
+// the synchronous return and mbg_synchronize() both surface it exactly once.  The flag
+// lives in device memory: the caller has synchronised the library stream first.
+int mbg::noalloc_take_error(int* site) {
+    using namespace mbg;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        cudaGetLastError();
+        return 0;
     }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_dev[dev].ready) return 0;  // never used on this device
+    int flag[4] = {0, 0, 0, 0};
+    if (cudaMemcpy(flag, g_noalloc_dev[dev].err, sizeof(flag), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (!flag[0]) return 0;
+    const int zero[4] = {0, 0, 0, 0};
+    if (cudaMemcpy(g_noalloc_dev[dev].err, zero, sizeof(zero), cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaGetLastError();
+    if (site) *site = flag[1];
+    return flag[0];
+}
+
+// Test hook: stores an error code in the no-allocation kernels' wait flag on the
+// current device, as an expired wait would, so the reporting path can be checked
+// without making any kernel wait.
+extern "C" int mbg_debug_set_noalloc_error(int code) {
+    using namespace mbg;
+    NoallocDevice* d = nullptr;
+    MBG_TRY(noalloc_setup(&d));
+    const int v[4] = {code, 77, 0, 0};
+    MBG_CUDA(cudaMemcpy(d->err, v, sizeof(v), cudaMemcpyHostToDevice));
     return MBG_OK;
 }
 

@@ -74,6 +74,7 @@ def lib():
         _lib.orc_fma.restype = C.c_int
         _lib.orc_set_threads.argtypes = [C.c_int]
         _lib.orc_max_threads.restype = C.c_int
+        _lib.orc_naive_threads.restype = C.c_int
     return _lib
 
 
@@ -83,6 +84,12 @@ def set_threads(n: int) -> None:
 
 def max_threads() -> int:
     return lib().orc_max_threads()
+
+
+def naive_threads() -> int:
+    """Threads that ran the column loop of the last gemm_naive call (1 below the
+    reference's parallel threshold of 64 columns, gemm.mojo:255)."""
+    return lib().orc_naive_threads()
 
 
 def _p(x: np.ndarray, dt):

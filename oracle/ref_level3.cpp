@@ -74,6 +74,10 @@ static void scale_or_zero(i64 m, i64 n, T beta, T* c, i64 ldc) {
     }
 }
 
+// Threads that ran the last _gemm_naive call's column loop (1 when n is below
+// the reference's parallel threshold), reported by orc_naive_threads().
+static int g_naive_threads = 0;
+
 // _gemm_naive, src/level3/gemm.mojo:127-377.  Column j of C is owned by one task
 // (parallel when n >= 64, :255/:276); within it, beta first, then an axpy per l in
 // ascending order, skipped when the B element is zero (:263, :299, :336, :365).
@@ -88,27 +92,34 @@ static int gemm_naive(char ta, char tb, i64 m, i64 n, i64 k, T alpha, const T* a
         return 0;
     }
     const bool nta = is_n(ta), ntb = is_n(tb);
-#pragma omp parallel for schedule(dynamic, 1) if (n >= PAR_THRESHOLD)
-    for (i64 j = 0; j < n; ++j) {
-        T* cj = c + j * ldc;
-        if (beta == T(0)) {
-            for (i64 i = 0; i < m; ++i) cj[i] = T(0);
-        } else if (beta != T(1)) {
-            for (i64 i = 0; i < m; ++i) cj[i] = beta * cj[i];
-        }
-        for (i64 l = 0; l < k; ++l) {
-            const T bv = ntb ? b[l + j * ldb] : b[j + l * ldb];
-            if (bv == T(0)) continue;
-            const T temp = alpha * bv;
-            if (nta) {  // NN :262-274, NT :298-310 — vectorised column axpy
-                const T* al = a + l * lda;
-                for (i64 i = 0; i < m; ++i) cj[i] = cj[i] + temp * al[i];
-            } else {    // TN :335-340, TT :364-369 — scalar strided loads
-                const T* al = a + l;
-                for (i64 i = 0; i < m; ++i) cj[i] = cj[i] + temp * al[i * lda];
+    int used = 1;
+#pragma omp parallel if (n >= PAR_THRESHOLD)
+    {
+#pragma omp single
+        used = omp_get_num_threads();
+#pragma omp for schedule(dynamic, 1)
+        for (i64 j = 0; j < n; ++j) {
+            T* cj = c + j * ldc;
+            if (beta == T(0)) {
+                for (i64 i = 0; i < m; ++i) cj[i] = T(0);
+            } else if (beta != T(1)) {
+                for (i64 i = 0; i < m; ++i) cj[i] = beta * cj[i];
+            }
+            for (i64 l = 0; l < k; ++l) {
+                const T bv = ntb ? b[l + j * ldb] : b[j + l * ldb];
+                if (bv == T(0)) continue;
+                const T temp = alpha * bv;
+                if (nta) {  // NN :262-274, NT :298-310 — vectorised column axpy
+                    const T* al = a + l * lda;
+                    for (i64 i = 0; i < m; ++i) cj[i] = cj[i] + temp * al[i];
+                } else {    // TN :335-340, TT :364-369 — scalar strided loads
+                    const T* al = a + l;
+                    for (i64 i = 0; i < m; ++i) cj[i] = cj[i] + temp * al[i * lda];
+                }
             }
         }
     }
+    g_naive_threads = used;
     return 0;
 }
 
@@ -650,6 +661,7 @@ extern "C" {
 
 void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
 int orc_max_threads(void) { return omp_get_max_threads(); }
+int orc_naive_threads(void) { return g_naive_threads; }
 
 // Full dispatch, as a user of the reference's gemm reaches it.
 int orc_sgemm(char ta, char tb, i64 m, i64 n, i64 k, float alpha, const float* a, i64 lda,

@@ -9,8 +9,8 @@ so this script reads those files as text, replays each test's assignments and
 records the call and its expected values.  The JSON it writes is committed;
 nothing reads the reference at test time.
 
-Run:  python tests/golden/make_known_answers.py [path/to/mojoBLAS]
-(default path: /root/reference)
+Run:  python tests/golden/make_known_answers.py path/to/mojoBLAS
+(or set MOJOBLAS_REFERENCE to the mojoBLAS source tree and omit the argument)
 """
 from __future__ import annotations
 
@@ -128,7 +128,11 @@ def parse(path: Path, routines=ROUTINES) -> list[dict]:
 
 
 def main() -> None:
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+    where = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MOJOBLAS_REFERENCE")
+    if not where:
+        sys.exit("usage: make_known_answers.py path/to/mojoBLAS (or set MOJOBLAS_REFERENCE)")
+    root = Path(where)
     src = root / "tests" / "test_level3.mojo"
     cases = parse(src)
     out = {

@@ -223,3 +223,17 @@ def test_level2_quick_returns_touch_no_device():
     assert mb.gemv("T", 3, 0, 1.0, Z, 3, Z, 1, 0.0, Z, 1) == 0
     assert mb.gemv("N", 3, 3, 0.0, Z, 3, Z, 1, 1.0, Z, 1) == 0
     assert mb.trsv("L", "N", "N", 0, Z, 1, Z, 1) == 0
+
+
+def test_noalloc_rejects_huge_dimensions_before_device_work():
+    """Dimensions near INT64_MAX cannot wrap the no-allocation entry point's scratch
+    size into a small number: they are rejected with MBG_ERR_SCRATCH_LIMIT before any
+    pointer is inspected or any device work is queued (no GPU needed)."""
+    lib = L.load()
+    huge = (1 << 62) + 5
+    for m, n, k in ((huge, 64, 64), (64, huge, 64), (64, 64, huge)):
+        lda = m
+        ldb = k
+        st = lib.mbg_sgemm_ex_noalloc(L.MODE_BF16X6, b"N", b"N", m, n, k, 1.0, None, lda, None, ldb, 0.0, None, m)
+        assert st == L.MBG_ERR_SCRATCH_LIMIT, (m, n, k, st)
+        assert "scratch limit" in L.last_error()

@@ -38,6 +38,25 @@ def test_reference_arm_line(monkeypatch, capsys):
     assert d["config"]["workload"].startswith("large_gemm")
 
 
+def test_cpu_sample_reaches_the_parallel_branch():
+    """The sampled _gemm_naive call has at least the reference's 64-column parallel
+    threshold (gemm.mojo:255), so it runs multi-threaded like the full 8192-column call,
+    and the line's `cores` is the thread count the oracle saw in the column loop."""
+    import oracle as orc
+    assert bench.cpu_sample_cols(1) >= 64 and bench.cpu_sample_cols(16) >= 64
+    assert bench.cpu_sample_cols(32) == 128
+    cb = bench.run_cpu_baseline(None, threads=2, rows=64, calls=("NT",))
+    assert cb["columns"] >= 64
+    assert cb["cores"] == cb["threads_used"] == 2, cb
+    # below the threshold the restated loop stays serial, as the reference's does
+    import numpy as np
+    a = np.asfortranarray(np.ones((32, 32), np.float32))
+    c = np.zeros((32, 16), np.float32, order="F")
+    orc.set_threads(2)
+    orc.gemm_naive("N", "N", 32, 16, 32, 1.0, a, 32, a, 32, 0.0, c, 32)
+    assert orc.naive_threads() == 1
+
+
 def test_reference_arm_other_ranks_do_nothing(monkeypatch, capsys):
     out = run_main(monkeypatch, capsys, ["--impl", "reference", "--steps", "1"],
                    env={"RANK": "1", "WORLD_SIZE": "2"})

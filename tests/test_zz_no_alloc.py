@@ -3,11 +3,13 @@ library allocate device memory (a host framework that owns a fixed device-memory
 budget, a latency-critical loop where cudaMalloc / cudaFree may synchronise the
 device, or code inside an allocator's out-of-memory handling).
 
-Its result must match the allocating entry point mbg_sgemm_ex with the same
-mode on the same device inputs, within the float32 tolerance the other GPU
-tests use, on two calls in a row (the second reuses the fixed scratch array
-the first one filled).  This file is collected last on purpose, and passes
-both alone in a fresh process and after the rest of the suite.
+Its result must equal the allocating entry point mbg_sgemm_ex's bit for bit
+with the same mode on the same device inputs (the same pre-pass and tcgen05
+kernels run on the same planes, only the planes' address differs), and stay
+within the float32 tolerance of the other GPU tests against a float64 product,
+on two calls in a row (the second reuses the fixed scratch array the first one
+filled).  This file is collected last on purpose, and passes both alone in a
+fresh process and after the rest of the suite.
 """
 import ctypes as C
 
@@ -59,9 +61,40 @@ def test_noalloc_matches_allocating_entry_point_twice():
         torch.cuda.synchronize()
         free_after = torch.cuda.mem_get_info()[0]
         assert free_before - free_after < (2 << 20), "the no-allocation entry point allocated device memory"
-        ref = c_ref.double()
-        diff = float((c_new.double() - ref).abs().max() / ref.abs().max())
+        assert torch.equal(c_new, c_ref), (i, float((c_new - c_ref).abs().max()))
+        # and within the float32 tolerance of the float64 product
+        A = a.double().T[:m, :k] if ta == "N" else a.double().T[:k, :m].T
+        B = b.double().T[:k, :n] if tb == "N" else b.double().T[:n, :k].T
+        ref = alpha * (A @ B) + beta * c0.double().T
+        diff = float((c_new.double().T - ref).abs().max() / ref.abs().max())
         assert diff <= tol32(k), (i, diff)
+
+
+def test_noalloc_wait_flag_reported_once_in_async_mode():
+    """An expired wait in the no-allocation kernels (planted in the flag from the
+    host; no kernel is made to wait) is reported by the next mbg_synchronize() as
+    MBG_ERR_TIMEOUT exactly once, then cleared."""
+    torch = need_gpu()
+    lib = L.load()
+    lib.mbg_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    lib.mbg_set_sync(0)
+    try:
+        assert lib.mbg_synchronize() == 0
+        assert lib.mbg_debug_set_noalloc_error(1) == 0
+        assert lib.mbg_synchronize() == L.MBG_ERR_TIMEOUT
+        assert "site 77" in L.last_error()
+        assert lib.mbg_synchronize() == 0
+    finally:
+        lib.mbg_set_sync(1)
+    # synchronous mode: the next call itself reports it, and only once
+    n = 64
+    a = torch.ones((n, n), device="cuda", dtype=torch.float32)
+    c = torch.zeros_like(a)
+    assert lib.mbg_debug_set_noalloc_error(1) == 0
+    st = _call(lib.mbg_sgemm_ex_noalloc, L.MODE_BF16X3, "N", "N", n, n, n, 1.0, a, n, a, n, 0.0, c, n)
+    assert st == L.MBG_ERR_TIMEOUT
+    st = _call(lib.mbg_sgemm_ex_noalloc, L.MODE_BF16X3, "N", "N", n, n, n, 1.0, a, n, a, n, 0.0, c, n)
+    assert st == 0 and float(c[0, 0]) == n
 
 
 def test_noalloc_rejects_oversized_and_host_operands():
