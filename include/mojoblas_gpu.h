@@ -202,6 +202,30 @@ int mbg_sgemm_ex_noalloc(int mode, char trans_a, char trans_b, int64_t m, int64_
                          float alpha, const float* a, int64_t lda, const float* b, int64_t ldb,
                          float beta, float* c, int64_t ldc);
 
+/* ---- complex gemm ---------------------------------------------------------
+ * C := alpha*op(A)*op(B) + beta*C for single (c) and double (z) complex, with
+ * op(X) = X ('N'), X^T ('T') or X^H ('C', conjugate transpose).  Matrices are
+ * column-major arrays of interleaved (re, im) pairs (lda, ldb, ldc count
+ * complex elements); alpha and beta point at one (re, im) pair each in host
+ * memory.  No counterpart in the reference: complex dtypes are on mojoBLAS's
+ * roadmap (README.md:152); the argument order and `info` numbering are those
+ * of its gemm (src/level3/gemm.mojo:56-78, :179-213).  Computed as one real
+ * product of 2m x n x 2k (the real embedding [Ar -Ai; Ai Ar] [Br; Bi], rows
+ * and reduction interleaved so C is written in place) in the mode given:
+ * MBG_MODE_PLAIN / BF16X3 / BF16X6 for c, MBG_MODE_PLAIN / OZAKI (slices) for z. */
+int mbg_cgemm(char trans_a, char trans_b, int64_t m, int64_t n, int64_t k, const float* alpha,
+              const float* a, int64_t lda, const float* b, int64_t ldb, const float* beta, float* c,
+              int64_t ldc);
+int mbg_zgemm(char trans_a, char trans_b, int64_t m, int64_t n, int64_t k, const double* alpha,
+              const double* a, int64_t lda, const double* b, int64_t ldb, const double* beta, double* c,
+              int64_t ldc);
+int mbg_cgemm_ex(int mode, char trans_a, char trans_b, int64_t m, int64_t n, int64_t k, const float* alpha,
+                 const float* a, int64_t lda, const float* b, int64_t ldb, const float* beta, float* c,
+                 int64_t ldc);
+int mbg_zgemm_ex(int mode, int slices, char trans_a, char trans_b, int64_t m, int64_t n, int64_t k,
+                 const double* alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                 const double* beta, double* c, int64_t ldc);
+
 /* ---- adjoints (reverse mode) --------------------------------------------
  * No counterpart in the reference.  Given the upstream gradient G = dL/dC of
  * C = alpha*op(A)*op(B), the gemm adjoint writes dA (shape of A, skipped if da
@@ -235,11 +259,17 @@ int mbg_dtrsm_adjoint(int mode, int slices, char side, char uplo, char trans_a, 
  * the problem table to the device once and records [reset; persistent kernel]
  * into a CUDA graph; mbg_plan_execute replays it on the library stream.  All
  * matrix pointers must be device pointers and stay valid for the plan's life.
- *   sgemm: any transposes, any sizes; tiles of 64 or 128 (tuning key
- *          "grouped_gemm_tile"), largest problems first, atomic tile counter.
+ *   sgemm, MBG_MODE_PLAIN: any transposes, any sizes; FP32 CUDA-core tiles of
+ *          64 or 128 per problem (the tuning table's entry for the problem's
+ *          transposes and size class, else "grouped_gemm_tile"), largest problems
+ *          first, atomic tile counter (one persistent kernel per tile size).
+ *   sgemm, MBG_MODE_BF16X3 / BF16X6: one persistent tcgen05 kernel; its producer
+ *          warps load and split each problem's operands into bf16 terms in
+ *          shared memory (no pre-pass, any leading dimension), tiles of 128 x 64
+ *          or 128 x 128 per problem (tuning table), longest reduction first.
  *   strsm: side 'L' only, m <= 256 (the triangle order), any uplo/trans/diag;
- *          one warp per right-hand-side column.
- * mode: MBG_MODE_PLAIN. */
+ *          32-column strips solved by the fused diagonal-block routine;
+ *          mode MBG_MODE_PLAIN. */
 typedef struct {
     char trans_a, trans_b;
     int64_t m, n, k;
@@ -301,6 +331,17 @@ int   mbg_release_workspace(void);
  * included (default 512; 64 or less: 64-row leaves with gemm updates between them);
  * "trsm_block_min_cols" — the fused launch is used only with at least this
  * many right-hand sides (default 64);
+ * "trsm_inverse_min_cols" — split / Ozaki trsm with at least this many
+ * right-hand sides inverts its 512-row diagonal blocks once (native precision)
+ * and applies each inverse as a split / Ozaki product (default 256; 0 = never:
+ * substitution in the diagonal blocks);
+ * "ozaki_cta_pair" — 1: Ozaki products on CTA pairs (tcgen05
+ * cta_group::2, 256 x 128 tiles over two SMs); 0 (default): one CTA per tile;
+ * "grouped_simt_tile_<TT>_c<d>", "grouped_tc_bn_<TT>_c<d>" — grouped sgemm
+ * plans' tile table, per transposes TT (NN, NT, TN, TT) and size class d of
+ * max(m, n) (0: <= 32, 1: <= 64, 2: <= 128, 3: <= 256, 4: larger): the plain
+ * form's tile edge and the split form's tile width, 64 or 128 (0 = default:
+ * "grouped_gemm_tile", resp. 64 for n <= 64 else 128);
  * "plain_fp64_simt" — 1: plain FP64 gemm / syrk on the CUDA cores instead of the
  * FP64 tensor pipe (default 0); "plain_fp32_staged" — 1: plain FP32 gemm / syrk
  * with the register-staged tiles instead of the cp.async pipeline (default 0).

@@ -66,6 +66,10 @@ SIGNATURES = {
     "mbg_dtrsm_adjoint": [_i, _i, _ch, _ch, _ch, _ch, i64, i64, _d, _vp, i64, _vp, i64, _vp, i64, _vp, i64, _vp,
                           i64],
     "mbg_sgemm_ex_noalloc": [_i, _ch, _ch, i64, i64, i64, _f, _vp, i64, _vp, i64, _f, _vp, i64],
+    "mbg_cgemm": [_ch, _ch, i64, i64, i64, _vp, _vp, i64, _vp, i64, _vp, _vp, i64],
+    "mbg_zgemm": [_ch, _ch, i64, i64, i64, _vp, _vp, i64, _vp, i64, _vp, _vp, i64],
+    "mbg_cgemm_ex": [_i, _ch, _ch, i64, i64, i64, _vp, _vp, i64, _vp, i64, _vp, _vp, i64],
+    "mbg_zgemm_ex": [_i, _i, _ch, _ch, i64, i64, i64, _vp, _vp, i64, _vp, i64, _vp, _vp, i64],
     "mbg_set_stream": [_vp],
     "mbg_set_thread_stream": [_i, _vp],
     "mbg_get_stream": [],

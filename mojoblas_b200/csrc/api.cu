@@ -2,6 +2,9 @@
 // routines), quick returns, host-operand staging and precision-mode dispatch.
 #include "mbg_internal.cuh"
 
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 namespace mbg {
@@ -187,45 +190,107 @@ static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i6
     if (hb) { MBG_TRY(wb.reserve(e * size_t(br) * size_t(bc))); db = wb.as<T>(); dldb = br; }
     if (hc) { MBG_TRY(wc.reserve(e * size_t(m) * size_t(n))); dc = wc.as<T>(); dldc = m; }
 
-    struct Events {  // destroyed on every return path (pending work keeps them alive until done)
-        std::vector<cudaEvent_t> v;
-        ~Events() {
+    const std::vector<i64> widths = pipeline_widths(n);
+    struct Guard {  // on every return: the copy streams' work is ordered before the library stream's
+        std::vector<cudaEvent_t> v;   // next use of the workspace blocks, then the events are destroyed
+        cudaStream_t s = nullptr, sin = nullptr, sout = nullptr;
+        ~Guard() {
+            cudaEvent_t tail[2] = {nullptr, nullptr};
+            cudaStream_t from[2] = {sin, sout};
+            for (int i = 0; i < 2; ++i)
+                if (from[i] && cudaEventCreateWithFlags(&tail[i], cudaEventDisableTiming) == cudaSuccess) {
+                    cudaEventRecord(tail[i], from[i]);
+                    cudaStreamWaitEvent(s, tail[i], 0);
+                    cudaEventDestroy(tail[i]);
+                }
             for (auto x : v)
                 if (x) cudaEventDestroy(x);
         }
-    } events;
-    const std::vector<i64> widths = pipeline_widths(n);
-    events.v.assign(2 * widths.size() + 2, nullptr);
-    auto& ev = events.v;
+    } guard;
+    guard.s = s;
+    guard.sin = sin;
+    guard.sout = sout;
+    auto& ev = guard.v;
+    ev.assign(2 * widths.size() + 2, nullptr);
     for (auto& x : ev) MBG_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
     cudaEvent_t ev_start = ev[0], ev_end = ev[1];
     MBG_CUDA(cudaEventRecord(ev_start, s));  // earlier work on the library stream (workspace reuse) first
     MBG_CUDA(cudaStreamWaitEvent(sin, ev_start, 0));
     MBG_CUDA(cudaStreamWaitEvent(sout, ev_start, 0));
-    if (ha)
-        MBG_CUDA(cudaMemcpy2DAsync(const_cast<T*>(da), size_t(ar) * e, a, size_t(lda) * e, size_t(ar) * e,
-                                   size_t(ac), cudaMemcpyHostToDevice, sin));
+
+    // C's blocks go back to the host in order as they finish.  Into pageable memory
+    // that takes the host's hands (unpacking from the bounce buffers), so a helper
+    // thread does it while this thread packs op(B)'s next blocks.
+    std::mutex out_mu;
+    std::condition_variable out_cv;
+    int recorded = 0;       // blocks whose ev_done is recorded
+    bool abort_out = false;
+    int out_st = MBG_OK;
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    const bool c_pageable = hc && !is_pinned_host(c);
+    auto copy_out_block = [&](int blk) -> int {
+        i64 j0 = 0;
+        for (int i = 0; i < blk; ++i) j0 += widths[size_t(i)];
+        const i64 w = widths[size_t(blk)];
+        return copy_d2h_2d(c + j0 * ldc, size_t(ldc) * e, dc + j0 * dldc, size_t(dldc) * e, size_t(m) * e,
+                           size_t(w), sout, ev[3 + 2 * blk]);
+    };
+    std::thread out_thread;
+    if (c_pageable) {
+        out_thread = std::thread([&] {
+            cudaSetDevice(dev);
+            for (int blk = 0; blk < int(widths.size()); ++blk) {
+                {
+                    std::unique_lock<std::mutex> lk(out_mu);
+                    out_cv.wait(lk, [&] { return recorded > blk || abort_out; });
+                    if (recorded <= blk) return;  // aborted before this block was computed
+                }
+                const int r = copy_out_block(blk);
+                if (r) {
+                    out_st = r;
+                    return;
+                }
+            }
+        });
+    }
+    struct Join {  // the helper thread ends before this function's state goes away
+        std::thread& t;
+        std::mutex& mu;
+        std::condition_variable& cv;
+        bool& abort;
+        ~Join() {
+            if (!t.joinable()) return;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                abort = true;
+            }
+            cv.notify_all();
+            t.join();
+        }
+    } join{out_thread, out_mu, out_cv, abort_out};
+
+    if (ha) MBG_TRY(copy_h2d_2d(const_cast<T*>(da), size_t(ar) * e, a, size_t(lda) * e, size_t(ar) * e, size_t(ac), sin));
     // split modes: op(A)'s planes once, on the library stream after op(A) has landed
     const bool split_once = sizeof(T) == 4 && (mode == MBG_MODE_BF16X3 || mode == MBG_MODE_BF16X6);
     SplitA sa;
     int st = MBG_OK;
-    int used = 0;
     i64 j0 = 0;
-    for (size_t blk = 0; blk < widths.size() && !st; ++blk, ++used) {
+    for (size_t blk = 0; blk < widths.size() && !st; ++blk) {
         const i64 w = widths[blk];
-        cudaEvent_t ev_in = ev[2 + 2 * used], ev_done = ev[3 + 2 * used];
+        cudaEvent_t ev_in = ev[2 + 2 * blk], ev_done = ev[3 + 2 * blk];
         // op(B)[:, j0 : j0 + w] is columns j0.. of B ('N') or rows j0.. of B ('T')
         if (hb) {
             if (is_n(tb))
-                MBG_CUDA(cudaMemcpy2DAsync(const_cast<T*>(db) + j0 * dldb, size_t(dldb) * e, b + j0 * ldb,
-                                           size_t(ldb) * e, size_t(k) * e, size_t(w), cudaMemcpyHostToDevice, sin));
+                MBG_TRY(copy_h2d_2d(const_cast<T*>(db) + j0 * dldb, size_t(dldb) * e, b + j0 * ldb, size_t(ldb) * e,
+                                    size_t(k) * e, size_t(w), sin));
             else
-                MBG_CUDA(cudaMemcpy2DAsync(const_cast<T*>(db) + j0, size_t(dldb) * e, b + j0, size_t(ldb) * e,
-                                           size_t(w) * e, size_t(k), cudaMemcpyHostToDevice, sin));
+                MBG_TRY(copy_h2d_2d(const_cast<T*>(db) + j0, size_t(dldb) * e, b + j0, size_t(ldb) * e,
+                                    size_t(w) * e, size_t(k), sin));
         }
         if (hc && beta != T(0))
-            MBG_CUDA(cudaMemcpy2DAsync(dc + j0 * dldc, size_t(dldc) * e, c + j0 * ldc, size_t(ldc) * e,
-                                       size_t(m) * e, size_t(w), cudaMemcpyHostToDevice, sin));
+            MBG_TRY(copy_h2d_2d(dc + j0 * dldc, size_t(dldc) * e, c + j0 * ldc, size_t(ldc) * e, size_t(m) * e,
+                                size_t(w), sin));
         MBG_CUDA(cudaEventRecord(ev_in, sin));
         MBG_CUDA(cudaStreamWaitEvent(s, ev_in, 0));
         const T* bj = is_n(tb) ? db + j0 * dldb : db + j0;
@@ -240,12 +305,24 @@ static int gemm_host_pipelined(int mode, int slices, char ta, char tb, i64 m, i6
                                  dldc);
         }
         MBG_CUDA(cudaEventRecord(ev_done, s));
-        if (hc) {
-            MBG_CUDA(cudaStreamWaitEvent(sout, ev_done, 0));
-            MBG_CUDA(cudaMemcpy2DAsync(c + j0 * ldc, size_t(ldc) * e, dc + j0 * dldc, size_t(dldc) * e,
-                                       size_t(m) * e, size_t(w), cudaMemcpyDeviceToHost, sout));
+        if (hc && !c_pageable) MBG_TRY(copy_out_block(int(blk)));
+        if (c_pageable) {
+            {
+                std::lock_guard<std::mutex> lk(out_mu);
+                recorded = int(blk) + 1;
+            }
+            out_cv.notify_all();
         }
         j0 += w;
+    }
+    if (out_thread.joinable()) {
+        if (st) {
+            std::lock_guard<std::mutex> lk(out_mu);
+            abort_out = true;
+        }
+        out_cv.notify_all();
+        out_thread.join();
+        if (!st) st = out_st;
     }
     MBG_CUDA(cudaEventRecord(ev_end, sout));
     MBG_CUDA(cudaStreamWaitEvent(s, ev_end, 0));  // the library stream completes after the last copy back

@@ -169,11 +169,20 @@ int num_sms() {
 struct mbg_plan {
     int kind = 0;  // 1 sgemm, 2 strsm
     void* table = nullptr;                 // device problem table
-    unsigned long long* counter = nullptr;  // device tile counter (sgemm)
+    unsigned long long* counter = nullptr;  // device tile counter
     int count = 0;
     i64 total = 0;       // tiles (sgemm) or columns (strsm)
     int tile = 64;
     int grid = 0;
+    // sgemm, plain form: the problems whose size class takes 128-tiles (the 64-tile ones are above)
+    void* table128 = nullptr;
+    unsigned long long* counter128 = nullptr;
+    int count128 = 0;
+    i64 total128 = 0;
+    int grid128 = 0;
+    // sgemm, split forms (BF16x3 / BF16x6): the tensor-core grouped kernel
+    bool tc = false;
+    mbg::GroupedTcPlan tcp;
     void* items = nullptr;  // strsm: (problem, strip) work items, inside the table allocation
     int nitems = 0;
     size_t smem = 0;        // strsm: dynamic shared memory per CTA
@@ -188,15 +197,22 @@ namespace {
 // Enqueues the plan's work on stream s (the capture stream: the library stream that
 // other host threads may be using is never touched).
 int enqueue_plan(mbg_plan* p, cudaStream_t s) {
+    if (p->kind == 1 && p->tc) return grouped_tc_enqueue(p->tcp, s);
     if (p->kind == 1) {
-        MBG_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
-        if (p->tile == 128)
-            grouped_sgemm_kernel<128><<<p->grid, GT_NT, f32t::f32_smem<128>(), s>>>(static_cast<const GemmDesc*>(p->table), p->count,
-                                                                p->total, p->counter);
-        else
-            grouped_sgemm_kernel<64><<<p->grid, GT_NT, f32t::f32_smem<64>(), s>>>(static_cast<const GemmDesc*>(p->table), p->count,
-                                                               p->total, p->counter);
-        return check_launch("grouped_sgemm");
+        // the 128-tile problems (the larger size classes) first, the 64-tile ones behind them
+        if (p->count128 > 0) {
+            MBG_CUDA(cudaMemsetAsync(p->counter128, 0, sizeof(unsigned long long), s));
+            grouped_sgemm_kernel<128><<<p->grid128, GT_NT, f32t::f32_smem<128>(), s>>>(
+                static_cast<const GemmDesc*>(p->table128), p->count128, p->total128, p->counter128);
+            MBG_TRY(check_launch("grouped_sgemm"));
+        }
+        if (p->count > 0) {
+            MBG_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
+            grouped_sgemm_kernel<64><<<p->grid, GT_NT, f32t::f32_smem<64>(), s>>>(
+                static_cast<const GemmDesc*>(p->table), p->count, p->total, p->counter);
+            MBG_TRY(check_launch("grouped_sgemm"));
+        }
+        return MBG_OK;
     }
     MBG_CUDA(cudaMemsetAsync(p->counter, 0, sizeof(unsigned long long), s));
     grouped_block_strsm_kernel<<<p->grid, bs::BS_THREADS, p->smem, s>>>(
@@ -243,10 +259,7 @@ extern "C" {
 int mbg_sgemm_grouped_plan(int mode, int count, const mbg_sgemm_problem* probs, mbg_plan** out) {
     if (!out) return MBG_ERR_INVALID_MODE;
     *out = nullptr;
-    if (mode != MBG_MODE_PLAIN) {
-        set_error_msg("grouped sgemm: only MBG_MODE_PLAIN is implemented");
-        return MBG_ERR_UNSUPPORTED;
-    }
+    if (mode != MBG_MODE_PLAIN && mode != MBG_MODE_BF16X3 && mode != MBG_MODE_BF16X6) return MBG_ERR_INVALID_MODE;
     if (count < 0 || (count > 0 && !probs)) return MBG_ERR_INVALID_MODE;
     for (int i = 0; i < count; ++i) {  // argument checks per problem, numbered as gemm numbers them
         const mbg_sgemm_problem& q = probs[i];
@@ -271,64 +284,79 @@ int mbg_sgemm_grouped_plan(int mode, int count, const mbg_sgemm_problem* probs, 
             return MBG_ERR_UNSUPPORTED;
         }
     }
-    const int tile = tuning().grouped_gemm_tile == 128 ? 128 : 64;
+    if (mode != MBG_MODE_PLAIN) {  // split forms: one tensor-core kernel over every problem
+        mbg_plan* p = new mbg_plan();
+        p->kind = 1;
+        p->tc = true;
+        int st = grouped_tc_build(mode == MBG_MODE_BF16X6 ? 3 : 2, count, probs, p->tcp);
+        p->count = p->tcp.count;
+        if (!st && p->tcp.ntiles > 0) st = capture_plan(p);
+        if (st) {
+            mbg_plan_destroy(p);
+            return st;
+        }
+        *out = p;
+        return MBG_OK;
+    }
+    // plain form: each problem's tile edge from its size class in the tuning table, the
+    // largest problems first within each tile size (the tail of the schedule is short tiles)
     std::vector<int> order(count);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
         const double cx = double(probs[x].m) * probs[x].n * imax(probs[x].k, 1);
         const double cy = double(probs[y].m) * probs[y].n * imax(probs[y].k, 1);
-        return cx > cy;  // largest first: the tail of the schedule is short tiles
+        return cx > cy;
     });
-    std::vector<GemmDesc> v;
-    v.reserve(count);
-    i64 tiles = 0;
+    std::vector<GemmDesc> v[2];  // [0]: 64-tiles, [1]: 128-tiles
+    i64 tiles[2] = {0, 0};
     for (int idx : order) {
         const mbg_sgemm_problem& q = probs[idx];
         if (q.m == 0 || q.n == 0) continue;
+        const int tile = grouped_simt_tile(q.m, q.n, is_t(q.trans_a), is_t(q.trans_b));
+        const int w = tile == 128 ? 1 : 0;
         GemmDesc d{};
         d.m = q.m; d.n = q.n; d.k = q.k; d.lda = q.lda; d.ldb = q.ldb; d.ldc = q.ldc;
         d.a = q.a; d.b = q.b; d.c = q.c; d.alpha = q.alpha; d.beta = q.beta;
         d.ta = is_t(q.trans_a); d.tb = is_t(q.trans_b);
         d.tiles_m = int(cdiv(q.m, tile));
-        d.tile0 = tiles;
-        tiles += i64(d.tiles_m) * cdiv(q.n, tile);
-        v.push_back(d);
+        d.tile0 = tiles[w];
+        tiles[w] += i64(d.tiles_m) * cdiv(q.n, tile);
+        v[w].push_back(d);
     }
     mbg_plan* p = new mbg_plan();
     p->kind = 1;
-    p->count = int(v.size());
-    p->total = tiles;
-    p->tile = tile;
-    int per_sm = 1;
+    p->count = int(v[0].size());
+    p->total = tiles[0];
+    p->count128 = int(v[1].size());
+    p->total128 = tiles[1];
+    int per_sm64 = 1, per_sm128 = 1;
     // dynamic shared memory above 48 KB needs the opt-in before the occupancy query and the launch
-    if (tile == 128) {
-        cudaFuncSetAttribute(grouped_sgemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(f32t::f32_smem<128>()));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<128>, GT_NT,
-                                                      f32t::f32_smem<128>());
-    } else {
-        cudaFuncSetAttribute(grouped_sgemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(f32t::f32_smem<64>()));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_sgemm_kernel<64>, GT_NT,
-                                                      f32t::f32_smem<64>());
-    }
+    cudaFuncSetAttribute(grouped_sgemm_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(f32t::f32_smem<128>()));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm128, grouped_sgemm_kernel<128>, GT_NT,
+                                                  f32t::f32_smem<128>());
+    cudaFuncSetAttribute(grouped_sgemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(f32t::f32_smem<64>()));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm64, grouped_sgemm_kernel<64>, GT_NT, f32t::f32_smem<64>());
     cudaGetLastError();
-    p->grid = int(imax(1, imin(tiles, i64(num_sms()) * imax(per_sm, 1))));
+    p->grid = int(imax(1, imin(tiles[0], i64(num_sms()) * imax(per_sm64, 1))));
+    p->grid128 = int(imax(1, imin(tiles[1], i64(num_sms()) * imax(per_sm128, 1))));
     int st = MBG_OK;
-    if (p->count > 0) {
-        st = upload(p, v);
-        if (!st) {
-            if (cudaMalloc(&p->counter, sizeof(unsigned long long)) != cudaSuccess) {
-                set_error("cudaMalloc(grouped counter)", cudaGetLastError());
-                st = MBG_ERR_ALLOC;
-            }
-        }
-        if (!st) st = capture_plan(p);
-    }
+    auto upload_part = [&](const std::vector<GemmDesc>& vv, void** table, unsigned long long** counter) -> int {
+        if (vv.empty()) return MBG_OK;
+        MBG_CUDA(cudaMalloc(table, sizeof(GemmDesc) * vv.size()));
+        MBG_CUDA(cudaMemcpy(*table, vv.data(), sizeof(GemmDesc) * vv.size(), cudaMemcpyHostToDevice));
+        MBG_CUDA(cudaMalloc(reinterpret_cast<void**>(counter), sizeof(unsigned long long)));
+        return MBG_OK;
+    };
+    st = upload_part(v[0], &p->table, &p->counter);
+    if (!st) st = upload_part(v[1], &p->table128, &p->counter128);
+    if (!st && (p->count + p->count128) > 0) st = capture_plan(p);
     if (st) {
         mbg_plan_destroy(p);
         return st;
     }
+    p->count += p->count128;
     *out = p;
     return MBG_OK;
 }
@@ -430,7 +458,7 @@ int mbg_strsm_grouped_plan(int mode, int count, const mbg_strsm_problem* probs, 
 int mbg_plan_execute(mbg_plan* p) {
     if (!p) return MBG_ERR_INVALID_MODE;
     if (p->count == 0) return MBG_OK;
-    ProfScope prof(p->kind == 1 ? "grouped_sgemm" : "grouped_strsm");
+    ProfScope prof(p->kind == 1 ? (p->tc ? "grouped_sgemm_tc" : "grouped_sgemm") : "grouped_strsm");
     MBG_CUDA(cudaGraphLaunch(p->exec, stream()));
     count_launch(1);
     return finish_call(false);
@@ -442,6 +470,9 @@ int mbg_plan_destroy(mbg_plan* p) {
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->table) cudaFree(p->table);
     if (p->counter) cudaFree(p->counter);
+    if (p->table128) cudaFree(p->table128);
+    if (p->counter128) cudaFree(p->counter128);
+    grouped_tc_free(p->tcp);
     delete p;
     return MBG_OK;
 }

@@ -104,6 +104,17 @@ struct Operand {
     int finish();  // copies back if staged && copy_out
 };
 bool is_device_pointer(const void* p);
+bool is_pinned_host(const void* p);  // page-locked host memory (cudaHostAlloc / cudaHostRegister)
+// Host <-> device 2-D copies (width bytes x height rows, pitches in bytes; staging.cu).
+// Pageable host memory goes through page-locked bounce buffers, packed / unpacked by
+// host threads while the DMAs of neighbouring chunks run; pinned memory is copied
+// directly on s.  copy_h2d_2d: ordered after the work on s, and later work on s sees
+// the data.  copy_d2h_2d: ordered after `after` (or, if null, the work on s); for
+// pageable dst it returns when the data is there, for pinned dst it enqueues on s.
+int copy_h2d_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
+                cudaStream_t s);
+int copy_d2h_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
+                cudaStream_t s, cudaEvent_t after);
 
 // ---- timing of library kernels (optional) ------------------------------------
 struct ProfScope {
@@ -127,10 +138,46 @@ struct Tuning {
     i64 trsm_leaf_ctas = 0;      // CTA cap of the trsm diagonal-block solve (0: 8 per SM)
     i64 trsm_block_rows = 512;   // diagonal blocks solved in one fused launch (<= 64: leaves + gemm)
     i64 trsm_block_min_cols = 64;    // ... when there are at least this many right-hand sides
+    i64 trsm_inverse_min_cols = 256;  // split / Ozaki trsm: inverted diagonal blocks from this many
+                                      // right-hand sides (0: never; substitution leaves instead)
     i64 plain_fp64_simt = 0;     // 1: plain FP64 gemm/syrk on the CUDA cores instead of the FP64 tensor pipe
     i64 plain_fp32_staged = 0;   // 1: plain FP32 128-tiles staged through registers (the earlier kernel)
+    i64 ozaki_cta_pair = 0;      // 1: Ozaki products on CTA pairs (tcgen05 cta_group::2); 0: one CTA per tile
+    // grouped sgemm plans, per transposes (NN, NT, TN, TT) and size class (grouped_size_class):
+    // tile edge of the plain form (64 / 128) and tile width of the split form (64 / 128); 0 = default
+    i64 grouped_simt_tile[4][5] = {};
+    i64 grouped_tc_bn[4][5] = {};
 };
 Tuning& tuning();
+
+// Size class of a grouped gemm problem by max(m, n): <= 32, <= 64, <= 128, <= 256, larger.
+inline int grouped_size_class(i64 m, i64 n) {
+    const i64 x = imax(m, n);
+    return x <= 32 ? 0 : x <= 64 ? 1 : x <= 128 ? 2 : x <= 256 ? 3 : 4;
+}
+// Tile edge of the plain grouped sgemm for one problem (the class's entry, else grouped_gemm_tile).
+inline int grouped_simt_tile(i64 m, i64 n, int ta, int tb) {
+    const i64 v = tuning().grouped_simt_tile[ta * 2 + tb][grouped_size_class(m, n)];
+    if (v == 64 || v == 128) return int(v);
+    return tuning().grouped_gemm_tile == 128 ? 128 : 64;
+}
+// Tile width of the split grouped sgemm for one problem (the class's entry, else 64 for n <= 64).
+inline int grouped_tc_tile_cols(i64 m, i64 n, i64 k, int ta, int tb) {
+    (void)k;
+    const i64 v = tuning().grouped_tc_bn[ta * 2 + tb][grouped_size_class(m, n)];
+    if (v == 64 || v == 128) return int(v);
+    return n <= 64 ? 64 : 128;
+}
+// The tensor-core grouped sgemm (grouped_tc.cu): device table, launch, release.
+struct GroupedTcPlan {
+    int terms = 3;
+    void* table = nullptr;
+    int count = 0, ntiles = 0, grid = 0;
+    size_t tiles_off = 0;
+};
+int grouped_tc_build(int terms, int count, const mbg_sgemm_problem* probs, GroupedTcPlan& out);
+int grouped_tc_enqueue(const GroupedTcPlan& p, cudaStream_t s);
+void grouped_tc_free(GroupedTcPlan& p);
 
 // ---- banded reduction: one operand triangular --------------------------------
 // When op(A) (or op(B)) is a dense copy of a triangular matrix, zero outside its
@@ -238,6 +285,20 @@ struct SplitA {
 int split_a_planes(int terms, char ta, i64 m, i64 k, const float* a, i64 lda, SplitA& out);
 int sgemm_split_tc_with_a(const SplitA& A, char tb, i64 n, float alpha, const float* b, i64 ldb, float beta,
                           float* c, i64 ldc);
+// rows r0 .. r0 + mb - 1 of op(A) (r0 a multiple of 128) against a k x n op(B), k <= A.k
+int sgemm_split_tc_with_a_rows(const SplitA& A, i64 r0, i64 mb, i64 k, char tb, i64 n, float alpha, const float* b,
+                               i64 ldb, float beta, float* c, i64 ldc);
+// op(A)'s Ozaki slices and row exponents made once for several row-block products
+struct OzakiA {
+    Workspace ws;
+    int slices = 0;
+    i64 m = 0, k = 0, Mp = 0, Kp = 0;
+    int8_t* planes = nullptr;
+    int* e = nullptr;
+};
+int ozaki_slice_a(int slices, char ta, i64 m, i64 k, const double* a, i64 lda, OzakiA& out);
+int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n, double alpha, const double* b,
+                          i64 ldb, double beta, double* c, i64 ldc);
 
 // trsm and trmm on device operands (trsm.cu)
 template <typename T>

@@ -163,16 +163,14 @@ int Operand::prepare(const void* p, i64 r, i64 c, i64 l, size_t e, bool copy_in,
     dev_ld = r;
     MBG_TRY(ws.reserve(size_t(r) * size_t(c) * e));
     dev = ws.ptr;
-    if (copy_in)
-        MBG_CUDA(cudaMemcpy2DAsync(dev, size_t(r) * e, p, size_t(l) * e, size_t(r) * e, size_t(c),
-                                   cudaMemcpyHostToDevice, stream()));
+    if (copy_in) return copy_h2d_2d(dev, size_t(r) * e, p, size_t(l) * e, size_t(r) * e, size_t(c), stream());
     return MBG_OK;
 }
 
 int Operand::finish() {
     if (staged && copy_out)
-        MBG_CUDA(cudaMemcpy2DAsync(const_cast<void*>(user), size_t(ld) * elem, dev, size_t(rows) * elem,
-                                   size_t(rows) * elem, size_t(cols), cudaMemcpyDeviceToHost, stream()));
+        return copy_d2h_2d(const_cast<void*>(user), size_t(ld) * elem, dev, size_t(rows) * elem, size_t(rows) * elem,
+                           size_t(cols), stream(), nullptr);
     return MBG_OK;
 }
 
@@ -351,29 +349,53 @@ int mbg_prof_query(const char* sub, double* total_ms, int64_t* launches) {
 
 int64_t mbg_launch_count(void) { return g_launches.load(); }
 
+// "grouped_simt_tile_<TT>_c<d>" / "grouped_tc_bn_<TT>_c<d>": the per-class entry of a grouped
+// sgemm plan's tile table (TT = NN, NT, TN or TT, d = size class 0..4), or nullptr.
+static i64* grouped_class_entry(const std::string& k) {
+    i64 (*table)[5] = nullptr;
+    std::string rest;
+    if (k.rfind("grouped_simt_tile_", 0) == 0) { table = tuning().grouped_simt_tile; rest = k.substr(18); }
+    else if (k.rfind("grouped_tc_bn_", 0) == 0) { table = tuning().grouped_tc_bn; rest = k.substr(14); }
+    else return nullptr;
+    if (rest.size() != 5 || rest[2] != '_' || rest[3] != 'c' || rest[4] < '0' || rest[4] > '4') return nullptr;
+    const char a = rest[0], b = rest[1];
+    if ((a != 'N' && a != 'T') || (b != 'N' && b != 'T')) return nullptr;
+    return &table[(a == 'T' ? 2 : 0) + (b == 'T' ? 1 : 0)][rest[4] - '0'];
+}
+
 int mbg_set_tuning(const char* key, int64_t value) {
     if (!key) return MBG_ERR_INVALID_MODE;
     const std::string k(key);
+    if (i64* e = grouped_class_entry(k)) {
+        if (value == 0 || value == 64 || value == 128) { *e = value; return MBG_OK; }
+        set_error_msg("tuning value out of range: " + k + " = " + std::to_string(value));
+        return MBG_ERR_INVALID_MODE;
+    }
     if (k == "trsm_tc_min_k" && value >= 0) { tuning().trsm_tc_min_k = value; return MBG_OK; }
     if (k == "grouped_gemm_tile" && (value == 64 || value == 128)) { tuning().grouped_gemm_tile = value; return MBG_OK; }
     if (k == "trsm_leaf_ctas" && value >= 0) { tuning().trsm_leaf_ctas = value; return MBG_OK; }
     if (k == "trsm_block_rows" && value >= 0 && value <= 1024) { tuning().trsm_block_rows = value; return MBG_OK; }
     if (k == "trsm_block_min_cols" && value >= 0) { tuning().trsm_block_min_cols = value; return MBG_OK; }
+    if (k == "trsm_inverse_min_cols" && value >= 0) { tuning().trsm_inverse_min_cols = value; return MBG_OK; }
     if (k == "plain_fp64_simt" && (value == 0 || value == 1)) { tuning().plain_fp64_simt = value; return MBG_OK; }
     if (k == "plain_fp32_staged" && (value == 0 || value == 1)) { tuning().plain_fp32_staged = value; return MBG_OK; }
+    if (k == "ozaki_cta_pair" && (value == 0 || value == 1)) { tuning().ozaki_cta_pair = value; return MBG_OK; }
     set_error_msg("unknown tuning key or value: " + k + " = " + std::to_string(value));
     return MBG_ERR_INVALID_MODE;
 }
 
 int64_t mbg_get_tuning(const char* key) {
     const std::string k(key ? key : "");
+    if (const i64* e = grouped_class_entry(k)) return *e;
     if (k == "trsm_tc_min_k") return tuning().trsm_tc_min_k;
     if (k == "grouped_gemm_tile") return tuning().grouped_gemm_tile;
     if (k == "trsm_leaf_ctas") return tuning().trsm_leaf_ctas;
     if (k == "trsm_block_rows") return tuning().trsm_block_rows;
     if (k == "trsm_block_min_cols") return tuning().trsm_block_min_cols;
+    if (k == "trsm_inverse_min_cols") return tuning().trsm_inverse_min_cols;
     if (k == "plain_fp64_simt") return tuning().plain_fp64_simt;
     if (k == "plain_fp32_staged") return tuning().plain_fp32_staged;
+    if (k == "ozaki_cta_pair") return tuning().ozaki_cta_pair;
     return -1;
 }
 

@@ -39,6 +39,7 @@
 // thread records an error code in the library's mapped error flag and the CTA
 // proceeds to teardown (TMEM is always freed).
 #include "mbg_internal.cuh"
+#include "tc_ptx.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -48,156 +49,6 @@
 namespace mbg {
 
 namespace tc {
-
-constexpr int BM = 128;
-constexpr uint64_t WAIT_LIMIT_NS = 2000000000ull;
-
-// ---------------------------------------------------------------------------
-// PTX wrappers
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ uint64_t globaltimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int site,
-                                          uint64_t limit_ns = WAIT_LIMIT_NS) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = globaltimer();
-    while (true) {
-#pragma unroll 1
-        for (int i = 0; i < 256; ++i)
-            if (mbar_try_wait(bar, parity)) return true;
-        if (globaltimer() - t0 > limit_ns) {
-            if (err) {
-                atomicExch(err, 1);
-                atomicExch(err + 1, site);
-            }
-            return false;
-        }
-    }
-}
-__device__ __forceinline__ void fence_barrier_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0,
-                                            int c1, int c2) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
-    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
-}
-__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
-                 "r"(ncols)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_relinquish() {
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-// COLLECTOR: 0 = read A from shared memory only, 1 = fill the tensor core's A
-// collector buffer, 2 = reuse it, 3 = reuse it for the last time.  Consecutive
-// MMAs with the same A tile (Ozaki products A_p B_q for one p) read A once.
-#define MBG_UMMA(KIND, COL)                                                        \
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"                \
-                 "tcgen05.mma.cta_group::1.kind::" KIND COL " [%0], %1, %2, %3, p;\n\t}" \
-                 ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)  \
-                 : "memory")
-template <bool INT8>
-__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                     uint32_t accumulate, int collector = 0) {
-    if (INT8) {
-        if (collector == 1) MBG_UMMA("i8", ".collector::a::fill");
-        else if (collector == 2) MBG_UMMA("i8", ".collector::a::use");
-        else if (collector == 3) MBG_UMMA("i8", ".collector::a::lastuse");
-        else MBG_UMMA("i8", "");
-    } else {
-        MBG_UMMA("f16", "");
-    }
-}
-#undef MBG_UMMA
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_ld_wait() {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// Shared-memory matrix descriptor (tcgen05), K-major operand with swizzle:
-// start address and stride-dimension byte offset (between 8-row groups) in
-// 16-byte units, descriptor version 1 (bits 46-47), layout type in bits 61-63
-// (2 = 128-byte swizzle, 4 = 64-byte, 6 = 32-byte).  Tiles are 1024-byte
-// aligned so the base-offset field stays 0.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t sbo_bytes, uint32_t layout) {
-    uint64_t d = 0;
-    d |= uint64_t((saddr >> 4) & 0x3FFFu);
-    d |= uint64_t(1) << 16;  // leading byte offset: unused for swizzled K-major tiles
-    d |= uint64_t((sbo_bytes >> 4) & 0x3FFFu) << 32;
-    d |= uint64_t(1) << 46;
-    d |= uint64_t(layout & 7u) << 61;
-    return d;
-}
-
-// Instruction descriptor: D format (bits 4-5: 1 = f32, 2 = s32), A/B formats
-// (bits 7-9 / 10-12: bf16 = 1 for kind::f16, signed = 1 for kind::i8), both
-// operands K-major (bits 15/16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
-__host__ __device__ constexpr uint32_t instr_desc(bool int8, int M, int N) {
-    return (uint32_t(int8 ? 2 : 1) << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) |
-           (uint32_t(M >> 4) << 24);
-}
-
-// 2^e as a double: built from the exponent bits in the normal range (exact, no
-// libm call), ldexp outside it.
-__device__ __forceinline__ double pow2_exact(int e) {
-    if (e >= -1022 && e <= 1023) return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
-    return ldexp(1.0, e);
-}
 
 // ---------------------------------------------------------------------------
 // Kernel configuration
@@ -262,44 +113,6 @@ struct Params {
     const int* eb;  // ozaki column exponents (op(B) columns)
     int* err;
 };
-
-// Product table, index -> (p, q) and collector use.
-//   split: ordered by descending p+q so small contributions enter the fp32
-//          accumulator first;
-//   ozaki: ordered by p (A slice), q ascending, so the products that share A_p
-//          run back to back and reuse it from the collector buffer; the first
-//          product into diagonal d is then (0, d).
-template <int TERMS, bool OZAKI>
-__device__ __forceinline__ void product(int idx, int& p, int& q, int& collector) {
-    collector = 0;
-    if (OZAKI) {
-        int t = 0;
-        for (int pp = 0; pp < TERMS; ++pp) {
-            const int cnt = TERMS - pp;  // q = 0 .. TERMS-1-pp
-            if (idx < t + cnt) {
-                p = pp;
-                q = idx - t;
-                if (cnt > 1) collector = (q == 0) ? 1 : (q == cnt - 1 ? 3 : 2);
-                return;
-            }
-            t += cnt;
-        }
-        p = q = 0;
-        return;
-    }
-    int t = 0;
-    for (int d = TERMS - 1; d >= 0; --d) {
-        for (int pp = 0; pp <= d; ++pp) {
-            if (t == idx) { p = pp; q = d - pp; return; }
-            ++t;
-        }
-    }
-    p = q = 0;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 
 template <class C>
 __global__ void __launch_bounds__(C::THREADS, 1)
@@ -625,6 +438,64 @@ __device__ __forceinline__ bool oz_mma_pass(const OzParams& P, int nkb, uint8_t*
     return true;
 }
 
+// Row `row` of the tile's output, columns cbase .. cbase + EPI_COLS - 1: scales the
+// fp64 sums by the row and column exponents and applies alpha / beta (or the
+// trmm diagonal term), as one epilogue thread of either Ozaki kernel owns them.
+template <class C>
+__device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cbase, const double (&acc)[C::EPI_COLS]) {
+    const int er = P.ea[row];
+    // beta == 1: reductions in L2, as in the split kernel's epilogue; else
+    // 4 columns at a time, loads first (the 64 fp64 accumulators leave
+    // room for no more)
+    if (P.dvec) {  // trmm: C = alpha acc + d C, d per row or per column
+        const double drow = P.dvec_mode == 1 ? P.dvec[row] : 0.0;
+#pragma unroll
+        for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+            double cv[4];
+            int ec[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const i64 col = cbase + c0 + j;
+                ec[j] = col < P.n ? P.eb[col] : 0;
+                cv[j] = col < P.n ? P.c[row + col * P.ldc] : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const i64 col = cbase + c0 + j;
+                if (col >= P.n) continue;
+                const double d = P.dvec_mode == 1 ? drow : P.dvec[col];
+                P.c[row + col * P.ldc] = fma(d, cv[j], P.alpha * (acc[c0 + j] * pow2_exact(er + ec[j])));
+            }
+        }
+    } else if (P.beta == 1.0) {
+#pragma unroll
+        for (int j = 0; j < C::EPI_COLS; ++j) {
+            const i64 col = cbase + j;
+            const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
+            if (live) atomicAdd(P.c + row + col * P.ldc, P.alpha * (acc[j] * pow2_exact(er + P.eb[col])));
+        }
+    } else
+#pragma unroll
+    for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+        double cv[4];
+        int ec[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const i64 col = cbase + c0 + j;
+            const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
+            ec[j] = live ? P.eb[col] : 0;
+            cv[j] = (live && P.beta != 0.0) ? P.c[row + col * P.ldc] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const i64 col = cbase + c0 + j;
+            if (col >= P.n || (P.tri == 1 && row < col) || (P.tri == 2 && row > col)) continue;
+            const double v = P.alpha * (acc[c0 + j] * pow2_exact(er + ec[j]));
+            P.c[row + col * P.ldc] = (P.beta == 0.0) ? v : fma(P.beta, cv[j], v);
+        }
+    }
+}
+
 template <class C>
 __global__ void __launch_bounds__(C::THREADS, 1)
 ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -741,60 +612,7 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
             __syncwarp();
             if (lane == 0) mbar_arrive(tempty);
         }
-        if (ok && row < P.m) {
-            const int er = P.ea[row];
-            const i64 cbase = n0 + part * C::EPI_COLS;
-            // beta == 1: reductions in L2, as in the split kernel's epilogue; else
-            // 4 columns at a time, loads first (the 64 fp64 accumulators leave
-            // room for no more)
-            if (P.dvec) {  // trmm: C = alpha acc + d C, d per row or per column
-                const double drow = P.dvec_mode == 1 ? P.dvec[row] : 0.0;
-#pragma unroll
-                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
-                    double cv[4];
-                    int ec[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const i64 col = cbase + c0 + j;
-                        ec[j] = col < P.n ? P.eb[col] : 0;
-                        cv[j] = col < P.n ? P.c[row + col * P.ldc] : 0.0;
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const i64 col = cbase + c0 + j;
-                        if (col >= P.n) continue;
-                        const double d = P.dvec_mode == 1 ? drow : P.dvec[col];
-                        P.c[row + col * P.ldc] = fma(d, cv[j], P.alpha * (acc[c0 + j] * pow2_exact(er + ec[j])));
-                    }
-                }
-            } else if (P.beta == 1.0) {
-#pragma unroll
-                for (int j = 0; j < C::EPI_COLS; ++j) {
-                    const i64 col = cbase + j;
-                    const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
-                    if (live) atomicAdd(P.c + row + col * P.ldc, P.alpha * (acc[j] * pow2_exact(er + P.eb[col])));
-                }
-            } else
-#pragma unroll
-            for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
-                double cv[4];
-                int ec[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const i64 col = cbase + c0 + j;
-                    const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
-                    ec[j] = live ? P.eb[col] : 0;
-                    cv[j] = (live && P.beta != 0.0) ? P.c[row + col * P.ldc] : 0.0;
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const i64 col = cbase + c0 + j;
-                    if (col >= P.n || (P.tri == 1 && row < col) || (P.tri == 2 && row > col)) continue;
-                    const double v = P.alpha * (acc[c0 + j] * pow2_exact(er + ec[j]));
-                    P.c[row + col * P.ldc] = (P.beta == 0.0) ? v : fma(P.beta, cv[j], v);
-                }
-            }
-        }
+        if (ok && row < P.m) oz_store_row<C>(P, row, n0 + part * C::EPI_COLS, acc);
     }
     tc_fence_before();
     __syncthreads();
@@ -802,6 +620,283 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
         __syncwarp();
         tc_fence_after();
         tmem_dealloc(tmem, 512);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ozaki kernel over a CTA pair: 256 x 128 tiles, tcgen05.mma.cta_group::2
+// ---------------------------------------------------------------------------
+// The single-CTA kernel above is bound by shared-memory bandwidth: every
+// 128 x 128 x 32 int8 MMA (64 tensor-core cycles) reads a 4 KB B tile, and the
+// TMA writes of the planes come on top, about 130 B/clk per SM against the 128
+// the shared memory delivers.  Here two CTAs of a cluster (one per SM) share one
+// 256 x 128 output tile: each stages its own 128 rows of op(A) and its own half
+// (64 rows) of op(B)^T, and the leader CTA (rank 0) issues M = 256 MMAs that read
+// A from each CTA's own shared memory and each half of B from the CTA holding it,
+// so every B byte serves both SMs' tensor cores.  Per SM and k slab the planes
+// written fall from 88 KB to 66 KB and the MMA operand reads from about 130 KB
+// to 100 KB: about 93 B/clk at the full int8 rate.  Each CTA's TMEM holds the
+// accumulators of its own 128 rows (the same four diagonals, two passes for
+// more than four slices, as above).
+//   both CTAs   warp 0 lane 0 loads this CTA's planes (plain TMA, no multicast);
+//               the loads complete on the leader's mbarrier, which expects the
+//               bytes of both CTAs; warp 0 allocates TMEM for the pair
+//   leader      warp 1 lane 0 issues the MMAs; each stage's completion is
+//               committed to the stage's "empty" barrier in both CTAs, each
+//               pass's to the "accumulators ready" barrier in both CTAs
+//   both CTAs   warps 2..9 drain their own TMEM and signal the leader's
+//               "accumulators read" barrier (16 arrivals: 8 per CTA)
+// All waits are bounded as in the other kernels; a cluster barrier before
+// teardown keeps each CTA's barriers and TMEM alive until its peer is done.
+template <int S_>
+struct Oz2Cfg {
+    static constexpr int S = S_;
+    static constexpr int BN = 128;                    // output columns of the pair's tile
+    static constexpr int BNH = BN / 2;                // op(B)^T rows staged by each CTA
+    static constexpr int BKB = 32;
+    static constexpr int EPI_WARPS = 8;
+    static constexpr int THREADS = 64 + 32 * EPI_WARPS;
+    static constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // 64
+    static constexpr int NPASS = S <= 4 ? 1 : 2;
+    static constexpr int SPLIT = S <= 4 ? 0 : 4;
+    static constexpr int A_PLANE = BM * BKB;          // 4 KB
+    static constexpr int B_PLANE = BNH * BKB;         // 2 KB
+    static constexpr int STAGE_BYTES = S * (A_PLANE + B_PLANE);
+    static constexpr int STAGES = (196608 / STAGE_BYTES) > 8 ? 8 : (196608 / STAGE_BYTES);
+    // at least 120 KB, so one CTA per SM: two pairs interleaved on the same two SMs could
+    // each hold one SM's TMEM while waiting for the other's (the pair allocates together)
+    static constexpr int SMEM_USED = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr int SMEM_BYTES = SMEM_USED > 122880 ? SMEM_USED : 122880;
+    static constexpr uint32_t IDESC = instr_desc(true, 2 * BM, BN);  // M = 256 over the pair
+    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 6;
+    static_assert(STAGES >= 2, "pipeline depth");
+    static_assert(A_PLANE % 256 == 0 && B_PLANE % 256 == 0, "32-byte swizzle atoms stay aligned");
+};
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// shared::cluster address of the same variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(const void* p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_bar) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
+}
+// TMA load into this CTA's shared memory whose completion is counted on an
+// mbarrier of either CTA of the pair (the leader's); no multicast.
+__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* map, uint32_t cluster_bar, int c0,
+                                                 int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(cluster_bar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish_pair() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// Completion of the MMAs issued so far, arriving once on the barrier at this
+// address in both CTAs of the pair.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"((unsigned short)3)
+        : "memory");
+}
+#define MBG_UMMA2(COL)                                                                   \
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"                      \
+                 "tcgen05.mma.cta_group::2.kind::i8" COL " [%0], %1, %2, %3, p;\n\t}"    \
+                 ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)     \
+                 : "memory")
+__device__ __forceinline__ void umma_i8_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate, int collector) {
+    if (collector == 1) MBG_UMMA2(".collector::a::fill");
+    else if (collector == 2) MBG_UMMA2(".collector::a::use");
+    else if (collector == 3) MBG_UMMA2(".collector::a::lastuse");
+    else MBG_UMMA2("");
+}
+#undef MBG_UMMA2
+
+template <class C, int PASS>
+__device__ __forceinline__ bool oz2_mma_pass(const OzParams& P, int nkb, uint8_t* smem, uint64_t* full,
+                                             uint64_t* empty, uint64_t* tfull, uint64_t* tempty, uint32_t tmem) {
+    constexpr int LO = OzPass<C::S, PASS>::LO, HI = OzPass<C::S, PASS>::HI;
+    if (PASS > 0) {  // both CTAs' epilogues must have read the previous pass's accumulators
+        if (!mbar_wait(tempty, (PASS - 1) & 1, P.err, 23)) return false;
+        tc_fence_after();
+    }
+    for (int kb = 0; kb < nkb; ++kb) {
+        const int it = PASS * nkb + kb;
+        const int s = it % C::STAGES;
+        if (!mbar_wait(&full[s], (it / C::STAGES) & 1, P.err, 24)) return false;
+        tc_fence_after();
+        const uint32_t sa = smem_u32(smem + s * C::STAGE_BYTES);
+        const uint32_t sb = sa + C::S * C::A_PLANE;
+#pragma unroll
+        for (int pi = 0; pi < C::S * C::S; ++pi) {
+            int p = 0, q = 0, collector = 0;
+            if (!oz_product<C::S>(LO, HI, pi, p, q, collector)) break;
+            const uint32_t accumulate = (kb > 0 || p > 0) ? 1u : 0u;
+            const uint64_t ad = smem_desc(sa + p * C::A_PLANE, C::SBO, C::LAYOUT);
+            const uint64_t bd = smem_desc(sb + q * C::B_PLANE, C::SBO, C::LAYOUT);
+            umma_i8_pair(tmem + uint32_t((p + q - LO) * C::BN), ad, bd, C::IDESC, accumulate, collector);
+        }
+        umma_commit_pair(&empty[s]);  // stage s is free in both CTAs once these MMAs have read it
+    }
+    umma_commit_pair(tfull);  // this pass's accumulators are complete in both CTAs
+    return true;
+}
+
+template <class C>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(C::THREADS, 1)
+ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                  const __grid_constant__ CUtensorMap tmAlo, const __grid_constant__ CUtensorMap tmBlo, OzParams P) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+    uint64_t* empty = full + C::STAGES;
+    uint64_t* tfull = empty + C::STAGES;
+    uint64_t* tempty = tfull + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
+
+    const uint32_t rank = cluster_rank();  // 0: leader (issues the MMAs), 1: peer
+    // pair tiles of 256 x 128, groups of 8 pair rows walk the n-tiles together (L2 reuse)
+    const int tile = blockIdx.x >> 1;
+    const int tiles_m2 = (P.tiles_m + 1) >> 1;
+    const int group = 8;
+    const int per_group = group * P.tiles_n;
+    const int g = tile / per_group;
+    const int first_m = g * group;
+    const int gsize = min(group, tiles_m2 - first_m);
+    const int in_g = tile - g * per_group;
+    int tm = first_m + in_g % gsize, tn = in_g / gsize;
+    if (P.band == KB_A_LOWER) tm = tiles_m2 - 1 - tm;
+    if (P.band == KB_B_UPPER) tn = P.tiles_n - 1 - tn;
+    const i64 pm0 = i64(tm) * 2 * BM, n0 = i64(tn) * C::BN;
+    const i64 m0 = pm0 + i64(rank) * BM;  // this CTA's rows
+    // both CTAs decide the same, before any cluster-wide step
+    if (P.tri == 1 && pm0 + 2 * BM <= n0) return;
+    if (P.tri == 2 && pm0 > n0 + C::BN - 1) return;
+    int kb0 = 0, nkb = P.num_kb;
+    if (P.band != KB_NONE) {
+        i64 s0, s1;
+        band_slabs(P.band, pm0, 2 * BM, n0, C::BN, P.band_k0, C::BKB, P.num_kb, s0, s1);
+        kb0 = int(s0);
+        nkb = int(s1 - s0);
+    }
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(tfull, 1);
+        mbar_init(tempty, 2 * C::EPI_WARPS);
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc_pair(tmem_slot, 512);
+        tmem_relinquish_pair();
+    }
+    tc_fence_before();
+    cluster_sync_all();  // barriers of both CTAs initialised, TMEM of the pair allocated
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int total = C::NPASS * nkb;
+    const uint32_t leader_tempty = peer_addr(tempty, 0);
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer (both CTAs) ----------------
+            prefetch_tmap(&tmA);
+            prefetch_tmap(&tmB);
+            bool ok = true;
+            for (int it = 0; it < total; ++it) {
+                const int pass = it / nkb, kb = it - pass * nkb;
+                int lo, hi, planes;
+                pass_range<C>(pass, lo, hi, planes);
+                const int s = it % C::STAGES;
+                const uint32_t ph = (it / C::STAGES) & 1;
+                if (!mbar_wait(&empty[s], ph ^ 1, P.err, 21)) { ok = false; break; }
+                uint8_t* sa = smem + s * C::STAGE_BYTES;
+                uint8_t* sb = sa + C::S * C::A_PLANE;
+                if (rank == 0) mbar_expect_tx(&full[s], uint32_t(2 * planes * (C::A_PLANE + C::B_PLANE)));
+                const uint32_t bar = peer_addr(&full[s], 0);
+                const bool all = planes == C::S;
+                tma_load_3d_pair(sa, all ? &tmA : &tmAlo, bar, (kb0 + kb) * C::BKB, int(m0), 0);
+                tma_load_3d_pair(sb, all ? &tmB : &tmBlo, bar, (kb0 + kb) * C::BKB, int(n0 + rank * C::BNH), 0);
+            }
+            // the loads of the last stages land before the CTA may exit: the leader's MMAs
+            // release every stage to both CTAs only after reading it
+            if (ok)
+                for (int it = max(0, total - C::STAGES); it < total; ++it)
+                    mbar_wait(&empty[it % C::STAGES], (it / C::STAGES) & 1, P.err, 22);
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && rank == 0) {
+            // ---------------- MMA issuer (leader) ----------------
+            if (oz2_mma_pass<C, 0>(P, nkb, smem, full, empty, tfull, tempty, tmem) && C::NPASS > 1)
+                oz2_mma_pass<C, 1>(P, nkb, smem, full, empty, tfull, tempty, tmem);
+        }
+    } else {
+        // ---------------- epilogue warps (both CTAs, own rows) ----------------
+        const int e = warp - 2;
+        const int quarter = warp & 3;
+        const int part = e >> 2;
+        const i64 row = m0 + quarter * 32 + lane;
+        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(part * C::EPI_COLS);
+        double acc[C::EPI_COLS];
+#pragma unroll
+        for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0;
+        bool ok = true;
+        for (int pass = 0; pass < C::NPASS; ++pass) {
+            int lo, hi, planes;
+            pass_range<C>(pass, lo, hi, planes);
+            if (!mbar_wait(tfull, pass & 1, P.err, 25)) { ok = false; break; }
+            tc_fence_after();
+#pragma unroll 1
+            for (int d = hi - 1; d >= lo; --d) {  // smallest weight first
+                const double w = pow2_exact(-8 * d - 12);
+#pragma unroll
+                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(lane_base + uint32_t((d - lo) * C::BN + c0), r);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_remote(leader_tempty);
+        }
+        if (ok && row < P.m) oz_store_row<C>(P, row, n0 + part * C::EPI_COLS, acc);
+    }
+    tc_fence_before();
+    __syncwarp();
+    cluster_sync_all();  // the peer's epilogue and loads are done; no more remote barrier traffic
+    if (warp == 0) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc_pair(tmem, 512);
     }
 }
 
@@ -1042,9 +1137,11 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// 3-D map over planes[term][row][k]; box = {bkb/elem, box_rows, terms}.
+// 3-D map over planes[term][row][k]; box = {bkb/elem, box_rows, terms}.  The map covers
+// Rp rows of each plane starting at `base`; consecutive planes are plane_rows rows apart
+// (default Rp: a map over whole planes; more when it covers a row block of taller planes).
 int make_map(CUtensorMap* map, const void* base, bool int8, i64 Kp, i64 Rp, int terms, int bkb,
-             int box_rows) {
+             int box_rows, i64 plane_rows = 0) {
     auto fn = encode_fn();
     if (!fn) {
         set_error_msg("cuTensorMapEncodeTiled is unavailable from the driver");
@@ -1052,7 +1149,8 @@ int make_map(CUtensorMap* map, const void* base, bool int8, i64 Kp, i64 Rp, int 
     }
     const int elem = int8 ? 1 : 2;
     cuuint64_t dims[3] = {cuuint64_t(Kp), cuuint64_t(Rp), cuuint64_t(terms)};
-    cuuint64_t strides[2] = {cuuint64_t(Kp) * elem, cuuint64_t(Kp) * cuuint64_t(Rp) * elem};
+    if (plane_rows <= 0) plane_rows = Rp;
+    cuuint64_t strides[2] = {cuuint64_t(Kp) * elem, cuuint64_t(Kp) * cuuint64_t(plane_rows) * elem};
     cuuint32_t box[3] = {cuuint32_t(bkb / elem), cuuint32_t(box_rows), cuuint32_t(terms)};
     cuuint32_t estr[3] = {1, 1, 1};
     const CUtensorMapSwizzle sw = bkb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
@@ -1190,25 +1288,34 @@ int split_a_planes(int terms, char ta, i64 m, i64 k, const float* a, i64 lda, Sp
 // C[:, 0:n] := alpha op(A) op(B) + beta C with op(A)'s planes from split_a_planes (alpha != 0, k > 0).
 int sgemm_split_tc_with_a(const SplitA& A, char tb, i64 n, float alpha, const float* b, i64 ldb, float beta,
                           float* c, i64 ldc) {
+    return sgemm_split_tc_with_a_rows(A, 0, A.m, A.k, tb, n, alpha, b, ldb, beta, c, ldc);
+}
+
+// Rows r0 .. r0 + mb - 1 of op(A) (r0 a multiple of 128) times op(B) (k x n, k <= A.k; op(B)'s
+// rows k .. A.k - 1 are taken as zero): C[0:mb, 0:n] := alpha op(A)[r0:r0+mb, :] op(B) + beta C.
+int sgemm_split_tc_with_a_rows(const SplitA& A, i64 r0, i64 mb, i64 k, char tb, i64 n, float alpha, const float* b,
+                               i64 ldb, float beta, float* c, i64 ldc) {
     using namespace tc;
-    if (A.m == 0 || n == 0) return MBG_OK;
+    if (mb == 0 || n == 0) return MBG_OK;
+    if (r0 % BM || r0 + mb > A.m || k > A.k) return MBG_ERR_UNSUPPORTED;
     const int BN = 256;
     const i64 Np = roundup(n, BN);
     if (Np > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
     Workspace ws;
     MBG_TRY(ws.reserve(size_t(A.terms) * Np * A.Kp * 2));
     __nv_bfloat16* pb = ws.as<__nv_bfloat16>();
-    if (A.terms == 2) MBG_TRY(launch_split<2>(b, ldb, is_n(tb), n, A.k, Np, A.Kp, pb));
-    else MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, A.k, Np, A.Kp, pb));
-    CUtensorMap ma, mb;
-    MBG_TRY(make_map(&ma, A.ws.as<__nv_bfloat16>(), false, A.Kp, A.Mp, A.terms, 64, BM));
-    MBG_TRY(make_map(&mb, pb, false, A.Kp, Np, A.terms, 64, BN));
+    if (A.terms == 2) MBG_TRY(launch_split<2>(b, ldb, is_n(tb), n, k, Np, A.Kp, pb));
+    else MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, k, Np, A.Kp, pb));
+    CUtensorMap ma, mb_;
+    const i64 rows = imin(roundup(mb, BM), A.Mp - r0);
+    MBG_TRY(make_map(&ma, A.ws.as<__nv_bfloat16>() + size_t(r0) * A.Kp, false, A.Kp, rows, A.terms, 64, BM, A.Mp));
+    MBG_TRY(make_map(&mb_, pb, false, A.Kp, Np, A.terms, 64, BN));
     Params P{};
-    P.m = A.m; P.n = n; P.num_kb = int(A.Kp / 32);
-    P.tiles_m = int(cdiv(A.m, BM)); P.tiles_n = int(cdiv(n, BN));
+    P.m = mb; P.n = n; P.num_kb = int(A.Kp / 32);
+    P.tiles_m = int(cdiv(mb, BM)); P.tiles_n = int(cdiv(n, BN));
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
-    if (A.terms == 2) return launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
-    return launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
+    if (A.terms == 2) return launch_tc<CfgBF16x3>(ma, mb_, P, "tc_gemm_bf16x3");
+    return launch_tc<CfgBF16x6>(ma, mb_, P, "tc_gemm_bf16x6");
 }
 
 // ---- Ozaki dgemm ----------------------------------------------------------------
@@ -1230,11 +1337,98 @@ int launch_ozaki(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap
     ozaki_kernel<C><<<unsigned(tiles), C::THREADS, C::SMEM_BYTES, stream()>>>(ma, mb, mal, mbl, P);
     return check_launch("tc_gemm_ozaki");
 }
+
+template <class C>
+int launch_ozaki_pair(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mal, const CUtensorMap& mbl,
+                      OzParams& P) {
+    static std::atomic<unsigned> configured{0};  // one bit per device
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    if (!configured_on(configured, dev)) {
+        MBG_CUDA(cudaFuncSetAttribute(ozaki_pair_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      C::SMEM_BYTES));
+        mark_configured(configured, dev);
+    }
+    P.err = device_error_flag();
+    const i64 ctas = 2 * i64((P.tiles_m + 1) / 2) * P.tiles_n;
+    if (ctas > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    ProfScope prof("tc_gemm_ozaki");
+    ozaki_pair_kernel<C><<<unsigned(ctas), C::THREADS, C::SMEM_BYTES, stream()>>>(ma, mb, mal, mbl, P);
+    return check_launch("tc_gemm_ozaki");
+}
+
+// Tensor maps over the slices of op(A) (a_rows rows from pa, planes a_plane_rows
+// rows apart) and of op(B)^T (Np rows, Kp bytes of k each), then the Ozaki
+// launch: the CTA-pair kernel unless the tuning table selects the single-CTA one.
+int run_ozaki(int slices, const int8_t* pa, i64 a_rows, i64 a_plane_rows, const int8_t* pb, i64 Np, i64 Kp,
+              OzParams& P) {
+    const bool pair = tuning().ozaki_cta_pair != 0;
+    const int lo = slices <= 4 ? slices : 4;
+    const int bbox = pair ? 64 : 128;
+    CUtensorMap ma, mb, mal, mbl;
+    MBG_TRY(make_map(&ma, pa, true, Kp, a_rows, slices, 32, BM, a_plane_rows));
+    MBG_TRY(make_map(&mal, pa, true, Kp, a_rows, lo, 32, BM, a_plane_rows));
+    MBG_TRY(make_map(&mb, pb, true, Kp, Np, slices, 32, bbox));
+    MBG_TRY(make_map(&mbl, pb, true, Kp, Np, lo, 32, bbox));
+#define OZ_CASE(S_)                                                                    \
+    case S_:                                                                           \
+        return pair ? launch_ozaki_pair<Oz2Cfg<S_>>(ma, mb, mal, mbl, P)               \
+                    : launch_ozaki<OzCfg<S_>>(ma, mb, mal, mbl, P);
+    switch (slices) {
+        OZ_CASE(2) OZ_CASE(3) OZ_CASE(4) OZ_CASE(5) OZ_CASE(6) OZ_CASE(7)
+        default: OZ_CASE(8)
+    }
+#undef OZ_CASE
+}
 }  // namespace tc
 
 // Longest reduction one Ozaki launch takes: its int32 accumulators hold at most
 // `slices` products of K terms of at most 128^2 each; longer k runs in several launches.
 i64 ozaki_max_k(int slices) { return (i64(0x7fffffff) / (i64(slices) * 128 * 128)) / 32 * 32; }
+
+// op(A)'s Ozaki slices and row exponents made once, for several products with
+// row blocks of op(A) (the trsm's inverted diagonal blocks).  k must fit one launch.
+int ozaki_slice_a(int slices, char ta, i64 m, i64 k, const double* a, i64 lda, OzakiA& out) {
+    using namespace tc;
+    if (slices < 2 || slices > 8) return MBG_ERR_INVALID_MODE;
+    if (k > ozaki_max_k(slices) || k <= 0 || m <= 0) return MBG_ERR_UNSUPPORTED;
+    out.slices = slices;
+    out.m = m;
+    out.k = k;
+    out.Mp = roundup(m, BM);
+    out.Kp = roundup(k, 32);
+    const size_t pbytes = size_t(slices) * out.Mp * out.Kp;
+    MBG_TRY(out.ws.reserve(pbytes + sizeof(int) * size_t(out.Mp) + 1024));
+    out.planes = out.ws.as<int8_t>();
+    out.e = reinterpret_cast<int*>(out.planes + (pbytes + 1023) / 1024 * 1024);
+    return launch_slices(a, lda, is_t(ta), m, k, out.Mp, out.Kp, slices, out.e, out.planes);
+}
+
+// Rows r0 .. r0 + mb - 1 of op(A) from ozaki_slice_a (r0 a multiple of 128) times op(B) (k x n,
+// k <= A.k; op(B)'s rows k .. A.k - 1 taken as zero): C[0:mb, 0:n] := alpha op(A)[r0:r0+mb, :] op(B)
+// + beta C.  C may be op(B) itself: the kernel reads op(B) only through its slices.
+int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n, double alpha, const double* b,
+                          i64 ldb, double beta, double* c, i64 ldc) {
+    using namespace tc;
+    if (mb == 0 || n == 0) return MBG_OK;
+    if (r0 % BM || r0 + mb > A.m || k > A.k || k <= 0) return MBG_ERR_UNSUPPORTED;
+    const int slices = A.slices, BN = 128;
+    const i64 Np = roundup(n, BN);
+    const size_t b_bytes = size_t(slices) * Np * A.Kp;
+    Workspace ws;
+    MBG_TRY(ws.reserve(b_bytes + sizeof(int) * size_t(Np) + 1024));
+    int8_t* pb = ws.as<int8_t>();
+    int* eb = reinterpret_cast<int*>(pb + (b_bytes + 1023) / 1024 * 1024);
+    MBG_TRY(launch_slices(b, ldb, is_n(tb), n, k, Np, A.Kp, slices, eb, pb));
+    const i64 rows = imin(roundup(mb, BM), A.Mp - r0);
+    const int8_t* pa = A.planes + size_t(r0) * A.Kp;
+    OzParams P{};
+    P.m = mb; P.n = n; P.num_kb = int(A.Kp / 32);
+    P.tiles_m = int(cdiv(mb, BM)); P.tiles_n = int(cdiv(n, BN));
+    P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
+    P.ea = A.e + r0; P.eb = eb;
+    return run_ozaki(slices, pa, rows, A.Mp, pb, Np, A.Kp, P);
+}
 
 int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alpha, const double* a,
                    i64 lda, const double* b, i64 ldb, double beta, double* c, i64 ldc, char tri_uplo, int band,
@@ -1260,7 +1454,6 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
     int8_t* pb = shared_planes ? pa : pa + a_bytes;
     int* ea = reinterpret_cast<int*>(pa + a_bytes + b_bytes + (1024 - ((a_bytes + b_bytes) & 1023)) % 1024);
     int* eb = shared_planes ? ea : ea + Mp;
-    const int lo_planes = slices <= 4 ? slices : 4;
     for (i64 k0 = 0; k0 < k; k0 += kc) {
         const i64 klen = imin(kc, k - k0);
         const i64 Kpc = roundup(klen, 32);
@@ -1269,11 +1462,6 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
         const double* bk = is_n(tb) ? b + k0 : b + k0 * ldb;
         MBG_TRY(launch_slices(ak, lda, is_t(ta), m, klen, Mp, Kpc, slices, ea, pa, keep_a));
         if (!shared_planes) MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb, keep_b));
-        CUtensorMap ma, mb, mal, mbl;
-        MBG_TRY(make_map(&ma, pa, true, Kpc, Mp, slices, 32, BM));
-        MBG_TRY(make_map(&mb, pb, true, Kpc, Np, slices, 32, BN));
-        MBG_TRY(make_map(&mal, pa, true, Kpc, Mp, lo_planes, 32, BM));
-        MBG_TRY(make_map(&mbl, pb, true, Kpc, Np, lo_planes, 32, BN));
         OzParams P{};
         P.m = m; P.n = n; P.num_kb = int(Kpc / 32);
         P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
@@ -1286,17 +1474,7 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
         P.c = c; P.ldc = ldc; P.alpha = alpha;
         P.beta = (k0 == 0) ? beta : 1.0;
         P.ea = ea; P.eb = eb;
-        int st;
-        switch (slices) {
-            case 2: st = launch_ozaki<OzCfg<2>>(ma, mb, mal, mbl, P); break;
-            case 3: st = launch_ozaki<OzCfg<3>>(ma, mb, mal, mbl, P); break;
-            case 4: st = launch_ozaki<OzCfg<4>>(ma, mb, mal, mbl, P); break;
-            case 5: st = launch_ozaki<OzCfg<5>>(ma, mb, mal, mbl, P); break;
-            case 6: st = launch_ozaki<OzCfg<6>>(ma, mb, mal, mbl, P); break;
-            case 7: st = launch_ozaki<OzCfg<7>>(ma, mb, mal, mbl, P); break;
-            default: st = launch_ozaki<OzCfg<8>>(ma, mb, mal, mbl, P); break;
-        }
-        if (st) return st;
+        MBG_TRY(run_ozaki(slices, pa, Mp, Mp, pb, Np, Kpc, P));
     }
     return MBG_OK;
 }

@@ -385,27 +385,172 @@ int launch_copy(i64 m, i64 n, T alpha, const T* x, i64 ldx, T* y, i64 ldy) {
     return check_launch("copy");
 }
 
+// ---- inverted diagonal blocks (split / Ozaki modes) ---------------------------------
+// The split / Ozaki solve: every diagonal block of NBI rows is inverted once in the
+// input precision (fused block solves of the identity, all blocks in one launch), the
+// inverses' planes are made once, and the solve recurses as solve_left does, except that
+// each leaf is one product X_b = inv(op(A)_bb) B_b on the tensor cores instead of a
+// substitution.  So every flop of the solve runs in split / Ozaki products: the leaves'
+// pivot chains leave the critical path (MAGMA's inverted-diagonal-block trsm, with the
+// products in the precision mode).  The forward error of X_b = inv(A_bb) B_b is bounded like
+// the substitution's by cond(A_bb) times the working precision (triangular inverses,
+// Higham, Accuracy and Stability of Numerical Algorithms, ch. 8 and 14).
+
+// W (m x NBI, column-major, ldw): block b's rows r0 = b NBI .. r0 + nbb hold the nbb x nbb
+// identity in columns 0 .. nbb - 1, zeros elsewhere.
+template <typename T>
+__global__ void identity_blocks_kernel(i64 m, int nbi, T* __restrict__ W, i64 ldw) {
+    for (i64 j = blockIdx.y; j < nbi; j += gridDim.y)
+        for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x)
+            W[i + j * ldw] = (i % nbi == j) ? T(1) : T(0);
+}
+
+// W block b := inv(op(A)_bb): blockIdx.y = b, blockIdx.x = 32-column strip of the block.
+template <typename T, bool LOWER, bool TRANS, bool UNIT>
+__global__ void __launch_bounds__(BS_THREADS, 1)
+block_invert_kernel(i64 m, int nbi, const T* __restrict__ A, i64 lda, T* __restrict__ W, i64 ldw) {
+    extern __shared__ __align__(16) unsigned char bs_smem_raw[];
+    const i64 r0 = i64(blockIdx.y) * nbi;
+    const int nbb = int(min(i64(nbi), m - r0));
+    const i64 c0 = i64(blockIdx.x) * BS_COLS;
+    if (c0 >= nbb) return;
+    bs::block_solve_strip<T, LOWER, TRANS, UNIT, BS_COLS>(nbb, nbb, A + r0 + r0 * lda, lda, W + r0, ldw, c0, T(1),
+                                                          bs_smem_raw);
+}
+
+template <typename T>
+constexpr i64 inv_block_rows() { return 512; }  // <= bs_max_rows<T>() for both precisions
+
+template <typename T, bool L, bool TR, bool U>
+int launch_block_invert_t(i64 m, int nbi, const T* a, i64 lda, T* w, i64 ldw) {
+    auto kern = block_invert_kernel<T, L, TR, U>;
+    static std::atomic<unsigned> configured{0};  // one bit per device
+    int dev = 0;
+    MBG_CUDA(cudaGetDevice(&dev));
+    if (!configured_on(configured, dev)) {
+        MBG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bs_smem_bytes<T>(bs_max_rows<T>())));
+        mark_configured(configured, dev);
+    }
+    const dim3 g(unsigned(cdiv(nbi, BS_COLS)), unsigned(cdiv(m, nbi)));
+    kern<<<g, BS_THREADS, bs_smem_bytes<T>(nbi), stream()>>>(m, nbi, a, lda, w, ldw);
+    return check_launch("trsm_block_invert");
+}
+
+// W := the inverses of op(A)'s diagonal blocks of nbi rows, stacked (m x nbi, ld m).
+template <typename T>
+int invert_diagonal_blocks(bool lower, bool trans, bool unit, i64 m, int nbi, const T* a, i64 lda, T* w) {
+    ProfScope prof("trsm_block_invert");
+    {
+        dim3 g((unsigned)imin(cdiv(m, 256), 256), (unsigned)imin(nbi, 65535));
+        identity_blocks_kernel<T><<<g, 256, 0, stream()>>>(m, nbi, w, m);
+        MBG_TRY(check_launch("trsm_identity"));
+    }
+#define BIV(L, TR, U) return launch_block_invert_t<T, L, TR, U>(m, nbi, a, lda, w, m)
+    if (lower) {
+        if (trans) { if (unit) BIV(true, true, true); else BIV(true, true, false); }
+        else { if (unit) BIV(true, false, true); else BIV(true, false, false); }
+    } else {
+        if (trans) { if (unit) BIV(false, true, true); else BIV(false, true, false); }
+        else { if (unit) BIV(false, false, true); else BIV(false, false, false); }
+    }
+#undef BIV
+}
+
+// The inverses' planes (bf16 split terms or Ozaki slices), made once per solve.
+template <typename T> struct InvPlanes;
+template <> struct InvPlanes<float> {
+    SplitA p;
+    int make(int mode, int, i64 m, i64 nbi, const float* w) {
+        return split_a_planes(mode == MBG_MODE_BF16X6 ? 3 : 2, 'N', m, nbi, w, m, p);
+    }
+    // B[0:mb, :] := inv block (rows r0 .. r0 + mb of the stack) times B[0:mb, :]
+    int leaf(i64 r0, i64 mb, i64 n, float* b, i64 ldb) const {
+        return sgemm_split_tc_with_a_rows(p, r0, mb, mb, 'N', n, 1.0f, b, ldb, 0.0f, b, ldb);
+    }
+};
+template <> struct InvPlanes<double> {
+    OzakiA p;
+    int make(int, int slices, i64 m, i64 nbi, const double* w) { return ozaki_slice_a(slices, 'N', m, nbi, w, m, p); }
+    int leaf(i64 r0, i64 mb, i64 n, double* b, i64 ldb) const {
+        return dgemm_ozaki_tc_with_a(p, r0, mb, mb, 'N', n, 1.0, b, ldb, 0.0, b, ldb);
+    }
+};
+
+// op(A)[r:r+m, r:r+m] X = B (in place; b points at row r of B), leaves from the inverses.
+template <typename T>
+int solve_left_inv_rec(const InvPlanes<T>& inv, int mode, int slices, bool lower, bool trans, i64 r, i64 m, i64 n,
+                       const T* a, i64 lda, T* b, i64 ldb) {
+    const i64 nbi = inv_block_rows<T>();
+    if (m <= nbi) {
+        ProfScope prof("trsm_inverse_leaf");
+        return inv.leaf(r, m, n, b, ldb);
+    }
+    const i64 m1 = cdiv(cdiv(m, 2), nbi) * nbi, m2 = m - m1;
+    const char tc = trans ? 'T' : 'N';
+    const T* ar = a + r + r * lda;  // op(A)[r, r]
+    if (lower) {
+        MBG_TRY(solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r, m1, n, a, lda, b, ldb));
+        MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m2, n, m1, T(-1), op_at(ar, lda, trans, m1, 0), lda, b, ldb,
+                             T(1), b + m1, ldb));
+        return solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r + m1, m2, n, a, lda, b + m1, ldb);
+    }
+    MBG_TRY(solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r + m1, m2, n, a, lda, b + m1, ldb));
+    MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m1, n, m2, T(-1), op_at(ar, lda, trans, 0, m1), lda, b + m1, ldb,
+                         T(1), b, ldb));
+    return solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r, m1, n, a, lda, b, ldb);
+}
+
+// Whether the inverted-block solve runs: a split / Ozaki mode, more than one diagonal block,
+// and enough right-hand sides to repay the inversions (about NBI^2 / 3 multiply-adds per
+// row of A, against m n / 2 for the solve itself).
+template <typename T>
+bool use_inverse_solve(int mode, i64 m, i64 n) {
+    if (mode == MBG_MODE_PLAIN || tuning().trsm_inverse_min_cols <= 0) return false;
+    return m > inv_block_rows<T>() && n >= tuning().trsm_inverse_min_cols;
+}
+
+template <typename T>
+int solve_left_inv(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, const T* a, i64 lda,
+                   T* b, i64 ldb) {
+    const int nbi = int(inv_block_rows<T>());
+    Workspace ww;
+    MBG_TRY(ww.reserve(sizeof(T) * size_t(m) * size_t(nbi)));
+    MBG_TRY(invert_diagonal_blocks<T>(lower, trans, unit, m, nbi, a, lda, ww.as<T>()));
+    InvPlanes<T> inv;
+    MBG_TRY(inv.make(mode, slices, m, nbi, ww.as<T>()));
+    return solve_left_inv_rec<T>(inv, mode, slices, lower, trans, 0, m, n, a, lda, b, ldb);
+}
+
 int accurate_mode(float) { return MBG_MODE_BF16X6; }
 int accurate_mode(double) { return MBG_MODE_OZAKI; }
 
 // Left-side solve with optional refinement; B already holds alpha*B.
 template <typename T>
+int solve_left_any(int mode, int slices, bool lower, bool trans, bool unit, i64 m, i64 n, const T* a, i64 lda,
+                   T* b, i64 ldb) {
+    if (use_inverse_solve<T>(mode, m, n))
+        return solve_left_inv<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb);
+    return solve_left<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb);
+}
+
+template <typename T>
 int solve_left_refined(int mode, int slices, int refine, bool lower, bool trans, bool unit, i64 m,
                        i64 n, const T* a, i64 lda, T* b, i64 ldb) {
     if (refine <= 0 || mode == MBG_MODE_PLAIN)
-        return solve_left<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb);
+        return solve_left_any<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb);
     Workspace w_rhs, w_res;
     MBG_TRY(w_rhs.reserve(sizeof(T) * size_t(m) * size_t(n)));
     MBG_TRY(w_res.reserve(sizeof(T) * size_t(m) * size_t(n)));
     T* rhs = w_rhs.as<T>();
     T* res = w_res.as<T>();
     MBG_TRY(launch_copy<T>(m, n, T(1), b, ldb, rhs, m));
-    MBG_TRY(solve_left<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb));
+    MBG_TRY(solve_left_any<T>(mode, slices, lower, trans, unit, m, n, a, lda, b, ldb));
     const int acc_mode = accurate_mode(T(0));
     for (int it = 0; it < refine; ++it) {
         MBG_TRY(launch_copy<T>(m, n, T(1), rhs, m, res, m));
         MBG_TRY(residual_left<T>(acc_mode, 8, lower, trans, unit, m, n, a, lda, b, ldb, res, m));
-        MBG_TRY(solve_left<T>(mode, slices, lower, trans, unit, m, n, a, lda, res, m));
+        MBG_TRY(solve_left_any<T>(mode, slices, lower, trans, unit, m, n, a, lda, res, m));
         MBG_TRY(launch_axpy<T>(m, n, T(1), res, m, b, ldb));
     }
     return MBG_OK;

@@ -6,7 +6,8 @@ trmm.mojo:20; docs/reference.md:264-325): column-major storage with leading
 dimensions, Netlib transpose / uplo / side / diag characters, results written in
 place into `c` (gemm, syrk, symm, syr2k) or `b` (trsm, trmm).
 The dtype is taken from the buffers (float32 or float64), as the reference
-takes it from its `dtype` parameter.
+takes it from its `dtype` parameter; gemm also takes complex64 / complex128
+buffers (cgemm / zgemm, with trans 'C' the conjugate transpose).
 
 Buffers may be numpy arrays (host memory; the library stages the copies),
 torch tensors (host or CUDA) or raw integer addresses with an explicit dtype.
@@ -41,7 +42,8 @@ def _dtype_of(x, dtype=None):
     try:
         import torch
         if isinstance(x, torch.Tensor):
-            return {torch.float32: np.dtype(np.float32), torch.float64: np.dtype(np.float64)}[x.dtype]
+            return {torch.float32: np.dtype(np.float32), torch.float64: np.dtype(np.float64),
+                    torch.complex64: np.dtype(np.complex64), torch.complex128: np.dtype(np.complex128)}[x.dtype]
     except ImportError:
         pass
     raise TypeError("pass dtype= for raw pointers")
@@ -85,6 +87,18 @@ def gemm(trans_a, trans_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, *, mode
         args = (_ch(trans_a), _ch(trans_b), m, n, k, float(alpha), _ptr(a), lda, _ptr(b), ldb,
                 float(beta), _ptr(c), ldc)
         st = lib.mbg_dgemm(*args) if mode == PLAIN else lib.mbg_dgemm_ex(mode, slices, *args)
+    elif dt in (np.complex64, np.complex128):
+        # complex (an extension: complex dtypes are on the reference's roadmap, README.md:152);
+        # trans 'C' is the conjugate transpose; alpha and beta are complex scalars
+        rt = np.float32 if dt == np.complex64 else np.float64
+        al = np.array([complex(alpha).real, complex(alpha).imag], rt)
+        be = np.array([complex(beta).real, complex(beta).imag], rt)
+        args = (_ch(trans_a), _ch(trans_b), m, n, k, al.ctypes.data, _ptr(a), lda, _ptr(b), ldb,
+                be.ctypes.data, _ptr(c), ldc)
+        if dt == np.complex64:
+            st = lib.mbg_cgemm(*args) if mode == PLAIN else lib.mbg_cgemm_ex(mode, *args)
+        else:
+            st = lib.mbg_zgemm(*args) if mode == PLAIN else lib.mbg_zgemm_ex(mode, slices, *args)
     else:
         raise TypeError(f"unsupported dtype {dt}")
     return _report("gemm", st)

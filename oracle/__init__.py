@@ -406,6 +406,20 @@ def ozaki_trmm_emulated(side, uplo, ta, diag, m, n, alpha, a, lda, b, ldb, slice
     return fma(d[None, :], B, v)
 
 
+def trsm_lower_longdouble(L: np.ndarray, B: np.ndarray) -> np.ndarray:
+    """X with L X = B for a lower-triangular L, by forward substitution in x86 extended
+    precision (numpy longdouble, 64-bit significand: unit roundoff 2^-64, 2048 times
+    below float64's), as a checker for float64 solves whose own error is near 1e-16."""
+    n = L.shape[0]
+    Ll = np.asarray(L, dtype=np.longdouble)
+    X = np.array(B, dtype=np.longdouble, copy=True)
+    for i in range(n):
+        X[i] = X[i] / Ll[i, i]
+        if i + 1 < n:
+            X[i + 1:] -= np.outer(Ll[i + 1:, i], X[i])
+    return X
+
+
 def max_rel_err(x: np.ndarray, ref: np.ndarray) -> float:
     """max|x - ref| / max|ref| (normwise, the error metric quoted with every result)."""
     den = float(np.max(np.abs(ref)))

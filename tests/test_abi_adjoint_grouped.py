@@ -8,7 +8,8 @@ device work starts (so null or unused buffers are fine here):
 * trsm adjoint: trsm's numbering for 1..9 (src/level3/trsm.mojo:62-89), then
   ldx 11, ldg 13, lddb 15, ldda 17;
 * grouped plans: the first invalid problem's gemm / trsm number, with the
-  problem's index in mbg_last_error; only MBG_MODE_PLAIN is accepted.
+  problem's index in mbg_last_error; sgemm plans take MBG_MODE_PLAIN, BF16X3 and
+  BF16X6, strsm plans MBG_MODE_PLAIN.
 """
 import ctypes as C
 
@@ -160,9 +161,11 @@ def test_grouped_plan_rejects_host_pointers(lib):
     assert "problem 0" in L.last_error() and "device only" in L.last_error()
 
 
-def test_grouped_plans_accept_plain_mode_only(lib):
+def test_grouped_plan_modes(lib):
     plan = C.c_void_p()
+    # the split modes pass the mode check and reach the per-problem checks (host pointers here)
     assert lib.mbg_sgemm_grouped_plan(L.MODE_BF16X6, 3, sgemm_problems(-1), C.byref(plan)) < 0
-    assert "MBG_MODE_PLAIN" in L.last_error()
+    assert "device only" in L.last_error()
+    assert lib.mbg_sgemm_grouped_plan(L.MODE_OZAKI, 3, sgemm_problems(-1), C.byref(plan)) == L.MBG_ERR_INVALID_MODE
     assert lib.mbg_strsm_grouped_plan(L.MODE_OZAKI, 2, strsm_problems(-1), C.byref(plan)) < 0
     assert lib.mbg_sgemm_grouped_plan(L.MODE_PLAIN, -1, None, C.byref(plan)) < 0
