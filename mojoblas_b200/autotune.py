@@ -5,16 +5,26 @@ mbg_load_tuning (mojoblas_b200.load_tuning applies it from Python).
     python -m mojoblas_b200.autotune [--out mojoblas_b200/tuning_b200.json]
 
 Keys swept:
-  grouped_gemm_tile  64 or 128 — tile edge of grouped sgemm plans, timed on a
-                     batch of 4096 problems with m, n, k log-uniform in 16..512
-                     (the batched configuration's distribution);
+  grouped_simt_tile_<TT>_c<d>   per transposes TT (NN, NT, TN, TT) and size
+  grouped_tc_bn_<TT>_c<d>       class d of max(m, n) (0: <= 32, 1: <= 64,
+                     2: <= 128, 3: <= 256, 4: <= 512): the tile edge (64 / 128)
+                     of the plain grouped sgemm and the tile width (64 / 128) of
+                     the split (BF16x6, tensor-core) grouped sgemm, each timed on
+                     a batch of problems of that class (m and n log-uniform within
+                     the class, k log-uniform in 16..512, the batched
+                     configuration's distribution);
+  grouped_gemm_tile  the plain form's tile for classes without an entry: the
+                     faster one on the whole configuration batch (4096 problems,
+                     m, n, k log-uniform in 16..512);
   trsm_block_rows    0 (64-row leaves), 256, 512 — diagonal blocks solved in
   trsm_tc_min_k      one fused launch, and the reduction length below which
                      the blocked trsm's off-diagonal updates stay on the plain
                      kernel; swept jointly on dtrsm 4096^2 with Ozaki
                      updates (the blocked-trsm configuration);
   trsm_block_min_cols  the fewest right-hand sides for which the fused launch
-                     beats the 64-row leaves, timed on dtrsm 4096 x nrhs.
+                     beats the 64-row leaves, timed on dtrsm 4096 x nrhs;
+  trsm_inverse_min_cols  the fewest right-hand sides for which the Ozaki trsm's
+                     inverted diagonal blocks beat substitution leaves.
 Labels in the measurement log avoid the key names, since the library's loader
 reads the table as "key value" pairs.
 """
@@ -38,10 +48,15 @@ def log_uniform(rng, lo, hi, size):
     return np.round(np.exp(rng.uniform(np.log(lo), np.log(hi), size))).astype(np.int64)
 
 
-def sgemm_batch(torch, L, count=4096, seed=0):
-    """count problems NN, m, n, k log-uniform 16..512, uniform[-1,1) data on the device."""
+CLASS_BOUNDS = [(16, 32), (33, 64), (65, 128), (129, 256), (257, 512)]  # max(m, n) per size class
+
+
+def sgemm_batch(torch, L, count=4096, seed=0, mn=(16, 512), trans=("N", "N")):
+    """count problems, m, n log-uniform in mn, k log-uniform 16..512, transposes `trans`,
+    uniform[-1,1) data on the device (leading dimensions the stored row counts)."""
     rng = np.random.default_rng(seed)
-    m, n, k = (log_uniform(rng, 16, 512, count) for _ in range(3))
+    m, n = (log_uniform(rng, mn[0], mn[1], count) for _ in range(2))
+    k = log_uniform(rng, 16, 512, count)
     sizes = m * k + k * n + m * n
     offs = np.concatenate([[0], np.cumsum((sizes + 63) // 64 * 64)])
     g = torch.Generator(device="cuda")
@@ -53,8 +68,10 @@ def sgemm_batch(torch, L, count=4096, seed=0):
         pa = base + 4 * int(offs[i])
         pb = pa + 4 * int(m[i] * k[i])
         pc = pb + 4 * int(k[i] * n[i])
-        probs[i] = L.SgemmProblem(b"N", b"N", int(m[i]), int(n[i]), int(k[i]), 1.0, 0.0, pa, int(m[i]), pb,
-                                  int(k[i]), pc, int(m[i]))
+        lda = int(m[i]) if trans[0] == "N" else int(k[i])
+        ldb = int(k[i]) if trans[1] == "N" else int(n[i])
+        probs[i] = L.SgemmProblem(trans[0].encode(), trans[1].encode(), int(m[i]), int(n[i]), int(k[i]), 1.0, 0.0,
+                                  pa, lda, pb, ldb, pc, int(m[i]))
     flops = float(np.sum(2.0 * m * n * k))
     return buf, probs, (m, n, k, offs), flops
 
@@ -80,22 +97,47 @@ def tune(out: Path) -> dict:
     lib.mbg_set_sync(0)
     table, log = {}, {}
 
+    def plan_ms(mode, probs):
+        plan = C.c_void_p()
+        st = lib.mbg_sgemm_grouped_plan(mode, len(probs), probs, C.byref(plan))
+        if st:
+            raise RuntimeError(L.last_error())
+        try:
+            return time_plan(torch, lib, plan)
+        finally:
+            lib.mbg_plan_destroy(plan)
+
     buf, probs, _, flops = sgemm_batch(torch, L)
     best = None
     for tile in (64, 128):
         lib.mbg_set_tuning(b"grouped_gemm_tile", tile)
-        plan = C.c_void_p()
-        st = lib.mbg_sgemm_grouped_plan(L.MODE_PLAIN, len(probs), probs, C.byref(plan))
-        if st:
-            raise RuntimeError(L.last_error())
-        ms = time_plan(torch, lib, plan)
-        lib.mbg_plan_destroy(plan)
+        ms = plan_ms(L.MODE_PLAIN, probs)
         log[f"grouped sgemm tile {tile}"] = {"ms": round(ms, 4), "tflops": round(flops / ms / 1e9, 2)}
         if best is None or ms < best[1]:
             best = (tile, ms)
     table["grouped_gemm_tile"] = best[0]
     lib.mbg_set_tuning(b"grouped_gemm_tile", best[0])
     del buf
+
+    # per transposes and size class: the plain form's tile edge, the split form's tile width
+    for ta in "NT":
+        for tb in "NT":
+            for cls, bounds in enumerate(CLASS_BOUNDS):
+                buf, probs, _, flops = sgemm_batch(torch, L, count=512, seed=100 + cls, mn=bounds, trans=(ta, tb))
+                for prefix, mode, label in (("grouped_simt_tile", L.MODE_PLAIN, "plain"),
+                                            ("grouped_tc_bn", L.MODE_BF16X6, "bf16x6")):
+                    key = f"{prefix}_{ta}{tb}_c{cls}"
+                    times = {}
+                    for v in (64, 128):
+                        lib.mbg_set_tuning(key.encode(), v)
+                        times[v] = plan_ms(mode, probs)
+                    choice = min(times, key=times.get)
+                    table[key] = choice
+                    lib.mbg_set_tuning(key.encode(), choice)
+                    log[f"grouped sgemm {label} {ta}{tb} max(m,n) in {bounds}, tile 64 / 128"] = {
+                        "ms": [round(times[64], 4), round(times[128], 4)],
+                        "tflops": [round(flops / times[64] / 1e9, 2), round(flops / times[128] / 1e9, 2)]}
+                del buf
 
     n = 4096
     A = torch.randn(n, n, dtype=torch.float64, device="cuda") / n ** 0.5
@@ -105,7 +147,7 @@ def tune(out: Path) -> dict:
 
     def time_trsm(mode, nrhs, reps=3):
         def call():
-            X[:, :nrhs].copy_(B0[:, :nrhs])
+            X[:nrhs].copy_(B0[:nrhs])  # column-major: the first nrhs columns
             st = lib.mbg_dtrsm_ex(mode, 7, 0, b"L", b"L", b"N", b"N", n, nrhs, 1.0, A.data_ptr(), n,
                                   X.data_ptr(), n)
             if st:
@@ -157,6 +199,21 @@ def tune(out: Path) -> dict:
         lib.mbg_set_tuning(b"trsm_block_rows", best[0])
     table["trsm_block_min_cols"] = min_cols
     lib.mbg_set_tuning(b"trsm_block_min_cols", min_cols)
+
+    # smallest right-hand-side count from which the Ozaki trsm's inverted diagonal blocks win
+    inv_cols = 0
+    for nrhs in (2048, 1024, 512, 256, 128, 64):
+        lib.mbg_set_tuning(b"trsm_inverse_min_cols", 1)
+        inv = time_trsm(L.MODE_OZAKI, nrhs)
+        lib.mbg_set_tuning(b"trsm_inverse_min_cols", 0)
+        sub = time_trsm(L.MODE_OZAKI, nrhs)
+        log[f"ozaki dtrsm 4096 x {nrhs}: inverted blocks vs substitution"] = {"ms": [round(inv, 3), round(sub, 3)]}
+        if inv <= sub:
+            inv_cols = nrhs
+        else:
+            break
+    table["trsm_inverse_min_cols"] = inv_cols
+    lib.mbg_set_tuning(b"trsm_inverse_min_cols", inv_cols)
 
     doc = {**table, "_measurements": log, "_device": torch.cuda.get_device_name(0)}
     out.write_text(json.dumps(doc, indent=1) + "\n")

@@ -5,6 +5,9 @@
     python mojoblas_b200/profile_case.py --op dtrsm --mode ozaki --m 4096 --n 4096
     python mojoblas_b200/profile_case.py --op strmm --mode bf16x6 --m 4096 --n 4096
     python mojoblas_b200/profile_case.py --op dgemv --ta N --m 8192 --n 8192
+    python mojoblas_b200/profile_case.py --op dgemm --mode ozaki --slices 7 --pair 1 --m 4096 --n 4096 --k 4096
+    python mojoblas_b200/profile_case.py --op grouped_sgemm --mode bf16x6
+    python mojoblas_b200/profile_case.py --op zgemm --mode ozaki --slices 7 --m 2048 --n 2048 --k 2048
 
 Inputs are uniform[-1, 1) (trsm, trmm: diagonally dominant lower triangle), device
 resident; each rep is one call through the C ABI.  Prints the mean CUDA-event
@@ -22,7 +25,8 @@ sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--op", choices=["sgemm", "dgemm", "ssyrk", "dtrsm", "strsm", "grouped_sgemm", "grouped_strsm",
+    ap.add_argument("--op", choices=["sgemm", "dgemm", "cgemm", "zgemm", "ssyrk", "dtrsm", "strsm", "grouped_sgemm",
+                                     "grouped_strsm",
                                      "strmm", "dtrmm", "ssymm", "dsymm", "ssyr2k", "dsyr2k",
                                      "sgemv", "dgemv", "strsv", "dtrsv"],
                     default="sgemm")
@@ -35,6 +39,7 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--k", type=int, default=8192)
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--pair", type=int, default=-1, help="Ozaki kernel: 1 CTA pairs, 0 one CTA per tile")
     a = ap.parse_args()
 
     import torch
@@ -44,7 +49,9 @@ def main():
     lib.mbg_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream))
     lib.mbg_set_sync(0)
     mode = {"plain": L.MODE_PLAIN, "bf16x3": L.MODE_BF16X3, "bf16x6": L.MODE_BF16X6, "ozaki": L.MODE_OZAKI}[a.mode]
-    dt = torch.float64 if a.op[0] == "d" else torch.float32
+    if a.pair >= 0:
+        assert lib.mbg_set_tuning(b"ozaki_cta_pair", a.pair) == 0
+    dt = torch.float64 if a.op[0] in "dz" else torch.float32
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
 
@@ -55,7 +62,7 @@ def main():
         from mojoblas_b200.autotune import sgemm_batch
         buf, probs, _, _ = sgemm_batch(torch, L, 4096, seed=41)
         plan = C.c_void_p()
-        assert lib.mbg_sgemm_grouped_plan(L.MODE_PLAIN, len(probs), probs, C.byref(plan)) == 0, L.last_error()
+        assert lib.mbg_sgemm_grouped_plan(mode, len(probs), probs, C.byref(plan)) == 0, L.last_error()
 
         def call():
             return lib.mbg_plan_execute(plan)
@@ -94,6 +101,20 @@ def main():
                                         B.data_ptr(), ldb, 0.0, Cm.data_ptr(), a.m)
             return lib.mbg_dgemm_ex(mode, a.slices, a.ta.encode(), a.tb.encode(), a.m, a.n, a.k, 1.0, A.data_ptr(),
                                     lda, B.data_ptr(), ldb, 0.0, Cm.data_ptr(), a.m)
+    elif a.op in ("cgemm", "zgemm"):  # complex, interleaved (re, im): a real buffer of twice the rows
+        lda = a.m if a.ta == "N" else a.k
+        ldb = a.k if a.tb == "N" else a.n
+        A, B, Cm = cm(2 * lda, a.k if a.ta == "N" else a.m), cm(2 * ldb, a.n if a.tb == "N" else a.k), cm(2 * a.m, a.n)
+        import numpy as np
+        al = np.array([1.0, 0.0], np.float64 if a.op == "zgemm" else np.float32)
+        be = np.zeros(2, al.dtype)
+
+        def call():
+            args = (a.ta.encode(), a.tb.encode(), a.m, a.n, a.k, al.ctypes.data, A.data_ptr(), lda, B.data_ptr(), ldb,
+                    be.ctypes.data, Cm.data_ptr(), a.m)
+            if a.op == "cgemm":
+                return lib.mbg_cgemm_ex(mode, *args)
+            return lib.mbg_zgemm_ex(mode, a.slices, *args)
     elif a.op == "ssyrk":
         A, Cm = cm(a.n, a.k), cm(a.n, a.n)
 
