@@ -358,6 +358,55 @@ def run_neighbours(torch, lib, L, stream):
     return out
 
 
+def run_complex(torch, lib, L, stream):
+    """Complex gemm NN (C := A B, alpha = 1, beta = 0; real and imaginary parts uniform[-1, 1)):
+    cgemm at 4096^3 (plain FP32 vs BF16x6) and zgemm at 2048^3 (plain FP64 vs Ozaki 7 slices),
+    8 m n k real flops per call, error against complex128 numpy on 64 sampled rows."""
+    out = {}
+    g = torch.Generator(device="cuda")
+    g.manual_seed(55)
+    for name, nn, tdt, legs in (("cgemm_NN_4096", 4096, torch.complex64,
+                                 (("plain_fp32", L.MODE_PLAIN, 0), ("bf16x6", L.MODE_BF16X6, 0))),
+                                ("zgemm_NN_2048", 2048, torch.complex128,
+                                 (("plain_fp64", L.MODE_PLAIN, 0), ("ozaki_s7", L.MODE_OZAKI, 7)))):
+        rt = torch.float32 if tdt == torch.complex64 else torch.float64
+        A = torch.complex(torch.rand((nn, nn), generator=g, device="cuda", dtype=rt) * 2 - 1,
+                          torch.rand((nn, nn), generator=g, device="cuda", dtype=rt) * 2 - 1)
+        B = torch.complex(torch.rand((nn, nn), generator=g, device="cuda", dtype=rt) * 2 - 1,
+                          torch.rand((nn, nn), generator=g, device="cuda", dtype=rt) * 2 - 1)
+        Cc = torch.empty_like(A)
+        rows = np.random.default_rng(9).choice(nn, 64, replace=False)
+        Ah = A.cpu().numpy().T.astype(np.complex128)  # column-major storage: tensor [col][row]
+        ref = Ah[rows, :] @ B.cpu().numpy().T.astype(np.complex128)
+        al = np.array([1.0, 0.0], np.float32 if tdt == torch.complex64 else np.float64)
+        be = np.zeros(2, al.dtype)
+        res = {}
+        for label, md, s_ in legs:
+            def call():
+                args = (b"N", b"N", nn, nn, nn, al.ctypes.data, A.data_ptr(), nn, B.data_ptr(), nn, be.ctypes.data,
+                        Cc.data_ptr(), nn)
+                st = lib.mbg_cgemm_ex(md, *args) if tdt == torch.complex64 else lib.mbg_zgemm_ex(md, s_, *args)
+                if st:
+                    raise RuntimeError(f"{name} failed {st}: {L.last_error()}")
+            call()
+            torch.cuda.synchronize()
+            got = Cc.cpu().numpy().T[rows, :]
+            err = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(3):
+                call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 3
+            res[label] = {"tflops": round(8.0 * nn ** 3 / (ms * 1e-3) / 1e12, 2), "ms": round(ms, 3),
+                          "fp64_err": err}
+        out[name] = res
+        del A, B, Cc
+    out["note"] = "flops 8 m n k (four real products per complex multiply-add); the real embedding (4M)"
+    return out
+
+
 def run_level2(torch, lib, L, stream):
     """gemv (NoTrans and Trans, 8192 x 8192, float32 and float64, alpha 1.5, beta 0.5, uniform[-1,1)) and
     trsv (Lower / Upper, NoTrans, order 4096, the trsm configuration's triangle scaled to a vector), device
@@ -447,33 +496,47 @@ def run_cfg4(torch, lib, L, stream):
     """Batched: 4096 sgemm problems (m, n, k log-uniform 16..512, NN, uniform[-1,1))
     and 2048 lower-triangular strsm problems (n log-uniform 8..256, nrhs uniform
     1..64, A diagonally dominant as in the trsm configuration, B N(0,1)), each in
-    one graph-replayed persistent launch; float64-oracle error on 64 sampled
+    one graph-replayed persistent launch (sgemm in the plain form and in the split
+    BF16x6 / BF16x3 forms on the tensor cores); float64-oracle error on 64 sampled
     problems of each."""
     from mojoblas_b200.autotune import log_uniform, sgemm_batch
     out = {}
     buf, probs, (m, n, k, offs), flops = sgemm_batch(torch, L, 4096, seed=41)
-    plan = C.c_void_p()
-    if lib.mbg_sgemm_grouped_plan(L.MODE_PLAIN, len(probs), probs, C.byref(plan)):
-        raise RuntimeError(L.last_error())
     reps = 20
-    lib.mbg_plan_execute(plan)
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        lib.mbg_plan_execute(plan)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
-    host = buf.cpu().numpy()
-    errs = []
-    for i in np.random.default_rng(3).choice(len(probs), 64, replace=False):
-        o, mi, ni, ki = int(offs[i]), int(m[i]), int(n[i]), int(k[i])
-        a = host[o:o + mi * ki].reshape((mi, ki), order="F").astype(np.float64)
-        b = host[o + mi * ki:o + mi * ki + ki * ni].reshape((ki, ni), order="F").astype(np.float64)
-        c = host[o + mi * ki + ki * ni:o + mi * ki + ki * ni + mi * ni].reshape((mi, ni), order="F")
-        ref = a @ b
-        errs.append(float(np.max(np.abs(c - ref)) / np.max(np.abs(ref))))
+    sample = np.random.default_rng(3).choice(len(probs), 64, replace=False)
+
+    def grouped(mode):
+        """CUDA-event time of one plan execution (mean of reps graph replays) and the
+        float64-oracle error on the sampled problems."""
+        plan = C.c_void_p()
+        if lib.mbg_sgemm_grouped_plan(mode, len(probs), probs, C.byref(plan)):
+            raise RuntimeError(L.last_error())
+        try:
+            lib.mbg_plan_execute(plan)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                lib.mbg_plan_execute(plan)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms_ = e0.elapsed_time(e1) / reps
+        finally:
+            lib.mbg_plan_destroy(plan)
+        host = buf.cpu().numpy()
+        errs_ = []
+        for i in sample:
+            o, mi, ni, ki = int(offs[i]), int(m[i]), int(n[i]), int(k[i])
+            a = host[o:o + mi * ki].reshape((mi, ki), order="F").astype(np.float64)
+            b = host[o + mi * ki:o + mi * ki + ki * ni].reshape((ki, ni), order="F").astype(np.float64)
+            c = host[o + mi * ki + ki * ni:o + mi * ki + ki * ni + mi * ni].reshape((mi, ni), order="F")
+            ref = a @ b
+            errs_.append(float(np.max(np.abs(c - ref)) / np.max(np.abs(ref))))
+        return ms_, max(errs_)
+
+    ms, err_plain = grouped(L.MODE_PLAIN)
+    ms_x6, err_x6 = grouped(L.MODE_BF16X6)
+    ms_x3, err_x3 = grouped(L.MODE_BF16X3)
     # the same problems as 4096 separate library calls (what a caller without batching does)
     lib.mbg_set_sync(0)
     e0.record(stream)
@@ -483,10 +546,14 @@ def run_cfg4(torch, lib, L, stream):
     e1.record(stream)
     torch.cuda.synchronize()
     loop_ms = e0.elapsed_time(e1)
-    lib.mbg_plan_destroy(plan)
     out["grouped_sgemm_4096"] = {"tflops": round(flops / ms / 1e9, 2), "ms": round(ms, 4),
-                                 "looped_calls_ms": round(loop_ms, 3), "max_fp64_err_64_sampled": max(errs),
+                                 "looped_calls_ms": round(loop_ms, 3), "max_fp64_err_64_sampled": err_plain,
                                  "tile": int(lib.mbg_get_tuning(b"grouped_gemm_tile"))}
+    out["grouped_sgemm_4096_bf16x6"] = {"tflops": round(flops / ms_x6 / 1e9, 2), "ms": round(ms_x6, 4),
+                                        "speedup_vs_plain_grouped": round(ms / ms_x6, 2),
+                                        "max_fp64_err_64_sampled": err_x6}
+    out["grouped_sgemm_4096_bf16x3"] = {"tflops": round(flops / ms_x3 / 1e9, 2), "ms": round(ms_x3, 4),
+                                        "max_fp64_err_64_sampled": err_x3}
     del buf
 
     rng = np.random.default_rng(42)
@@ -685,14 +752,28 @@ def leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk):
     tr = cfg3.get("dtrsm_LLNN_4096", {}) if cfg3 else {}
     if tr:
         put("dtrsm_plain_fp64", tr["plain_fp64"]["tflops"], f64, "fp64 pipe (probe); diagonal blocks latency-bound")
+    tr8 = cfg3.get("dtrsm_LLNN_8192", {}) if cfg3 else {}
+    if tr8 and "ozaki_s7" in tr8:
+        put("dtrsm_8192_ozaki_s7_int8", 28 * tr8["ozaki_s7"]["tflops"], i8,
+            "int8 tensor pipe (probe), whole call (m^2 n flops; the inverted-block leaves add m nb n)")
     if cfg4:
         put("grouped_sgemm_fp32", cfg4["grouped_sgemm_4096"]["tflops"], f32, "fp32 pipe (probe)")
+        gx = cfg4.get("grouped_sgemm_4096_bf16x6")
+        if gx:
+            put("grouped_sgemm_bf16x6_tensor", 6 * gx["tflops"], pk["bf16"],
+                "bf16 tensor pipe (measured burst); useful flops only (tile padding not counted)")
         g = cfg4.get("grouped_strsm_2048")
         if g:
             put("grouped_strsm_hbm", g["gbs"], pk["hbm_gbs"], "HBM (measured copy); latency-bound")
     ga = (cfg5 or {}).get("sgemm_adjoint_3072x1024x2048")
     if ga:
         put("sgemm_adjoint_bf16x6_tensor", 6 * ga["bf16x6"]["tflops"], pk["bf16"], "bf16 tensor pipe (measured burst)")
+    ta_ = (cfg5 or {}).get("strsm_adjoint_2048x512")
+    if ta_ and "bf16x6" in ta_:
+        put("strsm_adjoint_bf16x6_tensor", 6 * ta_["bf16x6"]["tflops"], pk["bf16"],
+            "bf16 tensor pipe (measured burst), whole call (inverted diagonal blocks, masked dL product)")
+        put("strsm_adjoint_plain_fp32", ta_["plain"]["tflops"] if "plain" in ta_ else None, f32,
+            "fp32 pipe (probe)")
     return out
 
 
@@ -939,6 +1020,7 @@ def run_ours(args, rank, world, dist):
     cfg5 = {} if args.skip_cfg5 else run_cfg5(torch, lib, L, stream)
     neighbours = {} if args.skip_neighbours else run_neighbours(torch, lib, L, stream)
     level2 = {} if args.skip_level2 else run_level2(torch, lib, L, stream)
+    cplx = {} if args.skip_complex else run_complex(torch, lib, L, stream)
 
     # ---- e2e through the C ABI with pinned host buffers ----
     hA = A.cpu().pin_memory()
@@ -1026,6 +1108,7 @@ def run_ours(args, rank, world, dist):
         "cfg5_adjoints": cfg5,
         "symm_syr2k_trmm": neighbours,
         "gemv_trsv": level2,
+        "complex_gemm": cplx,
         "roofline_fractions": leg_fractions(dg, cfg3, cfg4, cfg5, probes, pk),
         "e2e": {"value": round(e2e_value, 2), "unit": "TFLOP/s", "h2d_bytes_per_step": bytes_in,
                 "d2h_bytes_per_step": bytes_out, "ms_per_step": round(e2e_ms, 2), "host_memory": "pinned",
@@ -1178,6 +1261,7 @@ def main():
     ap.add_argument("--skip-cfg5", action="store_true")
     ap.add_argument("--skip-neighbours", action="store_true")
     ap.add_argument("--skip-level2", action="store_true")
+    ap.add_argument("--skip-complex", action="store_true")
     ap.add_argument("--skip-context", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
