@@ -337,6 +337,8 @@ int   mbg_release_workspace(void);
  * substitution in the diagonal blocks);
  * "ozaki_cta_pair" — 1: Ozaki products on CTA pairs (tcgen05
  * cta_group::2, 256 x 128 tiles over two SMs); 0 (default): one CTA per tile;
+ * "ozaki_fused_slicing" — 1 (default): a K-contiguous Ozaki operand's exponents
+ * and slices in one pass (0: the separate exponent and slicing kernels);
  * "grouped_simt_tile_<TT>_c<d>", "grouped_tc_bn_<TT>_c<d>" — grouped sgemm
  * plans' tile table, per transposes TT (NN, NT, TN, TT) and size class d of
  * max(m, n) (0: <= 32, 1: <= 64, 2: <= 128, 3: <= 256, 4: larger): the plain

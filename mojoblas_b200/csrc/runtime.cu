@@ -380,6 +380,10 @@ int mbg_set_tuning(const char* key, int64_t value) {
     if (k == "plain_fp64_simt" && (value == 0 || value == 1)) { tuning().plain_fp64_simt = value; return MBG_OK; }
     if (k == "plain_fp32_staged" && (value == 0 || value == 1)) { tuning().plain_fp32_staged = value; return MBG_OK; }
     if (k == "ozaki_cta_pair" && (value == 0 || value == 1)) { tuning().ozaki_cta_pair = value; return MBG_OK; }
+    if (k == "ozaki_fused_slicing" && (value == 0 || value == 1)) {
+        tuning().ozaki_fused_slicing = value;
+        return MBG_OK;
+    }
     set_error_msg("unknown tuning key or value: " + k + " = " + std::to_string(value));
     return MBG_ERR_INVALID_MODE;
 }
@@ -396,6 +400,7 @@ int64_t mbg_get_tuning(const char* key) {
     if (k == "plain_fp64_simt") return tuning().plain_fp64_simt;
     if (k == "plain_fp32_staged") return tuning().plain_fp32_staged;
     if (k == "ozaki_cta_pair") return tuning().ozaki_cta_pair;
+    if (k == "ozaki_fused_slicing") return tuning().ozaki_fused_slicing;
     return -1;
 }
 

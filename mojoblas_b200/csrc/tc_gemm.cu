@@ -1194,8 +1194,62 @@ int launch_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp,
     return check_launch("split_bf16");
 }
 
+// Exponents and slices of a K-contiguous operand in one pass over its rows: a warp per
+// row reads the row once for its largest magnitude (the exponent, 0 for an all-zero
+// row) and again, mostly from cache, to write its digits; padding rows (rows .. Rp)
+// and columns (K .. Kp) are written as zeros.  The digits and exponents are those of
+// row_exponent_kernel + slice_i8_kernel, bit for bit; this saves the second read of
+// the operand from DRAM and one launch.
+__global__ void __launch_bounds__(256)
+slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
+                         int* __restrict__ e, int8_t* __restrict__ planes, int keep) {
+    const i64 r = i64(blockIdx.x) * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= Rp) return;
+    const size_t plane = size_t(Rp) * size_t(Kp);
+    const double* row = src + r * ld;
+    const bool live = r < rows;
+    double mx = 0.0;
+    if (live) {
+#pragma unroll 8
+        for (i64 l = lane; l < K; l += 32)
+            if (kept(keep, r, l)) mx = fmax(mx, fabs(row[l]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    int er = 0;
+    if (mx > 0.0) frexp(mx, &er);
+    if (live && lane == 0) e[r] = er;
+    const int B = 8 * slices - 2;
+    const unsigned long long bias = 0x8080808080808080ULL >> (64 - 8 * slices);
+    for (i64 l0 = i64(lane) * 4; l0 < Kp; l0 += 128) {
+        unsigned long long H[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const i64 l = l0 + u;
+            const double v = (live && l < K && kept(keep, r, l)) ? row[l] : 0.0;
+            H[u] = static_cast<unsigned long long>(oz_fixed(v, er, B)) + bias;
+        }
+        unsigned* out = reinterpret_cast<unsigned*>(planes + size_t(r) * Kp + l0);
+        for (int p = 0; p < slices; ++p) {
+            const int byte = slices - 1 - p;
+            const int sh = 8 * (byte & 3), hiword = byte & 4 ? 32 : 0;
+            unsigned packed = 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) packed |= ((unsigned(H[u] >> hiword) >> sh) & 255u) << (8 * u);
+            out[(plane / 4) * p] = packed ^ 0x80808080u;
+        }
+    }
+}
+
 int launch_slices(const double* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
                   int* e, int8_t* planes, int keep = 0) {
+    if (kmajor && tuning().ozaki_fused_slicing) {
+        ProfScope prof("ozaki_slice");
+        slice_rows_kmajor_kernel<<<unsigned(cdiv(Rp, 8)), 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e,
+                                                                            planes, keep);
+        return check_launch("ozaki_slice");
+    }
     {
         ProfScope prof("ozaki_exponent");
         MBG_CUDA(cudaMemsetAsync(e, 0x80, sizeof(int) * size_t(rows), stream()));  // 0x80808080 < any exponent

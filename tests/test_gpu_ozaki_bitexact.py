@@ -113,3 +113,27 @@ def test_ozaki_trmm_bit_exact(oracle, ozaki_kernel, side, uplo, ta, diag):
     want = oracle.ozaki_trmm_emulated(side, uplo, ta, diag, m, n, 1.5, a, na + 1, b0, m + 2, 7)
     assert np.array_equal(b[:m], want), (np.max(np.abs(b[:m] - want)), np.sum(b[:m] != want))
     np.testing.assert_array_equal(b[m:], b0[m:])
+
+
+def test_fused_and_separate_slicing_agree(oracle):
+    """K-contiguous operands (op(A) = A^T, op(B) = B) are sliced in one pass by default;
+    the separate exponent and slicing kernels give the same planes, so the same product."""
+    from mojoblas_b200 import _lib as L
+    lib = L.load()
+    rng = np.random.default_rng(74)
+    m, n, k = 200, 150, 777
+    a = np.asfortranarray(rng.uniform(-1, 1, (k + 1, m)))
+    b = np.asfortranarray(rng.uniform(-1, 1, (k + 3, n)))
+    a[:, 5] = 0.0  # an all-zero row of op(A)
+    out = []
+    default = lib.mbg_get_tuning(b"ozaki_fused_slicing")
+    try:
+        for fused in (1, 0):
+            assert lib.mbg_set_tuning(b"ozaki_fused_slicing", fused) == 0
+            c = np.full((m, n), np.nan, order="F")
+            assert mb.gemm("T", "N", m, n, k, 1.0, a, k + 1, b, k + 3, 0.0, c, m, mode=mb.OZAKI, slices=7) == 0
+            out.append(c)
+    finally:
+        lib.mbg_set_tuning(b"ozaki_fused_slicing", default)
+    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], oracle.ozaki_gemm_emulated("T", "N", m, n, k, 1.0, a, k + 1, b, k + 3, 7))
