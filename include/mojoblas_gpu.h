@@ -335,8 +335,10 @@ int   mbg_release_workspace(void);
  * right-hand sides inverts its 512-row diagonal blocks once (native precision)
  * and applies each inverse as a split / Ozaki product (default 256; 0 = never:
  * substitution in the diagonal blocks);
- * "ozaki_cta_pair" — 1: Ozaki products on CTA pairs (tcgen05
- * cta_group::2, 256 x 128 tiles over two SMs); 0 (default): one CTA per tile;
+ * "ozaki_cta_pair" — Ozaki products on CTA pairs (tcgen05 cta_group::2,
+ * 256 x 128 tiles over two SMs): 1 one cluster per tile, 2 persistent clusters
+ * (one per two SMs, the epilogue of a tile overlapping the next tile's products);
+ * 0 (default): one CTA per 128 x 128 tile;
  * "ozaki_fused_slicing" — 1 (default): a K-contiguous Ozaki operand's exponents
  * and slices in one pass (0: the separate exponent and slicing kernels);
  * "grouped_simt_tile_<TT>_c<d>", "grouped_tc_bn_<TT>_c<d>" — grouped sgemm

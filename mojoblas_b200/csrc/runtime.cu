@@ -379,7 +379,7 @@ int mbg_set_tuning(const char* key, int64_t value) {
     if (k == "trsm_inverse_min_cols" && value >= 0) { tuning().trsm_inverse_min_cols = value; return MBG_OK; }
     if (k == "plain_fp64_simt" && (value == 0 || value == 1)) { tuning().plain_fp64_simt = value; return MBG_OK; }
     if (k == "plain_fp32_staged" && (value == 0 || value == 1)) { tuning().plain_fp32_staged = value; return MBG_OK; }
-    if (k == "ozaki_cta_pair" && (value == 0 || value == 1)) { tuning().ozaki_cta_pair = value; return MBG_OK; }
+    if (k == "ozaki_cta_pair" && value >= 0 && value <= 2) { tuning().ozaki_cta_pair = value; return MBG_OK; }
     if (k == "ozaki_fused_slicing" && (value == 0 || value == 1)) {
         tuning().ozaki_fused_slicing = value;
         return MBG_OK;

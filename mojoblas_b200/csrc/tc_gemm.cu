@@ -734,16 +734,20 @@ __device__ __forceinline__ void umma_i8_pair(uint32_t d_tmem, uint64_t adesc, ui
 }
 #undef MBG_UMMA2
 
+// One pass of one tile: every k slab, the products of diagonals [LO, HI), then the
+// accumulators committed to both CTAs' epilogues.  `it` counts stage uses across
+// passes and tiles; `gp` is the pass's index across tiles (the epilogue must have
+// read the previous pass's accumulators before this one overwrites them).
 template <class C, int PASS>
-__device__ __forceinline__ bool oz2_mma_pass(const OzParams& P, int nkb, uint8_t* smem, uint64_t* full,
-                                             uint64_t* empty, uint64_t* tfull, uint64_t* tempty, uint32_t tmem) {
+__device__ __forceinline__ bool oz2_mma_pass(const OzParams& P, int nkb, int& it, int gp, uint8_t* smem,
+                                             uint64_t* full, uint64_t* empty, uint64_t* tfull, uint64_t* tempty,
+                                             uint32_t tmem) {
     constexpr int LO = OzPass<C::S, PASS>::LO, HI = OzPass<C::S, PASS>::HI;
-    if (PASS > 0) {  // both CTAs' epilogues must have read the previous pass's accumulators
-        if (!mbar_wait(tempty, (PASS - 1) & 1, P.err, 23)) return false;
+    if (gp > 0) {
+        if (!mbar_wait(tempty, (gp - 1) & 1, P.err, 23)) return false;
         tc_fence_after();
     }
-    for (int kb = 0; kb < nkb; ++kb) {
-        const int it = PASS * nkb + kb;
+    for (int kb = 0; kb < nkb; ++kb, ++it) {
         const int s = it % C::STAGES;
         if (!mbar_wait(&full[s], (it / C::STAGES) & 1, P.err, 24)) return false;
         tc_fence_after();
@@ -764,6 +768,44 @@ __device__ __forceinline__ bool oz2_mma_pass(const OzParams& P, int nkb, uint8_t
     return true;
 }
 
+// Pair tile t of a launch: its rows (pm0), columns (n0) and slabs; false when the
+// triangle mask skips it.  Every role of both CTAs evaluates the same tiles.
+struct OzTile {
+    i64 pm0, n0;
+    int kb0, nkb;
+};
+template <class C>
+__device__ __forceinline__ bool oz2_tile(const OzParams& P, int t, OzTile& T) {
+    // pair tiles of 256 x 128, groups of 8 pair rows walk the n-tiles together (L2 reuse)
+    const int tiles_m2 = (P.tiles_m + 1) >> 1;
+    const int group = 8;
+    const int per_group = group * P.tiles_n;
+    const int g = t / per_group;
+    const int first_m = g * group;
+    const int gsize = min(group, tiles_m2 - first_m);
+    const int in_g = t - g * per_group;
+    int tm = first_m + in_g % gsize, tn = in_g / gsize;
+    if (P.band == KB_A_LOWER) tm = tiles_m2 - 1 - tm;
+    if (P.band == KB_B_UPPER) tn = P.tiles_n - 1 - tn;
+    T.pm0 = i64(tm) * 2 * BM;
+    T.n0 = i64(tn) * C::BN;
+    if (P.tri == 1 && T.pm0 + 2 * BM <= T.n0) return false;
+    if (P.tri == 2 && T.pm0 > T.n0 + C::BN - 1) return false;
+    T.kb0 = 0;
+    T.nkb = P.num_kb;
+    if (P.band != KB_NONE) {
+        i64 s0, s1;
+        band_slabs(P.band, T.pm0, 2 * BM, T.n0, C::BN, P.band_k0, C::BKB, P.num_kb, s0, s1);
+        T.kb0 = int(s0);
+        T.nkb = int(s1 - s0);
+    }
+    return true;
+}
+
+// Persistent over pair tiles: cluster c takes tiles c, c + clusters, ... (a launch
+// with one cluster per tile is the plain form).  Between two tiles the epilogue
+// stores the finished tile from registers while the next tile's first pass is
+// already loading and multiplying: it only has to read the accumulators out first.
 template <class C>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(C::THREADS, 1)
 ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -777,30 +819,8 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 1);
 
     const uint32_t rank = cluster_rank();  // 0: leader (issues the MMAs), 1: peer
-    // pair tiles of 256 x 128, groups of 8 pair rows walk the n-tiles together (L2 reuse)
-    const int tile = blockIdx.x >> 1;
-    const int tiles_m2 = (P.tiles_m + 1) >> 1;
-    const int group = 8;
-    const int per_group = group * P.tiles_n;
-    const int g = tile / per_group;
-    const int first_m = g * group;
-    const int gsize = min(group, tiles_m2 - first_m);
-    const int in_g = tile - g * per_group;
-    int tm = first_m + in_g % gsize, tn = in_g / gsize;
-    if (P.band == KB_A_LOWER) tm = tiles_m2 - 1 - tm;
-    if (P.band == KB_B_UPPER) tn = P.tiles_n - 1 - tn;
-    const i64 pm0 = i64(tm) * 2 * BM, n0 = i64(tn) * C::BN;
-    const i64 m0 = pm0 + i64(rank) * BM;  // this CTA's rows
-    // both CTAs decide the same, before any cluster-wide step
-    if (P.tri == 1 && pm0 + 2 * BM <= n0) return;
-    if (P.tri == 2 && pm0 > n0 + C::BN - 1) return;
-    int kb0 = 0, nkb = P.num_kb;
-    if (P.band != KB_NONE) {
-        i64 s0, s1;
-        band_slabs(P.band, pm0, 2 * BM, n0, C::BN, P.band_k0, C::BKB, P.num_kb, s0, s1);
-        kb0 = int(s0);
-        nkb = int(s1 - s0);
-    }
+    const int ntiles = ((P.tiles_m + 1) >> 1) * P.tiles_n;
+    const int first = blockIdx.x >> 1, stride = gridDim.x >> 1;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -820,7 +840,6 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     cluster_sync_all();  // barriers of both CTAs initialised, TMEM of the pair allocated
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int total = C::NPASS * nkb;
     const uint32_t leader_tempty = peer_addr(tempty, 0);
 
     if (warp == 0) {
@@ -829,66 +848,85 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
             prefetch_tmap(&tmA);
             prefetch_tmap(&tmB);
             bool ok = true;
-            for (int it = 0; it < total; ++it) {
-                const int pass = it / nkb, kb = it - pass * nkb;
-                int lo, hi, planes;
-                pass_range<C>(pass, lo, hi, planes);
-                const int s = it % C::STAGES;
-                const uint32_t ph = (it / C::STAGES) & 1;
-                if (!mbar_wait(&empty[s], ph ^ 1, P.err, 21)) { ok = false; break; }
-                uint8_t* sa = smem + s * C::STAGE_BYTES;
-                uint8_t* sb = sa + C::S * C::A_PLANE;
-                if (rank == 0) mbar_expect_tx(&full[s], uint32_t(2 * planes * (C::A_PLANE + C::B_PLANE)));
-                const uint32_t bar = peer_addr(&full[s], 0);
-                const bool all = planes == C::S;
-                tma_load_3d_pair(sa, all ? &tmA : &tmAlo, bar, (kb0 + kb) * C::BKB, int(m0), 0);
-                tma_load_3d_pair(sb, all ? &tmB : &tmBlo, bar, (kb0 + kb) * C::BKB, int(n0 + rank * C::BNH), 0);
+            int it = 0;
+            for (int t = first; t < ntiles && ok; t += stride) {
+                OzTile T;
+                if (!oz2_tile<C>(P, t, T)) continue;
+                const i64 m0 = T.pm0 + i64(rank) * BM;
+                for (int pass = 0; pass < C::NPASS && ok; ++pass) {
+                    int lo, hi, planes;
+                    pass_range<C>(pass, lo, hi, planes);
+                    const bool all = planes == C::S;
+                    for (int kb = 0; kb < T.nkb; ++kb, ++it) {
+                        const int s = it % C::STAGES;
+                        if (!mbar_wait(&empty[s], ((it / C::STAGES) & 1) ^ 1, P.err, 21)) { ok = false; break; }
+                        uint8_t* sa = smem + s * C::STAGE_BYTES;
+                        uint8_t* sb = sa + C::S * C::A_PLANE;
+                        if (rank == 0) mbar_expect_tx(&full[s], uint32_t(2 * planes * (C::A_PLANE + C::B_PLANE)));
+                        const uint32_t bar = peer_addr(&full[s], 0);
+                        tma_load_3d_pair(sa, all ? &tmA : &tmAlo, bar, (T.kb0 + kb) * C::BKB, int(m0), 0);
+                        tma_load_3d_pair(sb, all ? &tmB : &tmBlo, bar, (T.kb0 + kb) * C::BKB,
+                                         int(T.n0 + rank * C::BNH), 0);
+                    }
+                }
             }
             // the loads of the last stages land before the CTA may exit: the leader's MMAs
             // release every stage to both CTAs only after reading it
             if (ok)
-                for (int it = max(0, total - C::STAGES); it < total; ++it)
-                    mbar_wait(&empty[it % C::STAGES], (it / C::STAGES) & 1, P.err, 22);
+                for (int i = max(0, it - C::STAGES); i < it; ++i)
+                    mbar_wait(&empty[i % C::STAGES], (i / C::STAGES) & 1, P.err, 22);
         }
     } else if (warp == 1) {
         if (lane == 0 && rank == 0) {
             // ---------------- MMA issuer (leader) ----------------
-            if (oz2_mma_pass<C, 0>(P, nkb, smem, full, empty, tfull, tempty, tmem) && C::NPASS > 1)
-                oz2_mma_pass<C, 1>(P, nkb, smem, full, empty, tfull, tempty, tmem);
+            int it = 0, gp = 0;
+            bool ok = true;
+            for (int t = first; t < ntiles && ok; t += stride) {
+                OzTile T;
+                if (!oz2_tile<C>(P, t, T)) continue;
+                ok = oz2_mma_pass<C, 0>(P, T.nkb, it, gp++, smem, full, empty, tfull, tempty, tmem);
+                if (ok && C::NPASS > 1)
+                    ok = oz2_mma_pass<C, 1>(P, T.nkb, it, gp++, smem, full, empty, tfull, tempty, tmem);
+            }
         }
     } else {
         // ---------------- epilogue warps (both CTAs, own rows) ----------------
         const int e = warp - 2;
         const int quarter = warp & 3;
         const int part = e >> 2;
-        const i64 row = m0 + quarter * 32 + lane;
         const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(part * C::EPI_COLS);
-        double acc[C::EPI_COLS];
-#pragma unroll
-        for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0;
+        int gp = 0;
         bool ok = true;
-        for (int pass = 0; pass < C::NPASS; ++pass) {
-            int lo, hi, planes;
-            pass_range<C>(pass, lo, hi, planes);
-            if (!mbar_wait(tfull, pass & 1, P.err, 25)) { ok = false; break; }
-            tc_fence_after();
+        for (int t = first; t < ntiles && ok; t += stride) {
+            OzTile T;
+            if (!oz2_tile<C>(P, t, T)) continue;
+            const i64 row = T.pm0 + i64(rank) * BM + quarter * 32 + lane;
+            double acc[C::EPI_COLS];
+#pragma unroll
+            for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0;
+            for (int pass = 0; pass < C::NPASS; ++pass, ++gp) {
+                int lo, hi, planes;
+                pass_range<C>(pass, lo, hi, planes);
+                if (!mbar_wait(tfull, gp & 1, P.err, 25)) { ok = false; break; }
+                tc_fence_after();
 #pragma unroll 1
-            for (int d = hi - 1; d >= lo; --d) {  // smallest weight first
-                const double w = pow2_exact(-8 * d - 12);
+                for (int d = hi - 1; d >= lo; --d) {  // smallest weight first
+                    const double w = pow2_exact(-8 * d - 12);
 #pragma unroll
-                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 16) {
-                    uint32_t r[16];
-                    tmem_ld16(lane_base + uint32_t((d - lo) * C::BN + c0), r);
-                    tmem_ld_wait();
+                    for (int c0 = 0; c0 < C::EPI_COLS; c0 += 16) {
+                        uint32_t r[16];
+                        tmem_ld16(lane_base + uint32_t((d - lo) * C::BN + c0), r);
+                        tmem_ld_wait();
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
+                        for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
+                    }
                 }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_remote(leader_tempty);
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_remote(leader_tempty);
+            if (ok && row < P.m) oz_store_row<C>(P, row, T.n0 + part * C::EPI_COLS, acc);
         }
-        if (ok && row < P.m) oz_store_row<C>(P, row, n0 + part * C::EPI_COLS, acc);
     }
     tc_fence_before();
     __syncwarp();
@@ -1404,8 +1442,13 @@ int launch_ozaki_pair(const CUtensorMap& ma, const CUtensorMap& mb, const CUtens
         mark_configured(configured, dev);
     }
     P.err = device_error_flag();
-    const i64 ctas = 2 * i64((P.tiles_m + 1) / 2) * P.tiles_n;
+    i64 ctas = 2 * i64((P.tiles_m + 1) / 2) * P.tiles_n;
     if (ctas > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    if (tuning().ozaki_cta_pair == 2) {  // persistent: one cluster per pair of SMs
+        int sms = 148;
+        MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        ctas = imin(ctas, i64(sms / 2) * 2);
+    }
     ProfScope prof("tc_gemm_ozaki");
     ozaki_pair_kernel<C><<<unsigned(ctas), C::THREADS, C::SMEM_BYTES, stream()>>>(ma, mb, mal, mbl, P);
     return check_launch("tc_gemm_ozaki");

@@ -8,7 +8,9 @@ every epilogue form: beta = 0, general beta (C read first), beta = 1 (one L2
 reduction per element: the trsm updates), the triangle-masked dsyrk, and the
 in-place dtrmm (banded reduction, diagonal term by one fused multiply-add).
 Tile counts cover an odd number of 128-row tiles (the last pair's second CTA
-holds only padding rows).
+holds only padding rows), and the persistent form (each cluster looping over
+several tiles) is checked against one cluster per tile, including a launch with
+more tiles than clusters (1200 x 1100).
 """
 import numpy as np
 import pytest
@@ -31,21 +33,24 @@ def lib():
 
 
 def both(lib, call):
-    """(pair kernel result, single-CTA kernel result) of call()."""
+    """(pair kernel result, single-CTA kernel result) of call(); the pair kernel run both
+    with one cluster per tile and persistent (one cluster per two SMs), which must agree."""
     default = lib.mbg_get_tuning(b"ozaki_cta_pair")
     out = []
     try:
-        for pair in (1, 0):
+        for pair in (1, 2, 0):
             assert lib.mbg_set_tuning(b"ozaki_cta_pair", pair) == 0
             out.append(call())
     finally:
         lib.mbg_set_tuning(b"ozaki_cta_pair", default)
-    return out
+    assert np.array_equal(out[0], out[1]), "persistent pair kernel differs from one cluster per tile"
+    return out[0], out[2]
 
 
 @pytest.mark.parametrize("s", [3, 7])
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T")])
-@pytest.mark.parametrize("m,n,k,beta", [(300, 200, 700, 0.0), (129, 385, 96, 0.5), (600, 130, 512, 1.0)])
+@pytest.mark.parametrize("m,n,k,beta", [(300, 200, 700, 0.0), (129, 385, 96, 0.5), (600, 130, 512, 1.0),
+                                        (1200, 1100, 300, 0.5)])
 def test_pair_equals_single_cta_gemm(lib, s, ta, tb, m, n, k, beta):
     rng = np.random.default_rng(m * 7 + n + k + s)
     ra, ca = (m, k) if ta == "N" else (k, m)
