@@ -10,7 +10,7 @@ in-place dtrmm (banded reduction, diagonal term by one fused multiply-add).
 Tile counts cover an odd number of 128-row tiles (the last pair's second CTA
 holds only padding rows), and the persistent form (each cluster looping over
 several tiles) is checked against one cluster per tile, including a launch with
-more tiles than clusters (1200 x 1100).
+more tiles than clusters (3000 x 1500: 144 pair tiles).
 """
 import numpy as np
 import pytest
@@ -50,7 +50,7 @@ def both(lib, call):
 @pytest.mark.parametrize("s", [3, 7])
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T")])
 @pytest.mark.parametrize("m,n,k,beta", [(300, 200, 700, 0.0), (129, 385, 96, 0.5), (600, 130, 512, 1.0),
-                                        (1200, 1100, 300, 0.5)])
+                                        (3000, 1500, 300, 0.5)])
 def test_pair_equals_single_cta_gemm(lib, s, ta, tb, m, n, k, beta):
     rng = np.random.default_rng(m * 7 + n + k + s)
     ra, ca = (m, k) if ta == "N" else (k, m)
