@@ -82,6 +82,36 @@ int gemm_adjoint(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, T 
     const T* A_ = (const T*)A.dev;
     const T* B_ = (const T*)B.dev;
     const T* G_ = (const T*)Gm.dev;
+    // dA and dB are independent products that each fill only part of the GPU at the
+    // adjoint sizes (e.g. 96 and 64 tiles of 128 x 256 on 148 SMs): dB runs on a second
+    // stream beside dA, ordered after the work before this call and before the work after it
+    cudaStream_t s = stream(), aux = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    const bool overlap = da && db && mode != MBG_MODE_PLAIN;
+    if (overlap) {
+        MBG_TRY(aux_stream(&aux));
+        MBG_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+        MBG_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+        MBG_CUDA(cudaEventRecord(ev_in, s));
+        MBG_CUDA(cudaStreamWaitEvent(aux, ev_in, 0));
+        cudaEventDestroy(ev_in);
+        int st;
+        {
+            StreamScope on_aux(aux);
+            T* o = (T*)dB.dev;
+            if (is_n(tb))
+                st = gemm_any(mode, slices, flip(ta), 'N', k, n, m, alpha, A_, A.dev_ld, G_, Gm.dev_ld, T(0), o,
+                              dB.dev_ld);
+            else
+                st = gemm_any(mode, slices, 'T', ta, n, k, m, alpha, G_, Gm.dev_ld, A_, A.dev_ld, T(0), o, dB.dev_ld);
+        }
+        const cudaError_t e1 = cudaEventRecord(ev_out, aux);
+        const cudaError_t e2 = cudaStreamWaitEvent(s, ev_out, 0);
+        cudaEventDestroy(ev_out);
+        if (st) return st;
+        MBG_CUDA(e1);
+        MBG_CUDA(e2);
+    }
     if (da) {
         T* o = (T*)dA.dev;
         if (is_n(ta))  // dA = alpha * G * op(B)^T   (m x k)
@@ -90,7 +120,8 @@ int gemm_adjoint(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, T 
             MBG_TRY(gemm_any(mode, slices, tb, 'T', k, m, n, alpha, B_, B.dev_ld, G_, Gm.dev_ld, T(0), o, dA.dev_ld));
         MBG_TRY(dA.finish());
     }
-    if (db) {
+    if (db && overlap) MBG_TRY(dB.finish());
+    if (db && !overlap) {
         T* o = (T*)dB.dev;
         if (is_n(tb))  // dB = alpha * op(A)^T * G   (k x n)
             MBG_TRY(gemm_any(mode, slices, flip(ta), 'N', k, n, m, alpha, A_, A.dev_ld, G_, Gm.dev_ld, T(0), o, dB.dev_ld));

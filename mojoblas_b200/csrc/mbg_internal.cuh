@@ -63,6 +63,20 @@ void set_error_msg(const std::string& msg);
 // Checks the launch that was just enqueued (configuration errors only).
 int check_launch(const char* name);
 
+// A second non-blocking compute stream of the current device (created on first use,
+// kept), for independent work within one call that can run beside the library stream.
+int aux_stream(cudaStream_t* out);
+// For its lifetime, the calling thread's library work goes to stream s (workspace
+// blocks from s's pool); the previous setting comes back when it ends.
+struct StreamScope {
+    cudaStream_t saved;
+    bool saved_on;
+    explicit StreamScope(cudaStream_t s);
+    ~StreamScope();
+    StreamScope(const StreamScope&) = delete;
+    StreamScope& operator=(const StreamScope&) = delete;
+};
+
 // Two non-blocking streams of the current device (host->device and device->host
 // copies of the pipelined host path), created on first use and kept.
 int copy_streams(cudaStream_t* in, cudaStream_t* out);

@@ -174,6 +174,25 @@ int Operand::finish() {
     return MBG_OK;
 }
 
+// ---- a second compute stream per device, and scoped stream overrides ----------------
+int aux_stream(cudaStream_t* out) {
+    static std::map<int, cudaStream_t> aux;
+    std::lock_guard<std::mutex> lk(g_mu);
+    cudaStream_t& s = aux[current_device()];
+    if (!s) MBG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    *out = s;
+    return MBG_OK;
+}
+
+StreamScope::StreamScope(cudaStream_t s) : saved(t_stream), saved_on(t_stream_on) {
+    t_stream = s;
+    t_stream_on = true;
+}
+StreamScope::~StreamScope() {
+    t_stream = saved;
+    t_stream_on = saved_on;
+}
+
 // ---- copy streams of the pipelined host path ---------------------------------------
 int copy_streams(cudaStream_t* in, cudaStream_t* out) {
     std::lock_guard<std::mutex> lk(g_mu);
