@@ -197,6 +197,20 @@ def dtrsm_leg(torch, lib, L, stream, n, g, variants):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
         tr[label] = {"tflops": round(n ** 3 / (ms * 1e-3) / 1e12, 2), "ms": round(ms, 3), "fp64_err": err}
+        if md != L.MODE_PLAIN:  # where one call's time goes: device time of each library kernel kind
+            lib.mbg_prof_enable(1)
+            lib.mbg_prof_reset()
+            tcall(md, s_, r_)
+            torch.cuda.synchronize()
+            parts = {}
+            for kname in ("tc_gemm_ozaki", "tc_gemm_bf16", "ozaki_slice", "ozaki_exponent", "split_bf16",
+                          "trsm_block_invert", "trsm_block_solve", "trsm_diag"):
+                tot, cnt = C.c_double(), C.c_int64()
+                lib.mbg_prof_query(kname.encode(), C.byref(tot), C.byref(cnt))
+                if cnt.value:
+                    parts[kname] = {"ms": round(tot.value, 3), "launches": int(cnt.value)}
+            lib.mbg_prof_enable(0)
+            tr[label]["kernel_ms"] = parts
     del A, B0, X
     return tr
 
