@@ -314,7 +314,7 @@ struct OzakiA {
 };
 int ozaki_slice_a(int slices, char ta, i64 m, i64 k, const double* a, i64 lda, OzakiA& out);
 int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n, double alpha, const double* b,
-                          i64 ldb, double beta, double* c, i64 ldc);
+                          i64 ldb, double beta, double* c, i64 ldc, const double* dvec = nullptr);
 
 // trsm and trmm on device operands (trsm.cu)
 template <typename T>

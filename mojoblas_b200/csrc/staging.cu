@@ -39,8 +39,10 @@ constexpr int STAGE_NBUF = 4;
 class CopyPool {
 public:
     static CopyPool& get() {
-        static CopyPool pool;
-        return pool;
+        // never destroyed: its worker threads wait on its condition variable until the
+        // process exits, and destroying a condition variable with waiters blocks exit
+        static CopyPool* pool = new CopyPool();
+        return *pool;
     }
     // dst[r * dpitch .. + width] = src[r * spitch .. + width] for rows r in [0, height)
     void copy_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height) {

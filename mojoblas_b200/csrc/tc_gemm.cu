@@ -1503,9 +1503,11 @@ int ozaki_slice_a(int slices, char ta, i64 m, i64 k, const double* a, i64 lda, O
 
 // Rows r0 .. r0 + mb - 1 of op(A) from ozaki_slice_a (r0 a multiple of 128) times op(B) (k x n,
 // k <= A.k; op(B)'s rows k .. A.k - 1 taken as zero): C[0:mb, 0:n] := alpha op(A)[r0:r0+mb, :] op(B)
-// + beta C.  C may be op(B) itself: the kernel reads op(B) only through its slices.
+// + beta C, or with dvec (mb values) C := alpha op(A)[r0:r0+mb, :] op(B) + dvec .* C (each
+// element of C read by the thread that then overwrites it).  C may be op(B) itself: the kernel
+// reads op(B) only through its slices.
 int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n, double alpha, const double* b,
-                          i64 ldb, double beta, double* c, i64 ldc) {
+                          i64 ldb, double beta, double* c, i64 ldc, const double* dvec) {
     using namespace tc;
     if (mb == 0 || n == 0) return MBG_OK;
     if (r0 % BM || r0 + mb > A.m || k > A.k || k <= 0) return MBG_ERR_UNSUPPORTED;
@@ -1524,6 +1526,10 @@ int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n
     P.tiles_m = int(cdiv(mb, BM)); P.tiles_n = int(cdiv(n, BN));
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
     P.ea = A.e + r0; P.eb = eb;
+    if (dvec) {  // C = alpha acc + d .* C, d per row (C read before it is overwritten)
+        P.dvec = dvec;
+        P.dvec_mode = 1;
+    }
     return run_ozaki(slices, pa, rows, A.Mp, pb, Np, A.Kp, P);
 }
 

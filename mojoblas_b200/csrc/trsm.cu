@@ -461,7 +461,7 @@ int invert_diagonal_blocks(bool lower, bool trans, bool unit, i64 m, int nbi, co
 template <typename T> struct InvPlanes;
 template <> struct InvPlanes<float> {
     SplitA p;
-    int make(int mode, int, i64 m, i64 nbi, const float* w) {
+    int make(int mode, int, i64 m, i64 nbi, float* w) {
         return split_a_planes(mode == MBG_MODE_BF16X6 ? 3 : 2, 'N', m, nbi, w, m, p);
     }
     // B[0:mb, :] := inv block (rows r0 .. r0 + mb of the stack) times B[0:mb, :]
@@ -469,11 +469,33 @@ template <> struct InvPlanes<float> {
         return sgemm_split_tc_with_a_rows(p, r0, mb, mb, 'N', n, 1.0f, b, ldb, 0.0f, b, ldb);
     }
 };
+// The Ozaki leaves keep each inverse's diagonal out of the slices: an inverted block of a
+// diagonally dominant triangle is dominated by its diagonal, and the slices are scaled per
+// row, so with the diagonal inside them the off-diagonal entries would keep few bits.  The
+// slices hold the strict triangle (exponents from its entries only) and the epilogue adds
+// the diagonal term with one fused multiply-add: X_b = W_off B_b + d .* B_b, B_b read by the
+// thread that overwrites it.
+__global__ void split_block_diagonal_kernel(i64 m, int nbi, double* __restrict__ W, i64 ldw,
+                                            double* __restrict__ d) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < m; r += (i64)gridDim.x * blockDim.x) {
+        double* p = W + r + (r % nbi) * ldw;
+        d[r] = *p;
+        *p = 0.0;
+    }
+}
 template <> struct InvPlanes<double> {
     OzakiA p;
-    int make(int, int slices, i64 m, i64 nbi, const double* w) { return ozaki_slice_a(slices, 'N', m, nbi, w, m, p); }
+    Workspace wd;
+    double* d = nullptr;
+    int make(int, int slices, i64 m, i64 nbi, double* w) {
+        MBG_TRY(wd.reserve(sizeof(double) * size_t(m)));
+        d = wd.as<double>();
+        split_block_diagonal_kernel<<<unsigned(imin(cdiv(m, 256), 1024)), 256, 0, stream()>>>(m, int(nbi), w, m, d);
+        MBG_TRY(check_launch("trsm_block_invert"));
+        return ozaki_slice_a(slices, 'N', m, nbi, w, m, p);
+    }
     int leaf(i64 r0, i64 mb, i64 n, double* b, i64 ldb) const {
-        return dgemm_ozaki_tc_with_a(p, r0, mb, mb, 'N', n, 1.0, b, ldb, 0.0, b, ldb);
+        return dgemm_ozaki_tc_with_a(p, r0, mb, mb, 'N', n, 1.0, b, ldb, 0.0, b, ldb, d + r0);
     }
 };
 
