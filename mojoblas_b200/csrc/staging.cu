@@ -78,7 +78,7 @@ public:
 private:
     CopyPool() {
         unsigned hw = std::thread::hardware_concurrency();
-        nthreads_ = int(std::max(1u, std::min(8u, hw > 1 ? hw / 2 : 1u)));
+        nthreads_ = int(std::max(1u, std::min(16u, hw > 1 ? hw - 1 : 1u)));  // the caller is one more
         if (const char* e = std::getenv("MBG_COPY_THREADS")) nthreads_ = std::max(0, std::min(64, std::atoi(e)));
         for (int i = 0; i < nthreads_; ++i) {
             std::thread t([this] { work(); });
