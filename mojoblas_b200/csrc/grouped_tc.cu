@@ -331,6 +331,8 @@ int grouped_tc_build(int terms, int count, const mbg_sgemm_problem* probs, Group
     MBG_CUDA(cudaGetDevice(&dev));
     MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     out.grid = int(imin(out.ntiles, sms));
+    // the wait-error flag is created now: its first use must not fall inside the plan's graph capture
+    out.err = device_error_flag();
     const int smem = terms == 3 ? GCfg<3>::SMEM_BYTES : GCfg<2>::SMEM_BYTES;
     if (terms == 3)
         MBG_CUDA(cudaFuncSetAttribute(grouped_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -344,11 +346,10 @@ int grouped_tc_enqueue(const GroupedTcPlan& p, cudaStream_t s) {
     if (p.ntiles == 0) return MBG_OK;
     const TcDesc* d = static_cast<const TcDesc*>(p.table);
     const TcTile* t = reinterpret_cast<const TcTile*>(static_cast<const char*>(p.table) + p.tiles_off);
-    int* err = device_error_flag();
     if (p.terms == 3)
-        grouped_tc_kernel<3><<<p.grid, GTHREADS, GCfg<3>::SMEM_BYTES, s>>>(d, t, p.ntiles, err);
+        grouped_tc_kernel<3><<<p.grid, GTHREADS, GCfg<3>::SMEM_BYTES, s>>>(d, t, p.ntiles, p.err);
     else
-        grouped_tc_kernel<2><<<p.grid, GTHREADS, GCfg<2>::SMEM_BYTES, s>>>(d, t, p.ntiles, err);
+        grouped_tc_kernel<2><<<p.grid, GTHREADS, GCfg<2>::SMEM_BYTES, s>>>(d, t, p.ntiles, p.err);
     return check_launch("grouped_sgemm_tc");
 }
 

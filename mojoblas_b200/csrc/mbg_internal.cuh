@@ -190,6 +190,7 @@ struct GroupedTcPlan {
     void* table = nullptr;
     int count = 0, ntiles = 0, grid = 0;
     size_t tiles_off = 0;
+    int* err = nullptr;  // the library's wait-error flag, created before the graph capture
 };
 int grouped_tc_build(int terms, int count, const mbg_sgemm_problem* probs, GroupedTcPlan& out);
 int grouped_tc_enqueue(const GroupedTcPlan& p, cudaStream_t s);

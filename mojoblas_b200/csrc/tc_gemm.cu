@@ -653,14 +653,19 @@ struct Oz2Cfg {
     static constexpr int S = S_;
     static constexpr int BN = 128;                    // output columns of the pair's tile
     static constexpr int BNH = BN / 2;                // op(B)^T rows staged by each CTA
-    static constexpr int BKB = 32;
+    // k slab: 64 int8 per row (two 32-deep MMA steps), 64-byte swizzle.  Each TMA row
+    // request then carries two 32-byte sectors: with 32-byte slabs the loads were bound
+    // by the SM's L1-to-L2 request rate (ncu: l1tex2xbar requests 85 % busy for 21 % of
+    // the read bandwidth), not by bytes
+    static constexpr int BKB = 64;
+    static constexpr int KSTEPS = BKB / 32;
     static constexpr int EPI_WARPS = 8;
     static constexpr int THREADS = 64 + 32 * EPI_WARPS;
     static constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // 64
     static constexpr int NPASS = S <= 4 ? 1 : 2;
     static constexpr int SPLIT = S <= 4 ? 0 : 4;
-    static constexpr int A_PLANE = BM * BKB;          // 4 KB
-    static constexpr int B_PLANE = BNH * BKB;         // 2 KB
+    static constexpr int A_PLANE = BM * BKB;          // 8 KB
+    static constexpr int B_PLANE = BNH * BKB;         // 4 KB
     static constexpr int STAGE_BYTES = S * (A_PLANE + B_PLANE);
     static constexpr int STAGES = (196608 / STAGE_BYTES) > 8 ? 8 : (196608 / STAGE_BYTES);
     // at least 120 KB, so one CTA per SM: two pairs interleaved on the same two SMs could
@@ -668,9 +673,9 @@ struct Oz2Cfg {
     static constexpr int SMEM_USED = STAGES * STAGE_BYTES + 1024 + 256;
     static constexpr int SMEM_BYTES = SMEM_USED > 122880 ? SMEM_USED : 122880;
     static constexpr uint32_t IDESC = instr_desc(true, 2 * BM, BN);  // M = 256 over the pair
-    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 6;
+    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 4;
     static_assert(STAGES >= 2, "pipeline depth");
-    static_assert(A_PLANE % 256 == 0 && B_PLANE % 256 == 0, "32-byte swizzle atoms stay aligned");
+    static_assert(A_PLANE % 512 == 0 && B_PLANE % 512 == 0, "64-byte swizzle atoms stay aligned");
 };
 
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -754,13 +759,16 @@ __device__ __forceinline__ bool oz2_mma_pass(const OzParams& P, int nkb, int& it
         const uint32_t sa = smem_u32(smem + s * C::STAGE_BYTES);
         const uint32_t sb = sa + C::S * C::A_PLANE;
 #pragma unroll
-        for (int pi = 0; pi < C::S * C::S; ++pi) {
-            int p = 0, q = 0, collector = 0;
-            if (!oz_product<C::S>(LO, HI, pi, p, q, collector)) break;
-            const uint32_t accumulate = (kb > 0 || p > 0) ? 1u : 0u;
-            const uint64_t ad = smem_desc(sa + p * C::A_PLANE, C::SBO, C::LAYOUT);
-            const uint64_t bd = smem_desc(sb + q * C::B_PLANE, C::SBO, C::LAYOUT);
-            umma_i8_pair(tmem + uint32_t((p + q - LO) * C::BN), ad, bd, C::IDESC, accumulate, collector);
+        for (int ks = 0; ks < C::KSTEPS; ++ks) {
+#pragma unroll
+            for (int pi = 0; pi < C::S * C::S; ++pi) {
+                int p = 0, q = 0, collector = 0;
+                if (!oz_product<C::S>(LO, HI, pi, p, q, collector)) break;
+                const uint32_t accumulate = (kb > 0 || ks > 0 || p > 0) ? 1u : 0u;
+                const uint64_t ad = smem_desc(sa + p * C::A_PLANE + ks * 32, C::SBO, C::LAYOUT);
+                const uint64_t bd = smem_desc(sb + q * C::B_PLANE + ks * 32, C::SBO, C::LAYOUT);
+                umma_i8_pair(tmem + uint32_t((p + q - LO) * C::BN), ad, bd, C::IDESC, accumulate, collector);
+            }
         }
         umma_commit_pair(&empty[s]);  // stage s is free in both CTAs once these MMAs have read it
     }
@@ -1462,11 +1470,15 @@ int run_ozaki(int slices, const int8_t* pa, i64 a_rows, i64 a_plane_rows, const 
     const bool pair = tuning().ozaki_cta_pair != 0;
     const int lo = slices <= 4 ? slices : 4;
     const int bbox = pair ? 64 : 128;
+    // slab width in bytes of k: 64 for the pair kernel (a last slab reaching past Kp reads
+    // TMA's zero fill), 32 for the single-CTA kernel
+    const int bkb = pair ? 64 : 32;
+    P.num_kb = int(cdiv(Kp, bkb));
     CUtensorMap ma, mb, mal, mbl;
-    MBG_TRY(make_map(&ma, pa, true, Kp, a_rows, slices, 32, BM, a_plane_rows));
-    MBG_TRY(make_map(&mal, pa, true, Kp, a_rows, lo, 32, BM, a_plane_rows));
-    MBG_TRY(make_map(&mb, pb, true, Kp, Np, slices, 32, bbox));
-    MBG_TRY(make_map(&mbl, pb, true, Kp, Np, lo, 32, bbox));
+    MBG_TRY(make_map(&ma, pa, true, Kp, a_rows, slices, bkb, BM, a_plane_rows));
+    MBG_TRY(make_map(&mal, pa, true, Kp, a_rows, lo, bkb, BM, a_plane_rows));
+    MBG_TRY(make_map(&mb, pb, true, Kp, Np, slices, bkb, bbox));
+    MBG_TRY(make_map(&mbl, pb, true, Kp, Np, lo, bkb, bbox));
 #define OZ_CASE(S_)                                                                    \
     case S_:                                                                           \
         return pair ? launch_ozaki_pair<Oz2Cfg<S_>>(ma, mb, mal, mbl, P)               \
