@@ -338,7 +338,7 @@ int   mbg_release_workspace(void);
  * "ozaki_cta_pair" — Ozaki products on CTA pairs (tcgen05 cta_group::2,
  * 256 x 128 tiles over two SMs): 1 one cluster per tile, 2 persistent clusters
  * (one per two SMs, the epilogue of a tile overlapping the next tile's products);
- * 0 (default): one CTA per 128 x 128 tile;
+ * 0: one CTA per 128 x 128 tile; default 2;
  * "ozaki_fused_slicing" — 1 (default): a K-contiguous Ozaki operand's exponents
  * and slices in one pass (0: the separate exponent and slicing kernels);
  * "grouped_simt_tile_<TT>_c<d>", "grouped_tc_bn_<TT>_c<d>" — grouped sgemm

@@ -42,18 +42,26 @@ constexpr int GBN = 128;       // widest tile (TMEM buffer stride)
 constexpr int GBKB = 64;       // k slab: 32 bf16 per row, 64-byte swizzle
 constexpr int GBK = 32;
 constexpr int GCHUNK = 4;      // slabs per TMEM accumulation chunk
-constexpr int GSTAGES = 4;
 constexpr int GPROD_WARPS = 4;
 constexpr int GMMA_WARP = 4;
 constexpr int GEPI_WARPS = 8;
 constexpr int GTHREADS = 32 * (GPROD_WARPS + 1 + GEPI_WARPS);
+// Raw fp32 staging: each producer thread copies its own row's 32 values of op(A) and of
+// op(B)^T for a slab into shared memory with cp.async, RAW_STAGES - 1 slabs ahead of the
+// one it splits, so the global-memory latency overlaps the splitting of earlier slabs
+// (a thread reads back only what it copied itself: no barrier is needed).  Row stride
+// 36 floats: 16-byte aligned, and the 16-byte reads of 32 rows spread over all banks.
+constexpr int GRAW_STAGES = 3;
+constexpr int GRAW_LD = 36;
+constexpr int GRAW_BYTES = 2 * BM * GRAW_LD * 4;  // op(A) rows then op(B)^T rows
 
 template <int TERMS>
 struct GCfg {
     static constexpr int A_PLANE = BM * GBKB;   // 8 KB
     static constexpr int B_PLANE = GBN * GBKB;  // 8 KB
     static constexpr int STAGE_BYTES = TERMS * (A_PLANE + B_PLANE);
-    static constexpr int SMEM_BYTES = GSTAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr int STAGES = TERMS == 3 ? 2 : 3;  // split planes in flight to the MMA warp
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + GRAW_STAGES * GRAW_BYTES + 1024 + 256;
     static constexpr int NPROD = TERMS * (TERMS + 1) / 2;
     static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 };
@@ -101,26 +109,28 @@ __device__ __forceinline__ void split_store16(const float (&v)[16], uint8_t* pla
     }
 }
 
-// 32 values of logical row `row` (of `rows`), k = k0 .. k0 + 31 (of K): element (row, l) at
-// src[row * rs + l * ks]; zero outside.  vec4: k contiguous (ks == 1) and 16-byte aligned rows.
-__device__ __forceinline__ void load_row32(const float* __restrict__ src, i64 rs, i64 ks, i64 rows, i64 K, i64 row,
-                                           i64 k0, bool vec4, float (&v)[32]) {
-    if (row >= rows) {
+// Copies the 32 values of logical row `row` (of `rows`), k = k0 .. k0 + 31 (of K), into
+// dst[0 .. 31] with cp.async: element (row, l) at src[row * rs + l * ks]; zero outside.
+// vec4: k contiguous (ks == 1) and 16-byte aligned rows (16-byte copies).
+__device__ __forceinline__ void copy_row32(float* dst, const float* __restrict__ src, i64 rs, i64 ks, i64 rows,
+                                           i64 K, i64 row, i64 k0, bool vec4) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    if (row < rows && vec4 && k0 + 32 <= K) {
+        const float* p = src + row * rs + k0;
 #pragma unroll
-        for (int l = 0; l < 32; ++l) v[l] = 0.0f;
+        for (int q = 0; q < 8; ++q)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d + 16 * q), "l"(p + 4 * q) : "memory");
         return;
     }
-    const float* p = src + row * rs + k0 * ks;
-    if (vec4 && k0 + 32 <= K) {
+    const bool live = row < rows;
+    const float* p = src + (live ? row * rs + k0 * ks : 0);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const float4 f = __ldg(reinterpret_cast<const float4*>(p) + q);
-            v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
-        }
-        return;
+    for (int l = 0; l < 32; ++l) {
+        const bool v = live && k0 + l < K;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d + 4 * l), "l"(v ? p + l * ks : src),
+                     "r"(v ? 4 : 0)
+                     : "memory");
     }
-#pragma unroll
-    for (int l = 0; l < 32; ++l) v[l] = (k0 + l < K) ? __ldg(p + l * ks) : 0.0f;
 }
 
 template <int TERMS>
@@ -129,15 +139,16 @@ grouped_tc_kernel(const TcDesc* __restrict__ probs, const TcTile* __restrict__ t
     using C = GCfg<TERMS>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + GSTAGES * C::STAGE_BYTES);
-    uint64_t* empty = full + GSTAGES;
-    uint64_t* tfull = empty + GSTAGES;  // [2]
+    float* raw = reinterpret_cast<float*>(smem + C::STAGES * C::STAGE_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES + GRAW_STAGES * GRAW_BYTES);
+    uint64_t* empty = full + C::STAGES;
+    uint64_t* tfull = empty + C::STAGES;  // [2]
     uint64_t* tempty = tfull + 2;       // [2]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < GSTAGES; ++s) {
+        for (int s = 0; s < C::STAGES; ++s) {
             mbar_init(&full[s], 32 * GPROD_WARPS);
             mbar_init(&empty[s], 1);
         }
@@ -157,41 +168,75 @@ grouped_tc_kernel(const TcDesc* __restrict__ probs, const TcTile* __restrict__ t
     const uint32_t tmem = *tmem_slot;
 
     if (warp < GPROD_WARPS) {
-        // ---------------- producers: load, split, store ----------------
+        // ---------------- producers: copy (cp.async), split, store ----------------
         const int r = threadIdx.x;  // tile row 0..127
+        // the slabs of this CTA's tiles form one sequence; `ahead` walks it RAW_STAGES - 1
+        // slabs in front of the one being split
+        int at = blockIdx.x, akb = 0;  // look-ahead cursor: tile and slab
+        auto issue_next = [&](int slot) {
+            while (at < ntiles && akb >= tiles[at].nkb) {
+                at += gridDim.x;
+                akb = 0;
+            }
+            if (at < ntiles) {
+                const TcTile tl = tiles[at];
+                const TcDesc d = probs[tl.prob];
+                const i64 m0 = i64(tl.tm) * BM, n0 = i64(tl.tn) * d.bn, k0 = i64(akb) * GBK;
+                float* ra = raw + slot * (GRAW_BYTES / 4) + r * GRAW_LD;
+                float* rb = ra + BM * GRAW_LD;
+                // op(A)(i, l): A^T -> a[l + i lda] (k contiguous), else a[i + l lda]
+                copy_row32(ra, d.a, d.ta ? d.lda : 1, d.ta ? 1 : d.lda, d.m, d.k, m0 + r, k0,
+                           d.ta && d.lda % 4 == 0 && reinterpret_cast<uintptr_t>(d.a) % 16 == 0);
+                // op(B)^T(j, l) = op(B)(l, j): B^T -> b[j + l ldb], else b[l + j ldb] (k contiguous)
+                if (r < d.bn)
+                    copy_row32(rb, d.b, d.tb ? 1 : d.ldb, d.tb ? d.ldb : 1, d.n, d.k, n0 + r, k0,
+                               !d.tb && d.ldb % 4 == 0 && reinterpret_cast<uintptr_t>(d.b) % 16 == 0);
+                ++akb;
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");  // one group per slab, empty at the end
+        };
+        for (int i = 0; i < GRAW_STAGES - 1; ++i) issue_next(i);
         int it = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            const TcTile tl = tiles[t];
-            const TcDesc d = probs[tl.prob];
-            const i64 m0 = i64(tl.tm) * BM, n0 = i64(tl.tn) * d.bn;
-            // op(A)(i, l): A^T -> a[l + i lda] (k contiguous), else a[i + l lda]
-            const i64 ars = d.ta ? d.lda : 1, aks = d.ta ? 1 : d.lda;
-            // op(B)^T(j, l) = op(B)(l, j): B^T -> b[j + l ldb], else b[l + j ldb] (k contiguous)
-            const i64 brs = d.tb ? 1 : d.ldb, bks = d.tb ? d.ldb : 1;
-            const bool va = d.ta && (d.lda % 4 == 0) && (reinterpret_cast<uintptr_t>(d.a) % 16 == 0);
-            const bool vb = !d.tb && (d.ldb % 4 == 0) && (reinterpret_cast<uintptr_t>(d.b) % 16 == 0);
-            const bool brow = r < d.bn;
-            for (int kb = 0; kb < tl.nkb; ++kb, ++it) {
-                const int s = it % GSTAGES;
-                const i64 k0 = i64(kb) * GBK;
-                float va_[32], vb_[32];
-                load_row32(d.a, ars, aks, d.m, d.k, m0 + r, k0, va, va_);
-                if (brow) load_row32(d.b, brs, bks, d.n, d.k, n0 + r, k0, vb, vb_);
-                if (!mbar_wait(&empty[s], ((it / GSTAGES) & 1) ^ 1, err, 31)) { ok = false; break; }
+            const int nkb = tiles[t].nkb;
+            const bool brow = r < probs[tiles[t].prob].bn;
+            for (int kb = 0; kb < nkb; ++kb, ++it) {
+                issue_next((it + GRAW_STAGES - 1) % GRAW_STAGES);
+                asm volatile("cp.async.wait_group %0;\n" ::"n"(GRAW_STAGES - 1) : "memory");  // slab `it` landed
+                const float* ra = raw + (it % GRAW_STAGES) * (GRAW_BYTES / 4) + r * GRAW_LD;
+                const float* rb = ra + BM * GRAW_LD;
+                const int s = it % C::STAGES;
+                if (!mbar_wait(&empty[s], ((it / C::STAGES) & 1) ^ 1, err, 31)) { ok = false; break; }
                 uint8_t* sa = smem + s * C::STAGE_BYTES;
                 uint8_t* sb = sa + TERMS * C::A_PLANE;
-                split_store16<TERMS>(*reinterpret_cast<const float(*)[16]>(va_), sa, C::A_PLANE, r, 0);
-                split_store16<TERMS>(*reinterpret_cast<const float(*)[16]>(va_ + 16), sa, C::A_PLANE, r, 2);
+                float v[16];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float4 f = reinterpret_cast<const float4*>(ra + 16 * h)[q];
+                        v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
+                    }
+                    split_store16<TERMS>(v, sa, C::A_PLANE, r, 2 * h);
+                }
                 if (brow) {
-                    split_store16<TERMS>(*reinterpret_cast<const float(*)[16]>(vb_), sb, C::B_PLANE, r, 0);
-                    split_store16<TERMS>(*reinterpret_cast<const float(*)[16]>(vb_ + 16), sb, C::B_PLANE, r, 2);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float4 f = reinterpret_cast<const float4*>(rb + 16 * h)[q];
+                            v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
+                        }
+                        split_store16<TERMS>(v, sb, C::B_PLANE, r, 2 * h);
+                    }
                 }
                 // generic-proxy stores must be visible to the tensor core's (async proxy) reads
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_arrive(&full[s]);
             }
         }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy lands after the CTA exits
     } else if (warp == GMMA_WARP) {
         if (lane == 0) {
             // ---------------- MMA issuer ----------------
@@ -206,8 +251,8 @@ grouped_tc_kernel(const TcDesc* __restrict__ probs, const TcTile* __restrict__ t
                         if (!mbar_wait(&tempty[buf], ((ch >> 1) - 1) & 1, err, 32)) { ok = false; break; }
                         tc_fence_after();
                     }
-                    const int s = it % GSTAGES;
-                    if (!mbar_wait(&full[s], (it / GSTAGES) & 1, err, 33)) { ok = false; break; }
+                    const int s = it % C::STAGES;
+                    if (!mbar_wait(&full[s], (it / C::STAGES) & 1, err, 33)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t sa = smem_u32(smem + s * C::STAGE_BYTES);
                     const uint32_t sb = sa + TERMS * C::A_PLANE;

@@ -19,6 +19,7 @@
 #include "mbg_internal.cuh"
 
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -153,6 +154,31 @@ Stager* stager() {
     return s;
 }
 
+// How pageable host memory is moved: 0 (default) through the bounce buffers, 1 the driver's
+// own staged copy, 2 the region page-locked for the duration of the copy (cudaHostRegister).
+// Read once from MBG_PAGEABLE_MODE; the alternatives are kept for measurements on new hosts.
+int pageable_mode() {
+    static const int mode = [] {
+        const char* e = std::getenv("MBG_PAGEABLE_MODE");
+        const int v = e ? std::atoi(e) : 0;
+        return (v >= 0 && v <= 2) ? v : 0;
+    }();
+    return mode;
+}
+
+// Page-locks the pages under [p, p + bytes) for one copy; false if the driver refuses
+// (e.g. part of the range is registered already), in which case nothing was locked.
+bool register_range(const void* p, size_t bytes, void** base) {
+    const uintptr_t page = 4096, a = reinterpret_cast<uintptr_t>(p) & ~(page - 1);
+    const uintptr_t b = (reinterpret_cast<uintptr_t>(p) + bytes + page - 1) & ~(page - 1);
+    if (cudaHostRegister(reinterpret_cast<void*>(a), b - a, cudaHostRegisterDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    *base = reinterpret_cast<void*>(a);
+    return true;
+}
+
 }  // namespace
 
 bool is_pinned_host(const void* p) {
@@ -167,8 +193,17 @@ bool is_pinned_host(const void* p) {
 int copy_h2d_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
                 cudaStream_t s) {
     if (width == 0 || height == 0) return MBG_OK;
-    if (is_pinned_host(src) || width > STAGE_BUF) {
+    if (is_pinned_host(src) || width > STAGE_BUF || pageable_mode() == 1) {
         MBG_CUDA(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyHostToDevice, s));
+        return MBG_OK;
+    }
+    void* reg = nullptr;
+    if (pageable_mode() == 2 && register_range(src, (height - 1) * spitch + width, &reg)) {
+        const cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyHostToDevice, s);
+        const cudaError_t w = e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+        cudaHostUnregister(reg);
+        MBG_CUDA(e);
+        MBG_CUDA(w);
         return MBG_OK;
     }
     Stager* st = stager();
@@ -196,9 +231,20 @@ int copy_h2d_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t
 int copy_d2h_2d(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
                 cudaStream_t s, cudaEvent_t after) {
     if (width == 0 || height == 0) return MBG_OK;
-    if (is_pinned_host(dst) || width > STAGE_BUF) {
+    if (is_pinned_host(dst) || width > STAGE_BUF || pageable_mode() == 1) {
         if (after) MBG_CUDA(cudaStreamWaitEvent(s, after, 0));
         MBG_CUDA(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyDeviceToHost, s));
+        return MBG_OK;
+    }
+    void* reg = nullptr;
+    if (pageable_mode() == 2 && register_range(dst, (height - 1) * dpitch + width, &reg)) {
+        cudaError_t e = after ? cudaStreamWaitEvent(s, after, 0) : cudaSuccess;
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyDeviceToHost, s);
+        const cudaError_t w = e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+        cudaHostUnregister(reg);
+        MBG_CUDA(e);
+        MBG_CUDA(w);
         return MBG_OK;
     }
     Stager* st = stager();
