@@ -399,6 +399,7 @@ int mbg_set_tuning(const char* key, int64_t value) {
     if (k == "plain_fp64_simt" && (value == 0 || value == 1)) { tuning().plain_fp64_simt = value; return MBG_OK; }
     if (k == "plain_fp32_staged" && (value == 0 || value == 1)) { tuning().plain_fp32_staged = value; return MBG_OK; }
     if (k == "ozaki_cta_pair" && value >= 0 && value <= 2) { tuning().ozaki_cta_pair = value; return MBG_OK; }
+    if (k == "trsm_preslice" && (value == 0 || value == 1)) { tuning().trsm_preslice = value; return MBG_OK; }
     if (k == "ozaki_fused_slicing" && (value == 0 || value == 1)) {
         tuning().ozaki_fused_slicing = value;
         return MBG_OK;
@@ -420,6 +421,7 @@ int64_t mbg_get_tuning(const char* key) {
     if (k == "plain_fp32_staged") return tuning().plain_fp32_staged;
     if (k == "ozaki_cta_pair") return tuning().ozaki_cta_pair;
     if (k == "ozaki_fused_slicing") return tuning().ozaki_fused_slicing;
+    if (k == "trsm_preslice") return tuning().trsm_preslice;
     return -1;
 }
 

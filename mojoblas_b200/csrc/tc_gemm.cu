@@ -1255,11 +1255,23 @@ slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K
     const size_t plane = size_t(Rp) * size_t(Kp);
     const double* row = src + r * ld;
     const bool live = r < rows;
+    // 16-byte loads when the row starts 16-byte aligned and no triangle mask applies
+    const bool vec = keep == 0 && (reinterpret_cast<uintptr_t>(row) & 15) == 0;
     double mx = 0.0;
     if (live) {
+        if (vec) {
+            i64 l = 2 * i64(lane);
+#pragma unroll 4
+            for (; l + 1 < K; l += 64) {
+                const double2 v = *reinterpret_cast<const double2*>(row + l);
+                mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+            }
+            if (l < K) mx = fmax(mx, fabs(row[l]));
+        } else {
 #pragma unroll 8
-        for (i64 l = lane; l < K; l += 32)
-            if (kept(keep, r, l)) mx = fmax(mx, fabs(row[l]));
+            for (i64 l = lane; l < K; l += 32)
+                if (kept(keep, r, l)) mx = fmax(mx, fabs(row[l]));
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -1268,22 +1280,37 @@ slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K
     if (live && lane == 0) e[r] = er;
     const int B = 8 * slices - 2;
     const unsigned long long bias = 0x8080808080808080ULL >> (64 - 8 * slices);
-    for (i64 l0 = i64(lane) * 4; l0 < Kp; l0 += 128) {
-        unsigned long long H[4];
+    // eight consecutive k per lane and iteration (Kp is a multiple of 32, so all eight are inside Kp)
+    for (i64 l0 = i64(lane) * 8; l0 < Kp; l0 += 256) {
+        double x[8];
+        if (live && vec && l0 + 8 <= K) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const i64 l = l0 + u;
-            const double v = (live && l < K && kept(keep, r, l)) ? row[l] : 0.0;
-            H[u] = static_cast<unsigned long long>(oz_fixed(v, er, B)) + bias;
+            for (int q = 0; q < 4; ++q) {
+                const double2 v = *reinterpret_cast<const double2*>(row + l0 + 2 * q);
+                x[2 * q] = v.x;
+                x[2 * q + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const i64 l = l0 + u;
+                x[u] = (live && l < K && kept(keep, r, l)) ? row[l] : 0.0;
+            }
         }
-        unsigned* out = reinterpret_cast<unsigned*>(planes + size_t(r) * Kp + l0);
+        unsigned long long H[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) H[u] = static_cast<unsigned long long>(oz_fixed(x[u], er, B)) + bias;
+        uint2* out = reinterpret_cast<uint2*>(planes + size_t(r) * Kp + l0);
         for (int p = 0; p < slices; ++p) {
             const int byte = slices - 1 - p;
             const int sh = 8 * (byte & 3), hiword = byte & 4 ? 32 : 0;
-            unsigned packed = 0;
+            unsigned lo = 0, hi = 0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) packed |= ((unsigned(H[u] >> hiword) >> sh) & 255u) << (8 * u);
-            out[(plane / 4) * p] = packed ^ 0x80808080u;
+            for (int u = 0; u < 4; ++u) {
+                lo |= ((unsigned(H[u] >> hiword) >> sh) & 255u) << (8 * u);
+                hi |= ((unsigned(H[u + 4] >> hiword) >> sh) & 255u) << (8 * u);
+            }
+            out[(plane / 8) * p] = make_uint2(lo ^ 0x80808080u, hi ^ 0x80808080u);
         }
     }
 }

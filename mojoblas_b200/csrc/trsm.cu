@@ -30,6 +30,8 @@
 #include "mbg_internal.cuh"
 #include "block_solve.cuh"
 
+#include <vector>
+
 namespace mbg {
 
 namespace {
@@ -499,10 +501,43 @@ template <> struct InvPlanes<double> {
     }
 };
 
+// The off-diagonal update blocks op(A)21 (op(A)12 for an upper triangle) of the recursion,
+// in the order the solve uses them: (row r of the sub-problem, m1, m2).
+struct UpdateBlock {
+    i64 r, m1, m2;
+};
+inline void collect_updates(bool lower, i64 r, i64 m, i64 nbi, std::vector<UpdateBlock>& out) {
+    if (m <= nbi) return;
+    const i64 m1 = cdiv(cdiv(m, 2), nbi) * nbi, m2 = m - m1;
+    if (lower) {
+        collect_updates(lower, r, m1, nbi, out);
+        out.push_back({r, m1, m2});
+        collect_updates(lower, r + m1, m2, nbi, out);
+    } else {
+        collect_updates(lower, r + m1, m2, nbi, out);
+        out.push_back({r, m1, m2});
+        collect_updates(lower, r, m1, nbi, out);
+    }
+}
+
+// Ozaki solves: every update block's slices are made up front on a second stream, so the
+// slicing of op(A) (which does not depend on the solution) runs beside the leaves and
+// updates instead of before each update; each update waits only for its own block.
+struct PreSlicedUpdates {
+    std::vector<OzakiA> planes;      // in use order
+    std::vector<cudaEvent_t> ready;  // recorded on the second stream after each block's slices
+    size_t next = 0;
+    bool on = false;
+    ~PreSlicedUpdates() {
+        for (auto e : ready)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
 // op(A)[r:r+m, r:r+m] X = B (in place; b points at row r of B), leaves from the inverses.
 template <typename T>
-int solve_left_inv_rec(const InvPlanes<T>& inv, int mode, int slices, bool lower, bool trans, i64 r, i64 m, i64 n,
-                       const T* a, i64 lda, T* b, i64 ldb) {
+int solve_left_inv_rec(const InvPlanes<T>& inv, PreSlicedUpdates& pre, int mode, int slices, bool lower, bool trans,
+                       i64 r, i64 m, i64 n, const T* a, i64 lda, T* b, i64 ldb) {
     const i64 nbi = inv_block_rows<T>();
     if (m <= nbi) {
         ProfScope prof("trsm_inverse_leaf");
@@ -511,16 +546,72 @@ int solve_left_inv_rec(const InvPlanes<T>& inv, int mode, int slices, bool lower
     const i64 m1 = cdiv(cdiv(m, 2), nbi) * nbi, m2 = m - m1;
     const char tc = trans ? 'T' : 'N';
     const T* ar = a + r + r * lda;  // op(A)[r, r]
+    // B_dst -= op(A)block B_src: rows x k
+    auto update = [&](const T* ablk, i64 rows, i64 k, const T* bsrc, T* bdst) -> int {
+        if constexpr (sizeof(T) == 8) {
+            if (pre.on) {
+                const size_t i = pre.next++;
+                MBG_CUDA(cudaStreamWaitEvent(stream(), pre.ready[i], 0));
+                return dgemm_ozaki_tc_with_a(pre.planes[i], 0, rows, k, 'N', n, -1.0, bsrc, ldb, 1.0, bdst, ldb);
+            }
+        }
+        return gemm_in_mode(mode, slices, tc, 'N', rows, n, k, T(-1), ablk, lda, bsrc, ldb, T(1), bdst, ldb);
+    };
     if (lower) {
-        MBG_TRY(solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r, m1, n, a, lda, b, ldb));
-        MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m2, n, m1, T(-1), op_at(ar, lda, trans, m1, 0), lda, b, ldb,
-                             T(1), b + m1, ldb));
-        return solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r + m1, m2, n, a, lda, b + m1, ldb);
+        MBG_TRY(solve_left_inv_rec<T>(inv, pre, mode, slices, lower, trans, r, m1, n, a, lda, b, ldb));
+        MBG_TRY(update(op_at(ar, lda, trans, m1, 0), m2, m1, b, b + m1));
+        return solve_left_inv_rec<T>(inv, pre, mode, slices, lower, trans, r + m1, m2, n, a, lda, b + m1, ldb);
     }
-    MBG_TRY(solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r + m1, m2, n, a, lda, b + m1, ldb));
-    MBG_TRY(gemm_in_mode(mode, slices, tc, 'N', m1, n, m2, T(-1), op_at(ar, lda, trans, 0, m1), lda, b + m1, ldb,
-                         T(1), b, ldb));
-    return solve_left_inv_rec<T>(inv, mode, slices, lower, trans, r, m1, n, a, lda, b, ldb);
+    MBG_TRY(solve_left_inv_rec<T>(inv, pre, mode, slices, lower, trans, r + m1, m2, n, a, lda, b + m1, ldb));
+    MBG_TRY(update(op_at(ar, lda, trans, 0, m1), m1, m2, b + m1, b));
+    return solve_left_inv_rec<T>(inv, pre, mode, slices, lower, trans, r, m1, n, a, lda, b, ldb);
+}
+
+// Slices of every update block of an Ozaki solve, on the second stream (see above).
+inline int pre_slice_updates(int slices, bool lower, bool trans, i64 m, const double* a, i64 lda,
+                             PreSlicedUpdates& pre) {
+    std::vector<UpdateBlock> ub;
+    collect_updates(lower, 0, m, inv_block_rows<double>(), ub);
+    if (ub.empty()) return MBG_OK;
+    for (const auto& u : ub)
+        if ((lower ? u.m1 : u.m2) > ozaki_max_k(slices)) return MBG_OK;  // longer reductions: sliced per update
+    cudaStream_t s = stream(), aux = nullptr;
+    MBG_TRY(aux_stream(&aux));
+    cudaEvent_t start = nullptr;
+    MBG_CUDA(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    const cudaError_t e1 = cudaEventRecord(start, s);  // A is ready once the work before this call is
+    const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(aux, start, 0) : e1;
+    cudaEventDestroy(start);
+    MBG_CUDA(e2);
+    pre.planes.resize(ub.size());
+    pre.ready.assign(ub.size(), nullptr);
+    StreamScope on_aux(aux);
+    const char tc = trans ? 'T' : 'N';
+    for (size_t i = 0; i < ub.size(); ++i) {
+        const UpdateBlock& u = ub[i];
+        const double* ar = a + u.r + u.r * lda;
+        if (lower) MBG_TRY(ozaki_slice_a(slices, tc, u.m2, u.m1, op_at(ar, lda, trans, u.m1, 0), lda, pre.planes[i]));
+        else MBG_TRY(ozaki_slice_a(slices, tc, u.m1, u.m2, op_at(ar, lda, trans, 0, u.m1), lda, pre.planes[i]));
+        MBG_CUDA(cudaEventCreateWithFlags(&pre.ready[i], cudaEventDisableTiming));
+        MBG_CUDA(cudaEventRecord(pre.ready[i], aux));
+    }
+    pre.on = true;
+    return MBG_OK;
+}
+
+// Before the pre-sliced planes go back to the second stream's workspace pool, that stream
+// waits for the solve's work that reads them.
+inline int release_pre_sliced(PreSlicedUpdates& pre) {
+    if (!pre.on) return MBG_OK;
+    cudaStream_t aux = nullptr;
+    MBG_TRY(aux_stream(&aux));
+    cudaEvent_t done = nullptr;
+    MBG_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    const cudaError_t e1 = cudaEventRecord(done, stream());
+    const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(aux, done, 0) : e1;
+    cudaEventDestroy(done);
+    MBG_CUDA(e2);
+    return MBG_OK;
 }
 
 // Whether the inverted-block solve runs: a split / Ozaki mode, more than one diagonal block,
@@ -539,9 +630,15 @@ int solve_left_inv(int mode, int slices, bool lower, bool trans, bool unit, i64 
     Workspace ww;
     MBG_TRY(ww.reserve(sizeof(T) * size_t(m) * size_t(nbi)));
     MBG_TRY(invert_diagonal_blocks<T>(lower, trans, unit, m, nbi, a, lda, ww.as<T>()));
+    PreSlicedUpdates pre;
+    if constexpr (sizeof(T) == 8) {
+        if (mode == MBG_MODE_OZAKI && tuning().trsm_preslice) MBG_TRY(pre_slice_updates(slices, lower, trans, m, a, lda, pre));
+    }
     InvPlanes<T> inv;
-    MBG_TRY(inv.make(mode, slices, m, nbi, ww.as<T>()));
-    return solve_left_inv_rec<T>(inv, mode, slices, lower, trans, 0, m, n, a, lda, b, ldb);
+    int st = inv.make(mode, slices, m, nbi, ww.as<T>());
+    if (!st) st = solve_left_inv_rec<T>(inv, pre, mode, slices, lower, trans, 0, m, n, a, lda, b, ldb);
+    const int rel = release_pre_sliced(pre);
+    return st ? st : rel;
 }
 
 int accurate_mode(float) { return MBG_MODE_BF16X6; }
