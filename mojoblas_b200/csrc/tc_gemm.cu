@@ -568,8 +568,8 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
                 uint8_t* sb = sa + C::S * C::PLANE;
                 mbar_expect_tx(&full[s], uint32_t(2 * planes * C::PLANE));
                 const bool all = planes == C::S;
-                tma_load_3d(sa, all ? &tmA : &tmAlo, &full[s], (kb0 + kb) * C::BKB, int(m0), 0);
-                tma_load_3d(sb, all ? &tmB : &tmBlo, &full[s], (kb0 + kb) * C::BKB, int(n0), 0);
+                tma_load_4d(sa, all ? &tmA : &tmAlo, &full[s], 0, int(m0), kb0 + kb, 0);
+                tma_load_4d(sb, all ? &tmB : &tmBlo, &full[s], 0, int(n0), kb0 + kb, 0);
             }
             for (int it = max(0, total - C::STAGES); it < total; ++it)
                 mbar_wait(&full[it % C::STAGES], (it / C::STAGES) & 1, P.err, 12);
@@ -653,19 +653,20 @@ struct Oz2Cfg {
     static constexpr int S = S_;
     static constexpr int BN = 128;                    // output columns of the pair's tile
     static constexpr int BNH = BN / 2;                // op(B)^T rows staged by each CTA
-    // k slab: 64 int8 per row (two 32-deep MMA steps), 64-byte swizzle.  Each TMA row
-    // request then carries two 32-byte sectors: with 32-byte slabs the loads were bound
-    // by the SM's L1-to-L2 request rate (ncu: l1tex2xbar requests 85 % busy for 21 % of
-    // the read bandwidth), not by bytes
-    static constexpr int BKB = 64;
+    // k slab: 32 int8 per row (one 32-deep MMA step), 32-byte swizzle; the planes are
+    // stored slab-major (all rows' 32-byte pieces of a slab contiguous), so one TMA box
+    // is a few contiguous kilobytes per plane, not one 32-byte request per row (which
+    // bound the loads by the SM's L1-to-L2 request rate), and a stage stays small enough
+    // for four of them
+    static constexpr int BKB = 32;
     static constexpr int KSTEPS = BKB / 32;
     static constexpr int EPI_WARPS = 8;
     static constexpr int THREADS = 64 + 32 * EPI_WARPS;
     static constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // 64
     static constexpr int NPASS = S <= 4 ? 1 : 2;
     static constexpr int SPLIT = S <= 4 ? 0 : 4;
-    static constexpr int A_PLANE = BM * BKB;          // 8 KB
-    static constexpr int B_PLANE = BNH * BKB;         // 4 KB
+    static constexpr int A_PLANE = BM * BKB;          // 4 KB
+    static constexpr int B_PLANE = BNH * BKB;         // 2 KB
     static constexpr int STAGE_BYTES = S * (A_PLANE + B_PLANE);
     static constexpr int STAGES = (196608 / STAGE_BYTES) > 8 ? 8 : (196608 / STAGE_BYTES);
     // at least 120 KB, so one CTA per SM: two pairs interleaved on the same two SMs could
@@ -673,9 +674,9 @@ struct Oz2Cfg {
     static constexpr int SMEM_USED = STAGES * STAGE_BYTES + 1024 + 256;
     static constexpr int SMEM_BYTES = SMEM_USED > 122880 ? SMEM_USED : 122880;
     static constexpr uint32_t IDESC = instr_desc(true, 2 * BM, BN);  // M = 256 over the pair
-    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 4;
+    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 6;
     static_assert(STAGES >= 2, "pipeline depth");
-    static_assert(A_PLANE % 512 == 0 && B_PLANE % 512 == 0, "64-byte swizzle atoms stay aligned");
+    static_assert(A_PLANE % 256 == 0 && B_PLANE % 256 == 0, "32-byte swizzle atoms stay aligned");
 };
 
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -697,12 +698,12 @@ __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_bar) {
 }
 // TMA load into this CTA's shared memory whose completion is counted on an
 // mbarrier of either CTA of the pair (the leader's); no multicast.
-__device__ __forceinline__ void tma_load_3d_pair(void* dst, const CUtensorMap* map, uint32_t cluster_bar, int c0,
-                                                 int c1, int c2) {
+__device__ __forceinline__ void tma_load_4d_pair(void* dst, const CUtensorMap* map, uint32_t cluster_bar, int c0,
+                                                 int c1, int c2, int c3) {
     asm volatile(
-        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(cluster_bar), "r"(c0), "r"(c1), "r"(c2)
+        "cp.async.bulk.tensor.4d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(cluster_bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
 }
 __device__ __forceinline__ void tmem_alloc_pair(uint32_t* slot, uint32_t ncols) {
@@ -872,9 +873,9 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         uint8_t* sb = sa + C::S * C::A_PLANE;
                         if (rank == 0) mbar_expect_tx(&full[s], uint32_t(2 * planes * (C::A_PLANE + C::B_PLANE)));
                         const uint32_t bar = peer_addr(&full[s], 0);
-                        tma_load_3d_pair(sa, all ? &tmA : &tmAlo, bar, (T.kb0 + kb) * C::BKB, int(m0), 0);
-                        tma_load_3d_pair(sb, all ? &tmB : &tmBlo, bar, (T.kb0 + kb) * C::BKB,
-                                         int(T.n0 + rank * C::BNH), 0);
+                        tma_load_4d_pair(sa, all ? &tmA : &tmAlo, bar, 0, int(m0), T.kb0 + kb, 0);
+                        tma_load_4d_pair(sb, all ? &tmB : &tmBlo, bar, 0, int(T.n0 + rank * C::BNH), T.kb0 + kb,
+                                         0);
                     }
                 }
             }
@@ -1125,6 +1126,14 @@ __device__ __forceinline__ long long oz_fixed(double v, int er, int B) {
     return (b >> 63) ? -static_cast<long long>(F) : static_cast<long long>(F);
 }
 
+// Ozaki planes are stored slab-major: plane p holds, for each 32-deep k slab in turn, the
+// 32-byte pieces of all Rp rows back to back, so element (r, l) of a plane sits at
+//     (l / 32) (Rp 32) + r 32 + l % 32.
+// One TMA box (32 bytes of k, a block of rows, every plane) is then a contiguous run per plane.
+__host__ __device__ __forceinline__ size_t oz_plane_offset(i64 Rp, i64 r, i64 l) {
+    return size_t(l >> 5) * size_t(Rp) * 32 + size_t(r) * 32 + size_t(l & 31);
+}
+
 template <bool KMAJOR>
 __global__ void __launch_bounds__(256)
 slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
@@ -1153,7 +1162,7 @@ slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp,
 #pragma unroll
         for (int u = 0; u < 4; ++u)
             H[u] = static_cast<unsigned long long>(oz_fixed(tile[rr][lq + u], er, B)) + bias;
-        unsigned* out = reinterpret_cast<unsigned*>(planes + size_t(r) * Kp + l0 + lq);
+        unsigned* out = reinterpret_cast<unsigned*>(planes + oz_plane_offset(Rp, r, l0 + lq));
         for (int p = 0; p < slices; ++p) {
             const int byte = slices - 1 - p;
             const int sh = 8 * (byte & 3), hiword = byte & 4 ? 32 : 0;
@@ -1206,6 +1215,31 @@ int make_map(CUtensorMap* map, const void* base, bool int8, i64 Kp, i64 Rp, int 
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error_msg("cuTensorMapEncodeTiled failed (code " + std::to_string(int(r)) + ")");
+        return MBG_ERR_CUDA;
+    }
+    return MBG_OK;
+}
+
+// 4-D map over slab-major Ozaki planes (oz_plane_offset): dims {32 bytes of k, rows, slabs,
+// planes}, the rows of each slab plane_rows * 32 bytes apart, planes plane_rows * Kp bytes
+// apart; the map covers `rows` rows from `base` (a row block of taller planes when
+// rows < plane_rows); box = {32, box_rows, 1, planes}: in shared memory the planes' tiles
+// follow each other, rows 32 bytes apart (the 32-byte swizzled K-major layout).
+int make_slab_map(CUtensorMap* map, const void* base, i64 Kp, i64 rows, i64 plane_rows, int planes, int box_rows) {
+    auto fn = encode_fn();
+    if (!fn) {
+        set_error_msg("cuTensorMapEncodeTiled is unavailable from the driver");
+        return MBG_ERR_CUDA;
+    }
+    cuuint64_t dims[4] = {32, cuuint64_t(rows), cuuint64_t(Kp / 32), cuuint64_t(planes)};
+    cuuint64_t strides[3] = {32, cuuint64_t(plane_rows) * 32, cuuint64_t(plane_rows) * cuuint64_t(Kp)};
+    cuuint32_t box[4] = {32, cuuint32_t(box_rows), 1, cuuint32_t(planes)};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error_msg("cuTensorMapEncodeTiled (slab-major planes) failed (code " + std::to_string(int(r)) + ")");
         return MBG_ERR_CUDA;
     }
     return MBG_OK;
@@ -1300,7 +1334,7 @@ slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K
         unsigned long long H[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) H[u] = static_cast<unsigned long long>(oz_fixed(x[u], er, B)) + bias;
-        uint2* out = reinterpret_cast<uint2*>(planes + size_t(r) * Kp + l0);
+        uint2* out = reinterpret_cast<uint2*>(planes + oz_plane_offset(Rp, r, l0));
         for (int p = 0; p < slices; ++p) {
             const int byte = slices - 1 - p;
             const int sh = 8 * (byte & 3), hiword = byte & 4 ? 32 : 0;
@@ -1497,15 +1531,12 @@ int run_ozaki(int slices, const int8_t* pa, i64 a_rows, i64 a_plane_rows, const 
     const bool pair = tuning().ozaki_cta_pair != 0;
     const int lo = slices <= 4 ? slices : 4;
     const int bbox = pair ? 64 : 128;
-    // slab width in bytes of k: 64 for the pair kernel (a last slab reaching past Kp reads
-    // TMA's zero fill), 32 for the single-CTA kernel
-    const int bkb = pair ? 64 : 32;
-    P.num_kb = int(cdiv(Kp, bkb));
+    P.num_kb = int(Kp / 32);
     CUtensorMap ma, mb, mal, mbl;
-    MBG_TRY(make_map(&ma, pa, true, Kp, a_rows, slices, bkb, BM, a_plane_rows));
-    MBG_TRY(make_map(&mal, pa, true, Kp, a_rows, lo, bkb, BM, a_plane_rows));
-    MBG_TRY(make_map(&mb, pb, true, Kp, Np, slices, bkb, bbox));
-    MBG_TRY(make_map(&mbl, pb, true, Kp, Np, lo, bkb, bbox));
+    MBG_TRY(make_slab_map(&ma, pa, Kp, a_rows, a_plane_rows, slices, BM));
+    MBG_TRY(make_slab_map(&mal, pa, Kp, a_rows, a_plane_rows, lo, BM));
+    MBG_TRY(make_slab_map(&mb, pb, Kp, Np, Np, slices, bbox));
+    MBG_TRY(make_slab_map(&mbl, pb, Kp, Np, Np, lo, bbox));
 #define OZ_CASE(S_)                                                                    \
     case S_:                                                                           \
         return pair ? launch_ozaki_pair<Oz2Cfg<S_>>(ma, mb, mal, mbl, P)               \
@@ -1559,7 +1590,7 @@ int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n
     int* eb = reinterpret_cast<int*>(pb + (b_bytes + 1023) / 1024 * 1024);
     MBG_TRY(launch_slices(b, ldb, is_n(tb), n, k, Np, A.Kp, slices, eb, pb));
     const i64 rows = imin(roundup(mb, BM), A.Mp - r0);
-    const int8_t* pa = A.planes + size_t(r0) * A.Kp;
+    const int8_t* pa = A.planes + size_t(r0) * 32;  // row r0 of every slab (slab-major planes)
     OzParams P{};
     P.m = mb; P.n = n; P.num_kb = int(A.Kp / 32);
     P.tiles_m = int(cdiv(mb, BM)); P.tiles_n = int(cdiv(n, BN));
