@@ -7,19 +7,23 @@
 // 512 rows that pre-pass would cost more than the products, and TMA needs
 // 16-byte-aligned leading dimensions that batched callers rarely have.  Here the
 // split is fused into the kernel's producer warps:
-//   warps 0..3   producers: thread r owns row r of the tile's op(A) slab and row r
-//                of its op(B)^T slab (32 k each), loads them from global memory
-//                (coalesced across the warp when rows are contiguous, 16-byte
-//                loads along k when k is contiguous and aligned), splits each
-//                value into TERMS bf16 terms (x1 = bf16(x), x2 = bf16(x - x1),
-//                x3 = bf16(x - x1 - x2); each difference is exact) and stores them
-//                in the tcgen05 K-major layout with the 64-byte swizzle; then a
-//                proxy fence and an arrival on the stage's "full" barrier;
-//   warp 4       lane 0 issues the TERMS (TERMS + 1) / 2 products per 16-deep k
+//   warps 0..3   op(A) producers, warps 4..7 op(B)^T producers: thread r of a group
+//                owns row r of its operand's tile.  Each warp copies the raw fp32
+//                values of its 32 rows for a 32-deep k slab into shared memory with
+//                cp.async, two slabs ahead of the one it splits, coalesced along
+//                whichever dimension the operand stores contiguously (along k for a
+//                k-contiguous operand, along the rows otherwise; 16-byte copies when
+//                the leading dimension allows); then each thread splits its own row
+//                into TERMS bf16 terms (x1 = bf16(x), x2 = bf16(x - x1),
+//                x3 = bf16(x - x1 - x2); each difference is exact) and stores them in
+//                the tcgen05 K-major layout with the 64-byte swizzle.  Rows past the
+//                problem's edge are stored as zeros without being copied or split.
+//                Then a proxy fence and an arrival on the stage's "full" barrier;
+//   warp 8       lane 0 issues the TERMS (TERMS + 1) / 2 products per 16-deep k
 //                step into a TMEM accumulator of 128 x BN fp32 (BN = 64 or 128
 //                per problem), restarted every 128 k (the tensor core's fp32
 //                accumulation truncates) into the other of two buffers;
-//   warps 5..12  epilogue: add each 128-k chunk into fp32 registers with
+//   warps 9..16  epilogue: add each 128-k chunk into fp32 registers with
 //                round-to-nearest, then alpha / beta and the column-major store;
 //                the other TMEM buffer lets the next tile's products run meanwhile.
 // Tiles (problem, 128-row block, BN-column block) are ordered by reduction length,
@@ -42,18 +46,23 @@ constexpr int GBN = 128;       // widest tile (TMEM buffer stride)
 constexpr int GBKB = 64;       // k slab: 32 bf16 per row, 64-byte swizzle
 constexpr int GBK = 32;
 constexpr int GCHUNK = 4;      // slabs per TMEM accumulation chunk
-constexpr int GPROD_WARPS = 4;
-constexpr int GMMA_WARP = 4;
+constexpr int GPROD_WARPS = 8;  // 4 for op(A), 4 for op(B)^T
+constexpr int GMMA_WARP = 8;
 constexpr int GEPI_WARPS = 8;
+constexpr int GEPI_WARP0 = GMMA_WARP + 1;
 constexpr int GTHREADS = 32 * (GPROD_WARPS + 1 + GEPI_WARPS);
-// Raw fp32 staging: each producer thread copies its own row's 32 values of op(A) and of
-// op(B)^T for a slab into shared memory with cp.async, RAW_STAGES - 1 slabs ahead of the
-// one it splits, so the global-memory latency overlaps the splitting of earlier slabs
-// (a thread reads back only what it copied itself: no barrier is needed).  Row stride
-// 36 floats: 16-byte aligned, and the 16-byte reads of 32 rows spread over all banks.
+// Raw fp32 staging ring of GRAW_STAGES slabs.  Per slab and operand each producer warp
+// owns a region of GRAW_WARP floats holding its 32 rows, either as 32 rows of 36 floats
+// (k-contiguous source: row-major, 16-byte aligned rows whose 16-byte reads by 8
+// consecutive threads hit distinct banks) or as 32 k of 32 rows (row-contiguous source:
+// a thread reads its row at stride 32, conflict-free across the warp).  The regions are
+// disjoint whatever the layout, so only the warp itself ever reads or overwrites its
+// region (consecutive uses of a slot may have different layouts).
 constexpr int GRAW_STAGES = 3;
 constexpr int GRAW_LD = 36;
-constexpr int GRAW_BYTES = 2 * BM * GRAW_LD * 4;  // op(A) rows then op(B)^T rows
+constexpr int GRAW_WARP = 32 * GRAW_LD;   // floats per warp per operand per slab (>= 32 x 32)
+constexpr int GRAW_OP = 4 * GRAW_WARP;    // floats per operand per slab
+constexpr int GRAW_BYTES = 2 * GRAW_OP * 4;
 
 template <int TERMS>
 struct GCfg {
@@ -80,8 +89,106 @@ struct TcTile {
     int prob, tm, tn, nkb;  // nkb: k slabs (0 when alpha == 0 or k == 0: C := beta C only)
 };
 
-// split of 16 consecutive k values into TERMS bf16 terms, written as two 16-byte chunks
-// per plane at their 64-byte-swizzled positions of row r
+// One producer group's view of a tile: row i of its operand tile, k index l, sits at
+// p0[i * ld + l] (kcontig) or p0[i + l * ld]; rows >= live are padding (zero).
+struct ProdOp {
+    const float* p0;
+    i64 ld, K;
+    int live;     // rows of the tile inside the problem
+    int used;     // rows the MMA reads (128 for op(A), the tile width for op(B)^T)
+    int kcontig;  // k is the contiguous dimension
+    int vec;      // 16-byte copies: ld a multiple of 4 floats and p0 16-byte aligned
+};
+
+__device__ __forceinline__ ProdOp prod_op(const TcDesc& d, const TcTile& tl, bool isA) {
+    ProdOp o;
+    if (isA) {  // op(A)(i, l): A^T -> a[l + i lda] (k contiguous), else a[i + l lda]
+        const i64 r0 = i64(tl.tm) * BM;
+        o.kcontig = d.ta;
+        o.ld = d.lda;
+        o.p0 = d.a + (d.ta ? r0 * d.lda : r0);
+        o.live = int(min(i64(BM), d.m - r0));
+        o.used = BM;
+    } else {  // op(B)^T(j, l) = op(B)(l, j): B^T -> b[j + l ldb], else b[l + j ldb] (k contiguous)
+        const i64 r0 = i64(tl.tn) * d.bn;
+        o.kcontig = !d.tb;
+        o.ld = d.ldb;
+        o.p0 = d.b + (d.tb ? r0 : r0 * d.ldb);
+        o.live = int(min(i64(d.bn), d.n - r0));
+        o.used = d.bn;
+    }
+    o.K = d.k;
+    o.vec = (o.ld % 4 == 0) && (reinterpret_cast<uintptr_t>(o.p0) % 16 == 0);
+    return o;
+}
+
+__device__ __forceinline__ void cp_async4(unsigned dst, const float* src, int bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async16(unsigned dst, const float* src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+// The warp's share of one slab copy: rows rw0 .. rw0 + 31 of the tile, k = k0 .. k0 + 31,
+// into the warp's region wr of a ring slot: row rw0 + i, k0 + l at wr[i * GRAW_LD + l]
+// (kcontig) or wr[l * 32 + i].  Rows at or past o.live are not copied (their split is a
+// zero store); k past K is zero-filled.
+__device__ __forceinline__ void copy_slab(float* wr, const ProdOp& o, int rw0, int lane, i64 k0) {
+    const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(wr));
+    if (rw0 >= o.live) return;
+    if (o.kcontig) {
+        if (o.vec && k0 + GBK <= o.K) {
+            // lanes 8 q .. 8 q + 7: the eight 16-byte pieces of one row; four rows per copy
+            const int ch = lane & 7;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int row = rw0 + 4 * j + (lane >> 3);
+                if (row < o.live)
+                    cp_async16(base + unsigned((row - rw0) * GRAW_LD + 4 * ch) * 4, o.p0 + i64(row) * o.ld + k0 + 4 * ch,
+                               16);
+            }
+        } else {
+            // lane = k: one row per copy, 128 contiguous bytes across the warp
+            const bool kv = k0 + lane < o.K;
+            const float* q = o.p0 + i64(rw0) * o.ld + (kv ? k0 + lane : 0);
+            const int n = min(32, o.live - rw0);
+#pragma unroll 8
+            for (int i = 0; i < n; ++i, q += o.ld)
+                cp_async4(base + unsigned(i * GRAW_LD + lane) * 4, kv ? q : o.p0, kv ? 4 : 0);
+        }
+    } else {
+        if (o.vec) {
+            // lanes 8 q .. 8 q + 7: 32 consecutive rows of one k (four per 16-byte copy);
+            // four k per copy; partial row groups and k past K are zero-filled
+            const int rr = rw0 + 4 * (lane & 7);
+            const int nv = min(4, o.live - rr);
+            if (nv > 0) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int l = 4 * j + (lane >> 3);
+                    const bool kv = k0 + l < o.K;
+                    cp_async16(base + unsigned(l * 32 + rr - rw0) * 4, kv ? o.p0 + rr + (k0 + l) * o.ld : o.p0,
+                               kv ? 4 * nv : 0);
+                }
+            }
+        } else {
+            // lane = row: one k per copy, 128 contiguous bytes across the warp
+            const int r = rw0 + lane;
+            if (r < o.live) {
+                const float* q = o.p0 + r + k0 * o.ld;
+#pragma unroll 8
+                for (int l = 0; l < GBK; ++l, q += o.ld) {
+                    const bool kv = k0 + l < o.K;
+                    cp_async4(base + unsigned(l * 32 + lane) * 4, kv ? q : o.p0, kv ? 4 : 0);
+                }
+            }
+        }
+    }
+}
+
+// Split of 16 consecutive k values into TERMS bf16 terms, written as two 16-byte chunks
+// per plane at their 64-byte-swizzled positions of row r.  Pairs are rounded together
+// (one bf16x2 conversion) and each term's value recovered from its bits.
 template <int TERMS>
 __device__ __forceinline__ void split_store16(const float (&v)[16], uint8_t* plane0, int plane_bytes, int r,
                                               int chunk0) {
@@ -93,11 +200,12 @@ __device__ __forceinline__ void split_store16(const float (&v)[16], uint8_t* pla
         uint32_t w[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * i]), h1 = __float2bfloat16_rn(x[2 * i + 1]);
-            x[2 * i] -= __bfloat162float(h0);  // exact: x and h agree in their leading bits
-            x[2 * i + 1] -= __bfloat162float(h1);
-            const __nv_bfloat162 pr = __halves2bfloat162(h0, h1);
+            const __nv_bfloat162 pr = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);  // .x low half, .y high
             w[i] = *reinterpret_cast<const uint32_t*>(&pr);
+            if (t + 1 < TERMS) {
+                x[2 * i] -= __uint_as_float(w[i] << 16);  // exact: x and its bf16 agree in their leading bits
+                x[2 * i + 1] -= __uint_as_float(w[i] & 0xffff0000u);
+            }
         }
         uint8_t* rowp = plane0 + t * plane_bytes + r * GBKB;
         const int sw = (r >> 1) & 3;  // 64-byte swizzle: 16-byte chunk c of row r sits at c ^ ((r / 2) % 4)
@@ -106,30 +214,6 @@ __device__ __forceinline__ void split_store16(const float (&v)[16], uint8_t* pla
             const int c = (chunk0 + h) ^ sw;
             *reinterpret_cast<uint4*>(rowp + c * 16) = make_uint4(w[4 * h], w[4 * h + 1], w[4 * h + 2], w[4 * h + 3]);
         }
-    }
-}
-
-// Copies the 32 values of logical row `row` (of `rows`), k = k0 .. k0 + 31 (of K), into
-// dst[0 .. 31] with cp.async: element (row, l) at src[row * rs + l * ks]; zero outside.
-// vec4: k contiguous (ks == 1) and 16-byte aligned rows (16-byte copies).
-__device__ __forceinline__ void copy_row32(float* dst, const float* __restrict__ src, i64 rs, i64 ks, i64 rows,
-                                           i64 K, i64 row, i64 k0, bool vec4) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    if (row < rows && vec4 && k0 + 32 <= K) {
-        const float* p = src + row * rs + k0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d + 16 * q), "l"(p + 4 * q) : "memory");
-        return;
-    }
-    const bool live = row < rows;
-    const float* p = src + (live ? row * rs + k0 * ks : 0);
-#pragma unroll
-    for (int l = 0; l < 32; ++l) {
-        const bool v = live && k0 + l < K;
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d + 4 * l), "l"(v ? p + l * ks : src),
-                     "r"(v ? 4 : 0)
-                     : "memory");
     }
 }
 
@@ -169,28 +253,33 @@ grouped_tc_kernel(const TcDesc* __restrict__ probs, const TcTile* __restrict__ t
 
     if (warp < GPROD_WARPS) {
         // ---------------- producers: copy (cp.async), split, store ----------------
-        const int r = threadIdx.x;  // tile row 0..127
-        // the slabs of this CTA's tiles form one sequence; `ahead` walks it RAW_STAGES - 1
-        // slabs in front of the one being split
-        int at = blockIdx.x, akb = 0;  // look-ahead cursor: tile and slab
+        const bool isA = warp < GPROD_WARPS / 2;
+        const int r = isA ? threadIdx.x : threadIdx.x - BM;  // tile row 0..127 of this group's operand
+        const int rw0 = r & ~31;                              // the warp's first row
+        const int plane_bytes = isA ? C::A_PLANE : C::B_PLANE;
+        float* const ring = raw + (isA ? 0 : GRAW_OP) + (rw0 / 32) * GRAW_WARP;  // this warp's region of slot 0
+        // the slabs of this CTA's tiles form one sequence; the look-ahead cursor (tile
+        // `at`, slab `akb`, operand view `ao`) walks it GRAW_STAGES - 1 slabs in front of
+        // the slab being split
+        int at = blockIdx.x, akb = 0, anb = 0;
+        ProdOp ao{};
+        if (at < ntiles) {
+            const TcTile tl = tiles[at];
+            anb = tl.nkb;
+            ao = prod_op(probs[tl.prob], tl, isA);
+        }
         auto issue_next = [&](int slot) {
-            while (at < ntiles && akb >= tiles[at].nkb) {
+            while (at < ntiles && akb >= anb) {
                 at += gridDim.x;
                 akb = 0;
+                if (at < ntiles) {
+                    const TcTile tl = tiles[at];
+                    anb = tl.nkb;
+                    ao = prod_op(probs[tl.prob], tl, isA);
+                }
             }
             if (at < ntiles) {
-                const TcTile tl = tiles[at];
-                const TcDesc d = probs[tl.prob];
-                const i64 m0 = i64(tl.tm) * BM, n0 = i64(tl.tn) * d.bn, k0 = i64(akb) * GBK;
-                float* ra = raw + slot * (GRAW_BYTES / 4) + r * GRAW_LD;
-                float* rb = ra + BM * GRAW_LD;
-                // op(A)(i, l): A^T -> a[l + i lda] (k contiguous), else a[i + l lda]
-                copy_row32(ra, d.a, d.ta ? d.lda : 1, d.ta ? 1 : d.lda, d.m, d.k, m0 + r, k0,
-                           d.ta && d.lda % 4 == 0 && reinterpret_cast<uintptr_t>(d.a) % 16 == 0);
-                // op(B)^T(j, l) = op(B)(l, j): B^T -> b[j + l ldb], else b[l + j ldb] (k contiguous)
-                if (r < d.bn)
-                    copy_row32(rb, d.b, d.tb ? 1 : d.ldb, d.tb ? d.ldb : 1, d.n, d.k, n0 + r, k0,
-                               !d.tb && d.ldb % 4 == 0 && reinterpret_cast<uintptr_t>(d.b) % 16 == 0);
+                copy_slab(ring + slot * (GRAW_BYTES / 4), ao, rw0, lane, i64(akb) * GBK);
                 ++akb;
             }
             asm volatile("cp.async.commit_group;\n" ::: "memory");  // one group per slab, empty at the end
@@ -199,37 +288,40 @@ grouped_tc_kernel(const TcDesc* __restrict__ probs, const TcTile* __restrict__ t
         int it = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            const int nkb = tiles[t].nkb;
-            const bool brow = r < probs[tiles[t].prob].bn;
-            for (int kb = 0; kb < nkb; ++kb, ++it) {
+            const TcTile tl = tiles[t];
+            const ProdOp o = prod_op(probs[tl.prob], tl, isA);
+            for (int kb = 0; kb < tl.nkb; ++kb, ++it) {
+                __syncwarp();  // every lane has read the warp's region that the next copy overwrites
                 issue_next((it + GRAW_STAGES - 1) % GRAW_STAGES);
                 asm volatile("cp.async.wait_group %0;\n" ::"n"(GRAW_STAGES - 1) : "memory");  // slab `it` landed
-                const float* ra = raw + (it % GRAW_STAGES) * (GRAW_BYTES / 4) + r * GRAW_LD;
-                const float* rb = ra + BM * GRAW_LD;
+                __syncwarp();  // ... including the pieces of this warp's rows copied by other lanes
                 const int s = it % C::STAGES;
                 if (!mbar_wait(&empty[s], ((it / C::STAGES) & 1) ^ 1, err, 31)) { ok = false; break; }
-                uint8_t* sa = smem + s * C::STAGE_BYTES;
-                uint8_t* sb = sa + TERMS * C::A_PLANE;
-                float v[16];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float4 f = reinterpret_cast<const float4*>(ra + 16 * h)[q];
-                        v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
-                    }
-                    split_store16<TERMS>(v, sa, C::A_PLANE, r, 2 * h);
-                }
-                if (brow) {
+                uint8_t* plane0 = smem + s * C::STAGE_BYTES + (isA ? 0 : TERMS * C::A_PLANE);
+                if (r < o.live) {
+                    const float* rr = ring + (it % GRAW_STAGES) * (GRAW_BYTES / 4);
+                    float v[16];
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
+                        if (o.kcontig) {
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float4 f = reinterpret_cast<const float4*>(rb + 16 * h)[q];
-                            v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
+                            for (int q = 0; q < 4; ++q) {
+                                const float4 f = reinterpret_cast<const float4*>(rr + lane * GRAW_LD + 16 * h)[q];
+                                v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
+                            }
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) v[i] = rr[(16 * h + i) * 32 + lane];
                         }
-                        split_store16<TERMS>(v, sb, C::B_PLANE, r, 2 * h);
+                        split_store16<TERMS>(v, plane0, plane_bytes, r, 2 * h);
                     }
+                } else if (r < o.used) {  // padding row: zero terms
+#pragma unroll
+                    for (int tt = 0; tt < TERMS; ++tt)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            *reinterpret_cast<uint4*>(plane0 + tt * plane_bytes + r * GBKB + c * 16) =
+                                make_uint4(0u, 0u, 0u, 0u);
                 }
                 // generic-proxy stores must be visible to the tensor core's (async proxy) reads
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -278,7 +370,7 @@ grouped_tc_kernel(const TcDesc* __restrict__ probs, const TcTile* __restrict__ t
         }
     } else {
         // ---------------- epilogue ----------------
-        const int e = warp - (GPROD_WARPS + 1);
+        const int e = warp - GEPI_WARP0;
         const int quarter = warp & 3;  // the TMEM lanes this warp may read
         const int part = e >> 2;
         int ch = 0;

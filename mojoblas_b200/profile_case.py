@@ -39,6 +39,7 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--k", type=int, default=8192)
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--beta", type=float, default=0.0, help="gemm: C := A B + beta C (1: the trsm update form)")
     ap.add_argument("--pair", type=int, default=-1, help="Ozaki kernel: 1 CTA pairs, 0 one CTA per tile")
     a = ap.parse_args()
 
@@ -98,9 +99,9 @@ def main():
         def call():
             if a.op == "sgemm":
                 return lib.mbg_sgemm_ex(mode, a.ta.encode(), a.tb.encode(), a.m, a.n, a.k, 1.0, A.data_ptr(), lda,
-                                        B.data_ptr(), ldb, 0.0, Cm.data_ptr(), a.m)
+                                        B.data_ptr(), ldb, a.beta, Cm.data_ptr(), a.m)
             return lib.mbg_dgemm_ex(mode, a.slices, a.ta.encode(), a.tb.encode(), a.m, a.n, a.k, 1.0, A.data_ptr(),
-                                    lda, B.data_ptr(), ldb, 0.0, Cm.data_ptr(), a.m)
+                                    lda, B.data_ptr(), ldb, a.beta, Cm.data_ptr(), a.m)
     elif a.op in ("cgemm", "zgemm"):  # complex, interleaved (re, im): a real buffer of twice the rows
         lda = a.m if a.ta == "N" else a.k
         ldb = a.k if a.tb == "N" else a.n

@@ -144,3 +144,65 @@ def test_grouped_strsm_full_count():
         got = arena.get(2 * i + 1, (n, r))
         err = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
         assert err < 4 * tol32(n), (i, n, r, err)
+
+
+@pytest.mark.parametrize("mode", [L.MODE_BF16X6, L.MODE_BF16X3], ids=["bf16x6", "bf16x3"])
+def test_grouped_split_padded_and_misaligned(mode):
+    """The split form's copy paths: leading dimensions past the stored rows (by 0..5
+    floats, so some are multiples of four and some not), base addresses 0..3 floats
+    past a 256-byte boundary (16-byte copies only where both allow), k not a multiple
+    of the 32-deep slab (zero-filled tails), m and n not multiples of the tile (padding
+    rows), both transposes.  The padding between the stored rows and ld must come back
+    untouched in C."""
+    torch = need_gpu()
+    lib = L.load()
+    rng = np.random.default_rng(77)
+    count = 160
+    dims = np.array([1, 3, 31, 32, 33, 63, 64, 65, 127, 128, 129, 200, 257, 300])
+    meta, host_parts, offs, total = [], [], [], 0
+
+    def place(x):
+        nonlocal total
+        start = (total + 63) // 64 * 64 + int(rng.integers(0, 4))  # 0..3 floats past a 256-byte boundary
+        offs.append(start)
+        host_parts.append((start, x))
+        total = start + x.size
+
+    for i in range(count):
+        m, n, k = (int(v) for v in rng.choice(dims, 3))
+        ta, tb = rng.choice(list("NT"), 2)
+        ra, ca = (m, k) if ta == "N" else (k, m)
+        rb, cb = (k, n) if tb == "N" else (n, k)
+        lda, ldb, ldc = ra + int(rng.integers(0, 6)), rb + int(rng.integers(0, 6)), m + int(rng.integers(0, 6))
+        a = np.asfortranarray(rng.uniform(-1, 1, (lda, ca)).astype(np.float32))
+        b = np.asfortranarray(rng.uniform(-1, 1, (ldb, cb)).astype(np.float32))
+        c = np.asfortranarray(rng.uniform(-1, 1, (ldc, n)).astype(np.float32))
+        for x in (a, b, c):
+            place(x.reshape(-1, order="F"))
+        meta.append((m, n, k, ta, tb, lda, ldb, ldc, a, b, c, float(rng.uniform(-2, 2)),
+                     float(rng.choice([0.0, 0.5]))))
+    host = np.zeros(total + 64, np.float32)
+    for start, x in host_parts:
+        host[start:start + x.size] = x
+    buf = torch.from_numpy(host).cuda()
+    base = buf.data_ptr()
+    probs = (L.SgemmProblem * count)()
+    for i, (m, n, k, ta, tb, lda, ldb, ldc, a, b, c, al, be) in enumerate(meta):
+        probs[i] = L.SgemmProblem(ta.encode(), tb.encode(), m, n, k, al, be, base + 4 * offs[3 * i], lda,
+                                  base + 4 * offs[3 * i + 1], ldb, base + 4 * offs[3 * i + 2], ldc)
+    plan = C.c_void_p()
+    assert lib.mbg_sgemm_grouped_plan(mode, count, probs, C.byref(plan)) == 0, L.last_error()
+    try:
+        assert lib.mbg_plan_execute(plan) == 0, L.last_error()
+        torch.cuda.synchronize()
+    finally:
+        lib.mbg_plan_destroy(plan)
+    out = buf.cpu().numpy()
+    tol = (lambda k: TOL_X3) if mode == L.MODE_BF16X3 else tol32
+    for i, (m, n, k, ta, tb, lda, ldb, ldc, a, b, c, al, be) in enumerate(meta):
+        got = out[offs[3 * i + 2]:offs[3 * i + 2] + ldc * n].reshape((ldc, n), order="F")
+        a64, b64 = a[:(m if ta == "N" else k)].astype(np.float64), b[:(k if tb == "N" else n)].astype(np.float64)
+        ref = al * ((a64 if ta == "N" else a64.T) @ (b64 if tb == "N" else b64.T)) + be * c[:m].astype(np.float64)
+        err = float(np.max(np.abs(got[:m] - ref)) / max(np.max(np.abs(ref)), 1e-30))
+        assert err < tol(k), (i, m, n, k, ta, tb, lda, ldb, err)
+        np.testing.assert_array_equal(got[m:], c[m:])
