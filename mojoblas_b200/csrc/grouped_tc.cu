@@ -406,13 +406,25 @@ grouped_tc_kernel(const TcDesc* __restrict__ probs, const TcTile* __restrict__ t
             }
             if (!ok) break;
             if (row < d.m) {
+                // straight-line stores of the live columns; with beta != 0 eight loads of C
+                // are issued before their stores (a store may alias any later load, so a
+                // load per store would wait one round trip each)
+                const int nc = int(min(i64(epi_cols), d.n - cbase));
+                float* cp = d.c + row + cbase * d.ldc;
+                const i64 ldc = d.ldc;
+                if (d.beta == 0.0f) {
 #pragma unroll
-                for (int j = 0; j < GBN / 2; ++j) {
-                    const i64 col = cbase + j;
-                    if (j < epi_cols && col < d.n) {
-                        float* cp = d.c + row + col * d.ldc;
-                        const float v = d.alpha * acc[j];
-                        *cp = (d.beta == 0.0f) ? v : fmaf(d.beta, *cp, v);
+                    for (int j = 0; j < GBN / 2; ++j)
+                        if (j < nc) cp[j * ldc] = d.alpha * acc[j];
+                } else {
+#pragma unroll
+                    for (int j0 = 0; j0 < GBN / 2; j0 += 8) {
+                        float cv[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) cv[j] = j0 + j < nc ? cp[(j0 + j) * ldc] : 0.0f;
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            if (j0 + j < nc) cp[(j0 + j) * ldc] = fmaf(d.beta, cv[j], d.alpha * acc[j0 + j]);
                     }
                 }
             }

@@ -349,7 +349,8 @@ struct OzCfg {
     static constexpr int PLANE = BM * BKB;            // A and B tiles are both 128 x 32 bytes
     static constexpr int STAGE_BYTES = 2 * S * PLANE;
     static constexpr int STAGES = (196608 / STAGE_BYTES) > 6 ? 6 : (196608 / STAGE_BYTES);
-    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr int EXP_BYTES = EPI_WARPS * EPI_COLS * 4;  // staged column exponents
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256 + EXP_BYTES;
     static constexpr uint32_t IDESC = instr_desc(true, BM, BN);
     static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 6;
     static_assert(STAGES >= 2, "pipeline depth");
@@ -438,12 +439,101 @@ __device__ __forceinline__ bool oz_mma_pass(const OzParams& P, int nkb, uint8_t*
     return true;
 }
 
-// Row `row` of the tile's output, columns cbase .. cbase + EPI_COLS - 1: scales the
-// fp64 sums by the row and column exponents and applies alpha / beta (or the
-// trmm diagonal term), as one epilogue thread of either Ozaki kernel owns them.
+// The column exponents of an epilogue warp's EPI_COLS columns, staged in the warp's own
+// slice of shared memory at the start of each tile (while the tile's products run), so
+// the stores wait on no global load, and the row's exponent.  `fast`: the row takes the
+// short store path of oz_store_row (no trmm diagonal term, no triangle mask, and every
+// scale 2^(er + ec) a normal number).
+struct OzRowExp {
+    int er;
+    bool fast;
+};
 template <class C>
-__device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cbase, const double (&acc)[C::EPI_COLS]) {
-    const int er = P.ea[row];
+__device__ __forceinline__ OzRowExp oz_stage_exponents(const OzParams& P, i64 row, i64 cbase, int* ex, int lane) {
+    __syncwarp();  // every lane has finished the previous tile's stores
+    int lo = 1 << 30, hi = -(1 << 30);
+#pragma unroll
+    for (int j = lane; j < C::EPI_COLS; j += 32) {
+        const i64 col = cbase + j;
+        const int v = col < P.n ? P.eb[col] : 0;
+        ex[j] = v;
+        if (col < P.n) {
+            lo = min(lo, v);
+            hi = max(hi, v);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    OzRowExp r;
+    r.er = row < P.m ? P.ea[row] : 0;
+    r.fast = !P.dvec && P.tri == 0 && (lo > hi || (r.er + lo >= -1022 && r.er + hi <= 1023));
+    __syncwarp();
+    return r;
+}
+
+// An int32 accumulator as a double, exactly, without the int-to-fp64 conversion unit
+// (a quarter-rate pipe that bounded the accumulator drains): the bits of 2^52 + 2^51 + v
+// are 0x4338000000000000 + v for |v| < 2^51, and subtracting 2^52 + 2^51 is exact.
+__device__ __forceinline__ double oz_i2d(uint32_t v) {
+    const int hi = 0x43380000 + (static_cast<int>(v) >> 31);
+    return __hiloint2double(hi, static_cast<int>(v)) - 6755399441055744.0;  // 2^52 + 2^51
+}
+
+// 2^e for -1022 <= e <= 1023 (a normal number), from its bits.
+__device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double(static_cast<long long>(e + 1023) << 52); }
+
+// Row `row` of the tile's output, columns cbase .. cbase + EPI_COLS - 1: scales the
+// fp64 sums by the row exponent and the column exponents ex (staged by
+// oz_stage_exponents) and applies alpha / beta (or the trmm diagonal term), as one
+// epilogue thread of either Ozaki kernel owns them.  The short path (x.fast) is
+// straight-line code without branches per element: the general one, with its masks,
+// out-of-range scalings and a global load per column, ran a tile's stores at a few GB/s
+// per SM, longer than the tile's products when k is a few hundred.
+template <class C>
+__device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cbase, const double (&acc)[C::EPI_COLS],
+                                             const int* ex, OzRowExp x) {
+    const int er = x.er;
+    if (x.fast) {
+        const int nc = int(min(i64(C::EPI_COLS), P.n - cbase));  // live columns
+        double* cp = P.c + row + cbase * P.ldc;
+        const i64 ldc = P.ldc;
+        const double alpha = P.alpha, beta = P.beta;
+        if (beta == 1.0) {  // reductions in L2 (the trsm updates)
+#pragma unroll
+            for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+                const int4 e4 = *reinterpret_cast<const int4*>(ex + c0);
+                const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (c0 + j < nc) atomicAdd(cp + (c0 + j) * ldc, alpha * (acc[c0 + j] * oz_pow2(er + ev[j])));
+            }
+        } else if (beta == 0.0) {
+#pragma unroll
+            for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+                const int4 e4 = *reinterpret_cast<const int4*>(ex + c0);
+                const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (c0 + j < nc) cp[(c0 + j) * ldc] = alpha * (acc[c0 + j] * oz_pow2(er + ev[j]));
+            }
+        } else {
+#pragma unroll
+            for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+                const int4 e4 = *reinterpret_cast<const int4*>(ex + c0);
+                const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
+                double cv[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cv[j] = c0 + j < nc ? cp[(c0 + j) * ldc] : 0.0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (c0 + j < nc) cp[(c0 + j) * ldc] = fma(beta, cv[j], alpha * (acc[c0 + j] * oz_pow2(er + ev[j])));
+            }
+        }
+        return;
+    }
     // beta == 1: reductions in L2, as in the split kernel's epilogue; else
     // 4 columns at a time, loads first (the 64 fp64 accumulators leave
     // room for no more)
@@ -456,7 +546,7 @@ __device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cba
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const i64 col = cbase + c0 + j;
-                ec[j] = col < P.n ? P.eb[col] : 0;
+                ec[j] = ex[c0 + j];
                 cv[j] = col < P.n ? P.c[row + col * P.ldc] : 0.0;
             }
 #pragma unroll
@@ -472,7 +562,7 @@ __device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cba
         for (int j = 0; j < C::EPI_COLS; ++j) {
             const i64 col = cbase + j;
             const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
-            if (live) atomicAdd(P.c + row + col * P.ldc, P.alpha * (acc[j] * pow2_exact(er + P.eb[col])));
+            if (live) atomicAdd(P.c + row + col * P.ldc, P.alpha * (acc[j] * pow2_exact(er + ex[j])));
         }
     } else
 #pragma unroll
@@ -483,7 +573,7 @@ __device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cba
         for (int j = 0; j < 4; ++j) {
             const i64 col = cbase + c0 + j;
             const bool live = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
-            ec[j] = live ? P.eb[col] : 0;
+            ec[j] = ex[c0 + j];
             cv[j] = (live && P.beta != 0.0) ? P.c[row + col * P.ldc] : 0.0;
         }
 #pragma unroll
@@ -587,6 +677,8 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
         const int part = e >> 2;
         const i64 row = m0 + quarter * 32 + lane;
         const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(part * C::EPI_COLS);
+        int* ex = reinterpret_cast<int*>(smem + C::STAGES * C::STAGE_BYTES + 256) + e * C::EPI_COLS;
+        const OzRowExp rx = oz_stage_exponents<C>(P, row, n0 + part * C::EPI_COLS, ex, lane);
         double acc[C::EPI_COLS];
 #pragma unroll
         for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0;
@@ -605,14 +697,14 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
                     tmem_ld16(lane_base + uint32_t((d - lo) * C::BN + c0), r);
                     tmem_ld_wait();
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
+                    for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(oz_i2d(r[j]), w, acc[c0 + j]);
                 }
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(tempty);
         }
-        if (ok && row < P.m) oz_store_row<C>(P, row, n0 + part * C::EPI_COLS, acc);
+        if (ok && row < P.m) oz_store_row<C>(P, row, n0 + part * C::EPI_COLS, acc, ex, rx);
     }
     tc_fence_before();
     __syncthreads();
@@ -671,7 +763,8 @@ struct Oz2Cfg {
     static constexpr int STAGES = (196608 / STAGE_BYTES) > 8 ? 8 : (196608 / STAGE_BYTES);
     // at least 120 KB, so one CTA per SM: two pairs interleaved on the same two SMs could
     // each hold one SM's TMEM while waiting for the other's (the pair allocates together)
-    static constexpr int SMEM_USED = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr int EXP_BYTES = EPI_WARPS * EPI_COLS * 4;  // staged column exponents
+    static constexpr int SMEM_USED = STAGES * STAGE_BYTES + 1024 + 256 + EXP_BYTES;
     static constexpr int SMEM_BYTES = SMEM_USED > 122880 ? SMEM_USED : 122880;
     static constexpr uint32_t IDESC = instr_desc(true, 2 * BM, BN);  // M = 256 over the pair
     static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 6;
@@ -904,12 +997,14 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         const int quarter = warp & 3;
         const int part = e >> 2;
         const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(part * C::EPI_COLS);
+        int* ex = reinterpret_cast<int*>(smem + C::STAGES * C::STAGE_BYTES + 256) + e * C::EPI_COLS;
         int gp = 0;
         bool ok = true;
         for (int t = first; t < ntiles && ok; t += stride) {
             OzTile T;
             if (!oz2_tile<C>(P, t, T)) continue;
             const i64 row = T.pm0 + i64(rank) * BM + quarter * 32 + lane;
+            const OzRowExp rx = oz_stage_exponents<C>(P, row, T.n0 + part * C::EPI_COLS, ex, lane);
             double acc[C::EPI_COLS];
 #pragma unroll
             for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0;
@@ -927,14 +1022,14 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         tmem_ld16(lane_base + uint32_t((d - lo) * C::BN + c0), r);
                         tmem_ld_wait();
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(double(int(r[j])), w, acc[c0 + j]);
+                        for (int j = 0; j < 16; ++j) acc[c0 + j] = fma(oz_i2d(r[j]), w, acc[c0 + j]);
                     }
                 }
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_remote(leader_tempty);
             }
-            if (ok && row < P.m) oz_store_row<C>(P, row, T.n0 + part * C::EPI_COLS, acc);
+            if (ok && row < P.m) oz_store_row<C>(P, row, T.n0 + part * C::EPI_COLS, acc, ex, rx);
         }
     }
     tc_fence_before();
@@ -1126,6 +1221,24 @@ __device__ __forceinline__ long long oz_fixed(double v, int er, int B) {
     return (b >> 63) ? -static_cast<long long>(F) : static_cast<long long>(F);
 }
 
+// oz_fixed(v, er, B) for a row whose scale 2^(B - er) is a normal double: one product
+// (exact: a power-of-two scaling of a value below 2^er stays below 2^B, and a product
+// small enough to round is below 1, whose truncation is 0 either way) and one truncating
+// conversion, instead of the integer shifts.
+__device__ __forceinline__ bool oz_scale_ok(int er, int B) { return B - er >= -1022 && B - er <= 1023; }
+__device__ __forceinline__ long long oz_fixed_scaled(double v, double scale) { return __double2ll_rz(v * scale); }
+
+// 4 x 4 byte transpose: o[b] holds byte b of w0, w1, w2, w3 in its bytes 0, 1, 2, 3
+// (eight byte permutes instead of a shift, mask and merge per byte).
+__device__ __forceinline__ void byte_transpose4(unsigned w0, unsigned w1, unsigned w2, unsigned w3, unsigned* o) {
+    const unsigned t0 = __byte_perm(w0, w1, 0x5140), t1 = __byte_perm(w0, w1, 0x7362);  // w0.b0 w1.b0 w0.b1 w1.b1
+    const unsigned t2 = __byte_perm(w2, w3, 0x5140), t3 = __byte_perm(w2, w3, 0x7362);  // (t1, t3: bytes 2, 3)
+    o[0] = __byte_perm(t0, t2, 0x5410);
+    o[1] = __byte_perm(t0, t2, 0x7632);
+    o[2] = __byte_perm(t1, t3, 0x5410);
+    o[3] = __byte_perm(t1, t3, 0x7632);
+}
+
 // Ozaki planes are stored slab-major: plane p holds, for each 32-deep k slab in turn, the
 // 32-byte pieces of all Rp rows back to back, so element (r, l) of a plane sits at
 //     (l / 32) (Rp 32) + r 32 + l % 32.
@@ -1159,18 +1272,19 @@ slice_i8_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp,
         const int B = 8 * slices - 2;
         const unsigned long long bias = 0x8080808080808080ULL >> (64 - 8 * slices);
         unsigned long long H[4];
+        const bool fast = oz_scale_ok(er, B);
+        const double scale = fast ? oz_pow2(B - er) : 0.0;
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            H[u] = static_cast<unsigned long long>(oz_fixed(tile[rr][lq + u], er, B)) + bias;
+            H[u] = static_cast<unsigned long long>(fast ? oz_fixed_scaled(tile[rr][lq + u], scale)
+                                                        : oz_fixed(tile[rr][lq + u], er, B)) + bias;
         unsigned* out = reinterpret_cast<unsigned*>(planes + oz_plane_offset(Rp, r, l0 + lq));
-        for (int p = 0; p < slices; ++p) {
-            const int byte = slices - 1 - p;
-            const int sh = 8 * (byte & 3), hiword = byte & 4 ? 32 : 0;
-            unsigned packed = 0;
+        unsigned w[8];  // w[b]: byte b of H[0..3]
+        byte_transpose4(unsigned(H[0]), unsigned(H[1]), unsigned(H[2]), unsigned(H[3]), w);
+        byte_transpose4(unsigned(H[0] >> 32), unsigned(H[1] >> 32), unsigned(H[2] >> 32), unsigned(H[3] >> 32), w + 4);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) packed |= ((unsigned(H[u] >> hiword) >> sh) & 255u) << (8 * u);
-            out[(plane / 4) * p] = packed ^ 0x80808080u;
-        }
+        for (int b = 0; b < 8; ++b)  // byte b is the digit of slice slices - 1 - b
+            if (b < slices) out[(plane / 4) * (slices - 1 - b)] = w[b] ^ 0x80808080u;
     }
 }
 
@@ -1314,6 +1428,8 @@ slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K
     if (live && lane == 0) e[r] = er;
     const int B = 8 * slices - 2;
     const unsigned long long bias = 0x8080808080808080ULL >> (64 - 8 * slices);
+    const bool fast = oz_scale_ok(er, B);
+    const double scale = fast ? oz_pow2(B - er) : 0.0;
     // eight consecutive k per lane and iteration (Kp is a multiple of 32, so all eight are inside Kp)
     for (i64 l0 = i64(lane) * 8; l0 < Kp; l0 += 256) {
         double x[8];
@@ -1333,19 +1449,18 @@ slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K
         }
         unsigned long long H[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) H[u] = static_cast<unsigned long long>(oz_fixed(x[u], er, B)) + bias;
+        for (int u = 0; u < 8; ++u)
+            H[u] = static_cast<unsigned long long>(fast ? oz_fixed_scaled(x[u], scale) : oz_fixed(x[u], er, B)) + bias;
         uint2* out = reinterpret_cast<uint2*>(planes + oz_plane_offset(Rp, r, l0));
-        for (int p = 0; p < slices; ++p) {
-            const int byte = slices - 1 - p;
-            const int sh = 8 * (byte & 3), hiword = byte & 4 ? 32 : 0;
-            unsigned lo = 0, hi = 0;
+        unsigned wa[8], wb[8];  // byte b of H[0..3] and of H[4..7]
+        byte_transpose4(unsigned(H[0]), unsigned(H[1]), unsigned(H[2]), unsigned(H[3]), wa);
+        byte_transpose4(unsigned(H[0] >> 32), unsigned(H[1] >> 32), unsigned(H[2] >> 32), unsigned(H[3] >> 32), wa + 4);
+        byte_transpose4(unsigned(H[4]), unsigned(H[5]), unsigned(H[6]), unsigned(H[7]), wb);
+        byte_transpose4(unsigned(H[4] >> 32), unsigned(H[5] >> 32), unsigned(H[6] >> 32), unsigned(H[7] >> 32), wb + 4);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                lo |= ((unsigned(H[u] >> hiword) >> sh) & 255u) << (8 * u);
-                hi |= ((unsigned(H[u + 4] >> hiword) >> sh) & 255u) << (8 * u);
-            }
-            out[(plane / 8) * p] = make_uint2(lo ^ 0x80808080u, hi ^ 0x80808080u);
-        }
+        for (int b = 0; b < 8; ++b)  // byte b is the digit of slice slices - 1 - b
+            if (b < slices)
+                out[(plane / 8) * (slices - 1 - b)] = make_uint2(wa[b] ^ 0x80808080u, wb[b] ^ 0x80808080u);
     }
 }
 
