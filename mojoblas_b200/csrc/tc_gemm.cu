@@ -384,6 +384,11 @@ __device__ __forceinline__ bool oz_product(int lo, int hi, int idx, int& p, int&
     return false;
 }
 
+// Width in bytes of k of one slab of the Ozaki planes' layout (oz_plane_offset): the
+// CTA-pair kernel loads one slab per stage, 64-byte rows with the 64-byte swizzle; the
+// single-CTA kernel loads half a slab, 32-byte rows with the 32-byte swizzle.
+constexpr int OZ_SLAB = 64;
+
 struct OzParams {
     i64 m, n;
     int num_kb, tiles_m, tiles_n;
@@ -442,8 +447,8 @@ __device__ __forceinline__ bool oz_mma_pass(const OzParams& P, int nkb, uint8_t*
 // The column exponents of an epilogue warp's EPI_COLS columns, staged in the warp's own
 // slice of shared memory at the start of each tile (while the tile's products run), so
 // the stores wait on no global load, and the row's exponent.  `fast`: the row takes the
-// short store path of oz_store_row (no trmm diagonal term, no triangle mask, and every
-// scale 2^(er + ec) a normal number).
+// short store path of oz_store_row (no triangle mask, and every scale 2^(er + ec) a
+// normal number).
 struct OzRowExp {
     int er;
     bool fast;
@@ -469,7 +474,7 @@ __device__ __forceinline__ OzRowExp oz_stage_exponents(const OzParams& P, i64 ro
     }
     OzRowExp r;
     r.er = row < P.m ? P.ea[row] : 0;
-    r.fast = !P.dvec && P.tri == 0 && (lo > hi || (r.er + lo >= -1022 && r.er + hi <= 1023));
+    r.fast = P.tri == 0 && (lo > hi || (r.er + lo >= -1022 && r.er + hi <= 1023));
     __syncwarp();
     return r;
 }
@@ -489,9 +494,12 @@ __device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double(s
 // fp64 sums by the row exponent and the column exponents ex (staged by
 // oz_stage_exponents) and applies alpha / beta (or the trmm diagonal term), as one
 // epilogue thread of either Ozaki kernel owns them.  The short path (x.fast) is
-// straight-line code without branches per element: the general one, with its masks,
-// out-of-range scalings and a global load per column, ran a tile's stores at a few GB/s
-// per SM, longer than the tile's products when k is a few hundred.
+// straight-line code without branches per element, its reads of C (and of the diagonal
+// term) on the read-only path so that they need not wait for the stores before them
+// (each element is read once, by its own thread, before that thread writes it): the
+// general one, with its masks, out-of-range scalings and a global load per column, ran a
+// tile's stores at a few GB/s per SM, longer than the tile's products when k is a few
+// hundred.
 template <class C>
 __device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cbase, const double (&acc)[C::EPI_COLS],
                                              const int* ex, OzRowExp x) {
@@ -501,7 +509,26 @@ __device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cba
         double* cp = P.c + row + cbase * P.ldc;
         const i64 ldc = P.ldc;
         const double alpha = P.alpha, beta = P.beta;
-        if (beta == 1.0) {  // reductions in L2 (the trsm updates)
+        if (P.dvec) {  // trmm and the inverse-based trsm leaves: C = alpha acc + d C
+            const bool per_row = P.dvec_mode == 1;
+            const double drow = per_row ? __ldg(P.dvec + row) : 0.0;
+            const double* dcol = P.dvec + cbase;
+#pragma unroll
+            for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
+                const int4 e4 = *reinterpret_cast<const int4*>(ex + c0);
+                const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
+                double cv[4], dv[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const bool live = c0 + j < nc;
+                    cv[j] = live ? __ldg(cp + (c0 + j) * ldc) : 0.0;
+                    dv[j] = per_row ? drow : (live ? __ldg(dcol + c0 + j) : 0.0);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (c0 + j < nc) cp[(c0 + j) * ldc] = fma(dv[j], cv[j], alpha * (acc[c0 + j] * oz_pow2(er + ev[j])));
+            }
+        } else if (beta == 1.0) {  // reductions in L2 (the trsm updates)
 #pragma unroll
             for (int c0 = 0; c0 < C::EPI_COLS; c0 += 4) {
                 const int4 e4 = *reinterpret_cast<const int4*>(ex + c0);
@@ -526,7 +553,7 @@ __device__ __forceinline__ void oz_store_row(const OzParams& P, i64 row, i64 cba
                 const int ev[4] = {e4.x, e4.y, e4.z, e4.w};
                 double cv[4];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) cv[j] = c0 + j < nc ? cp[(c0 + j) * ldc] : 0.0;
+                for (int j = 0; j < 4; ++j) cv[j] = c0 + j < nc ? __ldg(cp + (c0 + j) * ldc) : 0.0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     if (c0 + j < nc) cp[(c0 + j) * ldc] = fma(beta, cv[j], alpha * (acc[c0 + j] * oz_pow2(er + ev[j])));
@@ -658,8 +685,11 @@ ozaki_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CU
                 uint8_t* sb = sa + C::S * C::PLANE;
                 mbar_expect_tx(&full[s], uint32_t(2 * planes * C::PLANE));
                 const bool all = planes == C::S;
-                tma_load_4d(sa, all ? &tmA : &tmAlo, &full[s], 0, int(m0), kb0 + kb, 0);
-                tma_load_4d(sb, all ? &tmB : &tmBlo, &full[s], 0, int(n0), kb0 + kb, 0);
+                // 32-byte slab kb is half (kb % 2) of the layout's 64-byte slab kb / 2
+                constexpr int HALVES = OZ_SLAB / 32;
+                const int ks = kb0 + kb, x = (ks % HALVES) * 32, z = ks / HALVES;
+                tma_load_4d(sa, all ? &tmA : &tmAlo, &full[s], x, int(m0), z, 0);
+                tma_load_4d(sb, all ? &tmB : &tmBlo, &full[s], x, int(n0), z, 0);
             }
             for (int it = max(0, total - C::STAGES); it < total; ++it)
                 mbar_wait(&full[it % C::STAGES], (it / C::STAGES) & 1, P.err, 12);
@@ -745,20 +775,19 @@ struct Oz2Cfg {
     static constexpr int S = S_;
     static constexpr int BN = 128;                    // output columns of the pair's tile
     static constexpr int BNH = BN / 2;                // op(B)^T rows staged by each CTA
-    // k slab: 32 int8 per row (one 32-deep MMA step), 32-byte swizzle; the planes are
-    // stored slab-major (all rows' 32-byte pieces of a slab contiguous), so one TMA box
-    // is a few contiguous kilobytes per plane, not one 32-byte request per row (which
-    // bound the loads by the SM's L1-to-L2 request rate), and a stage stays small enough
-    // for four of them
-    static constexpr int BKB = 32;
+    // k slab: 64 int8 per row (two 32-deep MMA steps), 64-byte swizzle; the planes are
+    // stored slab-major (all rows' 64-byte pieces of a slab contiguous), so one TMA box is
+    // a few contiguous kilobytes per plane, in 64-byte rows (with 32-byte rows the loads
+    // were bound by the SM's L1-to-L2 request rate, not by bytes)
+    static constexpr int BKB = OZ_SLAB;
     static constexpr int KSTEPS = BKB / 32;
     static constexpr int EPI_WARPS = 8;
     static constexpr int THREADS = 64 + 32 * EPI_WARPS;
     static constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // 64
     static constexpr int NPASS = S <= 4 ? 1 : 2;
     static constexpr int SPLIT = S <= 4 ? 0 : 4;
-    static constexpr int A_PLANE = BM * BKB;          // 4 KB
-    static constexpr int B_PLANE = BNH * BKB;         // 2 KB
+    static constexpr int A_PLANE = BM * BKB;          // 8 KB
+    static constexpr int B_PLANE = BNH * BKB;         // 4 KB
     static constexpr int STAGE_BYTES = S * (A_PLANE + B_PLANE);
     static constexpr int STAGES = (196608 / STAGE_BYTES) > 8 ? 8 : (196608 / STAGE_BYTES);
     // at least 120 KB, so one CTA per SM: two pairs interleaved on the same two SMs could
@@ -767,9 +796,9 @@ struct Oz2Cfg {
     static constexpr int SMEM_USED = STAGES * STAGE_BYTES + 1024 + 256 + EXP_BYTES;
     static constexpr int SMEM_BYTES = SMEM_USED > 122880 ? SMEM_USED : 122880;
     static constexpr uint32_t IDESC = instr_desc(true, 2 * BM, BN);  // M = 256 over the pair
-    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = 6;
+    static constexpr uint32_t SBO = 8 * BKB, LAYOUT = BKB == 64 ? 4 : 6;
     static_assert(STAGES >= 2, "pipeline depth");
-    static_assert(A_PLANE % 256 == 0 && B_PLANE % 256 == 0, "32-byte swizzle atoms stay aligned");
+    static_assert(A_PLANE % (8 * BKB) == 0 && B_PLANE % (8 * BKB) == 0, "swizzle atoms stay aligned");
 };
 
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -1239,12 +1268,13 @@ __device__ __forceinline__ void byte_transpose4(unsigned w0, unsigned w1, unsign
     o[3] = __byte_perm(t1, t3, 0x7632);
 }
 
-// Ozaki planes are stored slab-major: plane p holds, for each 32-deep k slab in turn, the
-// 32-byte pieces of all Rp rows back to back, so element (r, l) of a plane sits at
-//     (l / 32) (Rp 32) + r 32 + l % 32.
-// One TMA box (32 bytes of k, a block of rows, every plane) is then a contiguous run per plane.
+// Ozaki planes are stored slab-major: plane p holds, for each OZ_SLAB-deep k slab in turn,
+// the OZ_SLAB-byte pieces of all Rp rows back to back, so element (r, l) of a plane sits at
+//     (l / OZ_SLAB) (Rp OZ_SLAB) + r OZ_SLAB + l % OZ_SLAB.
+// One TMA box (a slab of k, a block of rows, every plane) is then a contiguous run per plane.
+// Kp (the padded k) is a multiple of OZ_SLAB.
 __host__ __device__ __forceinline__ size_t oz_plane_offset(i64 Rp, i64 r, i64 l) {
-    return size_t(l >> 5) * size_t(Rp) * 32 + size_t(r) * 32 + size_t(l & 31);
+    return size_t(l) / OZ_SLAB * size_t(Rp) * OZ_SLAB + size_t(r) * OZ_SLAB + size_t(l) % OZ_SLAB;
 }
 
 template <bool KMAJOR>
@@ -1334,24 +1364,26 @@ int make_map(CUtensorMap* map, const void* base, bool int8, i64 Kp, i64 Rp, int 
     return MBG_OK;
 }
 
-// 4-D map over slab-major Ozaki planes (oz_plane_offset): dims {32 bytes of k, rows, slabs,
-// planes}, the rows of each slab plane_rows * 32 bytes apart, planes plane_rows * Kp bytes
-// apart; the map covers `rows` rows from `base` (a row block of taller planes when
-// rows < plane_rows); box = {32, box_rows, 1, planes}: in shared memory the planes' tiles
-// follow each other, rows 32 bytes apart (the 32-byte swizzled K-major layout).
-int make_slab_map(CUtensorMap* map, const void* base, i64 Kp, i64 rows, i64 plane_rows, int planes, int box_rows) {
+// 4-D map over slab-major Ozaki planes (oz_plane_offset): dims {OZ_SLAB bytes of k, rows,
+// slabs, planes}, the rows of each slab plane_rows * OZ_SLAB bytes apart, planes
+// plane_rows * Kp bytes apart; the map covers `rows` rows from `base` (a row block of
+// taller planes when rows < plane_rows); box = {box_k, box_rows, 1, planes} with box_k 32
+// or 64 bytes: in shared memory the planes' tiles follow each other, rows box_k bytes
+// apart (the K-major layout with the box_k-byte swizzle).
+int make_slab_map(CUtensorMap* map, const void* base, i64 Kp, i64 rows, i64 plane_rows, int planes, int box_rows,
+                  int box_k) {
     auto fn = encode_fn();
     if (!fn) {
         set_error_msg("cuTensorMapEncodeTiled is unavailable from the driver");
         return MBG_ERR_CUDA;
     }
-    cuuint64_t dims[4] = {32, cuuint64_t(rows), cuuint64_t(Kp / 32), cuuint64_t(planes)};
-    cuuint64_t strides[3] = {32, cuuint64_t(plane_rows) * 32, cuuint64_t(plane_rows) * cuuint64_t(Kp)};
-    cuuint32_t box[4] = {32, cuuint32_t(box_rows), 1, cuuint32_t(planes)};
+    cuuint64_t dims[4] = {OZ_SLAB, cuuint64_t(rows), cuuint64_t(Kp / OZ_SLAB), cuuint64_t(planes)};
+    cuuint64_t strides[3] = {OZ_SLAB, cuuint64_t(plane_rows) * OZ_SLAB, cuuint64_t(plane_rows) * cuuint64_t(Kp)};
+    cuuint32_t box[4] = {cuuint32_t(box_k), cuuint32_t(box_rows), 1, cuuint32_t(planes)};
     cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, box_k == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error_msg("cuTensorMapEncodeTiled (slab-major planes) failed (code " + std::to_string(int(r)) + ")");
         return MBG_ERR_CUDA;
@@ -1646,12 +1678,14 @@ int run_ozaki(int slices, const int8_t* pa, i64 a_rows, i64 a_plane_rows, const 
     const bool pair = tuning().ozaki_cta_pair != 0;
     const int lo = slices <= 4 ? slices : 4;
     const int bbox = pair ? 64 : 128;
-    P.num_kb = int(Kp / 32);
+    const int bk = pair ? OZ_SLAB : 32;  // bytes of k per stage
+    if (Kp % OZ_SLAB) return MBG_ERR_UNSUPPORTED;
+    P.num_kb = int(Kp / bk);
     CUtensorMap ma, mb, mal, mbl;
-    MBG_TRY(make_slab_map(&ma, pa, Kp, a_rows, a_plane_rows, slices, BM));
-    MBG_TRY(make_slab_map(&mal, pa, Kp, a_rows, a_plane_rows, lo, BM));
-    MBG_TRY(make_slab_map(&mb, pb, Kp, Np, Np, slices, bbox));
-    MBG_TRY(make_slab_map(&mbl, pb, Kp, Np, Np, lo, bbox));
+    MBG_TRY(make_slab_map(&ma, pa, Kp, a_rows, a_plane_rows, slices, BM, bk));
+    MBG_TRY(make_slab_map(&mal, pa, Kp, a_rows, a_plane_rows, lo, BM, bk));
+    MBG_TRY(make_slab_map(&mb, pb, Kp, Np, Np, slices, bbox, bk));
+    MBG_TRY(make_slab_map(&mbl, pb, Kp, Np, Np, lo, bbox, bk));
 #define OZ_CASE(S_)                                                                    \
     case S_:                                                                           \
         return pair ? launch_ozaki_pair<Oz2Cfg<S_>>(ma, mb, mal, mbl, P)               \
@@ -1678,7 +1712,7 @@ int ozaki_slice_a(int slices, char ta, i64 m, i64 k, const double* a, i64 lda, O
     out.m = m;
     out.k = k;
     out.Mp = roundup(m, BM);
-    out.Kp = roundup(k, 32);
+    out.Kp = roundup(k, OZ_SLAB);
     const size_t pbytes = size_t(slices) * out.Mp * out.Kp;
     MBG_TRY(out.ws.reserve(pbytes + sizeof(int) * size_t(out.Mp) + 1024));
     out.planes = out.ws.as<int8_t>();
@@ -1705,9 +1739,9 @@ int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n
     int* eb = reinterpret_cast<int*>(pb + (b_bytes + 1023) / 1024 * 1024);
     MBG_TRY(launch_slices(b, ldb, is_n(tb), n, k, Np, A.Kp, slices, eb, pb));
     const i64 rows = imin(roundup(mb, BM), A.Mp - r0);
-    const int8_t* pa = A.planes + size_t(r0) * 32;  // row r0 of every slab (slab-major planes)
+    const int8_t* pa = A.planes + size_t(r0) * OZ_SLAB;  // row r0 of every slab (slab-major planes)
     OzParams P{};
-    P.m = mb; P.n = n; P.num_kb = int(A.Kp / 32);
+    P.m = mb; P.n = n;
     P.tiles_m = int(cdiv(mb, BM)); P.tiles_n = int(cdiv(n, BN));
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
     P.ea = A.e + r0; P.eb = eb;
@@ -1734,7 +1768,7 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
     const bool shared_planes = tri && a == b && lda == ldb && (is_n(ta) != is_n(tb)) && m == n;
     const i64 Mp = roundup(m, BM), Np = roundup(n, BN);
     const i64 kc = imin(k, kchunk_max);
-    const i64 Kp = roundup(kc, 32);
+    const i64 Kp = roundup(kc, OZ_SLAB);
     const size_t a_bytes = size_t(slices) * Mp * Kp, b_bytes = shared_planes ? 0 : size_t(slices) * Np * Kp;
     Workspace ws;
     MBG_TRY(ws.reserve(a_bytes + b_bytes + sizeof(int) * size_t(Mp + Np) + 1024));
@@ -1744,14 +1778,14 @@ int dgemm_ozaki_tc(int slices, char ta, char tb, i64 m, i64 n, i64 k, double alp
     int* eb = shared_planes ? ea : ea + Mp;
     for (i64 k0 = 0; k0 < k; k0 += kc) {
         const i64 klen = imin(kc, k - k0);
-        const i64 Kpc = roundup(klen, 32);
+        const i64 Kpc = roundup(klen, OZ_SLAB);
         // op(A)[:, k0:k0+klen] and op(B)[k0:k0+klen, :]
         const double* ak = is_n(ta) ? a + k0 * lda : a + k0;
         const double* bk = is_n(tb) ? b + k0 : b + k0 * ldb;
         MBG_TRY(launch_slices(ak, lda, is_t(ta), m, klen, Mp, Kpc, slices, ea, pa, keep_a));
         if (!shared_planes) MBG_TRY(launch_slices(bk, ldb, is_n(tb), n, klen, Np, Kpc, slices, eb, pb, keep_b));
         OzParams P{};
-        P.m = m; P.n = n; P.num_kb = int(Kpc / 32);
+        P.m = m; P.n = n;
         P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
         P.tri = tri ? (is_l(tri_uplo) ? 1 : 2) : 0;
         P.band = band; P.band_k0 = k0;
