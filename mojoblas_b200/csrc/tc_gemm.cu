@@ -1425,10 +1425,14 @@ int launch_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp,
 // row) and again, mostly from cache, to write its digits; padding rows (rows .. Rp)
 // and columns (K .. Kp) are written as zeros.  The digits and exponents are those of
 // row_exponent_kernel + slice_i8_kernel, bit for bit; this saves the second read of
-// the operand from DRAM and one launch.
+// the operand from DRAM and one launch.  SCALE: each value v(r, l) read for slicing is
+// then overwritten in place by dscale[l] v (the inverse-based trsm leaf: the operand is
+// also the output, whose diagonal term d .* C is applied here instead of being read
+// back in the product's epilogue).
+template <bool SCALE>
 __global__ void __launch_bounds__(256)
-slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
-                         int* __restrict__ e, int8_t* __restrict__ planes, int keep) {
+slice_rows_kmajor_kernel(const double* src, i64 ld, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
+                         int* __restrict__ e, int8_t* __restrict__ planes, int keep, const double* __restrict__ dscale) {
     const i64 r = i64(blockIdx.x) * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (r >= Rp) return;
@@ -1479,6 +1483,12 @@ slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K
                 x[u] = (live && l < K && kept(keep, r, l)) ? row[l] : 0.0;
             }
         }
+        if (SCALE && live) {
+            double* w = const_cast<double*>(row);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (l0 + u < K) w[l0 + u] = dscale[l0 + u] * x[u];
+        }
         unsigned long long H[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u)
@@ -1496,12 +1506,19 @@ slice_rows_kmajor_kernel(const double* __restrict__ src, i64 ld, i64 rows, i64 K
     }
 }
 
+// dscale (K-major fused slicing only, keep 0): src is overwritten in place by dscale[l] v(r, l).
 int launch_slices(const double* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, int slices,
-                  int* e, int8_t* planes, int keep = 0) {
+                  int* e, int8_t* planes, int keep = 0, const double* dscale = nullptr) {
+    if (dscale && (!kmajor || !tuning().ozaki_fused_slicing || keep)) return MBG_ERR_UNSUPPORTED;
     if (kmajor && tuning().ozaki_fused_slicing) {
         ProfScope prof("ozaki_slice");
-        slice_rows_kmajor_kernel<<<unsigned(cdiv(Rp, 8)), 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e,
-                                                                            planes, keep);
+        const unsigned g = unsigned(cdiv(Rp, 8));
+        if (dscale)
+            slice_rows_kmajor_kernel<true><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes, keep,
+                                                                  dscale);
+        else
+            slice_rows_kmajor_kernel<false><<<g, 256, 0, stream()>>>(src, ld, rows, K, Rp, Kp, slices, e, planes,
+                                                                   keep, nullptr);
         return check_launch("ozaki_slice");
     }
     {
@@ -1737,7 +1754,11 @@ int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n
     MBG_TRY(ws.reserve(b_bytes + sizeof(int) * size_t(Np) + 1024));
     int8_t* pb = ws.as<int8_t>();
     int* eb = reinterpret_cast<int*>(pb + (b_bytes + 1023) / 1024 * 1024);
-    MBG_TRY(launch_slices(b, ldb, is_n(tb), n, k, Np, A.Kp, slices, eb, pb));
+    // the trsm leaf (C is op(B) itself, k = mb): the slicer writes d .* C back as it reads op(B),
+    // and the product is added to it in L2, instead of the epilogue reading C (one round trip
+    // per few columns, longer than the leaf's products)
+    const bool prescale = dvec && c == b && ldc == ldb && k == mb && is_n(tb) && tuning().ozaki_fused_slicing;
+    MBG_TRY(launch_slices(b, ldb, is_n(tb), n, k, Np, A.Kp, slices, eb, pb, 0, prescale ? dvec : nullptr));
     const i64 rows = imin(roundup(mb, BM), A.Mp - r0);
     const int8_t* pa = A.planes + size_t(r0) * OZ_SLAB;  // row r0 of every slab (slab-major planes)
     OzParams P{};
@@ -1745,7 +1766,9 @@ int dgemm_ozaki_tc_with_a(const OzakiA& A, i64 r0, i64 mb, i64 k, char tb, i64 n
     P.tiles_m = int(cdiv(mb, BM)); P.tiles_n = int(cdiv(n, BN));
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
     P.ea = A.e + r0; P.eb = eb;
-    if (dvec) {  // C = alpha acc + d .* C, d per row (C read before it is overwritten)
+    if (prescale) {
+        P.beta = 1.0;
+    } else if (dvec) {  // C = alpha acc + d .* C, d per row (C read before it is overwritten)
         P.dvec = dvec;
         P.dvec_mode = 1;
     }
