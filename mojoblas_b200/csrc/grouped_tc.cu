@@ -10,7 +10,7 @@
 //   warps 0..3   op(A) producers, warps 4..7 op(B)^T producers: thread r of a group
 //                owns row r of its operand's tile.  Each warp copies the raw fp32
 //                values of its 32 rows for a 32-deep k slab into shared memory with
-//                cp.async, two slabs ahead of the one it splits, coalesced along
+//                cp.async, one slab ahead of the one it splits, coalesced along
 //                whichever dimension the operand stores contiguously (along k for a
 //                k-contiguous operand, along the rows otherwise; 16-byte copies when
 //                the leading dimension allows); then each thread splits its own row
@@ -58,7 +58,10 @@ constexpr int GTHREADS = 32 * (GPROD_WARPS + 1 + GEPI_WARPS);
 // a thread reads its row at stride 32, conflict-free across the warp).  The regions are
 // disjoint whatever the layout, so only the warp itself ever reads or overwrites its
 // region (consecutive uses of a slot may have different layouts).
-constexpr int GRAW_STAGES = 3;
+// Two slots: with three the loads ran no faster (they are bound by the SM's outstanding
+// 4-byte copy requests, not by latency) and the larger shared-memory carve-out left L1,
+// which allocates those requests' lines, a third smaller.
+constexpr int GRAW_STAGES = 2;
 constexpr int GRAW_LD = 36;
 constexpr int GRAW_WARP = 32 * GRAW_LD;   // floats per warp per operand per slab (>= 32 x 32)
 constexpr int GRAW_OP = 4 * GRAW_WARP;    // floats per operand per slab
