@@ -96,6 +96,10 @@ struct Cfg {
 
 using CfgBF16x3 = Cfg<false, 2, 256, 64, 4, 8, 4>;
 using CfgBF16x6 = Cfg<false, 3, 256, 64, 3, 8, 4>;
+// 128 x 64 tiles for products too small to give a quarter of the SMs a 128 x 256 tile (the
+// trsm recursion's 512-row blocks: 8 CTAs of the wide tile against 32 of these)
+using CfgBF16x3n = Cfg<false, 2, 64, 64, 8, 8, 4>;
+using CfgBF16x6n = Cfg<false, 3, 64, 64, 6, 8, 4>;
 
 struct Params {
     i64 m, n;
@@ -1409,6 +1413,26 @@ int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, Params& P, const cha
     return check_launch(name);
 }
 
+// The split product on planes pa (op(A), a_rows rows from pa, planes a_plane_rows apart)
+// and pb (op(B)^T, b_rows rows): 128 x 256 tiles, or 128 x 64 tiles when the wide ones
+// would occupy fewer than a quarter of the SMs (a product that fills more may share the
+// GPU with another stream's, as the gemm adjoint's two do).  Sets the B map and P.tiles_n.
+int launch_split_product(int terms, const __nv_bfloat16* pa, i64 a_rows, i64 a_plane_rows, const __nv_bfloat16* pb,
+                         i64 b_rows, i64 Kp, Params& P) {
+    int dev = 0, sms = 148;
+    MBG_CUDA(cudaGetDevice(&dev));
+    MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const bool narrow = 4 * i64(P.tiles_m) * cdiv(P.n, 256) < sms;
+    const int bn = narrow ? 64 : 256;
+    CUtensorMap ma, mb;
+    MBG_TRY(make_map(&ma, pa, false, Kp, a_rows, terms, 64, BM, a_plane_rows));
+    MBG_TRY(make_map(&mb, pb, false, Kp, b_rows, terms, 64, bn));
+    P.tiles_n = int(cdiv(P.n, bn));
+    if (terms == 2)
+        return narrow ? launch_tc<CfgBF16x3n>(ma, mb, P, "tc_gemm_bf16x3") : launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
+    return narrow ? launch_tc<CfgBF16x6n>(ma, mb, P, "tc_gemm_bf16x6") : launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
+}
+
 template <int TERMS>
 int launch_split(const float* src, i64 ld, bool kmajor, i64 rows, i64 K, i64 Rp, i64 Kp, __nv_bfloat16* planes,
                  int keep = 0) {
@@ -1576,12 +1600,9 @@ int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha
         MBG_TRY(launch_split<3>(a, lda, is_t(ta), m, k, Mp, Kp, pa, keep_a));
         if (!shared_planes) MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, k, Np, Kp, pb, keep_b));
     }
-    CUtensorMap ma, mb;
-    MBG_TRY(make_map(&ma, pa, false, Kp, Mp, terms, 64, BM));
-    MBG_TRY(make_map(&mb, pb, false, Kp, shared_planes ? Mp : Np, terms, 64, BN));
     Params P{};
     P.m = m; P.n = n; P.num_kb = int(Kp / 32);
-    P.tiles_m = int(cdiv(m, BM)); P.tiles_n = int(cdiv(n, BN));
+    P.tiles_m = int(cdiv(m, BM));
     P.tri = tri ? (is_l(tri_uplo) ? 1 : 2) : 0;
     P.band = band; P.band_k0 = 0;
     if (tri_op && tri_op->dvec_mode) {
@@ -1589,8 +1610,7 @@ int sgemm_split_tc(int terms, char ta, char tb, i64 m, i64 n, i64 k, float alpha
         P.dvec_mode = tri_op->dvec_mode;
     }
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
-    if (terms == 2) return launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
-    return launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
+    return launch_split_product(terms, pa, Mp, Mp, pb, shared_planes ? Mp : Np, Kp, P);
 }
 
 // op(A)'s split planes made once and used for several products with column blocks of
@@ -1631,16 +1651,12 @@ int sgemm_split_tc_with_a_rows(const SplitA& A, i64 r0, i64 mb, i64 k, char tb, 
     __nv_bfloat16* pb = ws.as<__nv_bfloat16>();
     if (A.terms == 2) MBG_TRY(launch_split<2>(b, ldb, is_n(tb), n, k, Np, A.Kp, pb));
     else MBG_TRY(launch_split<3>(b, ldb, is_n(tb), n, k, Np, A.Kp, pb));
-    CUtensorMap ma, mb_;
     const i64 rows = imin(roundup(mb, BM), A.Mp - r0);
-    MBG_TRY(make_map(&ma, A.ws.as<__nv_bfloat16>() + size_t(r0) * A.Kp, false, A.Kp, rows, A.terms, 64, BM, A.Mp));
-    MBG_TRY(make_map(&mb_, pb, false, A.Kp, Np, A.terms, 64, BN));
     Params P{};
     P.m = mb; P.n = n; P.num_kb = int(A.Kp / 32);
-    P.tiles_m = int(cdiv(mb, BM)); P.tiles_n = int(cdiv(n, BN));
+    P.tiles_m = int(cdiv(mb, BM));
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
-    if (A.terms == 2) return launch_tc<CfgBF16x3>(ma, mb_, P, "tc_gemm_bf16x3");
-    return launch_tc<CfgBF16x6>(ma, mb_, P, "tc_gemm_bf16x6");
+    return launch_split_product(A.terms, A.ws.as<__nv_bfloat16>() + size_t(r0) * A.Kp, rows, A.Mp, pb, Np, A.Kp, P);
 }
 
 // ---- Ozaki dgemm ----------------------------------------------------------------
