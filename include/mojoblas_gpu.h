@@ -332,9 +332,10 @@ int   mbg_release_workspace(void);
  * "trsm_block_min_cols" — the fused launch is used only with at least this
  * many right-hand sides (default 64);
  * "trsm_inverse_min_cols" — split / Ozaki trsm with at least this many
- * right-hand sides inverts its 512-row diagonal blocks once (native precision)
+ * right-hand sides inverts its diagonal blocks once (native precision)
  * and applies each inverse as a split / Ozaki product (default 256; 0 = never:
  * substitution in the diagonal blocks);
+ * "trsm_inverse_block" — rows of those diagonal blocks, 256 or 512 (default 512);
  * "ozaki_cta_pair" — Ozaki products on CTA pairs (tcgen05 cta_group::2,
  * 256 x 128 tiles over two SMs): 1 one cluster per tile, 2 persistent clusters
  * (one per two SMs, the epilogue of a tile overlapping the next tile's products);

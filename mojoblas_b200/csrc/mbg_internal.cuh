@@ -154,6 +154,7 @@ struct Tuning {
     i64 trsm_block_min_cols = 64;    // ... when there are at least this many right-hand sides
     i64 trsm_inverse_min_cols = 256;  // split / Ozaki trsm: inverted diagonal blocks from this many
                                       // right-hand sides (0: never; substitution leaves instead)
+    i64 trsm_inverse_block = 512;     // ... of this many rows (256 or 512)
     i64 plain_fp64_simt = 0;     // 1: plain FP64 gemm/syrk on the CUDA cores instead of the FP64 tensor pipe
     i64 plain_fp32_staged = 0;   // 1: plain FP32 128-tiles staged through registers (the earlier kernel)
     i64 ozaki_fused_slicing = 1;  // K-contiguous Ozaki operands: exponents and slices in one pass

@@ -396,6 +396,10 @@ int mbg_set_tuning(const char* key, int64_t value) {
     if (k == "trsm_block_rows" && value >= 0 && value <= 1024) { tuning().trsm_block_rows = value; return MBG_OK; }
     if (k == "trsm_block_min_cols" && value >= 0) { tuning().trsm_block_min_cols = value; return MBG_OK; }
     if (k == "trsm_inverse_min_cols" && value >= 0) { tuning().trsm_inverse_min_cols = value; return MBG_OK; }
+    if (k == "trsm_inverse_block" && (value == 256 || value == 512)) {
+        tuning().trsm_inverse_block = value;
+        return MBG_OK;
+    }
     if (k == "plain_fp64_simt" && (value == 0 || value == 1)) { tuning().plain_fp64_simt = value; return MBG_OK; }
     if (k == "plain_fp32_staged" && (value == 0 || value == 1)) { tuning().plain_fp32_staged = value; return MBG_OK; }
     if (k == "ozaki_cta_pair" && value >= 0 && value <= 2) { tuning().ozaki_cta_pair = value; return MBG_OK; }
@@ -417,6 +421,7 @@ int64_t mbg_get_tuning(const char* key) {
     if (k == "trsm_block_rows") return tuning().trsm_block_rows;
     if (k == "trsm_block_min_cols") return tuning().trsm_block_min_cols;
     if (k == "trsm_inverse_min_cols") return tuning().trsm_inverse_min_cols;
+    if (k == "trsm_inverse_block") return tuning().trsm_inverse_block;
     if (k == "plain_fp64_simt") return tuning().plain_fp64_simt;
     if (k == "plain_fp32_staged") return tuning().plain_fp32_staged;
     if (k == "ozaki_cta_pair") return tuning().ozaki_cta_pair;

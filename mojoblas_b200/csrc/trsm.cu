@@ -421,7 +421,9 @@ block_invert_kernel(i64 m, int nbi, const T* __restrict__ A, i64 lda, T* __restr
 }
 
 template <typename T>
-constexpr i64 inv_block_rows() { return 512; }  // <= bs_max_rows<T>() for both precisions
+i64 inv_block_rows() {  // the tuning table's 256 or 512 (<= bs_max_rows<T>() for both precisions)
+    return tuning().trsm_inverse_block == 256 ? 256 : 512;
+}
 
 template <typename T, bool L, bool TR, bool U>
 int launch_block_invert_t(i64 m, int nbi, const T* a, i64 lda, T* w, i64 ldw) {

@@ -120,3 +120,27 @@ def test_inverse_blocks_ill_conditioned(oracle, lib, case):
         den = float(np.max(np.abs(ref)))
         errs[label] = float(np.max(np.abs(x.astype(np.longdouble) - ref))) / den
     assert errs["ozaki_inverse"] <= 4 * errs["plain"] + 4e-16, errs
+
+
+@pytest.mark.parametrize("dt,mode", [(np.float32, mb.BF16X6), (np.float64, mb.OZAKI)], ids=["f32-bf16x6", "f64-ozaki"])
+@pytest.mark.parametrize("side,uplo,ta", [("L", "L", "N"), ("L", "U", "T"), ("R", "U", "N")])
+def test_inverse_blocks_of_256_rows(oracle, lib, dt, mode, side, uplo, ta):
+    """Tuning key trsm_inverse_block = 256: diagonal blocks of 256 rows (five blocks and a
+    short one at 1300 rows), the same tolerances as the 512-row blocks."""
+    default = lib.mbg_get_tuning(b"trsm_inverse_block")
+    rng = np.random.default_rng(23)
+    na, nrhs = 1300, 300
+    m, n = (na, nrhs) if side == "L" else (nrhs, na)
+    a, b, lda, ldb = tri_system(rng, side, m, n, dt, ld_pad=2)
+    ref = oracle.trsm_f64(side, uplo, ta, "N", m, n, 1.5, a, lda, b, ldb)
+    x = b.copy(order="F")
+    try:
+        assert lib.mbg_set_tuning(b"trsm_inverse_block", 256) == 0
+        assert lib.mbg_set_tuning(b"trsm_inverse_block", 300) != 0  # only 256 or 512
+        st, ran = _ran_inverse(lib, lambda: mb.trsm(side, uplo, ta, "N", m, n, 1.5, a, lda, x, ldb, mode=mode,
+                                                    slices=7))
+    finally:
+        lib.mbg_set_tuning(b"trsm_inverse_block", default)
+    assert st == 0 and ran
+    assert oracle.max_rel_err(oracle.view(x, m, n, ldb), ref) < tol_mode(mode, na, slices=7) * 4
+    np.testing.assert_array_equal(x[m:], b[m:])
