@@ -100,6 +100,10 @@ using CfgBF16x6 = Cfg<false, 3, 256, 64, 3, 8, 4>;
 // trsm recursion's 512-row blocks: 8 CTAs of the wide tile against 32 of these)
 using CfgBF16x3n = Cfg<false, 2, 64, 64, 8, 8, 4>;
 using CfgBF16x6n = Cfg<false, 3, 64, 64, 6, 8, 4>;
+// 128 x 128 tiles for products that give fewer CTAs than SMs with 128 x 256 tiles: twice the
+// CTAs, so a last partial wave idles less of the GPU (the gemm adjoint's two products)
+using CfgBF16x3m = Cfg<false, 2, 128, 64, 6, 8, 4>;
+using CfgBF16x6m = Cfg<false, 3, 128, 64, 4, 8, 4>;
 
 struct Params {
     i64 m, n;
@@ -1414,23 +1418,28 @@ int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, Params& P, const cha
 }
 
 // The split product on planes pa (op(A), a_rows rows from pa, planes a_plane_rows apart)
-// and pb (op(B)^T, b_rows rows): 128 x 256 tiles, or 128 x 64 tiles when the wide ones
-// would occupy fewer than a quarter of the SMs (a product that fills more may share the
-// GPU with another stream's, as the gemm adjoint's two do).  Sets the B map and P.tiles_n.
+// and pb (op(B)^T, b_rows rows): 128 x 256 tiles; 128 x 128 when the wide ones number
+// fewer than the SMs; 128 x 64 when they would occupy fewer than a quarter of the SMs.
+// Sets the B map and P.tiles_n.
 int launch_split_product(int terms, const __nv_bfloat16* pa, i64 a_rows, i64 a_plane_rows, const __nv_bfloat16* pb,
                          i64 b_rows, i64 Kp, Params& P) {
     int dev = 0, sms = 148;
     MBG_CUDA(cudaGetDevice(&dev));
     MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const bool narrow = 4 * i64(P.tiles_m) * cdiv(P.n, 256) < sms;
-    const int bn = narrow ? 64 : 256;
+    const i64 wide_tiles = i64(P.tiles_m) * cdiv(P.n, 256);
+    const int bn = 4 * wide_tiles < sms ? 64 : (wide_tiles < sms ? 128 : 256);
     CUtensorMap ma, mb;
     MBG_TRY(make_map(&ma, pa, false, Kp, a_rows, terms, 64, BM, a_plane_rows));
     MBG_TRY(make_map(&mb, pb, false, Kp, b_rows, terms, 64, bn));
     P.tiles_n = int(cdiv(P.n, bn));
-    if (terms == 2)
-        return narrow ? launch_tc<CfgBF16x3n>(ma, mb, P, "tc_gemm_bf16x3") : launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
-    return narrow ? launch_tc<CfgBF16x6n>(ma, mb, P, "tc_gemm_bf16x6") : launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
+    if (terms == 2) {
+        if (bn == 64) return launch_tc<CfgBF16x3n>(ma, mb, P, "tc_gemm_bf16x3");
+        if (bn == 128) return launch_tc<CfgBF16x3m>(ma, mb, P, "tc_gemm_bf16x3");
+        return launch_tc<CfgBF16x3>(ma, mb, P, "tc_gemm_bf16x3");
+    }
+    if (bn == 64) return launch_tc<CfgBF16x6n>(ma, mb, P, "tc_gemm_bf16x6");
+    if (bn == 128) return launch_tc<CfgBF16x6m>(ma, mb, P, "tc_gemm_bf16x6");
+    return launch_tc<CfgBF16x6>(ma, mb, P, "tc_gemm_bf16x6");
 }
 
 template <int TERMS>
