@@ -215,6 +215,20 @@ def tune(out: Path) -> dict:
     table["trsm_inverse_min_cols"] = inv_cols
     lib.mbg_set_tuning(b"trsm_inverse_min_cols", inv_cols)
 
+    # rows of the inverted diagonal blocks (Ozaki dtrsm 4096^2), interleaved rounds, medians
+    if inv_cols:
+        samples = {256: [], 512: []}
+        for _ in range(ROUNDS):
+            for blk in samples:
+                lib.mbg_set_tuning(b"trsm_inverse_block", blk)
+                samples[blk].append(time_trsm(L.MODE_OZAKI, n))
+        med = {blk: float(np.median(v)) for blk, v in samples.items()}
+        for blk, ms in med.items():
+            log[f"ozaki dtrsm 4096^2, inverted blocks of {blk} rows"] = {"ms_median": round(ms, 3),
+                                                                        "rounds": len(samples[blk])}
+        table["trsm_inverse_block"] = min(med, key=med.get)
+        lib.mbg_set_tuning(b"trsm_inverse_block", table["trsm_inverse_block"])
+
     doc = {**table, "_measurements": log, "_device": torch.cuda.get_device_name(0)}
     out.write_text(json.dumps(doc, indent=1) + "\n")
     return doc
