@@ -163,22 +163,33 @@ def tune(out: Path) -> dict:
         return e0.elapsed_time(e1) / reps
 
     lib.mbg_set_tuning(b"trsm_block_min_cols", 1)
-    # candidates are timed in interleaved rounds and ranked by their median, so that a clock
-    # or power-cap drift during the sweep does not favour whichever ran first
-    cands = [(rows, thr) for rows in (0, 256, 512) for thr in (256, 512, 1024)]
-    samples = {c: [] for c in cands}
+    # the keys swept here govern the substitution path: the fused diagonal blocks' rows (the
+    # plain solve's, and the split / Ozaki solves' below trsm_inverse_min_cols right-hand sides),
+    # chosen on the plain FP64 solve; then the k from which the substitution path's updates
+    # are split / Ozaki products, chosen on the Ozaki solve with the inverted-block path off.
+    # Candidates are timed in interleaved rounds and ranked by their median, so that a clock
+    # or power-cap drift during the sweep does not favour whichever ran first.
+    lib.mbg_set_tuning(b"trsm_inverse_min_cols", 0)
+    samples = {rows: [] for rows in (0, 256, 512)}
     for _ in range(ROUNDS):
-        for rows, thr in cands:
+        for rows in samples:
             lib.mbg_set_tuning(b"trsm_block_rows", rows)
+            samples[rows].append(time_trsm(L.MODE_PLAIN, n))
+    med = {rows: float(np.median(v)) for rows, v in samples.items()}
+    for rows, ms in med.items():
+        log[f"plain dtrsm 4096^2, fused rows {rows}"] = {"ms_median": round(ms, 3), "rounds": ROUNDS}
+    rows_best = min(med, key=med.get)
+    lib.mbg_set_tuning(b"trsm_block_rows", rows_best)
+    samples = {thr: [] for thr in (256, 512, 1024)}
+    for _ in range(ROUNDS):
+        for thr in samples:
             lib.mbg_set_tuning(b"trsm_tc_min_k", thr)
-            samples[(rows, thr)].append(time_trsm(L.MODE_OZAKI, n))
-    best = None
-    for (rows, thr), v in samples.items():
-        ms = float(np.median(v))
-        log[f"ozaki dtrsm 4096^2, fused rows {rows}, split from k {thr}"] = {"ms_median": round(ms, 3),
-                                                                            "rounds": len(v)}
-        if best is None or ms < best[2]:
-            best = (rows, thr, ms)
+            samples[thr].append(time_trsm(L.MODE_OZAKI, n))
+    med = {thr: float(np.median(v)) for thr, v in samples.items()}
+    for thr, ms in med.items():
+        log[f"ozaki dtrsm 4096^2 (substitution), fused rows {rows_best}, split from k {thr}"] = {
+            "ms_median": round(ms, 3), "rounds": ROUNDS}
+    best = (rows_best, min(med, key=med.get))
     table["trsm_block_rows"], table["trsm_tc_min_k"] = best[0], best[1]
     lib.mbg_set_tuning(b"trsm_block_rows", best[0])
     lib.mbg_set_tuning(b"trsm_tc_min_k", best[1])
