@@ -8,6 +8,8 @@
     python mojoblas_b200/profile_case.py --op dgemm --mode ozaki --slices 7 --pair 1 --m 4096 --n 4096 --k 4096
     python mojoblas_b200/profile_case.py --op grouped_sgemm --mode bf16x6
     python mojoblas_b200/profile_case.py --op zgemm --mode ozaki --slices 7 --m 2048 --n 2048 --k 2048
+    python mojoblas_b200/profile_case.py --op strsm_adjoint --mode bf16x6 --m 2048 --n 512
+    python mojoblas_b200/profile_case.py --op sgemm_adjoint --mode bf16x6 --m 3072 --n 2048 --k 1024
 
 Inputs are uniform[-1, 1) (trsm, trmm: diagonally dominant lower triangle), device
 resident; each rep is one call through the C ABI.  Prints the mean CUDA-event
@@ -28,7 +30,7 @@ def main():
     ap.add_argument("--op", choices=["sgemm", "dgemm", "cgemm", "zgemm", "ssyrk", "dtrsm", "strsm", "grouped_sgemm",
                                      "grouped_strsm",
                                      "strmm", "dtrmm", "ssymm", "dsymm", "ssyr2k", "dsyr2k",
-                                     "sgemv", "dgemv", "strsv", "dtrsv"],
+                                     "sgemv", "dgemv", "strsv", "dtrsv", "strsm_adjoint", "sgemm_adjoint"],
                     default="sgemm")
     ap.add_argument("--mode", choices=["plain", "bf16x3", "bf16x6", "ozaki"], default="bf16x6")
     ap.add_argument("--slices", type=int, default=8)
@@ -137,6 +139,24 @@ def main():
             xb.copy_(b0)
             args = (b"L", b"N", b"N", a.m, A.data_ptr(), a.m, xb.data_ptr(), 1)
             return lib.mbg_strsv(*args) if a.op == "strsv" else lib.mbg_dtrsv(*args)
+    elif a.op == "strsm_adjoint":  # L (m x m lower, dominant diagonal), X and G m x n: dB, dL
+        import numpy as np
+        Lm = torch.randn((a.m, a.m), generator=g, device="cuda") / np.sqrt(a.m)
+        Lm.diagonal().add_(a.m)
+        Lm = torch.tril(Lm.T).T.contiguous()
+        X, G = cm(a.m, a.n), cm(a.m, a.n)
+        dB, dL = torch.zeros_like(X), torch.zeros_like(Lm)
+
+        def call():
+            return lib.mbg_strsm_adjoint(mode, b"L", b"L", b"N", b"N", a.m, a.n, 1.0, Lm.data_ptr(), a.m, X.data_ptr(),
+                                         a.m, G.data_ptr(), a.m, dB.data_ptr(), a.m, dL.data_ptr(), a.m)
+    elif a.op == "sgemm_adjoint":  # C = A B (A m x k, B k x n, NN): dA = G B^T, dB = A^T G
+        A, B, G = cm(a.m, a.k), cm(a.k, a.n), cm(a.m, a.n)
+        dA, dB = torch.zeros_like(A), torch.zeros_like(B)
+
+        def call():
+            return lib.mbg_sgemm_adjoint(mode, b"N", b"N", a.m, a.n, a.k, 1.0, A.data_ptr(), a.m, B.data_ptr(), a.k,
+                                         G.data_ptr(), a.m, dA.data_ptr(), a.m, dB.data_ptr(), a.k)
     elif a.op in ("ssymm", "dsymm"):  # Left, Upper: C (m x n) = A (m x m, symmetric) B
         A, B, Cm = cm(a.m, a.m), cm(a.m, a.n), cm(a.m, a.n)
 
