@@ -18,8 +18,11 @@ constexpr int BS_THREADS = 8 * BS_COLS;           // eight lanes per column in t
 constexpr int BS_TILE = NB * 72;                  // diagonal block + reciprocals (64 x 65 + 64), or a 64 x 72 tile
 
 inline int bs_strip_ld(int nb) { return (int)(cdiv(nb, NB) * NB) + 2; }
+// nbuf: staging buffers per strip (items staged nbuf - 1 ahead of the one being computed)
 template <typename T>
-inline size_t bs_smem_bytes(int nb) { return sizeof(T) * (size_t(BS_COLS) * bs_strip_ld(nb) + 2 * BS_TILE); }
+inline size_t bs_smem_bytes(int nb, int nbuf = 2) {
+    return sizeof(T) * (size_t(BS_COLS) * bs_strip_ld(nb) + size_t(nbuf) * BS_TILE);
+}
 
 // One element copied global -> shared without a register round trip; zero-filled
 // (nothing read) when !valid, in which case src only has to be some valid pointer.
@@ -34,6 +37,8 @@ __device__ __forceinline__ void cp_async_elem(T* dst, const T* src, bool valid) 
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Solves op(A)[0:nb, 0:nb] X = B[0:nb, :] in place, nb up to 512 (double) or
 // 1024 (float) rows, in one launch.  Each CTA owns W right-hand-side columns (a
@@ -51,13 +56,14 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //       product), on the CUDA cores for float (each thread 4 rows x 4 columns
 //       over half of the 64-long reduction, tile and X_b read as 8-byte pairs).
 // The diagonal blocks and tiles form one sequence per strip that is staged
-// with cp.async into two alternating buffers: the next item is in flight while
-// the current one is computed, so the L2 latency of A (shared by every CTA)
-// is hidden.  The strip is read from and written to HBM once; only
+// with cp.async into NBUF rotating buffers: the next NBUF - 1 items are in flight
+// while the current one is computed, so the L2 latency of A (shared by every
+// CTA) is hidden.  Two for the blocked trsm (a third measured slower there); three
+// for the grouped plans' small problems (measured 9 % faster).  The strip is read from and written to HBM once; only
 // off-diagonal blocks above the launch's size go through gemm.  Rows at or
 // past nb stay zero in the strip and staged items are zero outside op(A)'s
 // block, so ragged edges need no special case in the inner loops.
-template <typename T, bool LOWER, bool TRANS, bool UNIT, int W>
+template <typename T, bool LOWER, bool TRANS, bool UNIT, int W, int NBUF = 2>
 __device__ __forceinline__ void block_solve_strip(int nb, i64 ncols, const T* __restrict__ A, i64 lda,
                                                   T* __restrict__ B, i64 ldb, i64 c0, T alpha,
                                                   unsigned char* bs_smem_raw) {
@@ -68,7 +74,8 @@ __device__ __forceinline__ void block_solve_strip(int nb, i64 ncols, const T* __
     constexpr int LT = TRANS ? NB + 2 : NB + 8;  // update tile: [l][r] (plain) or [r][l] (transposed)
     const int nsub = (nb + NB - 1) / NB, nbr = nsub * NB, ldbs = nbr + 2;
     T* Bs = reinterpret_cast<T*>(bs_smem_raw);
-    T* const buf0 = Bs + (size_t)W * ldbs;  // two staging buffers of BS_TILE elements
+    static_assert(NBUF >= 2, "staging depth");
+    T* const buf0 = Bs + (size_t)W * ldbs;  // NBUF staging buffers of BS_TILE elements
     const int tid = threadIdx.x;
 
     // item (step, tt): tt < 0 is the diagonal block of sub-block b(step), else its tt-th trailing tile
@@ -111,20 +118,27 @@ __device__ __forceinline__ void block_solve_strip(int nb, i64 ncols, const T* __
             for (int r = tid; r < nbr; r += NT) cp_async_elem(Bs + c * ldbs + r, live && r < nb ? bc + r : B, live && r < nb);
         }
         issue(0, -1, buf0);
-        cp_async_commit();
+        cp_async_commit();  // group 0: the strip and item 0; group g: item g (empty past the last)
+        int is = 0, itt = -1;  // the last item issued
+        for (int j = 1; j < NBUF - 1; ++j) {
+            advance(is, itt);
+            if (is < nsub) issue(is, itt, buf0 + j * BS_TILE);
+            cp_async_commit();
+        }
         int step = 0, tt = -1;
         for (int it = 0; step < nsub; ++it) {
-            T* cur = buf0 + (it & 1) * BS_TILE;
-            cp_async_wait_all();
-            __syncthreads();  // item `it` has landed everywhere; buffer (it + 1) & 1 is free
+            T* cur = buf0 + (it % NBUF) * BS_TILE;
+            cp_async_wait_group<NBUF - 2>();
+            __syncthreads();  // item `it` has landed everywhere; item it - 1's buffer is free
             if (it == 0 && alpha != T(1)) {  // the strip has landed: B := alpha B
                 for (int e = tid; e < W * ldbs; e += NT) Bs[e] *= alpha;
                 __syncthreads();
             }
+            advance(is, itt);
+            if (is < nsub) issue(is, itt, buf0 + ((it + NBUF - 1) % NBUF) * BS_TILE);
+            cp_async_commit();
             int ns = step, nt = tt;
             advance(ns, nt);
-            if (ns < nsub) issue(ns, nt, buf0 + ((it + 1) & 1) * BS_TILE);
-            cp_async_commit();
             const int b = sub_of(step), r0 = b * NB, nbb = min(NB, nb - r0);
             if (tt < 0) {
                 // ---- diagonal sub-block: substitution ----

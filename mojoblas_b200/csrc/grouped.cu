@@ -106,6 +106,7 @@ struct TrsmDesc {
 };
 
 constexpr int TR_MAXN = 256;  // largest problem order a grouped strsm plan takes
+constexpr int GS_NBUF = 3;    // staging buffers per strip of the fused block solve
 
 // One unit of grouped-strsm work: a strip of up to bs::BS_COLS right-hand sides of one problem.
 struct TrsmItem {
@@ -135,7 +136,7 @@ grouped_block_strsm_kernel(const TrsmDesc* __restrict__ probs, const TrsmItem* _
         const TrsmDesc d = probs[w.prob];
         const int nb = int(d.n);
 #define GS(L, TR, U)                                                                                  \
-    bs::block_solve_strip<float, L, TR, U, bs::BS_COLS>(nb, d.nrhs, d.a, d.lda, d.b, d.ldb, w.c0, d.alpha, gs_smem)
+    bs::block_solve_strip<float, L, TR, U, bs::BS_COLS, GS_NBUF>(nb, d.nrhs, d.a, d.lda, d.b, d.ldb, w.c0, d.alpha, gs_smem)
         switch ((d.lower ? 4 : 0) | (d.trans ? 2 : 0) | (d.unit ? 1 : 0)) {
             case 0: GS(false, false, false); break;
             case 1: GS(false, false, true); break;
@@ -417,7 +418,7 @@ int mbg_strsm_grouped_plan(int mode, int count, const mbg_strsm_problem* probs, 
     p->count = int(v.size());
     p->total = cols;
     p->nitems = int(items.size());
-    p->smem = bs::bs_smem_bytes<float>(TR_MAXN);
+    p->smem = bs::bs_smem_bytes<float>(TR_MAXN, GS_NBUF);
     int st = MBG_OK;
     if (p->count > 0) {
         int per_sm = 0;
