@@ -13,6 +13,8 @@
 //   gradient is set to 0.  The other triangle of dA is not written.
 #include "mbg_internal.cuh"
 
+#include <type_traits>
+
 namespace mbg {
 
 namespace {
@@ -88,6 +90,37 @@ int gemm_adjoint(int mode, int slices, char ta, char tb, i64 m, i64 n, i64 k, T 
     cudaStream_t s = stream(), aux = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     const bool overlap = da && db && mode != MBG_MODE_PLAIN;
+    if constexpr (std::is_same<T, float>::value) {
+        // split modes, products that together give fewer than four 128 x 256 tiles per SM:
+        // both in one launch (sgemm_split_tc_dual), whose last wave is balanced across the
+        // SMs; larger ones fill the GPU on their own with the wide tiles
+        int dev = 0, sms = 148;
+        bool small = false;
+        if (overlap && (mode == MBG_MODE_BF16X3 || mode == MBG_MODE_BF16X6) && m > 0 && n > 0 && k > 0 &&
+            alpha != T(0)) {
+            MBG_CUDA(cudaGetDevice(&dev));
+            MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const i64 wide = cdiv(m, 128) * cdiv(k, 256) + cdiv(k, 128) * cdiv(n, 256);
+            small = wide < 4 * i64(sms);
+        }
+        if (small) {
+            SplitProduct pa{}, pb{};
+            T* oa = (T*)dA.dev;
+            T* ob = (T*)dB.dev;
+            if (is_n(ta))  // dA = alpha * G * op(B)^T   (m x k)
+                pa = SplitProduct{'N', flip(tb), m, k, n, alpha, G_, Gm.dev_ld, B_, B.dev_ld, oa, dA.dev_ld};
+            else           // dA = alpha * op(B) * G^T   (k x m)
+                pa = SplitProduct{tb, 'T', k, m, n, alpha, B_, B.dev_ld, G_, Gm.dev_ld, oa, dA.dev_ld};
+            if (is_n(tb))  // dB = alpha * op(A)^T * G   (k x n)
+                pb = SplitProduct{flip(ta), 'N', k, n, m, alpha, A_, A.dev_ld, G_, Gm.dev_ld, ob, dB.dev_ld};
+            else           // dB = alpha * G^T * op(A)   (n x k)
+                pb = SplitProduct{'T', ta, n, k, m, alpha, G_, Gm.dev_ld, A_, A.dev_ld, ob, dB.dev_ld};
+            MBG_TRY(sgemm_split_tc_dual(mode == MBG_MODE_BF16X6 ? 3 : 2, pa, pb));
+            MBG_TRY(dA.finish());
+            MBG_TRY(dB.finish());
+            return finish_call(A.staged || B.staged || Gm.staged || dA.staged || dB.staged);
+        }
+    }
     if (overlap) {
         MBG_TRY(aux_stream(&aux));
         MBG_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));

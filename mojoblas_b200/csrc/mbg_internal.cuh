@@ -307,6 +307,22 @@ int sgemm_split_tc_with_a(const SplitA& A, char tb, i64 n, float alpha, const fl
 // rows r0 .. r0 + mb - 1 of op(A) (r0 a multiple of 128) against a k x n op(B), k <= A.k
 int sgemm_split_tc_with_a_rows(const SplitA& A, i64 r0, i64 mb, i64 k, char tb, i64 n, float alpha, const float* b,
                                i64 ldb, float beta, float* c, i64 ldc);
+// One product C := alpha op(A) op(B) (beta 0) of a pair run by sgemm_split_tc_dual.
+struct SplitProduct {
+    char ta, tb;
+    i64 m, n, k;
+    float alpha;
+    const float* a;
+    i64 lda;
+    const float* b;
+    i64 ldb;
+    float* c;
+    i64 ldc;
+};
+// Two independent split products (device operands, m, n, k > 0) in one persistent launch of
+// 128 x 256 tiles, the longer reduction's tiles first and a stream-K tail balanced across
+// the SMs.
+int sgemm_split_tc_dual(int terms, const SplitProduct& x, const SplitProduct& y);
 // op(A)'s Ozaki slices and row exponents made once for several row-block products
 struct OzakiA {
     Workspace ws;

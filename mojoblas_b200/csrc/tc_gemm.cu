@@ -87,6 +87,7 @@ struct Cfg {
     static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
                                         : TMEM_NEED <= 256 ? 256 : 512;
     static constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // columns per epilogue thread
+    static constexpr int TILE_M = BM, TILE_N = BN, TILE_GROUP = 16;  // output tile; m-tiles per L2 group
     static constexpr uint32_t IDESC = instr_desc(OZAKI, BM, BN);
     static_assert(TMEM_NEED <= 512, "accumulators exceed TMEM");
     static_assert(SMEM_BYTES <= 232448, "shared memory budget");
@@ -122,9 +123,68 @@ struct Params {
     int* err;
 };
 
+// One output row's EPI_COLS columns from cbase of a split product: C = alpha acc (+ beta C),
+// the trmm form alpha acc + d .* C, triangle masks; columns past n are skipped.
 template <class C>
-__global__ void __launch_bounds__(C::THREADS, 1)
-tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params P) {
+__device__ __forceinline__ void split_store_row(const Params& P, const i64 row, const i64 cbase,
+                                                const float (&acc)[C::EPI_COLS]) {
+    float* Cm = static_cast<float*>(P.c);
+    const float alpha = float(P.alpha), beta = float(P.beta);
+    // 8 columns at a time: all loads of C are issued before the
+    // first is used, so the read-modify-write of a beta != 0 call
+    // waits for memory once per 8 columns, not once per column
+    // beta == 1 (the trsm updates): C += v as a reduction in L2 — one
+    // add per element, rounded as c + v, with no read in the thread
+    if (P.dvec) {  // trmm: C = alpha acc + d C, d per row or per column
+        const float drow = P.dvec_mode == 1 ? P.dvec[row] : 0.0f;
+#pragma unroll
+        for (int c0 = 0; c0 < C::EPI_COLS; c0 += 8) {
+            float cv[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const i64 col = cbase + c0 + j;
+                cv[j] = col < P.n ? Cm[row + col * P.ldc] : 0.0f;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const i64 col = cbase + c0 + j;
+                if (col >= P.n) continue;
+                const float d = P.dvec_mode == 1 ? drow : P.dvec[col];
+                Cm[row + col * P.ldc] = fmaf(d, cv[j], alpha * acc[c0 + j]);
+            }
+        }
+    } else if (beta == 1.0f) {
+#pragma unroll
+        for (int j = 0; j < C::EPI_COLS; ++j) {
+            const i64 col = cbase + j;
+            if (col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col))
+                atomicAdd(Cm + row + col * P.ldc, alpha * acc[j]);
+        }
+    } else
+#pragma unroll
+    for (int c0 = 0; c0 < C::EPI_COLS; c0 += 8) {
+        float cv[8];
+        bool live[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const i64 col = cbase + c0 + j;
+            live[j] = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
+            cv[j] = (live[j] && beta != 0.0f) ? Cm[row + col * P.ldc] : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (!live[j]) continue;
+            const float v = alpha * acc[c0 + j];
+            Cm[row + (cbase + c0 + j) * P.ldc] = (beta == 0.0f) ? v : fmaf(beta, cv[j], v);
+        }
+    }
+}
+
+// Output tile `tile` of the product P, its operands' planes read through tmA / tmB (kernel
+// parameters): one CTA's whole work in the kernels below.
+template <class C>
+__device__ __forceinline__ void tc_gemm_tile(const CUtensorMap& tmA, const CUtensorMap& tmB, const Params& P,
+                                             const int tile) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
@@ -134,7 +194,6 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
 
     // tile coordinates: groups of 16 m-tiles walk the n-tiles together (L2 reuse)
-    const int tile = blockIdx.x;
     const int group = 16;
     const int per_group = group * P.tiles_n;
     const int g = tile / per_group;
@@ -270,59 +329,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&tempty[buf]);
             }
-            if (ok && row < P.m) {
-                float* Cm = static_cast<float*>(P.c);
-                const float alpha = float(P.alpha), beta = float(P.beta);
-                const i64 cbase = n0 + part * C::EPI_COLS;
-                // 8 columns at a time: all loads of C are issued before the
-                // first is used, so the read-modify-write of a beta != 0 call
-                // waits for memory once per 8 columns, not once per column
-                // beta == 1 (the trsm updates): C += v as a reduction in L2 — one
-                // add per element, rounded as c + v, with no read in the thread
-                if (P.dvec) {  // trmm: C = alpha acc + d C, d per row or per column
-                    const float drow = P.dvec_mode == 1 ? P.dvec[row] : 0.0f;
-#pragma unroll
-                    for (int c0 = 0; c0 < C::EPI_COLS; c0 += 8) {
-                        float cv[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const i64 col = cbase + c0 + j;
-                            cv[j] = col < P.n ? Cm[row + col * P.ldc] : 0.0f;
-                        }
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const i64 col = cbase + c0 + j;
-                            if (col >= P.n) continue;
-                            const float d = P.dvec_mode == 1 ? drow : P.dvec[col];
-                            Cm[row + col * P.ldc] = fmaf(d, cv[j], alpha * acc[c0 + j]);
-                        }
-                    }
-                } else if (beta == 1.0f) {
-#pragma unroll
-                    for (int j = 0; j < C::EPI_COLS; ++j) {
-                        const i64 col = cbase + j;
-                        if (col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col))
-                            atomicAdd(Cm + row + col * P.ldc, alpha * acc[j]);
-                    }
-                } else
-#pragma unroll
-                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 8) {
-                    float cv[8];
-                    bool live[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const i64 col = cbase + c0 + j;
-                        live[j] = col < P.n && !(P.tri == 1 && row < col) && !(P.tri == 2 && row > col);
-                        cv[j] = (live[j] && beta != 0.0f) ? Cm[row + col * P.ldc] : 0.0f;
-                    }
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        if (!live[j]) continue;
-                        const float v = alpha * acc[c0 + j];
-                        Cm[row + (cbase + c0 + j) * P.ldc] = (beta == 0.0f) ? v : fmaf(beta, cv[j], v);
-                    }
-                }
-            }
+            if (ok && row < P.m) split_store_row<C>(P, row, n0 + part * C::EPI_COLS, acc);
         }
     }
     tc_fence_before();
@@ -332,6 +339,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         tc_fence_after();
         tmem_dealloc(tmem, C::TMEM_COLS);
     }
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, 1)
+tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params P) {
+    tc_gemm_tile<C>(tmA, tmB, P, int(blockIdx.x));
 }
 
 // ---------------------------------------------------------------------------
@@ -1079,6 +1092,298 @@ ozaki_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     }
 }
 
+// Work of one persistent split launch (split_sk_kernel): one or two products (the second:
+// the gemm adjoint's other gradient).  Tiles are numbered product 0's first, then product 1's.
+//   whole tiles:  the first dp_tiles tiles, worker (CTA) c taking tiles c, c + G, ...
+//                 (G workers); the triangle mask may skip tiles; C is stored
+//                 with beta.
+//   stream-K:     the slabs of the remaining tiles, [sk_begin, total) in slab positions
+//                 over all tiles, cut into G equal contiguous ranges, one per worker, so
+//                 the last wave leaves no SM idle.  A range runs on across tile boundaries
+//                 without draining the pipeline.  Whole tiles are stored; a tile two ranges
+//                 share is zeroed first (sk_zero_kernel) and both add their partial sums
+//                 (beta = 0 only).  Every range is at least one tile long, so no tile gets
+//                 more than two partial sums, and their fp32 sum does not depend on the
+//                 order they arrive in.
+struct SkWork {
+    int tiles0, tiles1;   // tiles of each product (tiles1 = 0: one product)
+    int nkb0, nkb1;       // k slabs of each product's tiles
+    int dp_tiles;         // leading tiles taken whole
+    i64 sk_begin, total;  // stream-K slab positions (sk_begin == total: none)
+};
+struct SkSeg {
+    int prod, tile, kb0, kb1;  // slabs [kb0, kb1) of tile `tile` of product `prod`
+    i64 m0, n0;                // the tile's first row and column
+};
+struct SkCursor {
+    int u, u_end, step;  // whole tiles: next tile, end, stride
+    i64 pos, end;        // stream-K: the worker's slab range
+};
+
+// Tile t of P (C::TILE_M x C::TILE_N; P.tiles_m counts 128-row tiles, P.tiles_n
+// TILE_N-column tiles): groups of TILE_GROUP tile rows walk the n-tiles together (L2 reuse).
+template <class C>
+__device__ __forceinline__ void sk_tile_origin(const Params& P, int t, i64& m0, i64& n0) {
+    constexpr int R = C::TILE_M / BM;
+    const int tiles_m = (P.tiles_m + R - 1) / R;
+    const int per_group = C::TILE_GROUP * P.tiles_n;
+    const int g = t / per_group;
+    const int first_m = g * C::TILE_GROUP;
+    const int gsize = min(C::TILE_GROUP, tiles_m - first_m);
+    const int in_g = t - g * per_group;
+    m0 = i64(first_m + in_g % gsize) * C::TILE_M;
+    n0 = i64(in_g / gsize) * C::TILE_N;
+}
+
+// Stream-K slab position -> the tile holding it and the slab within it.
+__device__ __forceinline__ void sk_locate(const SkWork& W, i64 pos, int& prod, int& tile, int& kb, i64& base,
+                                          int& nkb) {
+    const i64 w0 = i64(W.tiles0) * W.nkb0;
+    prod = pos >= w0 ? 1 : 0;
+    base = prod ? w0 : 0;
+    nkb = prod ? W.nkb1 : W.nkb0;
+    const i64 rel = pos - base;
+    tile = int(rel / nkb);
+    kb = int(rel - i64(tile) * nkb);
+}
+
+__device__ __forceinline__ SkCursor sk_cursor(const SkWork& W, i64 worker, i64 workers) {
+    const i64 n = W.total - W.sk_begin;
+    SkCursor c;
+    c.u = int(worker);
+    c.u_end = W.dp_tiles;
+    c.step = int(workers);
+    c.pos = W.sk_begin + worker * n / workers;
+    c.end = W.sk_begin + (worker + 1) * n / workers;
+    return c;
+}
+
+// The worker's next segment; every role of the worker's CTAs walks the same sequence.
+template <class C>
+__device__ __forceinline__ bool sk_next(const SkWork& W, const Params& P0, const Params& P1, SkCursor& cur,
+                                        SkSeg& sg) {
+    while (cur.u < cur.u_end) {
+        const int u = cur.u;
+        cur.u += cur.step;
+        sg.prod = u >= W.tiles0 ? 1 : 0;
+        const Params& P = sg.prod ? P1 : P0;
+        sg.tile = sg.prod ? u - W.tiles0 : u;
+        sk_tile_origin<C>(P, sg.tile, sg.m0, sg.n0);
+        if (P.tri == 1 && sg.m0 + C::TILE_M <= sg.n0) continue;  // strictly above the diagonal
+        if (P.tri == 2 && sg.m0 > sg.n0 + C::TILE_N - 1) continue;  // strictly below the diagonal
+        sg.kb0 = 0;
+        sg.kb1 = sg.prod ? W.nkb1 : W.nkb0;
+        return true;
+    }
+    if (cur.pos >= cur.end) return false;
+    i64 base;
+    int nkb;
+    sk_locate(W, cur.pos, sg.prod, sg.tile, sg.kb0, base, nkb);
+    const i64 stop = min(cur.end, base + i64(sg.tile + 1) * nkb);
+    sg.kb1 = sg.kb0 + int(stop - cur.pos);
+    cur.pos = stop;
+    sk_tile_origin<C>(sg.prod ? P1 : P0, sg.tile, sg.m0, sg.n0);
+    return true;
+}
+
+// Zeroes the tiles two stream-K ranges share, ahead of their partial sums: block b takes
+// the boundary between ranges b and b + 1 (a boundary inside a tile; ranges are at least
+// a tile long, so each such tile holds one boundary).
+template <class C>
+__global__ void __launch_bounds__(256) sk_zero_kernel(Params P0, Params P1, SkWork W, int workers) {
+    const i64 n = W.total - W.sk_begin;
+    const i64 pos = W.sk_begin + (i64(blockIdx.x) + 1) * n / workers;
+    int prod, tile, kb, nkb;
+    i64 base;
+    sk_locate(W, pos, prod, tile, kb, base, nkb);
+    if (kb == 0) return;  // the boundary is a tile's start: nothing shared
+    const Params& P = prod ? P1 : P0;
+    i64 m0, n0;
+    sk_tile_origin<C>(P, tile, m0, n0);
+    float* Cm = static_cast<float*>(P.c);
+    for (int j = threadIdx.x; j < C::TILE_M * C::TILE_N; j += blockDim.x) {
+        const i64 r = m0 + (j % C::TILE_M), col = n0 + j / C::TILE_M;
+        if (r < P.m && col < P.n) Cm[r + col * P.ldc] = 0.0f;
+    }
+}
+
+// A partial tile's row: C += alpha acc (one reduction in L2 per element).
+template <class C>
+__device__ __forceinline__ void split_add_row(const Params& P, const i64 row, const i64 cbase,
+                                              const float (&acc)[C::EPI_COLS]) {
+    float* Cm = static_cast<float*>(P.c);
+    const float alpha = float(P.alpha);
+#pragma unroll
+    for (int j = 0; j < C::EPI_COLS; ++j) {
+        const i64 col = cbase + j;
+        if (col < P.n) atomicAdd(Cm + row + col * P.ldc, alpha * acc[j]);
+    }
+}
+
+// The split product on single CTAs, persistent over the CTA's segments (SkWork): the
+// 128 x 256 tile of tc_gemm_tile, whose operand bytes per flop suit the shared memory
+// best, with the stream-K schedule in place of a partly empty last wave.  Stage, chunk
+// and buffer counters run on across segments, so the producer loads the next segment's
+// slabs while the MMAs finish this one, and the epilogue stores a finished segment while
+// the next one's first chunk accumulates in the other TMEM buffer.
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, 1)
+split_sk_kernel(const __grid_constant__ CUtensorMap tmA0, const __grid_constant__ CUtensorMap tmB0, Params P0,
+                const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1, Params P1,
+                SkWork W) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+    uint64_t* empty = full + C::STAGES;
+    uint64_t* tfull = empty + C::STAGES;  // [2]: accumulator buffer ready for the epilogue
+    uint64_t* tempty = tfull + 2;         // [2]: epilogue finished reading a buffer
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+    int* const err = P0.err;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], C::EPI_WARPS);
+        }
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, C::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            prefetch_tmap(&tmA0);
+            prefetch_tmap(&tmB0);
+            if (W.tiles1) {
+                prefetch_tmap(&tmA1);
+                prefetch_tmap(&tmB1);
+            }
+            SkCursor cur = sk_cursor(W, blockIdx.x, gridDim.x);
+            SkSeg sg;
+            bool ok = true;
+            int it = 0;
+            while (ok && sk_next<C>(W, P0, P1, cur, sg)) {
+                const CUtensorMap* ma = sg.prod ? &tmA1 : &tmA0;
+                const CUtensorMap* mb = sg.prod ? &tmB1 : &tmB0;
+                for (int kb = sg.kb0; kb < sg.kb1; ++kb, ++it) {
+                    const int s = it % C::STAGES;
+                    if (!mbar_wait(&empty[s], ((it / C::STAGES) & 1) ^ 1, err, 51)) { ok = false; break; }
+                    uint8_t* sa = smem + s * C::STAGE_BYTES;
+                    uint8_t* sb = sa + C::TERMS * C::A_PLANE;
+                    mbar_expect_tx(&full[s], C::STAGE_BYTES);
+                    tma_load_3d(sa, ma, &full[s], kb * C::BK, int(sg.m0), 0);
+                    tma_load_3d(sb, mb, &full[s], kb * C::BK, int(sg.n0), 0);
+                }
+            }
+            // all issued loads land before the CTA may exit: the MMAs release every stage
+            // only after reading it
+            if (ok)
+                for (int i = max(0, it - C::STAGES); i < it; ++i)
+                    mbar_wait(&empty[i % C::STAGES], (i / C::STAGES) & 1, err, 52);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            SkCursor cur = sk_cursor(W, blockIdx.x, gridDim.x);
+            SkSeg sg;
+            bool ok = true;
+            int it = 0, chunk = 0;
+            while (ok && sk_next<C>(W, P0, P1, cur, sg)) {
+                for (int kb = sg.kb0; kb < sg.kb1; ++kb, ++it) {
+                    const int kin = (kb - sg.kb0) % C::CHUNK;  // slab index within the chunk
+                    const int buf = chunk & 1;
+                    if (kin == 0 && chunk >= 2) {
+                        // the epilogue must have drained this buffer's previous chunk
+                        if (!mbar_wait(&tempty[buf], ((chunk >> 1) - 1) & 1, err, 55)) { ok = false; break; }
+                        tc_fence_after();
+                    }
+                    const int s = it % C::STAGES;
+                    if (!mbar_wait(&full[s], (it / C::STAGES) & 1, err, 53)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(smem + s * C::STAGE_BYTES);
+                    const uint32_t sb = sa + C::TERMS * C::A_PLANE;
+#pragma unroll
+                    for (int ks = 0; ks < C::KSTEPS; ++ks) {
+#pragma unroll
+                        for (int pi = 0; pi < C::NPROD; ++pi) {
+                            int p, q, collector;
+                            product<C::TERMS, false>(pi, p, q, collector);
+                            // the first product of a chunk overwrites the buffer
+                            const uint32_t accumulate = (kin > 0 || ks > 0 || pi > 0) ? 1u : 0u;
+                            const uint64_t ad = smem_desc(sa + p * C::A_PLANE + ks * 32, C::SBO, C::LAYOUT);
+                            const uint64_t bd = smem_desc(sb + q * C::B_PLANE + ks * 32, C::SBO, C::LAYOUT);
+                            umma<false>(tmem + uint32_t(buf * C::BN), ad, bd, C::IDESC, accumulate);
+                        }
+                    }
+                    umma_commit(&empty[s]);  // slot s is free once these MMAs have read it
+                    if (kin == C::CHUNK - 1 || kb == sg.kb1 - 1) {
+                        umma_commit(&tfull[buf]);  // chunk complete
+                        ++chunk;
+                    }
+                }
+            }
+        }
+    } else {
+        // ---------------- epilogue warps ----------------
+        const int e = warp - 2;
+        const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
+        const int part = e >> 2;       // which EPI_COLS-wide column range
+        const uint32_t lane_base = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(part * C::EPI_COLS);
+        SkCursor cur = sk_cursor(W, blockIdx.x, gridDim.x);
+        SkSeg sg;
+        bool ok = true;
+        int chunk = 0;
+        while (ok && sk_next<C>(W, P0, P1, cur, sg)) {
+            const Params& P = sg.prod ? P1 : P0;
+            const int nchunks = (sg.kb1 - sg.kb0 + C::CHUNK - 1) / C::CHUNK;
+            float acc[C::EPI_COLS];
+#pragma unroll
+            for (int j = 0; j < C::EPI_COLS; ++j) acc[j] = 0.0f;
+            for (int ch = 0; ch < nchunks; ++ch, ++chunk) {
+                const int buf = chunk & 1;
+                if (!mbar_wait(&tfull[buf], (chunk >> 1) & 1, err, 54)) { ok = false; break; }
+                tc_fence_after();
+#pragma unroll
+                for (int c0 = 0; c0 < C::EPI_COLS; c0 += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(lane_base + uint32_t(buf * C::BN + c0), r);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[c0 + j] += __uint_as_float(r[j]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[buf]);
+            }
+            const i64 row = sg.m0 + quarter * 32 + lane;
+            if (!ok || row >= P.m) continue;
+            const i64 cbase = sg.n0 + part * C::EPI_COLS;
+            if (sg.kb0 == 0 && sg.kb1 == (sg.prod ? W.nkb1 : W.nkb0)) split_store_row<C>(P, row, cbase, acc);
+            else split_add_row<C>(P, row, cbase, acc);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, C::TMEM_COLS);
+    }
+}
+
+
 // ---------------------------------------------------------------------------
 // Pre-pass kernels
 // ---------------------------------------------------------------------------
@@ -1417,19 +1722,131 @@ int launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, Params& P, const cha
     return check_launch(name);
 }
 
+// CTAs of split_sk_kernel that can be resident at once on this device (one per SM),
+// cached per device.
+template <class C>
+int sk_workers(int dev, int sms, i64& out) {
+    static std::atomic<int> cache[64];
+    if (dev >= 0 && dev < 64 && cache[dev].load() > 0) {
+        out = cache[dev].load();
+        return MBG_OK;
+    }
+    int n = 0;
+    MBG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, split_sk_kernel<C>, C::THREADS, C::SMEM_BYTES));
+    out = imax(1, imin(i64(n) * sms, sms));
+    if (dev >= 0 && dev < 64) cache[dev].store(int(out));
+    return MBG_OK;
+}
+
+// Schedule of a persistent split launch over up to G workers (SkWork): whole tiles; when
+// the tiles leave a last wave partly empty (and stream_k allows), stream-K ranges over the
+// last (tiles mod g) + g tiles, with g <= G workers chosen so that every range is at least
+// as long as the longest tile, and only where the busiest worker then finishes clearly
+// sooner than with whole tiles.  G returns the number of workers to launch.
+inline SkWork sk_plan(i64 t0, int n0, i64 t1, int n1, i64& G, bool stream_k) {
+    SkWork W{};
+    W.tiles0 = int(t0);
+    W.tiles1 = int(t1);
+    W.nkb0 = n0;
+    W.nkb1 = t1 ? n1 : n0;
+    const i64 T = t0 + t1;
+    W.dp_tiles = int(T);
+    G = imin(G, T);
+    if (!stream_k || G <= 0 || T % G == 0) return W;
+    auto slab_pos = [&](i64 u) { return u <= t0 ? u * n0 : t0 * n0 + (u - t0) * n1; };
+    const i64 longest = t1 ? imax(n0, n1) : n0;
+    // all tiles in ranges of at least `longest` slabs: as many workers as that allows
+    const i64 total = slab_pos(T);
+    i64 g = imin(G, total / longest);
+    const i64 dp = T > 2 * g ? T - (T % g) - g : 0;
+    const i64 begin = slab_pos(dp);
+    if (g <= 0 || (total - begin) / g < longest) return W;
+    // worth it when the balanced ranges end before whole tiles would: whole tiles take
+    // ceil(T / G) tile times on the busiest worker, the ranges (total - begin) / g slabs
+    // after dp / g whole tiles
+    const double whole = double((T + G - 1) / G) * double(longest);
+    const double ranged = double(dp / g) * double(longest) + double(total - begin) / double(g);
+    // the persistent kernel runs a slab about 5 % slower than tc_gemm_kernel (the epilogue's
+    // segment state spills): demand a tenth
+    if (1.1 * ranged >= whole) return W;
+    W.dp_tiles = int(dp);
+    W.sk_begin = begin;
+    W.total = total;
+    G = g;
+    return W;
+}
+
+// Persistent launch (split_sk_kernel, config C) of one or two split products; the shared
+// tiles of a stream-K schedule are zeroed first.  declined (non-null): launch nothing and
+// set it when the schedule has no stream-K part (tc_gemm_kernel does whole tiles faster).
+template <class C>
+int launch_sk(const CUtensorMap* ma, const CUtensorMap* mb, Params* P, int nprod, bool stream_k, const char* name,
+              bool* declined = nullptr) {
+    static std::atomic<unsigned> configured{0};  // one bit per device
+    int dev = 0, sms = 148;
+    MBG_CUDA(cudaGetDevice(&dev));
+    MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (!configured_on(configured, dev)) {
+        MBG_CUDA(cudaFuncSetAttribute(split_sk_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      C::SMEM_BYTES));
+        mark_configured(configured, dev);
+    }
+    i64 G = 0;
+    MBG_TRY(sk_workers<C>(dev, sms, G));
+    if (nprod == 1) P[1] = P[0];
+    constexpr int R = C::TILE_M / BM;  // 128-row tiles per output tile
+    i64 tiles[2] = {0, 0};
+    for (int i = 0; i < nprod; ++i) {
+        P[i].err = device_error_flag();
+        tiles[i] = i64((P[i].tiles_m + R - 1) / R) * P[i].tiles_n;
+        if (P[i].num_kb <= 0) return MBG_ERR_UNSUPPORTED;
+        if (P[i].beta != 0.0 || P[i].tri || P[i].band != KB_NONE || P[i].dvec) stream_k = false;
+    }
+    P[1].err = P[0].err;
+    if (tiles[0] + tiles[1] > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+    const SkWork W = sk_plan(tiles[0], P[0].num_kb, tiles[1], P[1].num_kb, G, stream_k);
+    if (declined) {
+        *declined = W.total == W.sk_begin;
+        if (*declined) return MBG_OK;
+    }
+    if (G <= 0) return MBG_OK;
+    ProfScope prof(name);
+    if (W.total > W.sk_begin && G > 1) {
+        sk_zero_kernel<C><<<unsigned(G - 1), 256, 0, stream()>>>(P[0], P[1], W, int(G));
+        MBG_TRY(check_launch("sk_zero"));
+    }
+    split_sk_kernel<C><<<unsigned(G), C::THREADS, C::SMEM_BYTES, stream()>>>(ma[0], mb[0], P[0], ma[1], mb[1], P[1],
+                                                                            W);
+    return check_launch(name);
+}
+
 // The split product on planes pa (op(A), a_rows rows from pa, planes a_plane_rows apart)
-// and pb (op(B)^T, b_rows rows): 128 x 256 tiles; 128 x 128 when the wide ones number
-// fewer than the SMs; 128 x 64 when they would occupy fewer than a quarter of the SMs.
-// Sets the B map and P.tiles_n.
+// and pb (op(B)^T, b_rows rows): 128 x 256 tiles (a 128 x 128 tile's MMAs read a third
+// more operand bytes per flop from shared memory, so the wide tile wins wherever it fills
+// more than half of the SMs); 128 x 128 when the wide ones would fill at most half, 128 x 64
+// at most a quarter.  More wide tiles than SMs with a last wave mostly empty (beta = 0, no
+// band, mask or d-vector): split_sk_kernel with a stream-K tail.  Sets the B map and
+// P.tiles_n.
 int launch_split_product(int terms, const __nv_bfloat16* pa, i64 a_rows, i64 a_plane_rows, const __nv_bfloat16* pb,
                          i64 b_rows, i64 Kp, Params& P) {
     int dev = 0, sms = 148;
     MBG_CUDA(cudaGetDevice(&dev));
     MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const i64 wide_tiles = i64(P.tiles_m) * cdiv(P.n, 256);
-    const int bn = 4 * wide_tiles < sms ? 64 : (wide_tiles < sms ? 128 : 256);
+    const int bn = 4 * wide_tiles <= sms ? 64 : (2 * wide_tiles <= sms ? 128 : 256);
     CUtensorMap ma, mb;
     MBG_TRY(make_map(&ma, pa, false, Kp, a_rows, terms, 64, BM, a_plane_rows));
+    if (bn == 256 && wide_tiles > sms && P.beta == 0.0 && !P.tri && P.band == KB_NONE && !P.dvec) {
+        // more wide tiles than SMs and a last wave mostly empty: persistent, stream-K tail
+        MBG_TRY(make_map(&mb, pb, false, Kp, b_rows, terms, 64, 256));
+        P.tiles_n = int(cdiv(P.n, 256));
+        const CUtensorMap mas[2] = {ma, ma}, mbs[2] = {mb, mb};
+        Params Ps[2] = {P, P};
+        bool declined = false;
+        const int st = terms == 2 ? launch_sk<CfgBF16x3>(mas, mbs, Ps, 1, true, "tc_gemm_bf16x3", &declined)
+                                  : launch_sk<CfgBF16x6>(mas, mbs, Ps, 1, true, "tc_gemm_bf16x6", &declined);
+        if (st || !declined) return st;
+    }
     MBG_TRY(make_map(&mb, pb, false, Kp, b_rows, terms, 64, bn));
     P.tiles_n = int(cdiv(P.n, bn));
     if (terms == 2) {
@@ -1666,6 +2083,59 @@ int sgemm_split_tc_with_a_rows(const SplitA& A, i64 r0, i64 mb, i64 k, char tb, 
     P.tiles_m = int(cdiv(mb, BM));
     P.c = c; P.ldc = ldc; P.alpha = alpha; P.beta = beta;
     return launch_split_product(A.terms, A.ws.as<__nv_bfloat16>() + size_t(r0) * A.Kp, rows, A.Mp, pb, Np, A.Kp, P);
+}
+
+int sgemm_split_tc_dual(int terms, const SplitProduct& x, const SplitProduct& y) {
+    using namespace tc;
+    if (terms != 2 && terms != 3) return MBG_ERR_INVALID_MODE;
+    const SplitProduct* q[2] = {&x, &y};
+    if (y.k > x.k) std::swap(q[0], q[1]);  // the longer reduction's tiles take the first blocks
+    constexpr int BN = 256;
+    i64 Mp[2], Np[2], Kp[2];
+    size_t off[2][2], total = 0;
+    for (int i = 0; i < 2; ++i) {
+        const SplitProduct& p = *q[i];
+        if (p.m <= 0 || p.n <= 0 || p.k <= 0) return MBG_ERR_UNSUPPORTED;
+        Mp[i] = roundup(p.m, BM);
+        Np[i] = roundup(p.n, BN);
+        Kp[i] = roundup(p.k, 32);
+        if (Kp[i] > 0x7fffffff || Mp[i] > 0x7fffffff || Np[i] > 0x7fffffff) return MBG_ERR_UNSUPPORTED;
+        off[i][0] = total;
+        total += (size_t(terms) * Mp[i] * Kp[i] * 2 + 1023) / 1024 * 1024;
+        off[i][1] = total;
+        total += (size_t(terms) * Np[i] * Kp[i] * 2 + 1023) / 1024 * 1024;
+    }
+    Workspace ws;
+    MBG_TRY(ws.reserve(total));
+    CUtensorMap ma[2], mb[2];
+    Params P[2] = {};
+    for (int i = 0; i < 2; ++i) {
+        const SplitProduct& p = *q[i];
+        __nv_bfloat16* pa = reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + off[i][0]);
+        __nv_bfloat16* pb = reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + off[i][1]);
+        // op(A) rows are K-contiguous when A is transposed; op(B)^T rows when B is not
+        if (terms == 2) {
+            MBG_TRY(launch_split<2>(p.a, p.lda, is_t(p.ta), p.m, p.k, Mp[i], Kp[i], pa));
+            MBG_TRY(launch_split<2>(p.b, p.ldb, is_n(p.tb), p.n, p.k, Np[i], Kp[i], pb));
+        } else {
+            MBG_TRY(launch_split<3>(p.a, p.lda, is_t(p.ta), p.m, p.k, Mp[i], Kp[i], pa));
+            MBG_TRY(launch_split<3>(p.b, p.ldb, is_n(p.tb), p.n, p.k, Np[i], Kp[i], pb));
+        }
+        MBG_TRY(make_map(&ma[i], pa, false, Kp[i], Mp[i], terms, 64, BM));
+        MBG_TRY(make_map(&mb[i], pb, false, Kp[i], Np[i], terms, 64, BN));
+        P[i].m = p.m;
+        P[i].n = p.n;
+        P[i].num_kb = int(Kp[i] / 32);
+        P[i].tiles_m = int(cdiv(p.m, BM));
+        P[i].tiles_n = int(cdiv(p.n, BN));
+        P[i].c = p.c;
+        P[i].ldc = p.ldc;
+        P[i].alpha = p.alpha;
+        P[i].beta = 0.0;
+        P[i].err = device_error_flag();
+    }
+    if (terms == 2) return launch_sk<CfgBF16x3>(ma, mb, P, 2, true, "tc_gemm_bf16x3");
+    return launch_sk<CfgBF16x6>(ma, mb, P, 2, true, "tc_gemm_bf16x6");
 }
 
 // ---- Ozaki dgemm ----------------------------------------------------------------

@@ -65,6 +65,53 @@ def test_gemm_adjoint(mode, ta, tb):
         assert abs(fd - ad) <= 1e-4 * scale
 
 
+@pytest.mark.parametrize("mode", [L.MODE_BF16X3, L.MODE_BF16X6], ids=["bf16x3", "bf16x6"])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "N"), ("N", "T"), ("T", "T")])
+@pytest.mark.parametrize("m,n,k", [(300, 260, 130), (130, 390, 520), (3072, 2048, 1000)])
+def test_gemm_adjoint_split_ragged(mode, ta, tb, m, n, k):
+    """Split modes compute dA and dB in one launch: several tiles per product, reductions of
+    different lengths (n for dA, m for dB), and leading dimensions above the row counts.  At
+    3072 x 2048 x 1000 the two products' 160 wide tiles end in stream-K ranges (tiles shared
+    by two ranges get two partial sums): a second call gives the same bits."""
+    lib = L.load()
+    rng = np.random.default_rng(m + 7 * n + 13 * k)
+    pad = 5
+
+    def padded(rows, cols, data=None):
+        buf = np.zeros((rows + pad, cols), dtype=np.float32, order="F")
+        if data is not None:
+            buf[:rows] = data
+        return buf
+
+    ar, ac = (m, k) if ta == "N" else (k, m)
+    br, bc = (k, n) if tb == "N" else (n, k)
+    A = padded(ar, ac, rng.uniform(-1, 1, (ar, ac)))
+    B = padded(br, bc, rng.uniform(-1, 1, (br, bc)))
+    G = padded(m, n, rng.standard_normal((m, n)))
+    dA = padded(ar, ac)
+    dB = padded(br, bc)
+    dA[ar:] = dB[br:] = 7.0  # rows past the matrices stay untouched
+    alpha = -0.75
+    st = lib.mbg_sgemm_adjoint(mode, ta.encode(), tb.encode(), m, n, k, alpha, A.ctypes.data, ar + pad,
+                               B.ctypes.data, br + pad, G.ctypes.data, m + pad, dA.ctypes.data, ar + pad,
+                               dB.ctypes.data, br + pad)
+    assert st == 0, L.last_error()
+    dA2, dB2 = padded(ar, ac), padded(br, bc)
+    st = lib.mbg_sgemm_adjoint(mode, ta.encode(), tb.encode(), m, n, k, alpha, A.ctypes.data, ar + pad,
+                               B.ctypes.data, br + pad, G.ctypes.data, m + pad, dA2.ctypes.data, ar + pad,
+                               dB2.ctypes.data, br + pad)
+    assert st == 0, L.last_error()
+    np.testing.assert_array_equal(dA2[:ar], dA[:ar])
+    np.testing.assert_array_equal(dB2[:br], dB[:br])
+    A64, B64, G64 = (x.astype(np.float64) for x in (A[:ar], B[:br], G[:m]))
+    dopA = alpha * G64 @ opm(B64, tb).T
+    dopB = alpha * opm(A64, ta).T @ G64
+    tol = 2e-5 if mode == L.MODE_BF16X6 else 2e-4
+    assert rel(dA[:ar], opm(dopA, ta)) < tol
+    assert rel(dB[:br], opm(dopB, tb)) < tol
+    assert np.all(dA[ar:] == 7.0) and np.all(dB[br:] == 7.0)
+
+
 def _tri(rng, n, uplo, unit):
     a = rng.standard_normal((n, n)) / np.sqrt(n)
     a[np.arange(n), np.arange(n)] = n + np.abs(rng.standard_normal(n))

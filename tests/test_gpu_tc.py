@@ -91,6 +91,38 @@ def test_split_sgemm_parity(oracle, mode, ta, tb, m, n, k, alpha, beta, pad):
 
 
 @pytest.mark.parametrize("mode", [mb.BF16X3, mb.BF16X6], ids=["bf16x3", "bf16x6"])
+@pytest.mark.parametrize("ta,tb", [("N", "T"), ("T", "N")])
+@pytest.mark.parametrize("m,n,k,beta", [
+    (1000, 1500, 777, 0.0),    # 48 wide tiles: 128 x 128 tiles
+    (1300, 1100, 1500, 0.5),   # 55 wide tiles, beta != 0
+    (2560, 2048, 700, 0.0),    # 160 wide tiles on 148 SMs: persistent, stream-K ranges
+    (2700, 2000, 1000, 0.0),   # ragged stream-K tiles (last rows and columns partial)
+])
+def test_split_sgemm_tile_schedules(oracle, mode, ta, tb, m, n, k, beta):
+    """Mid-size products: 128 x 128 tiles where the wide ones would fill at most half of the
+    SMs; with more wide tiles than SMs and beta = 0, a persistent launch whose last tiles are
+    divided into equal k-slab ranges, the tiles two ranges share zeroed and both partial sums
+    added.  A tile gets at most two partial sums, so a second call gives the same bits."""
+    rng = np.random.default_rng(m + n + k)
+    lda = (m if ta == "N" else k) + 3
+    ldb = (k if tb == "N" else n) + 2
+    ldc = m + 5
+    a = rand(rng, (lda, k if ta == "N" else m), np.float32)
+    b = rand(rng, (ldb, n if tb == "N" else k), np.float32)
+    c = rand(rng, (ldc, n), np.float32)
+    alpha = -1.25
+    ref = oracle.gemm_f64(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc)
+    outs = []
+    for _ in range(2):
+        c_gpu = c.copy(order="F")
+        assert mb.gemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c_gpu, ldc, mode=mode) == 0
+        outs.append(c_gpu)
+    assert oracle.max_rel_err(oracle.view(outs[0], m, n, ldc), ref) < tol_mode(mode, k)
+    np.testing.assert_array_equal(outs[0][m:], c[m:])
+    np.testing.assert_array_equal(outs[1], outs[0])
+
+
+@pytest.mark.parametrize("mode", [mb.BF16X3, mb.BF16X6], ids=["bf16x3", "bf16x6"])
 def test_split_sgemm_scaled_rows(oracle, mode):
     """Rows scaled by 2^[-20, 20]: bf16 keeps fp32's exponent range, so the split is unaffected."""
     g, _, ref, _, _ = _gemm(oracle, np.float32, mode, "N", "T", 384, 320, 1024, 1.0, 0.0, scaled=True)
