@@ -340,8 +340,9 @@ int   mbg_release_workspace(void);
  * 256 x 128 tiles over two SMs): 1 one cluster per tile, 2 persistent clusters
  * (one per two SMs, the epilogue of a tile overlapping the next tile's products);
  * 0: one CTA per 128 x 128 tile; default 2;
- * "trsm_preslice" — 1 (default): an Ozaki trsm slices all its off-diagonal
- * update blocks of op(A) up front on a second stream (0: before each update);
+ * "trsm_preslice" — 1 (default): a split or Ozaki trsm makes the planes of all
+ * its off-diagonal update blocks of op(A) up front on a second stream, beside
+ * the diagonal blocks' inversion (0: before each update);
  * "ozaki_fused_slicing" — 1 (default): a K-contiguous Ozaki operand's exponents
  * and slices in one pass (0: the separate exponent and slicing kernels);
  * "grouped_simt_tile_<TT>_c<d>", "grouped_tc_bn_<TT>_c<d>" — grouped sgemm

@@ -158,7 +158,7 @@ struct Tuning {
     i64 plain_fp64_simt = 0;     // 1: plain FP64 gemm/syrk on the CUDA cores instead of the FP64 tensor pipe
     i64 plain_fp32_staged = 0;   // 1: plain FP32 128-tiles staged through registers (the earlier kernel)
     i64 ozaki_fused_slicing = 1;  // K-contiguous Ozaki operands: exponents and slices in one pass
-    i64 trsm_preslice = 1;        // Ozaki trsm: update blocks of op(A) sliced up front on a second stream
+    i64 trsm_preslice = 1;        // split / Ozaki trsm: update blocks of op(A) split up front on a second stream
     i64 ozaki_cta_pair = 2;      // Ozaki products on CTA pairs (tcgen05 cta_group::2): 1 one launch of
                                  // all pair tiles, 2 persistent clusters; 0: one CTA per 128 x 128 tile
     // grouped sgemm plans, per transposes (NN, NT, TN, TT) and size class (grouped_size_class):

@@ -522,12 +522,18 @@ inline void collect_updates(bool lower, i64 r, i64 m, i64 nbi, std::vector<Updat
     }
 }
 
-// Ozaki solves: every update block's slices are made up front on a second stream, so the
-// slicing of op(A) (which does not depend on the solution) runs beside the leaves and
-// updates instead of before each update; each update waits only for its own block.
+// Split and Ozaki solves: every update block's planes (bf16 split terms or int8 slices) are
+// made up front on a second stream, issued before the diagonal blocks' inversion, so the
+// splitting of op(A) (which depends on neither the inverses nor the solution) runs beside
+// the inversion, the leaves and the updates instead of before each update; each update
+// waits only for its own block.
+template <typename T> struct UpdatePlanes;
+template <> struct UpdatePlanes<float> { using type = SplitA; };
+template <> struct UpdatePlanes<double> { using type = OzakiA; };
+template <typename T>
 struct PreSlicedUpdates {
-    std::vector<OzakiA> planes;      // in use order
-    std::vector<cudaEvent_t> ready;  // recorded on the second stream after each block's slices
+    std::vector<typename UpdatePlanes<T>::type> planes;  // in use order
+    std::vector<cudaEvent_t> ready;  // recorded on the second stream after each block's planes
     size_t next = 0;
     bool on = false;
     ~PreSlicedUpdates() {
@@ -538,7 +544,7 @@ struct PreSlicedUpdates {
 
 // op(A)[r:r+m, r:r+m] X = B (in place; b points at row r of B), leaves from the inverses.
 template <typename T>
-int solve_left_inv_rec(const InvPlanes<T>& inv, PreSlicedUpdates& pre, int mode, int slices, bool lower, bool trans,
+int solve_left_inv_rec(const InvPlanes<T>& inv, PreSlicedUpdates<T>& pre, int mode, int slices, bool lower, bool trans,
                        i64 r, i64 m, i64 n, const T* a, i64 lda, T* b, i64 ldb) {
     const i64 nbi = inv_block_rows<T>();
     if (m <= nbi) {
@@ -550,12 +556,14 @@ int solve_left_inv_rec(const InvPlanes<T>& inv, PreSlicedUpdates& pre, int mode,
     const T* ar = a + r + r * lda;  // op(A)[r, r]
     // B_dst -= op(A)block B_src: rows x k
     auto update = [&](const T* ablk, i64 rows, i64 k, const T* bsrc, T* bdst) -> int {
-        if constexpr (sizeof(T) == 8) {
-            if (pre.on) {
-                const size_t i = pre.next++;
-                MBG_CUDA(cudaStreamWaitEvent(stream(), pre.ready[i], 0));
+        if (pre.on) {
+            const size_t i = pre.next++;
+            MBG_CUDA(cudaStreamWaitEvent(stream(), pre.ready[i], 0));
+            if constexpr (sizeof(T) == 8)
                 return dgemm_ozaki_tc_with_a(pre.planes[i], 0, rows, k, 'N', n, -1.0, bsrc, ldb, 1.0, bdst, ldb);
-            }
+            else
+                return sgemm_split_tc_with_a_rows(pre.planes[i], 0, rows, k, 'N', n, -1.0f, bsrc, ldb, 1.0f, bdst,
+                                                  ldb);
         }
         return gemm_in_mode(mode, slices, tc, 'N', rows, n, k, T(-1), ablk, lda, bsrc, ldb, T(1), bdst, ldb);
     };
@@ -569,14 +577,16 @@ int solve_left_inv_rec(const InvPlanes<T>& inv, PreSlicedUpdates& pre, int mode,
     return solve_left_inv_rec<T>(inv, pre, mode, slices, lower, trans, r, m1, n, a, lda, b, ldb);
 }
 
-// Slices of every update block of an Ozaki solve, on the second stream (see above).
-inline int pre_slice_updates(int slices, bool lower, bool trans, i64 m, const double* a, i64 lda,
-                             PreSlicedUpdates& pre) {
+// Planes of every update block of a split or Ozaki solve, on the second stream (see above).
+template <typename T>
+int pre_slice_updates(int mode, int slices, bool lower, bool trans, i64 m, const T* a, i64 lda,
+                      PreSlicedUpdates<T>& pre) {
     std::vector<UpdateBlock> ub;
-    collect_updates(lower, 0, m, inv_block_rows<double>(), ub);
+    collect_updates(lower, 0, m, inv_block_rows<T>(), ub);
     if (ub.empty()) return MBG_OK;
-    for (const auto& u : ub)
-        if ((lower ? u.m1 : u.m2) > ozaki_max_k(slices)) return MBG_OK;  // longer reductions: sliced per update
+    if constexpr (sizeof(T) == 8)
+        for (const auto& u : ub)
+            if ((lower ? u.m1 : u.m2) > ozaki_max_k(slices)) return MBG_OK;  // longer reductions: sliced per update
     cudaStream_t s = stream(), aux = nullptr;
     MBG_TRY(aux_stream(&aux));
     cudaEvent_t start = nullptr;
@@ -591,9 +601,11 @@ inline int pre_slice_updates(int slices, bool lower, bool trans, i64 m, const do
     const char tc = trans ? 'T' : 'N';
     for (size_t i = 0; i < ub.size(); ++i) {
         const UpdateBlock& u = ub[i];
-        const double* ar = a + u.r + u.r * lda;
-        if (lower) MBG_TRY(ozaki_slice_a(slices, tc, u.m2, u.m1, op_at(ar, lda, trans, u.m1, 0), lda, pre.planes[i]));
-        else MBG_TRY(ozaki_slice_a(slices, tc, u.m1, u.m2, op_at(ar, lda, trans, 0, u.m1), lda, pre.planes[i]));
+        const T* ar = a + u.r + u.r * lda;
+        const i64 rows = lower ? u.m2 : u.m1, k = lower ? u.m1 : u.m2;
+        const T* blk = lower ? op_at(ar, lda, trans, u.m1, 0) : op_at(ar, lda, trans, 0, u.m1);
+        if constexpr (sizeof(T) == 8) MBG_TRY(ozaki_slice_a(slices, tc, rows, k, blk, lda, pre.planes[i]));
+        else MBG_TRY(split_a_planes(mode == MBG_MODE_BF16X6 ? 3 : 2, tc, rows, k, blk, lda, pre.planes[i]));
         MBG_CUDA(cudaEventCreateWithFlags(&pre.ready[i], cudaEventDisableTiming));
         MBG_CUDA(cudaEventRecord(pre.ready[i], aux));
     }
@@ -603,7 +615,8 @@ inline int pre_slice_updates(int slices, bool lower, bool trans, i64 m, const do
 
 // Before the pre-sliced planes go back to the second stream's workspace pool, that stream
 // waits for the solve's work that reads them.
-inline int release_pre_sliced(PreSlicedUpdates& pre) {
+template <typename T>
+int release_pre_sliced(PreSlicedUpdates<T>& pre) {
     if (!pre.on) return MBG_OK;
     cudaStream_t aux = nullptr;
     MBG_TRY(aux_stream(&aux));
@@ -631,11 +644,9 @@ int solve_left_inv(int mode, int slices, bool lower, bool trans, bool unit, i64 
     const int nbi = int(inv_block_rows<T>());
     Workspace ww;
     MBG_TRY(ww.reserve(sizeof(T) * size_t(m) * size_t(nbi)));
+    PreSlicedUpdates<T> pre;
+    if (tuning().trsm_preslice) MBG_TRY(pre_slice_updates<T>(mode, slices, lower, trans, m, a, lda, pre));
     MBG_TRY(invert_diagonal_blocks<T>(lower, trans, unit, m, nbi, a, lda, ww.as<T>()));
-    PreSlicedUpdates pre;
-    if constexpr (sizeof(T) == 8) {
-        if (mode == MBG_MODE_OZAKI && tuning().trsm_preslice) MBG_TRY(pre_slice_updates(slices, lower, trans, m, a, lda, pre));
-    }
     InvPlanes<T> inv;
     int st = inv.make(mode, slices, m, nbi, ww.as<T>());
     if (!st) st = solve_left_inv_rec<T>(inv, pre, mode, slices, lower, trans, 0, m, n, a, lda, b, ldb);
