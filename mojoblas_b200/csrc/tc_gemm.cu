@@ -1495,6 +1495,56 @@ split_bf16_kernel(const float* __restrict__ src, i64 ld, i64 rows, i64 K, i64 Rp
     }
 }
 
+// Both plane layouts of one column-major matrix G (gm x gn) from one read of it: planes R
+// with G's rows as plane rows (value(r, l) = G[r + l * ld], RpR x KpR) and planes C with its
+// columns as plane rows (value(r, l) = G[l + r * ld], RpC x KpC): what split_bf16_kernel
+// writes for the two orientations, bit for bit (the gemm adjoint splits G once for dA = G
+// op(B)^T and once for dB = op(A)^T G).  One 64 x 64 tile of G per block, staged in shared
+// memory; padding rows and columns are written as zeros.
+template <int TERMS>
+__global__ void __launch_bounds__(256)
+split_bf16_both_kernel(const float* __restrict__ src, i64 ld, i64 gm, i64 gn, __nv_bfloat16* __restrict__ pr,
+                       i64 RpR, i64 KpR, __nv_bfloat16* __restrict__ pc, i64 RpC, i64 KpC) {
+    const i64 i0 = i64(blockIdx.y) * SP_R, j0 = i64(blockIdx.x) * SP_K;  // rows i of G, columns j
+    const bool vec = reinterpret_cast<uintptr_t>(src) % 16 == 0 && ld % 4 == 0;
+    __shared__ float tile[SP_K][SP_R + 1];  // tile[j][i]
+    for (int q = threadIdx.x; q < SP_K * (SP_R / 4); q += 256) {
+        const int jj = q / (SP_R / 4), iq = (q % (SP_R / 4)) * 4;
+        const i64 i = i0 + iq, j = j0 + jj;
+        float t[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (j < gn) {
+            if (vec && i + 3 < gm) {
+                const float4 v = *reinterpret_cast<const float4*>(src + i + j * ld);
+                t[0] = v.x; t[1] = v.y; t[2] = v.z; t[3] = v.w;
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (i + u < gm) t[u] = src[i + u + j * ld];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) tile[jj][iq + u] = t[u];
+    }
+    __syncthreads();
+    const size_t plane_r = size_t(RpR) * size_t(KpR), plane_c = size_t(RpC) * size_t(KpC);
+    for (int q = threadIdx.x; q < SP_R * (SP_K / 4); q += 256) {
+        // planes R: row i, k = j .. j + 3
+        const int ii = q / (SP_K / 4), jq = (q % (SP_K / 4)) * 4;
+        const i64 i = i0 + ii, j = j0 + jq;
+        if (i < RpR && j < KpR) {
+            const float4 v = make_float4(tile[jq][ii], tile[jq + 1][ii], tile[jq + 2][ii], tile[jq + 3][ii]);
+            split_store4<TERMS>(v, pr + size_t(i) * KpR + j, plane_r);
+        }
+        // planes C: row j, k = i .. i + 3
+        const int jc = q / (SP_R / 4), iq = (q % (SP_R / 4)) * 4;
+        const i64 jr = j0 + jc, ik = i0 + iq;
+        if (jr < RpC && ik < KpC) {
+            const float4 v = make_float4(tile[jc][iq], tile[jc][iq + 1], tile[jc][iq + 2], tile[jc][iq + 3]);
+            split_store4<TERMS>(v, pc + size_t(jr) * KpC + ik, plane_c);
+        }
+    }
+}
+
 // Row exponents for the Ozaki scaling: e(r) with max_l |value(r,l)| < 2^e(r).
 // Partial maxima over k chunks are combined with atomicMax on the exponent
 // (initialised by the host to 0x80808080, below any double exponent); an
@@ -2107,20 +2157,56 @@ int sgemm_split_tc_dual(int terms, const SplitProduct& x, const SplitProduct& y)
     }
     Workspace ws;
     MBG_TRY(ws.reserve(total));
+    // the four operands' planes; op(A) rows are K-contiguous when A is transposed, op(B)^T
+    // rows when B is not
+    struct Operand {
+        const float* src;
+        i64 ld;
+        bool kmajor;
+        i64 rows, K, Rp, Kp;
+        __nv_bfloat16* planes;
+        bool done;
+    } op[4];
+    for (int i = 0; i < 2; ++i) {
+        const SplitProduct& p = *q[i];
+        op[2 * i] = {p.a, p.lda, is_t(p.ta), p.m, p.k, Mp[i], Kp[i],
+                     reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + off[i][0]), false};
+        op[2 * i + 1] = {p.b, p.ldb, is_n(p.tb), p.n, p.k, Np[i], Kp[i],
+                         reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + off[i][1]), false};
+    }
+    // one matrix in both orientations, one in each product (the adjoint's G): one read of it
+    for (int u = 0; u < 2; ++u)
+        for (int v = 2; v < 4; ++v) {
+            Operand& a = op[u];
+            Operand& b = op[v];
+            if (a.done || b.done || a.src != b.src || a.ld != b.ld || a.kmajor == b.kmajor) continue;
+            Operand& r = a.kmajor ? b : a;  // G's rows as plane rows
+            Operand& c = a.kmajor ? a : b;  // G's columns as plane rows
+            if (r.rows != c.K || r.K != c.rows) continue;
+            const i64 gi = imax(r.Rp, roundup(c.Kp, SP_R)), gj = imax(c.Rp, roundup(r.Kp, SP_K));
+            if (gi / SP_R > 65535) continue;
+            const dim3 g(unsigned(gj / SP_K), unsigned(gi / SP_R));
+            ProfScope prof("split_bf16");
+            if (terms == 2)
+                split_bf16_both_kernel<2><<<g, 256, 0, stream()>>>(r.src, r.ld, r.rows, r.K, r.planes, r.Rp, r.Kp,
+                                                                   c.planes, c.Rp, c.Kp);
+            else
+                split_bf16_both_kernel<3><<<g, 256, 0, stream()>>>(r.src, r.ld, r.rows, r.K, r.planes, r.Rp, r.Kp,
+                                                                   c.planes, c.Rp, c.Kp);
+            MBG_TRY(check_launch("split_bf16"));
+            a.done = b.done = true;
+        }
+    for (auto& o : op) {
+        if (o.done) continue;
+        if (terms == 2) MBG_TRY(launch_split<2>(o.src, o.ld, o.kmajor, o.rows, o.K, o.Rp, o.Kp, o.planes));
+        else MBG_TRY(launch_split<3>(o.src, o.ld, o.kmajor, o.rows, o.K, o.Rp, o.Kp, o.planes));
+    }
     CUtensorMap ma[2], mb[2];
     Params P[2] = {};
     for (int i = 0; i < 2; ++i) {
         const SplitProduct& p = *q[i];
-        __nv_bfloat16* pa = reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + off[i][0]);
-        __nv_bfloat16* pb = reinterpret_cast<__nv_bfloat16*>(ws.as<uint8_t>() + off[i][1]);
-        // op(A) rows are K-contiguous when A is transposed; op(B)^T rows when B is not
-        if (terms == 2) {
-            MBG_TRY(launch_split<2>(p.a, p.lda, is_t(p.ta), p.m, p.k, Mp[i], Kp[i], pa));
-            MBG_TRY(launch_split<2>(p.b, p.ldb, is_n(p.tb), p.n, p.k, Np[i], Kp[i], pb));
-        } else {
-            MBG_TRY(launch_split<3>(p.a, p.lda, is_t(p.ta), p.m, p.k, Mp[i], Kp[i], pa));
-            MBG_TRY(launch_split<3>(p.b, p.ldb, is_n(p.tb), p.n, p.k, Np[i], Kp[i], pb));
-        }
+        const __nv_bfloat16* pa = op[2 * i].planes;
+        const __nv_bfloat16* pb = op[2 * i + 1].planes;
         MBG_TRY(make_map(&ma[i], pa, false, Kp[i], Mp[i], terms, 64, BM));
         MBG_TRY(make_map(&mb[i], pb, false, Kp[i], Np[i], terms, 64, BN));
         P[i].m = p.m;
