@@ -1874,7 +1874,7 @@ int launch_sk(const CUtensorMap* ma, const CUtensorMap* mb, Params* P, int nprod
 // and pb (op(B)^T, b_rows rows): 128 x 256 tiles (a 128 x 128 tile's MMAs read a third
 // more operand bytes per flop from shared memory, so the wide tile wins wherever it fills
 // more than half of the SMs); 128 x 128 when the wide ones would fill at most half, 128 x 64
-// at most a quarter.  More wide tiles than SMs with a last wave mostly empty (beta = 0, no
+// at most a quarter (counting, under a triangle mask, only the tiles it keeps).  More wide tiles than SMs with a last wave mostly empty (beta = 0, no
 // band, mask or d-vector): split_sk_kernel with a stream-K tail.  Sets the B map and
 // P.tiles_n.
 int launch_split_product(int terms, const __nv_bfloat16* pa, i64 a_rows, i64 a_plane_rows, const __nv_bfloat16* pb,
@@ -1882,7 +1882,18 @@ int launch_split_product(int terms, const __nv_bfloat16* pa, i64 a_rows, i64 a_p
     int dev = 0, sms = 148;
     MBG_CUDA(cudaGetDevice(&dev));
     MBG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const i64 wide_tiles = i64(P.tiles_m) * cdiv(P.n, 256);
+    i64 wide_tiles = i64(P.tiles_m) * cdiv(P.n, 256);
+    if (P.tri) {  // only the tiles the triangle mask keeps do work
+        i64 live = 0;
+        for (i64 tm = 0; tm < P.tiles_m; ++tm)
+            for (i64 tn = 0; tn < cdiv(P.n, 256); ++tn) {
+                const i64 m0 = tm * BM, n0 = tn * 256;
+                if (P.tri == 1 && m0 + BM <= n0) continue;
+                if (P.tri == 2 && m0 > n0 + 255) continue;
+                ++live;
+            }
+        wide_tiles = live;
+    }
     const int bn = 4 * wide_tiles <= sms ? 64 : (2 * wide_tiles <= sms ? 128 : 256);
     CUtensorMap ma, mb;
     MBG_TRY(make_map(&ma, pa, false, Kp, a_rows, terms, 64, BM, a_plane_rows));
