@@ -63,7 +63,9 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 // off-diagonal blocks above the launch's size go through gemm.  Rows at or
 // past nb stay zero in the strip and staged items are zero outside op(A)'s
 // block, so ragged edges need no special case in the inner loops.
-template <typename T, bool LOWER, bool TRANS, bool UNIT, int W, int NBUF = 2>
+// IDENT: the right-hand side is the identity (columns c0 .. of the nb x nb block inverse),
+// generated in shared memory instead of read from B; B is only written.
+template <typename T, bool LOWER, bool TRANS, bool UNIT, int W, int NBUF = 2, bool IDENT = false>
 __device__ __forceinline__ void block_solve_strip(int nb, i64 ncols, const T* __restrict__ A, i64 lda,
                                                   T* __restrict__ B, i64 ldb, i64 c0, T alpha,
                                                   unsigned char* bs_smem_raw) {
@@ -114,8 +116,13 @@ __device__ __forceinline__ void block_solve_strip(int nb, i64 ncols, const T* __
 #pragma unroll 4
         for (int c = 0; c < W; ++c) {
             const bool live = c0 + c < ncols;
-            const T* bc = B + (live ? c0 + c : 0) * ldb;
-            for (int r = tid; r < nbr; r += NT) cp_async_elem(Bs + c * ldbs + r, live && r < nb ? bc + r : B, live && r < nb);
+            if constexpr (IDENT) {
+                for (int r = tid; r < nbr; r += NT) Bs[c * ldbs + r] = (live && r == c0 + c) ? T(1) : T(0);
+            } else {
+                const T* bc = B + (live ? c0 + c : 0) * ldb;
+                for (int r = tid; r < nbr; r += NT)
+                    cp_async_elem(Bs + c * ldbs + r, live && r < nb ? bc + r : B, live && r < nb);
+            }
         }
         issue(0, -1, buf0);
         cp_async_commit();  // group 0: the strip and item 0; group g: item g (empty past the last)

@@ -398,16 +398,8 @@ int launch_copy(i64 m, i64 n, T alpha, const T* x, i64 ldx, T* y, i64 ldy) {
 // the substitution's by cond(A_bb) times the working precision (triangular inverses,
 // Higham, Accuracy and Stability of Numerical Algorithms, ch. 8 and 14).
 
-// W (m x NBI, column-major, ldw): block b's rows r0 = b NBI .. r0 + nbb hold the nbb x nbb
-// identity in columns 0 .. nbb - 1, zeros elsewhere.
-template <typename T>
-__global__ void identity_blocks_kernel(i64 m, int nbi, T* __restrict__ W, i64 ldw) {
-    for (i64 j = blockIdx.y; j < nbi; j += gridDim.y)
-        for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < m; i += (i64)gridDim.x * blockDim.x)
-            W[i + j * ldw] = (i % nbi == j) ? T(1) : T(0);
-}
-
-// W block b := inv(op(A)_bb): blockIdx.y = b, blockIdx.x = 32-column strip of the block.
+// W (m x NBI, column-major, ldw) block b := inv(op(A)_bb), solved against identity columns
+// made in shared memory: blockIdx.y = b, blockIdx.x = 32-column strip of the block.
 template <typename T, bool LOWER, bool TRANS, bool UNIT>
 __global__ void __launch_bounds__(BS_THREADS, 1)
 block_invert_kernel(i64 m, int nbi, const T* __restrict__ A, i64 lda, T* __restrict__ W, i64 ldw) {
@@ -416,8 +408,8 @@ block_invert_kernel(i64 m, int nbi, const T* __restrict__ A, i64 lda, T* __restr
     const int nbb = int(min(i64(nbi), m - r0));
     const i64 c0 = i64(blockIdx.x) * BS_COLS;
     if (c0 >= nbb) return;
-    bs::block_solve_strip<T, LOWER, TRANS, UNIT, BS_COLS>(nbb, nbb, A + r0 + r0 * lda, lda, W + r0, ldw, c0, T(1),
-                                                          bs_smem_raw);
+    bs::block_solve_strip<T, LOWER, TRANS, UNIT, BS_COLS, 2, true>(nbb, nbb, A + r0 + r0 * lda, lda, W + r0, ldw, c0,
+                                                                   T(1), bs_smem_raw);
 }
 
 template <typename T>
@@ -445,11 +437,13 @@ int launch_block_invert_t(i64 m, int nbi, const T* a, i64 lda, T* w, i64 ldw) {
 template <typename T>
 int invert_diagonal_blocks(bool lower, bool trans, bool unit, i64 m, int nbi, const T* a, i64 lda, T* w) {
     ProfScope prof("trsm_block_invert");
-    {
-        dim3 g((unsigned)imin(cdiv(m, 256), 256), (unsigned)imin(nbi, 65535));
-        identity_blocks_kernel<T><<<g, 256, 0, stream()>>>(m, nbi, w, m);
-        MBG_TRY(check_launch("trsm_identity"));
-    }
+    // the strips solve against identity columns made in shared memory and write every column
+    // of their block; a last block shorter than nbi leaves columns nbb .. nbi - 1 of its rows,
+    // which the leaf products read as zeros
+    const i64 r_last = (m - 1) / nbi * nbi, nb_last = m - r_last;
+    if (nb_last < nbi)
+        MBG_CUDA(cudaMemset2DAsync(w + r_last + nb_last * m, size_t(m) * sizeof(T), 0, size_t(nb_last) * sizeof(T),
+                                   size_t(nbi - nb_last), stream()));
 #define BIV(L, TR, U) return launch_block_invert_t<T, L, TR, U>(m, nbi, a, lda, w, m)
     if (lower) {
         if (trans) { if (unit) BIV(true, true, true); else BIV(true, true, false); }
